@@ -1,0 +1,309 @@
+"""Python host API over the C ABI: contexts, meshes, fields, equations, SIMPLE.
+
+Mirrors the reference's SDK vocabulary (Field, equ::/math:: operators,
+LinearSolverConfig, SolveResult) one call per C entry point.  Every call goes
+through libbabelsim_b200.so; there is no other implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (MeshGeometry, Options, SimpleConfig, SimpleReport, SolveResult, SolverConfig, check, f64, i32,
+                   lib, ptr)
+
+BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
+INTERP = {"linear": 0, "corrected": 1}
+GRAD = {"greenGauss": 0, "leastSquares": 1}
+CONV = {"upwind": 0, "linearUpwind": 1, "central": 2}
+DIFF = {"orthogonal": 0, "corrected": 1, "limitedCorrected": 2}
+KSP = {"cg": 0, "bcgs": 1, "gmres": 2, "fgmres": 3}
+PC = {"none": 0, "icc": 1, "hypre": 2, "gamg": 3, "bjacobi": 4, "asm": 5, "jacobi": 6}
+
+
+def options(interpolation="linear", gradient="greenGauss", convection="upwind", diffusion="orthogonal",
+            coefficient_interpolation=None, coefficient_gradient=None) -> Options:
+    return Options(INTERP[interpolation], GRAD[gradient], CONV[convection], DIFF[diffusion],
+                   -1 if coefficient_interpolation is None else INTERP[coefficient_interpolation],
+                   -1 if coefficient_gradient is None else GRAD[coefficient_gradient])
+
+
+def solver_config(ksp="cg", pc="jacobi", atol=1e-14, rtol=1e-10, max_iterations=1000, warm_start=False,
+                  amg_max_levels=12, amg_coarse_size=48, amg_smoothing_steps=2, precision=0) -> SolverConfig:
+    return SolverConfig(KSP[ksp], PC[pc], atol, rtol, max_iterations, int(warm_start), 8, 2.0, amg_max_levels,
+                        amg_coarse_size, amg_smoothing_steps, precision)
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().bsg_context_create(device, C.byref(h)))
+        self.h = h
+
+    def launches(self) -> int:
+        v = C.c_int64()
+        check(lib().bsg_context_launches(self.h, C.byref(v)), self.h)
+        return v.value
+
+    def synchronize(self):
+        check(lib().bsg_context_synchronize(self.h), self.h)
+
+    def close(self):
+        if self.h:
+            lib().bsg_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mesh:
+    """A device-resident mesh (bsg_mesh)."""
+
+    def __init__(self, ctx: Context, handle, n_patches):
+        self.ctx = ctx
+        self.h = handle
+        sizes = np.zeros(5, np.int64)
+        check(lib().bsg_mesh_sizes(self.h, ptr(sizes)), ctx.h)
+        self.n_cells, self.n_faces, self.n_interior, self.n_patches, orth = (int(v) for v in sizes)
+        self.orthogonal = bool(orth)
+
+    @classmethod
+    def from_polyhedral(cls, ctx: Context, poly):
+        """Geometry computed by the library from a polyhedral description (see meshgen.PolyMesh)."""
+        offsets = i32(np.concatenate([[0], np.cumsum([len(f) for f in poly.faces])]))
+        ids = i32(np.concatenate(poly.faces))
+        verts = f64(poly.vertices)
+        owner, nbr, patch = i32(poly.owner), i32(poly.neighbour), i32(poly.patch)
+        h = C.c_void_p()
+        check(lib().bsg_mesh_create_polyhedral(ctx.h, len(verts), ptr(verts), len(owner), ptr(offsets), ptr(ids),
+                                               ptr(owner), ptr(nbr), ptr(patch), len(poly.patch_names),
+                                               C.byref(h)), ctx.h)
+        m = cls(ctx, h, len(poly.patch_names))
+        m.patch_names = list(poly.patch_names)
+        return m
+
+    @classmethod
+    def from_geometry(cls, ctx: Context, geo: dict, n_patches: int):
+        """Geometry supplied by the caller (the reference's MeshStorage arrays)."""
+        keep = {k: (i32(v) if k in ("face_owner", "face_neighbour", "face_patch") else f64(v)) for k, v in geo.items()
+                if k != "orthogonal_geometry"}
+        g = MeshGeometry(len(keep["cell_volumes"]), len(keep["face_owner"]), n_patches,
+                         *(ptr(keep[k]) for k in ("face_owner", "face_neighbour", "face_patch", "face_area_vectors",
+                                                  "face_centres", "face_areas", "face_normals", "face_owner_weights",
+                                                  "face_orthogonal_coefficients", "face_non_orthogonal",
+                                                  "face_skewness", "cell_centres", "cell_volumes")),
+                         int(np.asarray(geo["orthogonal_geometry"]).ravel()[0]))
+        h = C.c_void_p()
+        check(lib().bsg_mesh_create(ctx.h, C.byref(g), C.byref(h)), ctx.h)
+        return cls(ctx, h, n_patches)
+
+    def export(self, name: str) -> np.ndarray:
+        width = {"face_owner": 1, "face_neighbour": 1, "face_patch": 1, "face_areas": 1, "face_owner_weights": 1,
+                 "face_orthogonal_coefficients": 1, "cell_volumes": 1}.get(name, 3)
+        count = self.n_cells if name.startswith("cell_") else self.n_faces
+        dtype = np.int32 if name in ("face_owner", "face_neighbour", "face_patch") else np.float64
+        out = np.zeros(count * width, dtype)
+        check(lib().bsg_mesh_export(self.h, name.encode(), ptr(out)), self.ctx.h)
+        return out.reshape(count, width) if width == 3 else out
+
+    def close(self):
+        if self.h:
+            lib().bsg_mesh_destroy(self.h)
+            self.h = None
+
+
+class Field:
+    """Device field (bsg_field): location 'cell' or 'face', 1/3/9 components."""
+
+    def __init__(self, mesh: Mesh, location="cell", components=1, values=None):
+        self.mesh = mesh
+        self.location = location
+        self.components = components
+        h = C.c_void_p()
+        check(lib().bsg_field_create(mesh.h, 0 if location == "cell" else 1, components, C.byref(h)), mesh.ctx.h)
+        self.h = h
+        if values is not None:
+            self.upload(values)
+
+    @property
+    def count(self):
+        return self.mesh.n_cells if self.location == "cell" else self.mesh.n_faces
+
+    def set_boundary(self, patch: int, kind: str, value=0.0):
+        v = f64(np.broadcast_to(np.asarray(value, dtype=np.float64), (3,)) if np.ndim(value) == 0 else
+                np.pad(np.asarray(value, np.float64), (0, 3 - len(value))))
+        check(lib().bsg_field_set_boundary(self.h, patch, BC[kind], ptr(v)), self.mesh.ctx.h)
+
+    def upload(self, values):
+        v = f64(values).reshape(-1)
+        assert v.size == self.count * self.components
+        check(lib().bsg_field_upload(self.h, ptr(v)), self.mesh.ctx.h)
+
+    def download(self) -> np.ndarray:
+        out = np.zeros(self.count * self.components)
+        check(lib().bsg_field_download(self.h, ptr(out)), self.mesh.ctx.h)
+        return out if self.components == 1 else out.reshape(self.count, self.components)
+
+    def set_boundary_flux(self, face_flux: "Field"):
+        check(lib().bsg_field_set_boundary_flux(self.h, face_flux.h), self.mesh.ctx.h)
+
+    def close(self):
+        if self.h:
+            lib().bsg_field_destroy(self.h)
+            self.h = None
+
+
+def grad(x: Field, method="greenGauss") -> Field:
+    out = Field(x.mesh, "cell", 3 * x.components)
+    check(lib().bsg_math_grad(x.h, GRAD[method], out.h), x.mesh.ctx.h)
+    return out
+
+
+def interpolate(x: Field, opts: Options) -> Field:
+    out = Field(x.mesh, "face", x.components)
+    check(lib().bsg_math_interpolate(x.h, C.byref(opts), out.h), x.mesh.ctx.h)
+    return out
+
+
+def flux(U: Field, opts: Options) -> Field:
+    out = Field(U.mesh, "face", 1)
+    check(lib().bsg_math_flux(U.h, C.byref(opts), out.h), U.mesh.ctx.h)
+    return out
+
+
+def div_flux(phi: Field) -> Field:
+    out = Field(phi.mesh, "cell", 1)
+    check(lib().bsg_math_div_flux(phi.h, out.h), phi.mesh.ctx.h)
+    return out
+
+
+def normal_gradient(x: Field, opts: Options, gradient: Field | None = None) -> Field:
+    out = Field(x.mesh, "face", 1)
+    check(lib().bsg_math_normal_gradient(x.h, gradient.h if gradient else None, C.byref(opts), out.h), x.mesh.ctx.h)
+    return out
+
+
+class Equation:
+    """equ::Equation on the device (bsg_equation)."""
+
+    def __init__(self, unknown: Field, opts: Options):
+        self.x = unknown
+        h = C.c_void_p()
+        check(lib().bsg_equation_create(unknown.h, C.byref(opts), C.byref(h)), unknown.mesh.ctx.h)
+        self.h = h
+
+    def _c(self, code):
+        check(code, self.x.mesh.ctx.h)
+
+    def reset(self):
+        self._c(lib().bsg_equ_reset(self.h))
+
+    def div(self, phi: Field, scale=1.0, term: Options | None = None):
+        self._c(lib().bsg_equ_div(self.h, phi.h, scale, C.byref(term) if term else None))
+
+    def laplacian(self, coefficient, factor, term: Options | None = None):
+        if isinstance(coefficient, Field):
+            self._c(lib().bsg_equ_laplacian(self.h, coefficient.h, 0.0, factor, C.byref(term) if term else None))
+        else:
+            self._c(lib().bsg_equ_laplacian(self.h, None, float(coefficient), factor, C.byref(term) if term else None))
+
+    def source(self, value: Field, factor=1.0):
+        self._c(lib().bsg_equ_source(self.h, value.h, factor))
+
+    def relax(self, previous: Field, alpha):
+        self._c(lib().bsg_equ_relax(self.h, previous.h, alpha))
+
+    def scale(self, f):
+        self._c(lib().bsg_equ_scale(self.h, f))
+
+    def reference_if_unanchored(self, value=0.0) -> bool:
+        flag = C.c_int32()
+        self._c(lib().bsg_equ_reference_if_unanchored(self.h, value, C.byref(flag)))
+        return bool(flag.value)
+
+    def face_flux(self, solution: Field) -> Field:
+        out = Field(self.x.mesh, "face", 1)
+        self._c(lib().bsg_equ_face_flux(self.h, solution.h, out.h))
+        return out
+
+    def relative_residual(self, x: Field) -> float:
+        v = C.c_double()
+        self._c(lib().bsg_equ_relative_residual(self.h, x.h, C.byref(v)))
+        return v.value
+
+    def solve(self, cfg: SolverConfig):
+        res = (SolveResult * self.x.components)()
+        self._c(lib().bsg_equ_solve(self.h, C.byref(cfg), res))
+        return list(res)
+
+    def download(self):
+        m = self.x.mesh
+        d, u, l = np.zeros(m.n_cells), np.zeros(m.n_faces), np.zeros(m.n_faces)
+        s = np.zeros(m.n_cells * self.x.components)
+        self._c(lib().bsg_equ_download(self.h, ptr(d), ptr(u), ptr(l), ptr(s)))
+        return dict(diag=d, upper=u, lower=l, source=s if self.x.components == 1 else s.reshape(-1, 3))
+
+    def close(self):
+        if self.h:
+            lib().bsg_equation_destroy(self.h)
+            self.h = None
+
+
+def solve_ldu(mesh: Mesh, cfg: SolverConfig, diag, upper, lower, source, x0=None):
+    """ComputeBackend::solve on host LDU arrays (bsg_solve_ldu)."""
+    src = f64(source)
+    comps = 1 if src.ndim == 1 else 3
+    x = f64(np.zeros_like(src) if x0 is None else x0).copy()
+    res = (SolveResult * comps)()
+    check(lib().bsg_solve_ldu(mesh.h, C.byref(cfg), comps, ptr(f64(diag)), ptr(f64(upper)), ptr(f64(lower)),
+                              ptr(src), ptr(x), res), mesh.ctx.h)
+    return x, list(res)
+
+
+class Simple:
+    """Steady SIMPLE on the device (bsg_simple), simple/main.cpp:11-131."""
+
+    def __init__(self, mesh: Mesh, rho=1.0, mu=0.01, alpha_u=0.7, alpha_p=0.3, non_orthogonal_corrections=1,
+                 continuity_tolerance=1e-8, velocity_tolerance=1e-7, momentum_tolerance=1e-6,
+                 pressure_tolerance=1e-6, momentum=None, pressure=None, momentum_solver=None, pressure_solver=None):
+        self.mesh = mesh
+        cfg = SimpleConfig(rho, mu, alpha_u, alpha_p, non_orthogonal_corrections, continuity_tolerance,
+                           velocity_tolerance, momentum_tolerance, pressure_tolerance,
+                           momentum or options(), pressure or options(),
+                           momentum_solver or solver_config("bcgs", "bjacobi", 1e-14, 1e-10),
+                           pressure_solver or solver_config("cg", "jacobi", 1e-14, 1e-10, 5000))
+        h = C.c_void_p()
+        check(lib().bsg_simple_create(mesh.h, C.byref(cfg), C.byref(h)), mesh.ctx.h)
+        self.h = h
+
+    def set_boundary(self, field: str, patch: int, kind: str, value=0.0):
+        v = f64(np.broadcast_to(np.asarray(value, np.float64), (3,)) if np.ndim(value) == 0 else
+                np.pad(np.asarray(value, np.float64), (0, 3 - len(value))))
+        check(lib().bsg_simple_set_boundary(self.h, field.encode(), patch, BC[kind], ptr(v)), self.mesh.ctx.h)
+
+    def set_fields(self, U, p):
+        check(lib().bsg_simple_set_fields(self.h, ptr(f64(U)), ptr(f64(p))), self.mesh.ctx.h)
+
+    def set_flux(self, phi):
+        check(lib().bsg_simple_set_flux(self.h, ptr(f64(phi))), self.mesh.ctx.h)
+
+    def iterate(self, max_iterations: int) -> SimpleReport:
+        r = SimpleReport()
+        check(lib().bsg_simple_iterate(self.h, max_iterations, C.byref(r)), self.mesh.ctx.h)
+        return r
+
+    def fields(self):
+        m = self.mesh
+        U, p, phi = np.zeros((m.n_cells, 3)), np.zeros(m.n_cells), np.zeros(m.n_faces)
+        check(lib().bsg_simple_get_fields(self.h, ptr(U), ptr(p), ptr(phi)), m.ctx.h)
+        return U, p, phi
+
+    def close(self):
+        if self.h:
+            lib().bsg_simple_destroy(self.h)
+            self.h = None

@@ -1,0 +1,416 @@
+// Aggregation AMG: host structure setup once per mesh, device numeric setup per
+// matrix version, device V-cycle.  See amg.h for the design.
+#include "amg.h"
+#include "bsg_device.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace bsg {
+
+struct AmgPreconditioner::Level {
+    int n = 0;
+    long long nnz = 0;
+    // matrix of this level (level 0 borrows the caller's arrays)
+    DeviceArray<int> ptr, col;
+    DeviceArray<double> diag, val;
+    const int* dptr = nullptr;
+    const int* dcol = nullptr;
+    const double* ddiag = nullptr;
+    const double* dval = nullptr;
+    DeviceArray<double> rdiag;           // omega / diag for damped Jacobi
+    // transfer to the next coarser level
+    DeviceArray<int> agg;                // fine row -> coarse row
+    DeviceArray<int> agg_ptr, agg_rows;  // coarse row -> fine rows
+    DeviceArray<int> cslot_ptr, cslot_src, cintra_ptr, cintra_src;
+    // work vectors
+    DeviceArray<double> x, b, t;
+    // coarsest level
+    DeviceArray<double> dense;           // n x 2n augmented matrix, inverse in the right half
+};
+
+namespace {
+constexpr int kBlock = 256;
+constexpr double kOmega = 2.0 / 3.0;
+
+struct HostCsr {
+    int n = 0;
+    std::vector<int> ptr, col;
+    std::vector<double> diag, val;
+};
+
+// Greedy pairwise matching on strongest negative couplings.
+std::vector<int> pairwise(const HostCsr& a, int& n_coarse) {
+    std::vector<int> mate(a.n, -1), agg(a.n, -1);
+    int next = 0;
+    for (int i = 0; i < a.n; ++i) {
+        if (agg[i] >= 0) continue;
+        int best = -1;
+        double bs = 0.0;
+        for (int k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+            const int j = a.col[k];
+            if (j == i || agg[j] >= 0) continue;
+            const double s = -a.val[k];
+            if (s > bs) { bs = s; best = j; }
+        }
+        agg[i] = next;
+        if (best >= 0) agg[best] = next;
+        ++next;
+    }
+    n_coarse = next;
+    return agg;
+}
+
+// Galerkin coarse graph of piecewise-constant aggregation (host, structure + values).
+HostCsr coarsen(const HostCsr& a, const std::vector<int>& agg, int nc, std::vector<int>* slot_target) {
+    HostCsr c;
+    c.n = nc;
+    c.ptr.assign(nc + 1, 0);
+    c.diag.assign(nc, 0.0);
+    std::vector<std::vector<int>> members(nc);
+    for (int i = 0; i < a.n; ++i) members[agg[i]].push_back(i);
+    std::vector<int> marker(nc, -1);
+    std::vector<int> cols;
+    if (slot_target) slot_target->assign(a.ptr[a.n], -1);
+    for (int I = 0; I < nc; ++I) {
+        cols.clear();
+        for (int i : members[I]) {
+            c.diag[I] += a.diag[i];
+            for (int k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+                const int J = agg[a.col[k]];
+                if (J == I) { c.diag[I] += a.val[k]; continue; }
+                if (marker[J] != I) { marker[J] = I; cols.push_back(J); }
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        const int base = static_cast<int>(c.col.size());
+        for (int J : cols) { c.col.push_back(J); c.val.push_back(0.0); }
+        c.ptr[I + 1] = static_cast<int>(c.col.size());
+        for (int i : members[I]) {
+            for (int k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+                const int J = agg[a.col[k]];
+                if (J == I) continue;
+                const int pos = base + static_cast<int>(std::lower_bound(cols.begin(), cols.end(), J) - cols.begin());
+                c.val[pos] += a.val[k];
+                if (slot_target) (*slot_target)[k] = pos;
+            }
+        }
+    }
+    return c;
+}
+
+__global__ void kRdiag(int n, const double* __restrict__ d, double* __restrict__ rd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rd[i] = kOmega / d[i];
+}
+
+// Coarse Galerkin values: fixed-order gathers over precomputed fine contributions.
+__global__ void kGalerkin(int nc, const int* __restrict__ agg_ptr, const int* __restrict__ agg_rows,
+                          const int* __restrict__ cintra_ptr, const int* __restrict__ cintra_src,
+                          const int* __restrict__ cptr, const int* __restrict__ cslot_ptr,
+                          const int* __restrict__ cslot_src, const double* __restrict__ fdiag,
+                          const double* __restrict__ fval, double* __restrict__ cdiag, double* __restrict__ cval) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc) return;
+    double d = 0.0;
+    for (int k = agg_ptr[I]; k < agg_ptr[I + 1]; ++k) d += fdiag[agg_rows[k]];
+    for (int k = cintra_ptr[I]; k < cintra_ptr[I + 1]; ++k) d += fval[cintra_src[k]];
+    cdiag[I] = d;
+    for (int c = cptr[I]; c < cptr[I + 1]; ++c) {
+        double v = 0.0;
+        for (int k = cslot_ptr[c]; k < cslot_ptr[c + 1]; ++k) v += fval[cslot_src[k]];
+        cval[c] = v;
+    }
+}
+
+// Dense [A | I] of the coarsest level, then in-place Gauss-Jordan (one block).
+__global__ void kDenseInvert(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+                             const double* __restrict__ diag, const double* __restrict__ val, double* __restrict__ M) {
+    const int w = 2 * n;
+    for (int e = threadIdx.x; e < n * w; e += blockDim.x) M[e] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        M[i * w + i] = diag[i];
+        M[i * w + n + i] = 1.0;
+        for (int k = ptr[i]; k < ptr[i + 1]; ++k) M[i * w + col[k]] += val[k];
+    }
+    __syncthreads();
+    __shared__ double piv;
+    for (int k = 0; k < n; ++k) {
+        if (threadIdx.x == 0) piv = 1.0 / M[k * w + k];
+        __syncthreads();
+        for (int j = threadIdx.x; j < w; j += blockDim.x) M[k * w + j] *= piv;
+        __syncthreads();
+        for (int e = threadIdx.x; e < n * w; e += blockDim.x) {
+            const int i = e / w, j = e % w;
+            if (i == k) continue;
+            const double f = M[i * w + k];
+            if (j != k && f != 0.0) M[e] -= f * M[k * w + j];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if (i != k) M[i * w + k] = 0.0;
+        __syncthreads();
+    }
+}
+
+__global__ void kDenseSolve(int n, const double* __restrict__ M, const double* __restrict__ b, double* __restrict__ x) {
+    const int w = 2 * n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < n; ++j) s += M[i * w + n + j] * b[j];
+        x[i] = s;
+    }
+}
+
+// x = omega D^-1 b (first Jacobi sweep from a zero guess)
+__global__ void kSmoothZero(int n, const double* __restrict__ rd, const double* __restrict__ b, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = rd[i] * b[i];
+}
+
+// x_out = x + omega D^-1 (b - A x)
+__global__ void kSmooth(int n, const int* __restrict__ ptr, const int* __restrict__ col, const double* __restrict__ diag,
+                        const double* __restrict__ val, const double* __restrict__ rd, const double* __restrict__ b,
+                        const double* __restrict__ x, double* __restrict__ xo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double ax = diag[i] * x[i];
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) ax += val[k] * x[col[k]];
+    xo[i] = x[i] + rd[i] * (b[i] - ax);
+}
+
+// Post-smoothing sweep fused with prolongation: y = x + P xc, x_out = y + omega D^-1 (b - A y).
+__global__ void kProlongSmooth(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+                               const double* __restrict__ diag, const double* __restrict__ val,
+                               const double* __restrict__ rd, const int* __restrict__ agg,
+                               const double* __restrict__ xc, const double* __restrict__ b,
+                               const double* __restrict__ x, double* __restrict__ xo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double yi = x[i] + xc[agg[i]];
+    double ay = diag[i] * yi;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
+        const int j = col[k];
+        ay += val[k] * (x[j] + xc[agg[j]]);
+    }
+    xo[i] = yi + rd[i] * (b[i] - ay);
+}
+
+__global__ void kProlong(int n, const int* __restrict__ agg, const double* __restrict__ xc, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += xc[agg[i]];
+}
+
+// b_c[I] = sum over fine rows i of aggregate I of (b - A x)_i
+__global__ void kResidualRestrict(int nc, const int* __restrict__ agg_ptr, const int* __restrict__ agg_rows,
+                                  const int* __restrict__ ptr, const int* __restrict__ col,
+                                  const double* __restrict__ diag, const double* __restrict__ val,
+                                  const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ bc) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc) return;
+    double s = 0.0;
+    for (int m = agg_ptr[I]; m < agg_ptr[I + 1]; ++m) {
+        const int i = agg_rows[m];
+        double ax = diag[i] * x[i];
+        for (int k = ptr[i]; k < ptr[i + 1]; ++k) ax += val[k] * x[col[k]];
+        s += b[i] - ax;
+    }
+    bc[I] = s;
+}
+
+__global__ void kCopy(int n, const double* __restrict__ a, double* __restrict__ b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+}  // namespace
+
+AmgPreconditioner::AmgPreconditioner(DeviceMesh& mesh, const SolverConfig& cfg)
+    : mesh_(mesh), ctx_(*mesh.ctx), cfg_(cfg) {}
+
+AmgPreconditioner::~AmgPreconditioner() {
+    for (Level* l : levels_) delete l;
+}
+
+int AmgPreconditioner::levels() const { return static_cast<int>(levels_.size()); }
+long long AmgPreconditioner::coarseRows(int level) const { return levels_.at(level)->n; }
+
+void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
+    HostCsr cur;
+    cur.n = A.n;
+    cur.ptr.resize(A.n + 1);
+    cur.col.resize(A.nnz_off);
+    cur.diag.resize(A.n);
+    cur.val.resize(A.nnz_off);
+    BSG_CUDA(cudaMemcpyAsync(cur.ptr.data(), A.ptr, sizeof(int) * (A.n + 1), cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(cur.col.data(), A.col, sizeof(int) * A.nnz_off, cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(cur.diag.data(), A.diag, sizeof(double) * A.n, cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(cur.val.data(), A.val, sizeof(double) * A.nnz_off, cudaMemcpyDeviceToHost, ctx_.stream));
+    ctx_.sync();
+    const int coarse_target = std::max(std::min(cfg_.amg_coarse_size, 256), 16);
+    const int max_levels = std::max(2, cfg_.amg_max_levels);
+    auto* l0 = new Level();
+    l0->n = A.n;
+    l0->nnz = A.nnz_off;
+    levels_.push_back(l0);
+    while (cur.n > coarse_target && static_cast<int>(levels_.size()) < max_levels) {
+        int n1 = 0, n2 = 0;
+        const std::vector<int> a1 = pairwise(cur, n1);
+        const HostCsr c1 = coarsen(cur, a1, n1, nullptr);
+        const std::vector<int> a2 = pairwise(c1, n2);
+        std::vector<int> agg(cur.n);
+        for (int i = 0; i < cur.n; ++i) agg[i] = a2[a1[i]];
+        if (n2 >= cur.n) break;  // no coarsening possible
+        std::vector<int> target;
+        HostCsr next = coarsen(cur, agg, n2, &target);
+        Level* fine = levels_.back();
+        // transfer maps
+        std::vector<int> agg_ptr(n2 + 1, 0), agg_rows(cur.n);
+        for (int i = 0; i < cur.n; ++i) ++agg_ptr[agg[i] + 1];
+        for (int I = 0; I < n2; ++I) agg_ptr[I + 1] += agg_ptr[I];
+        {
+            std::vector<int> fill(agg_ptr.begin(), agg_ptr.end() - 1);
+            for (int i = 0; i < cur.n; ++i) agg_rows[fill[agg[i]]++] = i;
+        }
+        const long long cnnz = static_cast<long long>(next.col.size());
+        std::vector<int> cslot_ptr(cnnz + 1, 0), cslot_src(cur.ptr[cur.n]);
+        std::vector<int> cintra_ptr(n2 + 1, 0), cintra_src;
+        std::vector<int> counts(cnnz, 0);
+        for (int k = 0; k < cur.ptr[cur.n]; ++k)
+            if (target[k] >= 0) ++cslot_ptr[target[k] + 1];
+        for (long long c = 0; c < cnnz; ++c) cslot_ptr[c + 1] += cslot_ptr[c];
+        {
+            std::vector<int> fill(cslot_ptr.begin(), cslot_ptr.end() - 1);
+            for (int I = 0; I < n2; ++I)
+                for (int mm = agg_ptr[I]; mm < agg_ptr[I + 1]; ++mm) {
+                    const int i = agg_rows[mm];
+                    for (int k = cur.ptr[i]; k < cur.ptr[i + 1]; ++k) {
+                        if (target[k] >= 0) cslot_src[fill[target[k]]++] = k;
+                        else cintra_src.push_back(k);
+                    }
+                    cintra_ptr[I + 1] = static_cast<int>(cintra_src.size());
+                }
+            for (int I = 0; I < n2; ++I) cintra_ptr[I + 1] = std::max(cintra_ptr[I + 1], cintra_ptr[I]);
+        }
+        cudaStream_t s = ctx_.stream;
+        fine->agg.upload(agg, s);
+        fine->agg_ptr.upload(agg_ptr, s);
+        fine->agg_rows.upload(agg_rows, s);
+        fine->cslot_ptr.upload(cslot_ptr, s);
+        fine->cslot_src.upload(cslot_src, s);
+        fine->cintra_ptr.upload(cintra_ptr, s);
+        if (cintra_src.empty()) cintra_src.push_back(0);
+        fine->cintra_src.upload(cintra_src, s);
+        auto* lv = new Level();
+        lv->n = n2;
+        lv->nnz = cnnz;
+        lv->ptr.upload(next.ptr, s);
+        if (next.col.empty()) { next.col.push_back(0); next.val.push_back(0.0); }
+        lv->col.upload(next.col, s);
+        lv->diag.resize(n2);
+        lv->val.resize(std::max<long long>(cnnz, 1));
+        lv->dptr = lv->ptr.data();
+        lv->dcol = lv->col.data();
+        lv->ddiag = lv->diag.data();
+        lv->dval = lv->val.data();
+        levels_.push_back(lv);
+        ctx_.sync();
+        cur = std::move(next);
+    }
+    for (Level* l : levels_) {
+        l->x.resize(l->n);
+        l->b.resize(l->n);
+        l->t.resize(l->n);
+        l->rdiag.resize(l->n);
+    }
+    Level* last = levels_.back();
+    last->dense.resize(2 * static_cast<std::size_t>(last->n) * last->n);
+    built_ = true;
+}
+
+void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
+    if (!built_) buildStructure(A);
+    fine_ = A;
+    Level* l0 = levels_[0];
+    l0->dptr = A.ptr; l0->dcol = A.col; l0->ddiag = A.diag; l0->dval = A.val;
+    if (!numeric) return;
+    for (std::size_t l = 0; l + 1 < levels_.size(); ++l) {
+        Level* f = levels_[l];
+        Level* c = levels_[l + 1];
+        kGalerkin<<<gridFor(c->n, kBlock), kBlock, 0, ctx_.stream>>>(
+            c->n, f->agg_ptr.data(), f->agg_rows.data(), f->cintra_ptr.data(), f->cintra_src.data(), c->dptr,
+            f->cslot_ptr.data(), f->cslot_src.data(), f->ddiag, f->dval, c->diag.data(), c->val.data());
+        ctx_.launched();
+    }
+    for (Level* l : levels_) {
+        kRdiag<<<gridFor(l->n, kBlock), kBlock, 0, ctx_.stream>>>(l->n, l->ddiag, l->rdiag.data());
+        ctx_.launched();
+    }
+    Level* last = levels_.back();
+    kDenseInvert<<<1, 1024, 0, ctx_.stream>>>(last->n, last->dptr, last->dcol, last->ddiag, last->dval,
+                                              last->dense.data());
+    ctx_.launched();
+    BSG_CUDA(cudaGetLastError());
+}
+
+void AmgPreconditioner::apply(Context& ctx, const double* r, double* z) {
+    const int L = static_cast<int>(levels_.size());
+    const int nu = std::max(1, cfg_.amg_smoothing_steps);
+    cudaStream_t s = ctx.stream;
+    // Downward leg: level l solves A_l x_l = b_l approximately.
+    for (int l = 0; l < L - 1; ++l) {
+        Level* f = levels_[l];
+        Level* c = levels_[l + 1];
+        const double* b = l == 0 ? r : f->b.data();
+        double* x = f->x.data();
+        double* t = f->t.data();
+        const unsigned g = gridFor(f->n, kBlock);
+        kSmoothZero<<<g, kBlock, 0, s>>>(f->n, f->rdiag.data(), b, x);
+        ctx.launched();
+        for (int it = 1; it < nu; ++it) {
+            kSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), b, x, t);
+            kCopy<<<g, kBlock, 0, s>>>(f->n, t, x);
+            ctx.launches += 2;
+        }
+        kResidualRestrict<<<gridFor(c->n, kBlock), kBlock, 0, s>>>(c->n, f->agg_ptr.data(), f->agg_rows.data(), f->dptr,
+                                                                    f->dcol, f->ddiag, f->dval, b, x, c->b.data());
+        ctx.launched();
+    }
+    Level* last = levels_.back();
+    {
+        const double* b = L == 1 ? r : last->b.data();
+        double* x = L == 1 ? z : last->x.data();
+        kDenseSolve<<<gridFor(last->n, 128), 128, 0, s>>>(last->n, last->dense.data(), b, x);
+        ctx.launched();
+    }
+    // Upward leg: prolongate and post-smooth.
+    for (int l = L - 2; l >= 0; --l) {
+        Level* f = levels_[l];
+        Level* c = levels_[l + 1];
+        const double* b = l == 0 ? r : f->b.data();
+        double* x = f->x.data();
+        double* t = f->t.data();
+        double* out = l == 0 ? z : x;
+        const unsigned g = gridFor(f->n, kBlock);
+        // first post sweep fused with prolongation writes t, further sweeps ping-pong
+        kProlongSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), f->agg.data(),
+                                            c->x.data(), b, x, t);
+        ctx.launched();
+        double* cur = t;
+        double* other = x;
+        for (int it = 1; it < nu; ++it) {
+            kSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), b, cur, other);
+            ctx.launched();
+            std::swap(cur, other);
+        }
+        if (cur != out) {
+            kCopy<<<g, kBlock, 0, s>>>(f->n, cur, out);
+            ctx.launched();
+        }
+    }
+    BSG_CUDA(cudaGetLastError());
+}
+
+}  // namespace bsg

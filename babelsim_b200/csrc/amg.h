@@ -1,0 +1,43 @@
+// Aggregation AMG preconditioner on the device (replaces Hypre BoomerAMG /
+// PETSc GAMG behind pcType hypre|gamg, src/backend/petsc_linear_system.cpp:92-115,197-231).
+//
+// Structure (aggregates, coarse patterns and the fine->coarse value maps) is
+// built once per mesh on the host from the first matrix by pairwise matching
+// of strongest couplings, applied twice per level (aggregates of up to four).
+// Every later matrix version only re-runs the numeric Galerkin product
+// A_c = P^T A P of piecewise-constant P on the device as fixed-order gathers,
+// so the preconditioner always matches the current matrix (no lagged reuse).
+// The V-cycle uses damped-Jacobi smoothing and a dense inverse on the coarsest
+// level, symmetric as PCG requires.
+#pragma once
+
+#include "linalg.h"
+
+#include <vector>
+
+namespace bsg {
+
+class AmgPreconditioner : public Preconditioner {
+public:
+    AmgPreconditioner(DeviceMesh& mesh, const SolverConfig& cfg);
+    ~AmgPreconditioner() override;
+    // Numeric setup for matrix A (same pattern as the mesh).  The structure is
+    // built on the first call.
+    void update(const Dcsr<double>& A, bool numeric);
+    void apply(Context& ctx, const double* r, double* z) override;
+    int levels() const;
+    long long coarseRows(int level) const;
+
+    struct Level;
+
+private:
+    void buildStructure(const Dcsr<double>& A);
+    DeviceMesh& mesh_;
+    Context& ctx_;
+    SolverConfig cfg_;
+    std::vector<Level*> levels_;
+    bool built_ = false;
+    Dcsr<double> fine_{};
+};
+
+}  // namespace bsg

@@ -1,0 +1,655 @@
+// extern "C" boundary: converts exceptions to status codes, host arrays in the
+// caller's numbering to the device layout, and owns the opaque handles.
+#include "../../include/babelsim_b200.h"
+#include "amg.h"
+#include "fvm.h"
+#include "linalg.h"
+#include "simple.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+struct bsg_context {
+    std::unique_ptr<bsg::Context> ctx;
+};
+struct bsg_mesh {
+    bsg_context* owner;
+    std::unique_ptr<bsg::DeviceMesh> mesh;
+};
+struct bsg_field {
+    bsg_mesh* mesh;
+    std::unique_ptr<bsg::DeviceField> field;
+};
+struct bsg_equation {
+    bsg_field* unknown;
+    std::unique_ptr<bsg::DeviceEquation> eq;
+    std::unique_ptr<bsg::KrylovSolver> krylov;
+    std::unique_ptr<bsg::AmgPreconditioner> amg;
+    bsg::Reducer red;
+    bsg::DeviceArray<int> flags;
+};
+struct bsg_simple {
+    bsg_mesh* mesh;
+    std::unique_ptr<bsg::SimpleSolver> solver;
+};
+
+namespace bsg {
+
+Context::Context(int dev) : device(dev) {
+    int count = 0;
+    checkCuda(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (dev < 0 || dev >= count) fail(kArgument, "CUDA device index out of range");
+    checkCuda(cudaSetDevice(dev), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    checkCuda(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+    if (prop.major < 10) fail(kState, "babelsim_b200 kernels are built for sm_100a (Blackwell); device is sm_" +
+                                         std::to_string(prop.major) + std::to_string(prop.minor));
+    sm_count = prop.multiProcessorCount;
+    checkCuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    checkCuda(cudaMallocHost(reinterpret_cast<void**>(&pinned), 64 * sizeof(double)), "cudaMallocHost");
+}
+
+Context::~Context() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (pinned) cudaFreeHost(pinned);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace bsg
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+int guard(bsg_context* ctx, F&& body) {
+    try {
+        body();
+        return bsg::kOk;
+    } catch (const bsg::Error& e) {
+        (ctx ? ctx->ctx->last_error : g_error) = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        (ctx ? ctx->ctx->last_error : g_error) = "host allocation failed";
+        return bsg::kMemory;
+    } catch (const std::exception& e) {
+        (ctx ? ctx->ctx->last_error : g_error) = e.what();
+        return bsg::kState;
+    }
+}
+
+bsg_context* ctxOf(const bsg_mesh* m) { return m ? m->owner : nullptr; }
+bsg_context* ctxOf(const bsg_field* f) { return f ? f->mesh->owner : nullptr; }
+
+void require(bool ok, const char* message) {
+    if (!ok) bsg::fail(bsg::kArgument, message);
+}
+
+bsg::Options options(const bsg_options* o) {
+    bsg::Options r;
+    if (!o) return r;
+    r.interpolation = o->interpolation;
+    r.gradient = o->gradient;
+    r.convection = o->convection;
+    r.diffusion = o->diffusion;
+    r.coefficient_interpolation = o->coefficient_interpolation;
+    r.coefficient_gradient = o->coefficient_gradient;
+    require(r.interpolation == 0 || r.interpolation == 1, "unsupported interpolation method");
+    require(r.gradient == 0 || r.gradient == 1, "unsupported gradient method");
+    require(r.convection >= 0 && r.convection <= 2, "unsupported convection method");
+    require(r.diffusion >= 0 && r.diffusion <= 2, "unsupported diffusion method");
+    return r;
+}
+
+bsg::SolverConfig solverConfig(const bsg_solver_config* c) {
+    bsg::SolverConfig r;
+    if (!c) return r;
+    r.solver = c->solver;
+    r.preconditioner = c->preconditioner;
+    r.atol = c->absolute_tolerance;
+    r.rtol = c->relative_tolerance;
+    r.max_iterations = c->max_iterations;
+    r.warm_start = c->warm_start != 0;
+    r.rebuild_interval = c->preconditioner_rebuild_interval;
+    r.reuse_growth = c->preconditioner_reuse_iteration_growth;
+    r.amg_max_levels = c->amg_max_levels;
+    r.amg_coarse_size = c->amg_coarse_size;
+    r.amg_smoothing_steps = c->amg_smoothing_steps;
+    r.precision = c->precision;
+    // LinearSolverConfig::validate (src/backend/solver_control.cpp:8-30)
+    require(r.atol > 0 && std::isfinite(r.atol) && r.rtol > 0 && std::isfinite(r.rtol) && r.max_iterations > 0,
+            "linear solver tolerances or iteration limit are invalid");
+    require(r.solver >= 0 && r.solver <= 3, "unknown linear solver type");
+    require(r.preconditioner >= 0 && r.preconditioner <= 6, "unknown preconditioner type");
+    return r;
+}
+
+void toResult(const bsg::SolveOutcome& o, bsg_solve_result* r) {
+    r->status = o.status;
+    r->iterations = o.iterations;
+    r->initial_residual = o.initial;
+    r->final_residual = o.final_;
+    r->relative_residual = o.relative;
+}
+
+// Solve an equation's device LDU system: 3 components through the lockstep
+// BiCGStab, scalars through CG/BiCGStab with Jacobi or AMG.
+void solveEquation(bsg_equation* e, const bsg::SolverConfig& cfg, bsg_solve_result* results) {
+    bsg::DeviceEquation& eq = *e->eq;
+    bsg::DeviceMesh& m = *eq.x->mesh;
+    bsg::Context& ctx = *m.ctx;
+    if (!e->krylov) e->krylov = std::make_unique<bsg::KrylovSolver>(ctx);
+    bsg::Dcsr<double> A{m.n_cells, m.cf_ptr.data(), m.cf_col.data(), eq.diag.data(), eq.val.data(),
+                        2LL * m.n_interior};
+    if (eq.x->comps == 3) {
+        bsg::SolveOutcome o[3];
+        e->krylov->solveVector3(A, cfg, eq.src.data(), eq.x->v.data(), o);
+        for (int c = 0; c < 3; ++c) toResult(o[c], results + c);
+        return;
+    }
+    std::unique_ptr<bsg::Preconditioner> jac;
+    bsg::Preconditioner* pc = nullptr;
+    if (cfg.preconditioner == 2 || cfg.preconditioner == 3) {
+        if (!e->amg) e->amg = std::make_unique<bsg::AmgPreconditioner>(m, cfg);
+        e->amg->update(A, true);
+        pc = e->amg.get();
+    } else if (cfg.preconditioner != 0) {
+        auto j = std::make_unique<bsg::JacobiPreconditioner>();
+        j->diag = eq.diag.data();
+        j->n = m.n_cells;
+        pc = j.get();
+        jac = std::move(j);
+    }
+    const bsg::SolveOutcome o = e->krylov->solveScalar(A, cfg, pc, eq.src.data(), eq.x->v.data());
+    toResult(o, results);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bsg_global_error(void) { return g_error.c_str(); }
+
+int bsg_context_create(int32_t device, bsg_context** out) {
+    return guard(nullptr, [&] {
+        require(out != nullptr, "null output handle");
+        auto* c = new bsg_context();
+        try {
+            c->ctx = std::make_unique<bsg::Context>(device);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int bsg_context_destroy(bsg_context* ctx) {
+    delete ctx;
+    return bsg::kOk;
+}
+
+const char* bsg_last_error(const bsg_context* ctx) { return ctx ? ctx->ctx->last_error.c_str() : g_error.c_str(); }
+
+int bsg_context_launches(const bsg_context* ctx, int64_t* out) {
+    if (!ctx || !out) return bsg::kArgument;
+    *out = ctx->ctx->launches;
+    return bsg::kOk;
+}
+
+int bsg_context_synchronize(bsg_context* ctx) {
+    return guard(ctx, [&] { ctx->ctx->sync(); });
+}
+
+int bsg_mesh_create(bsg_context* ctx, const bsg_mesh_geometry* g, bsg_mesh** out) {
+    return guard(ctx, [&] {
+        require(ctx && g && out, "null argument");
+        require(g->n_cells > 0 && g->n_faces > 0 && g->n_patches > 0, "mesh sizes must be positive");
+        bsg::HostGeometry h;
+        h.n_cells = g->n_cells;
+        h.n_faces = g->n_faces;
+        h.n_patches = g->n_patches;
+        const std::size_t F = g->n_faces, N = g->n_cells;
+        h.owner.assign(g->face_owner, g->face_owner + F);
+        h.nbr.assign(g->face_neighbour, g->face_neighbour + F);
+        h.patch.assign(g->face_patch, g->face_patch + F);
+        h.Sf.assign(g->face_area_vectors, g->face_area_vectors + 3 * F);
+        h.xf.assign(g->face_centres, g->face_centres + 3 * F);
+        h.area.assign(g->face_areas, g->face_areas + F);
+        h.normal.assign(g->face_normals, g->face_normals + 3 * F);
+        h.weight.assign(g->face_owner_weights, g->face_owner_weights + F);
+        h.dcoef.assign(g->face_orthogonal_coefficients, g->face_orthogonal_coefficients + F);
+        h.kvec.assign(g->face_non_orthogonal, g->face_non_orthogonal + 3 * F);
+        h.skew.assign(g->face_skewness, g->face_skewness + 3 * F);
+        h.xc.assign(g->cell_centres, g->cell_centres + 3 * N);
+        h.V.assign(g->cell_volumes, g->cell_volumes + N);
+        h.orthogonal = g->orthogonal_geometry != 0;
+        auto* m = new bsg_mesh{ctx, nullptr};
+        try {
+            m->mesh = bsg::buildDeviceMesh(*ctx->ctx, h);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int bsg_mesh_create_polyhedral(bsg_context* ctx, int32_t n_vertices, const double* vertices, int32_t n_faces,
+                               const int32_t* offsets, const int32_t* ids, const int32_t* owner,
+                               const int32_t* neighbour, const int32_t* patch, int32_t n_patches, bsg_mesh** out) {
+    return guard(ctx, [&] {
+        require(ctx && vertices && offsets && ids && owner && neighbour && patch && out, "null argument");
+        const bsg::HostGeometry h = bsg::computePolyhedralGeometry(n_vertices, vertices, n_faces, offsets, ids, owner,
+                                                                    neighbour, patch, n_patches);
+        auto* m = new bsg_mesh{ctx, nullptr};
+        try {
+            m->mesh = bsg::buildDeviceMesh(*ctx->ctx, h);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int bsg_mesh_destroy(bsg_mesh* mesh) {
+    delete mesh;
+    return bsg::kOk;
+}
+
+int bsg_mesh_sizes(const bsg_mesh* mesh, int64_t out[5]) {
+    if (!mesh || !out) return bsg::kArgument;
+    const bsg::DeviceMesh& m = *mesh->mesh;
+    out[0] = m.n_cells; out[1] = m.n_faces; out[2] = m.n_interior; out[3] = m.n_patches; out[4] = m.orthogonal;
+    return bsg::kOk;
+}
+
+int bsg_mesh_export(const bsg_mesh* mesh, const char* name, void* host_out) {
+    return guard(ctxOf(mesh), [&] {
+        require(mesh && name && host_out, "null argument");
+        const bsg::DeviceMesh& m = *mesh->mesh;
+        const std::string n(name);
+        auto put = [&](const auto& v) { std::memcpy(host_out, v.data(), v.size() * sizeof(v[0])); };
+        if (n == "face_owner") put(m.ext_owner);
+        else if (n == "face_neighbour") put(m.ext_nbr);
+        else if (n == "face_patch") put(m.ext_patch);
+        else if (n == "face_area_vectors") put(m.ext_Sf);
+        else if (n == "face_centres") put(m.ext_xf);
+        else if (n == "face_areas") put(m.ext_area);
+        else if (n == "face_normals") put(m.ext_n);
+        else if (n == "face_owner_weights") put(m.ext_w);
+        else if (n == "face_orthogonal_coefficients") put(m.ext_dcoef);
+        else if (n == "face_non_orthogonal") put(m.ext_k);
+        else if (n == "face_skewness") put(m.ext_skew);
+        else if (n == "cell_centres") put(m.ext_xc);
+        else if (n == "cell_volumes") put(m.ext_V);
+        else bsg::fail(bsg::kArgument, "unknown geometry array " + n);
+    });
+}
+
+int bsg_field_create(bsg_mesh* mesh, int32_t location, int32_t components, bsg_field** out) {
+    return guard(ctxOf(mesh), [&] {
+        require(mesh && out, "null argument");
+        require(location == 0 || location == 1, "field location must be cell or face");
+        auto* f = new bsg_field{mesh, nullptr};
+        try {
+            f->field = std::make_unique<bsg::DeviceField>(*mesh->mesh, location, components);
+        } catch (...) {
+            delete f;
+            throw;
+        }
+        *out = f;
+    });
+}
+
+int bsg_field_destroy(bsg_field* field) {
+    delete field;
+    return bsg::kOk;
+}
+
+int bsg_field_set_boundary(bsg_field* field, int32_t patch, int32_t type, const double* value) {
+    return guard(ctxOf(field), [&] {
+        require(field != nullptr, "null field");
+        field->field->setBoundary(patch, type, value);
+    });
+}
+
+int bsg_field_upload(bsg_field* field, const double* host) {
+    return guard(ctxOf(field), [&] {
+        require(field && host, "null argument");
+        field->field->uploadExternal(host);
+    });
+}
+
+int bsg_field_download(const bsg_field* field, double* host) {
+    return guard(ctxOf(field), [&] {
+        require(field && host, "null argument");
+        field->field->downloadExternal(host);
+    });
+}
+
+int bsg_field_set_boundary_flux(bsg_field* field, const bsg_field* face_flux) {
+    return guard(ctxOf(field), [&] {
+        require(field && face_flux, "null argument");
+        field->field->setFluxContext(*face_flux->field);
+        field->mesh->owner->ctx->sync();
+    });
+}
+
+int bsg_math_grad(const bsg_field* in, int32_t method, bsg_field* out) {
+    return guard(ctxOf(in), [&] {
+        require(in && out, "null argument");
+        bsg::DeviceField& x = *in->field;
+        require(out->field->location == 0 && out->field->comps == 3 * x.comps, "gradient result has the wrong shape");
+        bsg::gradient(x, method, out->field->v);
+        x.mesh->ctx->sync();
+    });
+}
+
+int bsg_math_interpolate(const bsg_field* in, const bsg_options* o, bsg_field* out) {
+    return guard(ctxOf(in), [&] {
+        require(in && out, "null argument");
+        const bsg::Options op = options(o);
+        require(out->field->location == 1 && out->field->comps == in->field->comps, "interpolation result has the wrong shape");
+        bsg::interpolate(*in->field, op.interpolation, op.gradient, out->field->v);
+        in->field->mesh->ctx->sync();
+    });
+}
+
+int bsg_math_flux(bsg_field* velocity, const bsg_options* o, bsg_field* out) {
+    return guard(ctxOf(velocity), [&] {
+        require(velocity && out, "null argument");
+        const bsg::Options op = options(o);
+        bsg::faceFlux(*velocity->field, op.interpolation, op.gradient, *out->field);
+        velocity->field->mesh->ctx->sync();
+    });
+}
+
+int bsg_math_div_flux(const bsg_field* phi, bsg_field* out) {
+    return guard(ctxOf(phi), [&] {
+        require(phi && out && out->field->location == 0 && out->field->comps == 1, "divergence result must be a scalar cell field");
+        bsg::divFlux(*phi->field, out->field->v);
+        phi->field->mesh->ctx->sync();
+    });
+}
+
+int bsg_math_normal_gradient(const bsg_field* in, const bsg_field* gradient, const bsg_options* o, bsg_field* out) {
+    return guard(ctxOf(in), [&] {
+        require(in && out && in->field->comps == 1, "normal gradient of a scalar cell field");
+        const bsg::Options op = options(o);
+        bsg::DeviceArray<double> g;
+        const double* gp = nullptr;
+        if (gradient) gp = gradient->field->v.data();
+        else {
+            bsg::gradient(*in->field, op.gradient, g);
+            gp = g.data();
+        }
+        bsg::normalGradient(*in->field, gp, op.diffusion, out->field->v);
+        in->field->mesh->ctx->sync();
+    });
+}
+
+int bsg_equation_create(bsg_field* unknown, const bsg_options* o, bsg_equation** out) {
+    return guard(ctxOf(unknown), [&] {
+        require(unknown && out, "null argument");
+        auto* e = new bsg_equation();
+        e->unknown = unknown;
+        try {
+            e->eq = std::make_unique<bsg::DeviceEquation>(*unknown->field, options(o));
+            e->flags.resize(4);
+        } catch (...) {
+            delete e;
+            throw;
+        }
+        *out = e;
+    });
+}
+
+int bsg_equation_destroy(bsg_equation* eq) {
+    delete eq;
+    return bsg::kOk;
+}
+
+int bsg_equ_reset(bsg_equation* e) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] { e->eq->reset(); });
+}
+
+int bsg_equ_div(bsg_equation* e, const bsg_field* flux, double scale, const bsg_options* term) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && flux, "null argument");
+        const bsg::Options op = term ? options(term) : e->eq->options;
+        bsg::addConvection(*e->eq, *flux->field, scale, op);
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_laplacian(bsg_equation* e, const bsg_field* coefficient, double k, double factor, const bsg_options* term) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e != nullptr, "null equation");
+        const bsg::Options op = term ? options(term) : e->eq->options;
+        bsg::addLaplacian(*e->eq, coefficient ? coefficient->field.get() : nullptr, k, factor, op);
+    });
+}
+
+int bsg_equ_source(bsg_equation* e, const bsg_field* value, double factor) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && value && value->field->location == 0 && value->field->comps == e->eq->x->comps,
+                "equ::source requires a compatible cell field");
+        bsg::addSource(*e->eq, value->field->v.data(), factor);
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_relax(bsg_equation* e, const bsg_field* previous, double alpha) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && previous && previous->field->comps == e->eq->x->comps, "equ::relax requires a compatible cell field");
+        bsg::relax(*e->eq, previous->field->v.data(), alpha);
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_scale(bsg_equation* e, double factor) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        bsg::scale(*e->eq, factor);
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_reference_if_unanchored(bsg_equation* e, double value, int32_t* anchored_out) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        bsg::referenceIfUnanchored(*e->eq, value, e->flags.data());
+        bsg::Context& ctx = *e->eq->x->mesh->ctx;
+        int h[2];
+        BSG_CUDA(cudaMemcpyAsync(h, e->flags.data(), sizeof(h), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        if (h[1]) bsg::fail(bsg::kArgument, "reference requires a positive diagonal");
+        if (anchored_out) *anchored_out = h[0];
+    });
+}
+
+int bsg_equ_face_flux(const bsg_equation* e, const bsg_field* solution, bsg_field* out) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && solution && out && out->field->location == 1 && out->field->comps == 1, "bad face-flux arguments");
+        bsg::faceFluxEquation(*e->eq, solution->field->v.data(), out->field->v);
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_relative_residual(const bsg_equation* e, const bsg_field* x, double* out) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && x && out, "null argument");
+        auto* me = const_cast<bsg_equation*>(e);
+        bsg::relativeResidualNorms(*me->eq, x->field->v.data(), me->red);
+        bsg::Context& ctx = *e->eq->x->mesh->ctx;
+        double h[3];
+        BSG_CUDA(cudaMemcpyAsync(h, me->red.result.data(), sizeof(h), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        *out = std::sqrt(h[0]) / std::max(std::sqrt(h[1]) + std::sqrt(h[2]), 1e-30);
+    });
+}
+
+int bsg_equ_solve(bsg_equation* e, const bsg_solver_config* config, bsg_solve_result* results) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && config && results, "null argument");
+        solveEquation(e, solverConfig(config), results);
+    });
+}
+
+int bsg_equ_download(const bsg_equation* e, double* diagonal, double* upper, double* lower, double* source) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e != nullptr, "null equation");
+        const bsg::DeviceEquation& eq = *e->eq;
+        const bsg::DeviceMesh& m = *eq.x->mesh;
+        bsg::Context& ctx = *m.ctx;
+        std::vector<double> val(eq.val.size());
+        if (diagonal) eq.diag.download(diagonal, ctx.stream);
+        if (source) eq.src.download(source, ctx.stream);
+        eq.val.download(val.data(), ctx.stream);
+        ctx.sync();
+        for (int f = 0; f < m.n_faces; ++f) {
+            double u = 0.0, l = 0.0;
+            if (m.face_kind[f] == 0) {
+                const int i = m.face_slot[f];
+                u = val[m.h_slot_own[i]];
+                l = val[m.h_slot_nbr[i]];
+            }
+            if (upper) upper[f] = u;
+            if (lower) lower[f] = l;
+        }
+    });
+}
+
+int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t components, const double* diagonal,
+                  const double* upper, const double* lower, const double* source, double* x,
+                  bsg_solve_result* results) {
+    return guard(ctxOf(mesh), [&] {
+        require(mesh && config && diagonal && upper && lower && source && x && results, "null argument");
+        require(components == 1 || components == 3, "components must be 1 or 3");
+        bsg::DeviceMesh& m = *mesh->mesh;
+        bsg::Context& ctx = *m.ctx;
+        const bsg::SolverConfig cfg = solverConfig(config);
+        // Pack the caller's LDU (face order) into the device slots.
+        std::vector<double> val(2 * static_cast<std::size_t>(m.n_interior));
+        for (int i = 0; i < m.n_interior; ++i) {
+            const int f = m.interior_ext[i];
+            val[m.h_slot_own[i]] = upper[f];
+            val[m.h_slot_nbr[i]] = lower[f];
+        }
+        for (int i = 0; i < m.n_cells; ++i)
+            if (!std::isfinite(diagonal[i])) bsg::fail(bsg::kNumeric, "nonfinite matrix diagonal");
+        bsg::DeviceField unknown(m, 0, components);
+        bsg::DeviceEquation eq(unknown, bsg::Options{});
+        eq.diag.upload(diagonal, m.n_cells, ctx.stream);
+        eq.val.upload(val, ctx.stream);
+        eq.src.upload(source, static_cast<std::size_t>(m.n_cells) * components, ctx.stream);
+        unknown.v.upload(x, static_cast<std::size_t>(m.n_cells) * components, ctx.stream);
+        bsg_field f{mesh, nullptr};
+        bsg_equation e;
+        e.unknown = &f;
+        e.eq.reset(&eq);
+        try {
+            solveEquation(&e, cfg, results);
+        } catch (...) {
+            e.eq.release();
+            throw;
+        }
+        e.eq.release();
+        unknown.v.download(x, ctx.stream);
+        ctx.sync();
+    });
+}
+
+int bsg_simple_create(bsg_mesh* mesh, const bsg_simple_config* c, bsg_simple** out) {
+    return guard(ctxOf(mesh), [&] {
+        require(mesh && c && out, "null argument");
+        bsg::SimpleConfig cfg;
+        cfg.rho = c->density;
+        cfg.mu = c->viscosity;
+        cfg.alpha_u = c->velocity_relaxation;
+        cfg.alpha_p = c->pressure_relaxation;
+        cfg.non_orthogonal_corrections = c->non_orthogonal_corrections;
+        cfg.mass_tolerance = c->continuity_tolerance;
+        cfg.velocity_tolerance = c->velocity_tolerance;
+        cfg.momentum_tolerance = c->momentum_tolerance;
+        cfg.pressure_tolerance = c->pressure_correction_tolerance;
+        cfg.momentum = options(&c->momentum);
+        cfg.pressure = options(&c->pressure);
+        cfg.momentum_solver = solverConfig(&c->momentum_solver);
+        cfg.pressure_solver = solverConfig(&c->pressure_solver);
+        require(cfg.alpha_u > 0 && cfg.alpha_u <= 1 && cfg.alpha_p > 0 && cfg.alpha_p <= 1, "relaxation must be in (0,1]");
+        require(cfg.non_orthogonal_corrections >= 0 && cfg.non_orthogonal_corrections <= 20,
+                "nonOrthogonalCorrections must be in [0,20]");
+        auto* s = new bsg_simple{mesh, nullptr};
+        try {
+            s->solver = std::make_unique<bsg::SimpleSolver>(*mesh->mesh, cfg);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int32_t type, const double* value) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && field, "null argument");
+        const std::string n(field);
+        if (n == "U") s->solver->U().setBoundary(patch, type, value);
+        else if (n == "p") s->solver->p().setBoundary(patch, type, value);
+        else bsg::fail(bsg::kArgument, "SIMPLE boundary field must be U or p");
+    });
+}
+
+int bsg_simple_set_fields(bsg_simple* s, const double* U, const double* p) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && U && p, "null argument");
+        s->solver->U().uploadExternal(U);
+        s->solver->p().uploadExternal(p);
+        s->solver->start();
+    });
+}
+
+int bsg_simple_set_flux(bsg_simple* s, const double* phi) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && phi, "null argument");
+        s->solver->phi().uploadExternal(phi);
+    });
+}
+
+int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report* report) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && max_iterations >= 0, "bad argument");
+        const bsg::SimpleReport r = s->solver->iterate(max_iterations);
+        if (report) {
+            report->iterations = r.iterations;
+            report->converged = r.converged;
+            report->status = r.status;
+            report->mass = r.mass;
+            report->dU = r.dU;
+            report->rU = r.rU;
+            report->dP = r.dP;
+            report->linear_pressure_residual = r.linP;
+            report->momentum_iterations = r.momentum_iterations;
+            report->pressure_iterations = r.pressure_iterations;
+        }
+    });
+}
+
+int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s != nullptr, "null argument");
+        if (U) s->solver->U().downloadExternal(U);
+        if (p) s->solver->p().downloadExternal(p);
+        if (phi) s->solver->phi().downloadExternal(phi);
+    });
+}
+
+int bsg_simple_destroy(bsg_simple* s) {
+    delete s;
+    return bsg::kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,712 @@
+// Krylov solvers on sm_100a with device-resident scalars.
+//
+// Every dot product is a fixed-grid, fixed-order two-stage reduction fused
+// into the kernel that produces its operands (SpMV+dot, axpy+norm), and the
+// scalar recurrences (alpha, beta, omega) are computed on the device by the
+// finishing kernel, so an iteration needs no host round trip.  The host only
+// reads a convergence word every `check_interval` iterations; kernels of
+// iterations issued after convergence return immediately.
+#include "bsg_device.cuh"
+#include "linalg.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace bsg {
+namespace {
+
+constexpr int kBlock = 256;
+
+// Device scalars of one solve.  Component-wise entries for the 3-RHS solver.
+struct Scalars {
+    double rho[3], alpha[3], omega[3], beta[3];
+    double rz[3];
+    double rr[3];           // current squared recursive residual norm
+    double target2[3];      // squared internal target
+    int done[3];            // 0 running, 1 converged (recursive), 2 breakdown
+    int iters[3];
+    int max_iters;
+    int all_done;
+};
+
+__device__ __forceinline__ bool allDone(const Scalars* s) { return s->all_done != 0; }
+
+template <int NV>
+__device__ __forceinline__ void writePartial(double v[NV], double* partial) {
+    blockSum<NV, kBlock>(v);
+    if (threadIdx.x == 0)
+        for (int j = 0; j < NV; ++j) partial[NV * blockIdx.x + j] = v[j];
+}
+
+template <int NV>
+__device__ __forceinline__ void finishSums(int blocks, const double* partial, double out[NV]) {
+    // single warp, lanes stride over blocks, fixed order within a lane then shuffle tree
+    const int lane = threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = 0.0;
+        for (int b = lane; b < blocks; b += 32) x += partial[NV * b + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        out[j] = x;
+    }
+}
+
+// y = A x (C components) fused with partial sums of dot(d, y) per component.
+template <int C>
+__device__ __forceinline__ void rowProduct(const Dcsr<double>& A, int i, const double* __restrict__ x, double acc[C]) {
+    const double d = A.diag[i];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = d * x[C * i + c];
+    const int e = A.ptr[i + 1];
+    for (int k = A.ptr[i]; k < e; ++k) {
+        const double a = A.val[k];
+        const int j = A.col[k];
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] += a * x[C * j + c];
+    }
+}
+
+template <int C>
+__global__ void kSpmv(Dcsr<double> A, const double* __restrict__ x, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    double acc[C];
+    rowProduct<C>(A, i, x, acc);
+#pragma unroll
+    for (int c = 0; c < C; ++c) y[C * i + c] = acc[c];
+}
+
+// r = b - A x and ||r||^2 partials (single RHS).
+__global__ void kResidual(Dcsr<double> A, const double* __restrict__ b, const double* __restrict__ x,
+                          double* __restrict__ r, double* __restrict__ partial) {
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
+        double acc[1];
+        rowProduct<1>(A, i, x, acc);
+        const double ri = b[i] - acc[0];
+        r[i] = ri;
+        v[0] += ri * ri;
+    }
+    writePartial<1>(v, partial);
+}
+
+__global__ void kFinishNorm(int blocks, const double* __restrict__ partial, double* __restrict__ out) {
+    double s[1];
+    finishSums<1>(blocks, partial, s);
+    if (threadIdx.x == 0) out[0] = s[0];
+}
+
+__global__ void kJacobi(int n, const double* __restrict__ d, const double* __restrict__ r, double* __restrict__ z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) z[i] = r[i] / d[i];
+}
+
+// ------------------------------------------------------------------ PCG
+// Start: z = M r (done by caller), p = z, rz = r.z
+__global__ void kCgStart(int n, const double* __restrict__ r, const double* __restrict__ z, double* __restrict__ p,
+                         double* __restrict__ partial) {
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        p[i] = z[i];
+        v[0] += r[i] * z[i];
+    }
+    writePartial<1>(v, partial);
+}
+__global__ void kCgStartFinish(int blocks, const double* __restrict__ partial, Scalars* s) {
+    double v[1];
+    finishSums<1>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+        s->rz[0] = v[0];
+        if (!(isfinite(v[0])) || v[0] == 0.0) { s->done[0] = 2; s->all_done = 1; }
+    }
+}
+// q = A p, partial p.q
+__global__ void kCgSpmv(Dcsr<double> A, const double* __restrict__ p, double* __restrict__ q,
+                        double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
+        double acc[1];
+        rowProduct<1>(A, i, p, acc);
+        q[i] = acc[0];
+        v[0] += p[i] * acc[0];
+    }
+    writePartial<1>(v, partial);
+}
+__global__ void kCgAlpha(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[1];
+    finishSums<1>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+        const double pq = v[0];
+        if (!(fabs(pq) > 0.0) || !isfinite(pq)) { s->done[0] = 2; s->all_done = 1; return; }
+        s->alpha[0] = s->rz[0] / pq;
+    }
+}
+// x += alpha p, r -= alpha q, partial r.r
+__global__ void kCgUpdate(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                          const double* __restrict__ q, double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    const double a = s->alpha[0];
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        x[i] += a * p[i];
+        const double ri = r[i] - a * q[i];
+        r[i] = ri;
+        v[0] += ri * ri;
+    }
+    writePartial<1>(v, partial);
+}
+__global__ void kCgCheck(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[1];
+    finishSums<1>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+        s->rr[0] = v[0];
+        s->iters[0] += 1;
+        if (!isfinite(v[0])) { s->done[0] = 2; s->all_done = 1; }
+        else if (v[0] <= s->target2[0]) { s->done[0] = 1; s->all_done = 1; }
+        else if (s->iters[0] >= s->max_iters) { s->all_done = 1; }
+    }
+}
+// partial r.z (z = M r computed before)
+__global__ void kDot(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ partial,
+                     const Scalars* s) {
+    if (allDone(s)) return;
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) v[0] += a[i] * b[i];
+    writePartial<1>(v, partial);
+}
+__global__ void kCgBeta(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[1];
+    finishSums<1>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+        s->beta[0] = v[0] / s->rz[0];
+        s->rz[0] = v[0];
+    }
+}
+__global__ void kCgDirection(int n, double* __restrict__ p, const double* __restrict__ z, const Scalars* s) {
+    if (allDone(s)) return;
+    const double be = s->beta[0];
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) p[i] = z[i] + be * p[i];
+}
+__global__ void kCgJacobiBetaDirection(int n, double* __restrict__ p, const double* __restrict__ r,
+                                       const double* __restrict__ d, const Scalars* s) {
+    if (allDone(s)) return;
+    const double be = s->beta[0];
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) p[i] = r[i] / d[i] + be * p[i];
+}
+// Jacobi z = r/d fused with partial r.z
+__global__ void kJacobiDot(int n, const double* __restrict__ d, const double* __restrict__ r, double* __restrict__ partial,
+                           const Scalars* s) {
+    if (allDone(s)) return;
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) v[0] += r[i] * (r[i] / d[i]);
+    writePartial<1>(v, partial);
+}
+
+// ------------------------------------------------------- BiCGStab, C RHS
+// Right-Jacobi-preconditioned BiCGStab for C right-hand sides in lockstep.
+// Vectors are xyz interleaved; component c has its own scalars and flags.
+template <int C>
+__device__ __forceinline__ bool compActive(const Scalars* s, int c) { return s->done[c] == 0 && s->iters[c] < s->max_iters; }
+
+template <int C>
+__global__ void kBiStart(int n, const double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
+                         double* __restrict__ v, double* __restrict__ partial) {
+    double acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const double ri = r[C * i + c];
+            r0[C * i + c] = ri;
+            p[C * i + c] = 0.0;
+            v[C * i + c] = 0.0;
+            acc[c] += ri * ri;
+        }
+    }
+    writePartial<C>(acc, partial);
+}
+// rho_new = r0.r (given as partial of previous step), beta, p = r + beta (p - omega v), ph = p/d
+template <int C>
+__global__ void kBiDirection(int n, const double* __restrict__ d, const double* __restrict__ r,
+                             double* __restrict__ p, const double* __restrict__ v, double* __restrict__ ph,
+                             const Scalars* s) {
+    if (allDone(s)) return;
+    double be[C], om[C];
+    bool act[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) { be[c] = s->beta[c]; om[c] = s->omega[c]; act[c] = compActive<C>(s, c); }
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const double rd = 1.0 / d[i];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (!act[c]) continue;
+            const double pi = r[C * i + c] + be[c] * (p[C * i + c] - om[c] * v[C * i + c]);
+            p[C * i + c] = pi;
+            ph[C * i + c] = pi * rd;
+        }
+    }
+}
+// v = A ph, partial r0.v
+template <int C>
+__global__ void kBiSpmvV(Dcsr<double> A, const double* __restrict__ ph, double* __restrict__ v,
+                         const double* __restrict__ r0, double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double acc2[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc2[c] = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
+        double acc[C];
+        rowProduct<C>(A, i, ph, acc);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            v[C * i + c] = acc[c];
+            acc2[c] += r0[C * i + c] * acc[c];
+        }
+    }
+    writePartial<C>(acc2, partial);
+}
+template <int C>
+__global__ void kBiAlpha(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[C];
+    finishSums<C>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (!compActive<C>(s, c)) continue;
+            if (!(fabs(v[c]) > 0.0) || !isfinite(v[c])) { s->done[c] = 2; continue; }
+            s->alpha[c] = s->rho[c] / v[c];
+        }
+    }
+}
+// s = r - alpha v (stored in r), sh = s/d, partial s.s
+template <int C>
+__global__ void kBiS(int n, const double* __restrict__ d, double* __restrict__ r, const double* __restrict__ v,
+                     double* __restrict__ sh, double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double al[C], acc[C];
+    bool act[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) { al[c] = s->alpha[c]; act[c] = compActive<C>(s, c); acc[c] = 0.0; }
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const double rd = 1.0 / d[i];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (!act[c]) continue;
+            const double si = r[C * i + c] - al[c] * v[C * i + c];
+            r[C * i + c] = si;
+            sh[C * i + c] = si * rd;
+            acc[c] += si * si;
+        }
+    }
+    writePartial<C>(acc, partial);
+}
+// early exit: if ||s|| <= target, x += alpha ph and the component is done
+template <int C>
+__global__ void kBiCheckS(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[C];
+    finishSums<C>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (!compActive<C>(s, c)) continue;
+            s->rr[c] = v[c];
+            if (!isfinite(v[c])) s->done[c] = 2;
+            else if (v[c] <= s->target2[c]) s->done[c] = 3;  // half step accepted
+        }
+    }
+}
+// t = A sh, partials t.t, t.s (s lives in r)
+template <int C>
+__global__ void kBiSpmvT(Dcsr<double> A, const double* __restrict__ sh, double* __restrict__ t,
+                         const double* __restrict__ sv, double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double acc2[2 * C];
+#pragma unroll
+    for (int c = 0; c < 2 * C; ++c) acc2[c] = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
+        double acc[C];
+        rowProduct<C>(A, i, sh, acc);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            t[C * i + c] = acc[c];
+            acc2[2 * c] += acc[c] * acc[c];
+            acc2[2 * c + 1] += acc[c] * sv[C * i + c];
+        }
+    }
+    writePartial<2 * C>(acc2, partial);
+}
+template <int C>
+__global__ void kBiOmega(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[2 * C];
+    finishSums<2 * C>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (!compActive<C>(s, c)) continue;
+            s->omega[c] = v[2 * c] > 0.0 ? v[2 * c + 1] / v[2 * c] : 0.0;
+        }
+    }
+}
+// x += alpha ph + omega sh; r = s - omega t; partials r.r and r0.r.  Components
+// that accepted the half step (done == 3) take x += alpha ph only.
+template <int C>
+__global__ void kBiUpdate(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ ph,
+                          const double* __restrict__ sh, const double* __restrict__ t, const double* __restrict__ r0,
+                          double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double al[C], om[C], acc[2 * C];
+    int mode[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        al[c] = s->alpha[c]; om[c] = s->omega[c];
+        mode[c] = s->done[c] == 3 ? 2 : (compActive<C>(s, c) ? 1 : 0);
+        acc[2 * c] = 0.0; acc[2 * c + 1] = 0.0;
+    }
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (mode[c] == 0) continue;
+            if (mode[c] == 2) { x[C * i + c] += al[c] * ph[C * i + c]; continue; }
+            x[C * i + c] += al[c] * ph[C * i + c] + om[c] * sh[C * i + c];
+            const double ri = r[C * i + c] - om[c] * t[C * i + c];
+            r[C * i + c] = ri;
+            acc[2 * c] += ri * ri;
+            acc[2 * c + 1] += r0[C * i + c] * ri;
+        }
+    }
+    writePartial<2 * C>(acc, partial);
+}
+template <int C>
+__global__ void kBiCheck(int blocks, const double* __restrict__ partial, Scalars* s) {
+    if (allDone(s)) return;
+    double v[2 * C];
+    finishSums<2 * C>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+        int all = 1;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (s->done[c] == 3) { s->done[c] = 1; s->iters[c] += 1; continue; }
+            if (!compActive<C>(s, c)) continue;
+            s->iters[c] += 1;
+            const double rr = v[2 * c], rho_new = v[2 * c + 1];
+            s->rr[c] = rr;
+            if (!isfinite(rr)) { s->done[c] = 2; continue; }
+            if (rr <= s->target2[c]) { s->done[c] = 1; continue; }
+            if (s->omega[c] == 0.0 || !(fabs(rho_new) > 0.0)) { s->done[c] = 2; continue; }
+            s->beta[c] = (rho_new / s->rho[c]) * (s->alpha[c] / s->omega[c]);
+            s->rho[c] = rho_new;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) if (compActive<C>(s, c)) all = 0;
+        s->all_done = all;
+    }
+}
+template <int C>
+__global__ void kBiInit(int blocks, const double* __restrict__ partial, Scalars* s) {
+    double v[C];
+    finishSums<C>(blocks, partial, v);
+    if (threadIdx.x == 0) {
+        int all = 1;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            s->rho[c] = v[c];            // r0.r0
+            s->alpha[c] = 1.0; s->omega[c] = 1.0; s->beta[c] = 0.0;
+            s->rr[c] = v[c];
+            if (s->done[c] == 0 && !(v[c] > 0.0)) s->done[c] = 1;
+            if (s->done[c] == 0) all = 0;
+        }
+        s->all_done = all;
+    }
+}
+
+// r = b - A x for 3 interleaved components, partials of |r_c|^2 and |b_c|^2.
+__global__ void kResidual3(Dcsr<double> A, const double* __restrict__ b, const double* __restrict__ x,
+                           double* __restrict__ r, double* __restrict__ partial) {
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
+        double acc[3];
+        rowProduct<3>(A, i, x, acc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double bi = b[3 * i + c], ri = bi - acc[c];
+            r[3 * i + c] = ri;
+            v[c] += ri * ri;
+            v[3 + c] += bi * bi;
+        }
+    }
+    writePartial<6>(v, partial);
+}
+__global__ void kFinish6(int blocks, const double* __restrict__ partial, double* __restrict__ out) {
+    double s[6];
+    finishSums<6>(blocks, partial, s);
+    if (threadIdx.x == 0) for (int j = 0; j < 6; ++j) out[j] = s[j];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+struct KrylovSolver::Impl {
+    Context& ctx;
+    DeviceArray<double> r, z, p, q, r0, v, ph, sh, t, partial, tmp;
+    DeviceArray<Scalars> sc;
+    explicit Impl(Context& c) : ctx(c) { sc.resize(1); }
+    int grid(int n) const {
+        const long long g = (static_cast<long long>(n) + kBlock - 1) / kBlock;
+        return static_cast<int>(std::max<long long>(1, std::min<long long>(g, 4LL * ctx.sm_count)));
+    }
+    void ensure(std::size_t n) {
+        for (DeviceArray<double>* a : {&r, &z, &p, &q, &r0, &v, &ph, &sh, &t, &tmp})
+            if (a->size() < n) a->resize(n);
+        if (partial.size() < 8 * 4096) partial.resize(8 * 4096);
+    }
+};
+
+KrylovSolver::KrylovSolver(Context& ctx) : impl_(std::make_unique<Impl>(ctx)) {}
+KrylovSolver::~KrylovSolver() = default;
+
+void spmv(Context& ctx, const Dcsr<double>& A, const double* x, double* y, int C) {
+    const unsigned g = gridFor(A.n, kBlock);
+    if (C == 1) kSpmv<1><<<g, kBlock, 0, ctx.stream>>>(A, x, y);
+    else kSpmv<3><<<g, kBlock, 0, ctx.stream>>>(A, x, y);
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+}
+
+double trueResidualNorm(Context& ctx, const Dcsr<double>& A, const double* b, const double* x, double* r_ws) {
+    static thread_local DeviceArray<double> partial;
+    if (partial.size() < 4096) partial.resize(4096);
+    const int g = static_cast<int>(std::max<long long>(1, std::min<long long>((A.n + kBlock - 1) / kBlock, 4LL * ctx.sm_count)));
+    kResidual<<<g, kBlock, 0, ctx.stream>>>(A, b, x, r_ws, partial.data());
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+    kFinishNorm<<<1, 32, 0, ctx.stream>>>(g, partial.data(), reinterpret_cast<double*>(partial.data()) + 4000);
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+    BSG_CUDA(cudaMemcpyAsync(ctx.pinned, partial.data() + 4000, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    return std::sqrt(ctx.pinned[0]);
+}
+
+void JacobiPreconditioner::apply(Context& ctx, const double* r, double* z) {
+    kJacobi<<<gridFor(n, kBlock), kBlock, 0, ctx.stream>>>(n, diag, r, z);
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+}
+
+namespace {
+double hostNorm(Context& ctx, const double* x, int n, DeviceArray<double>& partial) {
+    // ||x|| via the residual kernel with a zero matrix is wasteful; use a dot kernel.
+    Scalars zero{};
+    (void)zero;
+    const int g = static_cast<int>(std::max<long long>(1, std::min<long long>((n + kBlock - 1) / kBlock, 4LL * ctx.sm_count)));
+    static thread_local DeviceArray<Scalars> idle;
+    if (idle.size() < 1) {
+        idle.resize(1);
+        Scalars s{};
+        BSG_CUDA(cudaMemcpyAsync(idle.data(), &s, sizeof(s), cudaMemcpyHostToDevice, ctx.stream));
+    }
+    kDot<<<g, kBlock, 0, ctx.stream>>>(n, x, x, partial.data(), idle.data());
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+    kFinishNorm<<<1, 32, 0, ctx.stream>>>(g, partial.data(), partial.data() + 8 * 4096 - 1);
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+    BSG_CUDA(cudaMemcpyAsync(ctx.pinned, partial.data() + 8 * 4096 - 1, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    return std::sqrt(ctx.pinned[0]);
+}
+
+inline double residualScale(double initial, double rhs) {
+    const double v = std::max(initial, rhs);
+    return v > 0.0 ? v : 1.0;
+}
+}  // namespace
+
+SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc,
+                                       const double* b, double* x) {
+    Impl& m = *impl_;
+    Context& ctx = m.ctx;
+    const int n = A.n;
+    m.ensure(n);
+    const int g = m.grid(n);
+    SolveOutcome out;
+    const double bnorm = hostNorm(ctx, b, n, m.partial);
+    double r0n = bnorm;
+    if (cfg.warm_start) r0n = trueResidualNorm(ctx, A, b, x, m.r.data());
+    else BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, ctx.stream));
+    const double scale = residualScale(r0n, bnorm);
+    const double target = std::max(cfg.atol, cfg.rtol * scale);
+    out.initial = r0n;
+    if (std::isfinite(r0n) && r0n <= target) {
+        out.status = 0; out.final_ = r0n; out.relative = r0n / scale;
+        return out;
+    }
+    double inner = target;
+    int used = 0;
+    double fin = r0n;
+    auto* jac = dynamic_cast<JacobiPreconditioner*>(pc);
+    for (int restart = 0; restart < 3 && used < cfg.max_iterations; ++restart) {
+        // r = b - A x
+        trueResidualNorm(ctx, A, b, x, m.r.data());
+        Scalars s{};
+        s.target2[0] = inner * inner;
+        s.iters[0] = used;
+        s.max_iters = cfg.max_iterations;
+        BSG_CUDA(cudaMemcpyAsync(m.sc.data(), &s, sizeof(s), cudaMemcpyHostToDevice, ctx.stream));
+        if (pc) pc->apply(ctx, m.r.data(), m.z.data());
+        else BSG_CUDA(cudaMemcpyAsync(m.z.data(), m.r.data(), sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx.stream));
+        kCgStart<<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.z.data(), m.p.data(), m.partial.data());
+        kCgStartFinish<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+        ctx.launched(); ctx.launched();
+        const int solver = cfg.solver;
+        (void)solver;
+        for (;;) {
+            for (int it = 0; it < check_interval; ++it) {
+                kCgSpmv<<<g, kBlock, 0, ctx.stream>>>(A, m.p.data(), m.q.data(), m.partial.data(), m.sc.data());
+                kCgAlpha<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kCgUpdate<<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.p.data(), m.q.data(), m.partial.data(),
+                                                         m.sc.data());
+                kCgCheck<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                ctx.launches += 4;
+                if (jac) {
+                    kJacobiDot<<<g, kBlock, 0, ctx.stream>>>(n, jac->diag, m.r.data(), m.partial.data(), m.sc.data());
+                    kCgBeta<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                    kCgJacobiBetaDirection<<<g, kBlock, 0, ctx.stream>>>(n, m.p.data(), m.r.data(), jac->diag,
+                                                                         m.sc.data());
+                    ctx.launches += 3;
+                } else {
+                    if (pc) pc->apply(ctx, m.r.data(), m.z.data());
+                    else BSG_CUDA(cudaMemcpyAsync(m.z.data(), m.r.data(), sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                                  ctx.stream));
+                    kDot<<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.z.data(), m.partial.data(), m.sc.data());
+                    kCgBeta<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                    kCgDirection<<<g, kBlock, 0, ctx.stream>>>(n, m.p.data(), m.z.data(), m.sc.data());
+                    ctx.launches += 3;
+                }
+            }
+            BSG_CUDA(cudaGetLastError());
+            BSG_CUDA(cudaMemcpyAsync(ctx.pinned, m.sc.data(), sizeof(Scalars), cudaMemcpyDeviceToHost, ctx.stream));
+            ctx.sync();
+            Scalars h;
+            std::memcpy(&h, ctx.pinned, sizeof(h));
+            if (h.all_done) {
+                used = h.iters[0];
+                break;
+            }
+        }
+        fin = trueResidualNorm(ctx, A, b, x, m.r.data());
+        if ((std::isfinite(fin) && fin <= target) || !std::isfinite(fin)) break;
+        inner *= 0.5;
+    }
+    out.iterations = used;
+    out.final_ = fin;
+    out.relative = fin / scale;
+    out.status = (std::isfinite(fin) && fin <= target) ? 0 : (std::isfinite(fin) ? 1 : 2);
+    return out;
+}
+
+void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                                SolveOutcome out[3]) {
+    Impl& m = *impl_;
+    Context& ctx = m.ctx;
+    const int n = A.n;
+    m.ensure(3 * static_cast<std::size_t>(n));
+    const int g = m.grid(n);
+    if (!cfg.warm_start) BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * 3 * n, ctx.stream));
+    double* result = m.partial.data() + 8 * 4096 - 8;
+    // r = b - A x with per-component squared norms; also ||b|| per component.
+    auto residual3 = [&](double res[3], double bres[3]) {
+        kResidual3<<<g, kBlock, 0, ctx.stream>>>(A, b, x, m.r.data(), m.partial.data());
+        kFinish6<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), result);
+        ctx.launches += 2;
+        BSG_CUDA(cudaGetLastError());
+        BSG_CUDA(cudaMemcpyAsync(ctx.pinned, result, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        for (int c = 0; c < 3; ++c) {
+            res[c] = std::sqrt(ctx.pinned[c]);
+            if (bres) bres[c] = std::sqrt(ctx.pinned[3 + c]);
+        }
+    };
+    double bn[3], r0n[3], scale[3], target[3], inner[3], fin[3];
+    int used[3] = {0, 0, 0};
+    bool finished[3] = {false, false, false};
+    residual3(r0n, bn);
+    for (int c = 0; c < 3; ++c) {
+        if (!cfg.warm_start) r0n[c] = bn[c];
+        scale[c] = residualScale(r0n[c], bn[c]);
+        target[c] = std::max(cfg.atol, cfg.rtol * scale[c]);
+        inner[c] = target[c];
+        fin[c] = r0n[c];
+        out[c] = SolveOutcome{};
+        out[c].initial = r0n[c];
+        if (std::isfinite(r0n[c]) && r0n[c] <= target[c]) finished[c] = true;
+    }
+    for (int restart = 0; restart < 3; ++restart) {
+        bool any = false;
+        for (int c = 0; c < 3; ++c) any = any || (!finished[c] && used[c] < cfg.max_iterations);
+        if (!any) break;
+        if (restart > 0) { double dummy[3]; residual3(dummy, nullptr); }
+        Scalars s{};
+        for (int c = 0; c < 3; ++c) {
+            s.target2[c] = inner[c] * inner[c];
+            s.done[c] = (finished[c] || used[c] >= cfg.max_iterations) ? 1 : 0;
+            s.iters[c] = used[c];
+        }
+        s.max_iters = cfg.max_iterations;
+        BSG_CUDA(cudaMemcpyAsync(m.sc.data(), &s, sizeof(s), cudaMemcpyHostToDevice, ctx.stream));
+        kBiStart<3><<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.r0.data(), m.p.data(), m.v.data(), m.partial.data());
+        kBiInit<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+        ctx.launches += 2;
+        Scalars h{};
+        for (;;) {
+            for (int it = 0; it < check_interval; ++it) {
+                kBiDirection<3><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.p.data(), m.v.data(),
+                                                              m.ph.data(), m.sc.data());
+                kBiSpmvV<3><<<g, kBlock, 0, ctx.stream>>>(A, m.ph.data(), m.v.data(), m.r0.data(), m.partial.data(),
+                                                          m.sc.data());
+                kBiAlpha<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiS<3><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.v.data(), m.sh.data(), m.partial.data(),
+                                                      m.sc.data());
+                kBiCheckS<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiSpmvT<3><<<g, kBlock, 0, ctx.stream>>>(A, m.sh.data(), m.t.data(), m.r.data(), m.partial.data(),
+                                                          m.sc.data());
+                kBiOmega<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiUpdate<3><<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.ph.data(), m.sh.data(), m.t.data(),
+                                                           m.r0.data(), m.partial.data(), m.sc.data());
+                kBiCheck<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                ctx.launches += 9;
+            }
+            BSG_CUDA(cudaGetLastError());
+            BSG_CUDA(cudaMemcpyAsync(ctx.pinned, m.sc.data(), sizeof(Scalars), cudaMemcpyDeviceToHost, ctx.stream));
+            ctx.sync();
+            std::memcpy(&h, ctx.pinned, sizeof(h));
+            if (h.all_done) break;
+        }
+        double res[3];
+        residual3(res, nullptr);
+        for (int c = 0; c < 3; ++c) {
+            if (finished[c]) continue;
+            used[c] = h.iters[c];
+            fin[c] = res[c];
+            if (!std::isfinite(res[c]) || res[c] <= target[c] || h.done[c] == 2) finished[c] = true;
+            else inner[c] *= 0.5;
+        }
+    }
+    for (int c = 0; c < 3; ++c) {
+        out[c].iterations = used[c];
+        out[c].final_ = fin[c];
+        out[c].relative = fin[c] / scale[c];
+        out[c].status = (std::isfinite(fin[c]) && fin[c] <= target[c]) ? 0 : (std::isfinite(fin[c]) ? 1 : 2);
+    }
+}
+
+}  // namespace bsg

@@ -1,0 +1,85 @@
+// Sparse linear algebra on the device: DCSR matrices (diagonal + off-diagonal
+// CSR), Krylov solvers with device-resident scalars, preconditioners.
+#pragma once
+
+#include "bsg_internal.h"
+
+#include <memory>
+#include <vector>
+
+namespace bsg {
+
+// A square matrix in "diagonal + off-diagonal CSR" form; arrays are borrowed.
+template <class T>
+struct Dcsr {
+    int n = 0;
+    const int* ptr = nullptr;
+    const int* col = nullptr;
+    const T* diag = nullptr;
+    const T* val = nullptr;
+    long long nnz_off = 0;
+};
+
+// LinearSolverConfig (include/babelsim/solver_control.h:165-184).
+struct SolverConfig {
+    int solver = 1;            // 0 CG, 1 BiCGSTAB, 2 GMRES, 3 FGMRES
+    int preconditioner = 4;    // PreconditionerType order
+    double atol = 1e-12, rtol = 1e-8;
+    int max_iterations = 1000;
+    bool warm_start = false;
+    int rebuild_interval = 8;
+    double reuse_growth = 2.0;
+    int amg_max_levels = 12, amg_coarse_size = 48, amg_smoothing_steps = 2;
+    int precision = 0;         // 0 FP64, 1 FP32 inner iterations with FP64 refinement
+};
+
+// SolveResult (include/babelsim/solver_control.h:227-258).
+struct SolveOutcome {
+    int status = 2;            // 0 converged, 1 max iterations, 2 numerical failure
+    int iterations = 0;
+    double initial = 0.0, final_ = 0.0, relative = 0.0;
+};
+
+class AmgHierarchy;
+
+// Preconditioner application z = M^-1 r for a single right-hand side.
+struct Preconditioner {
+    virtual ~Preconditioner() = default;
+    virtual void apply(Context& ctx, const double* r, double* z) = 0;
+};
+
+// Workspace and driver for solving A x = b with the reference's acceptance
+// contract (src/backend/petsc_linear_system.cpp:355-481):
+// ||b-Ax|| <= max(atol, rtol*max(||r0||,||b||)), zero initial guess unless
+// warm_start, up to 3 true-residual restarts with a halved internal target.
+class KrylovSolver {
+public:
+    explicit KrylovSolver(Context& ctx);
+    ~KrylovSolver();
+    // Scalar system; x holds the guess on entry (warm start) and the solution on exit.
+    SolveOutcome solveScalar(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc,
+                             const double* b, double* x);
+    // Three right-hand sides (xyz interleaved) sharing one matrix; Jacobi-preconditioned
+    // BiCGStab in lockstep, one matrix read per product for all three.
+    void solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                      SolveOutcome out[3]);
+    int check_interval = 8;  // iterations between host convergence checks
+
+private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+// Jacobi preconditioner (point diagonal).
+struct JacobiPreconditioner : Preconditioner {
+    const double* diag = nullptr;
+    int n = 0;
+    void apply(Context& ctx, const double* r, double* z) override;
+};
+
+// Device SpMV y = A x for C interleaved components.
+void spmv(Context& ctx, const Dcsr<double>& A, const double* x, double* y, int C);
+// ||b - A x||_2 for one right-hand side, returned to the host.
+double trueResidualNorm(Context& ctx, const Dcsr<double>& A, const double* b, const double* x, double* r_ws);
+
+}  // namespace bsg

@@ -1,0 +1,59 @@
+// Steady SIMPLE outer loop on device-resident state (src/physics/simple/main.cpp:11-131).
+#pragma once
+
+#include "fvm.h"
+#include "linalg.h"
+
+#include <memory>
+
+namespace bsg {
+
+class AmgPreconditioner;
+
+struct SimpleConfig {
+    double rho = 1.0, mu = 0.01, alpha_u = 0.7, alpha_p = 0.3;
+    int non_orthogonal_corrections = 1;
+    double mass_tolerance = 1e-8, velocity_tolerance = 1e-7, momentum_tolerance = 1e-6,
+           pressure_tolerance = 1e-6;
+    Options momentum, pressure;
+    SolverConfig momentum_solver, pressure_solver;
+};
+
+struct SimpleReport {
+    int iterations = 0;
+    bool converged = false;
+    int status = 1;
+    double mass = 0, dU = 0, rU = 0, dP = 0, linP = 0;
+    int momentum_iterations = 0, pressure_iterations = 0;
+};
+
+class SimpleSolver {
+public:
+    SimpleSolver(DeviceMesh& mesh, const SimpleConfig& cfg);
+    ~SimpleSolver();
+    DeviceField& U() { return U_; }
+    DeviceField& p() { return p_; }
+    DeviceField& phi() { return phi_; }
+    // Initial state: phi = flux(U) (simple/main.cpp:40).
+    void start();
+    // Outer iterations until converged or `max_iterations` more are done.
+    SimpleReport iterate(int max_iterations);
+    const SimpleReport& report() const { return report_; }
+
+private:
+    void outerIteration();
+    DeviceMesh& m_;
+    Context& ctx_;
+    SimpleConfig cfg_;
+    DeviceField U_, p_, phi_, pP_, muEff_, rAU_, phiH_;
+    std::unique_ptr<DeviceEquation> mom_, peq_;
+    KrylovSolver krylov_;
+    std::unique_ptr<Preconditioner> ppc_;
+    Reducer red_;
+    DeviceArray<double> Uprev_, gradP_, gradPP_, divPhiH_, pflux_, diag_ws_;
+    DeviceArray<int> flags_;
+    SimpleReport report_;
+    bool started_ = false;
+};
+
+}  // namespace bsg

@@ -1,0 +1,253 @@
+/*
+ * babelsim_b200 - C ABI of the B200-native BabelSim finite-volume hot path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.  Every
+ * entry point returns BSG_OK (0) or a positive error code and records a message
+ * readable with bsg_last_error().  No entry point throws across the ABI.
+ *
+ * The ABI replaces two seams of the reference (midway-official/BabelSim):
+ *
+ *   1. the linear-system backend, detail::ComputeBackend
+ *      (src/internal/compute_backend.h:17-41; PETSc implementation
+ *      src/backend/petsc_backend.cpp:123-198) -> bsg_solve_ldu();
+ *   2. the equ:: / math:: operator SDK whose face loops live in
+ *      src/discretization/{operators,procedural_equation,fvm_execution}.cpp
+ *      -> bsg_field_* / bsg_math_* / bsg_equ_* on device-resident fields and
+ *      equations, plus the steady SIMPLE driver (src/physics/simple/main.cpp)
+ *      -> bsg_simple_*.
+ *
+ * Numbering: every host array crossing the ABI uses the caller's (reference)
+ * cell and face numbering.  Vec3 data are xyz-interleaved (MeshStorage<Vec3>
+ * layout, include/babelsim/vector.h); Tensor3 data are 9 doubles per cell,
+ * row c = gradient of component c (vector.h Tensor3::rows).
+ */
+#ifndef BABELSIM_B200_H
+#define BABELSIM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+    BSG_OK = 0,
+    BSG_ERR_ARGUMENT = 1,   /* std::invalid_argument in the reference */
+    BSG_ERR_CUDA = 2,       /* CUDA runtime failure */
+    BSG_ERR_NUMERIC = 3,    /* non-finite coefficient or value */
+    BSG_ERR_STATE = 4,      /* std::logic_error in the reference */
+    BSG_ERR_MEMORY = 5      /* device allocation or admission refused */
+};
+
+/* ---- enumerations: same order as the reference's enums ---------------- */
+/* BoundaryType, include/babelsim/field.h:23-32 */
+enum { BSG_FIXED_VALUE = 0, BSG_FIXED_GRADIENT = 1, BSG_ZERO_GRADIENT = 2,
+       BSG_INLET_OUTLET = 3, BSG_SYMMETRY = 4 };
+/* InterpolationMethod / GradientMethod / ConvectionMethod / DiffusionMethod,
+ * include/babelsim/methods.h:7-27 */
+enum { BSG_INTERP_LINEAR = 0, BSG_INTERP_CORRECTED = 1 };
+enum { BSG_GRAD_GREEN_GAUSS = 0, BSG_GRAD_LEAST_SQUARES = 1 };
+enum { BSG_CONV_UPWIND = 0, BSG_CONV_LINEAR_UPWIND = 1, BSG_CONV_CENTRAL = 2 };
+enum { BSG_DIFF_ORTHOGONAL = 0, BSG_DIFF_CORRECTED = 1, BSG_DIFF_LIMITED_CORRECTED = 2 };
+/* LinearSolverType / PreconditionerType / SolveStatus,
+ * include/babelsim/solver_control.h:12-36 */
+enum { BSG_KSP_CG = 0, BSG_KSP_BICGSTAB = 1, BSG_KSP_GMRES = 2, BSG_KSP_FGMRES = 3 };
+enum { BSG_PC_NONE = 0, BSG_PC_ICC = 1, BSG_PC_HYPRE = 2, BSG_PC_GAMG = 3,
+       BSG_PC_BJACOBI = 4, BSG_PC_ASM = 5, BSG_PC_JACOBI = 6 };
+enum { BSG_CONVERGED = 0, BSG_MAX_ITERATIONS = 1, BSG_NUMERICAL_FAILURE = 2 };
+/* Precision of the inner Krylov/AMG iterations (north-star form (c)). */
+enum { BSG_PRECISION_FP64 = 0, BSG_PRECISION_FP32_REFINED = 1 };
+/* Field locations, include/babelsim/field.h:17-21 */
+enum { BSG_CELL = 0, BSG_FACE = 1 };
+
+typedef struct bsg_context bsg_context;
+typedef struct bsg_mesh bsg_mesh;
+typedef struct bsg_field bsg_field;
+typedef struct bsg_equation bsg_equation;
+typedef struct bsg_simple bsg_simple;
+
+/* OperatorOptions, include/babelsim/methods.h:31-60.  -1 in a coefficient
+ * member means "not set" (std::nullopt). */
+typedef struct {
+    int32_t interpolation;
+    int32_t gradient;
+    int32_t convection;
+    int32_t diffusion;
+    int32_t coefficient_interpolation;
+    int32_t coefficient_gradient;
+} bsg_options;
+
+/* LinearSolverConfig, include/babelsim/solver_control.h:165-184, plus the
+ * precision of the inner iterations. */
+typedef struct {
+    int32_t solver;
+    int32_t preconditioner;
+    double absolute_tolerance;
+    double relative_tolerance;
+    int32_t max_iterations;
+    int32_t warm_start;
+    int32_t preconditioner_rebuild_interval;
+    double preconditioner_reuse_iteration_growth;
+    int32_t amg_max_levels;
+    int32_t amg_coarse_size;
+    int32_t amg_smoothing_steps;
+    int32_t precision;
+} bsg_solver_config;
+
+/* SolveResult, include/babelsim/solver_control.h:227-258 */
+typedef struct {
+    int32_t status;
+    int32_t iterations;
+    double initial_residual;
+    double final_residual;
+    double relative_residual;
+} bsg_solve_result;
+
+/* Geometry of a mesh as the reference computes it (Mesh::Storage,
+ * include/babelsim/mesh.h:138-177; src/core/mesh.cpp:321-564). */
+typedef struct {
+    int32_t n_cells;
+    int32_t n_faces;
+    int32_t n_patches;
+    const int32_t* face_owner;                  /* n_faces */
+    const int32_t* face_neighbour;              /* n_faces, -1 on boundary */
+    const int32_t* face_patch;                  /* n_faces, -1 on interior */
+    const double* face_area_vectors;            /* 3*n_faces */
+    const double* face_centres;                 /* 3*n_faces */
+    const double* face_areas;                   /* n_faces */
+    const double* face_normals;                 /* 3*n_faces */
+    const double* face_owner_weights;           /* n_faces */
+    const double* face_orthogonal_coefficients; /* n_faces */
+    const double* face_non_orthogonal;          /* 3*n_faces */
+    const double* face_skewness;                /* 3*n_faces */
+    const double* cell_centres;                 /* 3*n_cells */
+    const double* cell_volumes;                 /* n_cells */
+    int32_t orthogonal_geometry;
+} bsg_mesh_geometry;
+
+/* ---- context ---------------------------------------------------------- */
+int bsg_context_create(int32_t device, bsg_context** out);
+int bsg_context_destroy(bsg_context* ctx);
+/* Message of the last failed call on this context (never NULL). */
+const char* bsg_last_error(const bsg_context* ctx);
+/* Message of the last failure of a call that had no context to report on. */
+const char* bsg_global_error(void);
+/* Number of kernels this context has launched so far. */
+int bsg_context_launches(const bsg_context* ctx, int64_t* out);
+/* Wait for all work of this context. */
+int bsg_context_synchronize(bsg_context* ctx);
+
+/* ---- mesh --------------------------------------------------------------
+ * bsg_mesh_create takes geometry already computed by the caller (the drop-in
+ * for a reference Mesh: pass its MeshStorage arrays).
+ * bsg_mesh_create_polyhedral computes the geometry itself from a polyhedral
+ * description (Mesh::polyhedral, src/core/mesh.cpp:321-564; the
+ * BABELSIM_MESH 3 face list, src/io/mesh_reader.cpp:44-111). */
+int bsg_mesh_create(bsg_context* ctx, const bsg_mesh_geometry* geometry, bsg_mesh** out);
+int bsg_mesh_create_polyhedral(bsg_context* ctx, int32_t n_vertices, const double* vertices,
+                               int32_t n_faces, const int32_t* face_point_offsets,
+                               const int32_t* face_point_ids, const int32_t* owner,
+                               const int32_t* neighbour, const int32_t* patch, int32_t n_patches,
+                               bsg_mesh** out);
+int bsg_mesh_destroy(bsg_mesh* mesh);
+/* n_cells, n_faces, n_interior_faces, n_patches, orthogonal flag. */
+int bsg_mesh_sizes(const bsg_mesh* mesh, int64_t out[5]);
+/* Copy one geometry array (a bsg_mesh_geometry member name, e.g.
+ * "face_area_vectors") back to host memory in the caller's numbering. */
+int bsg_mesh_export(const bsg_mesh* mesh, const char* name, void* host_out);
+
+/* ---- fields (Field<T>, include/babelsim/field.h:57-374) ----------------
+ * components: 1 (scalar), 3 (vector) or 9 (tensor, cell only). */
+int bsg_field_create(bsg_mesh* mesh, int32_t location, int32_t components, bsg_field** out);
+int bsg_field_destroy(bsg_field* field);
+int bsg_field_set_boundary(bsg_field* field, int32_t patch, int32_t type, const double* value);
+int bsg_field_upload(bsg_field* field, const double* host_values);
+int bsg_field_download(const bsg_field* field, double* host_values);
+/* The inletOutlet flux context (Field::setBoundaryFlux, field.h:274-281). */
+int bsg_field_set_boundary_flux(bsg_field* field, const bsg_field* face_flux);
+
+/* ---- explicit operators (math::, include/babelsim/math.h:106-180) ------ */
+int bsg_math_grad(const bsg_field* in, int32_t gradient_method, bsg_field* out);
+int bsg_math_interpolate(const bsg_field* in, const bsg_options* options, bsg_field* out_face);
+int bsg_math_flux(bsg_field* velocity, const bsg_options* options, bsg_field* out_face);
+int bsg_math_div_flux(const bsg_field* face_flux, bsg_field* out_cell);
+int bsg_math_normal_gradient(const bsg_field* in, const bsg_field* gradient,
+                             const bsg_options* options, bsg_field* out_face);
+
+/* ---- implicit assembly (equ::, include/babelsim/equ.h:16-101) -----------
+ * An equation owns its LDU coefficients on the device; the unknown field
+ * supplies layout, boundary constraints and the current iterate. */
+int bsg_equation_create(bsg_field* unknown, const bsg_options* options, bsg_equation** out);
+int bsg_equation_destroy(bsg_equation* eq);
+int bsg_equ_reset(bsg_equation* eq);
+int bsg_equ_div(bsg_equation* eq, const bsg_field* flux, double scale, const bsg_options* term);
+/* coefficient: a cell or face scalar field, or NULL for the constant k. */
+int bsg_equ_laplacian(bsg_equation* eq, const bsg_field* coefficient, double k, double factor,
+                      const bsg_options* term);
+int bsg_equ_source(bsg_equation* eq, const bsg_field* value, double factor);
+int bsg_equ_relax(bsg_equation* eq, const bsg_field* previous, double alpha);
+int bsg_equ_scale(bsg_equation* eq, double factor);
+int bsg_equ_reference_if_unanchored(bsg_equation* eq, double value, int32_t* anchored_out);
+int bsg_equ_face_flux(const bsg_equation* eq, const bsg_field* solution, bsg_field* out_face);
+/* ||b-Ax|| / max(||Ax||+||b||, 1e-30) (procedural_equation.cpp:429-433). */
+int bsg_equ_relative_residual(const bsg_equation* eq, const bsg_field* x, double* out);
+int bsg_equ_solve(bsg_equation* eq, const bsg_solver_config* config, bsg_solve_result* results);
+/* LDU in the caller's face numbering (DiscreteEquation, discrete_equation.h:14-50). */
+int bsg_equ_download(const bsg_equation* eq, double* diagonal, double* upper, double* lower,
+                     double* source);
+
+/* ---- linear-system seam (ComputeBackend::solve, compute_backend.h:31-32) --
+ * Solves the LDU system given in host memory for 1 or 3 right-hand sides that
+ * share one matrix.  x is the initial guess when warm_start and the solution
+ * on return; source and x are xyz-interleaved for 3 components.  results gets
+ * one entry per component. */
+int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t components,
+                  const double* diagonal, const double* upper, const double* lower,
+                  const double* source, double* x, bsg_solve_result* results);
+
+/* ---- steady SIMPLE (src/physics/simple/main.cpp:11-131) ----------------- */
+typedef struct {
+    double density;
+    double viscosity;                   /* dynamic viscosity (physics "dynamicViscosity") */
+    double velocity_relaxation;
+    double pressure_relaxation;
+    int32_t non_orthogonal_corrections;
+    double continuity_tolerance;
+    double velocity_tolerance;
+    double momentum_tolerance;
+    double pressure_correction_tolerance;
+    bsg_options momentum;               /* equation.momentum (terms identical) */
+    bsg_options pressure;               /* equation.pressureCorrection diffusion term */
+    bsg_solver_config momentum_solver;
+    bsg_solver_config pressure_solver;
+} bsg_simple_config;
+
+typedef struct {
+    int32_t iterations;                 /* outer iterations done so far */
+    int32_t converged;
+    int32_t status;                     /* BSG_CONVERGED / MAX_ITERATIONS / NUMERICAL_FAILURE */
+    double mass;                        /* flux-balance relative imbalance */
+    double dU, rU, dP;
+    double linear_pressure_residual;
+    int32_t momentum_iterations;        /* Krylov iterations in the last outer iteration */
+    int32_t pressure_iterations;
+} bsg_simple_report;
+
+int bsg_simple_create(bsg_mesh* mesh, const bsg_simple_config* config, bsg_simple** out);
+/* Boundary constraint of "U" or "p" on one patch (the case's fields/initial). */
+int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int32_t type,
+                            const double* value);
+/* Initial U (3*n_cells) and p (n_cells); phi becomes flux(U) as in simple/main.cpp:40. */
+int bsg_simple_set_fields(bsg_simple* s, const double* U, const double* p);
+/* Resume from a saved face flux phi (n_faces) instead of flux(U). */
+int bsg_simple_set_flux(bsg_simple* s, const double* phi);
+/* Run outer iterations until converged or max_iterations more have been done. */
+int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report* report);
+int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi);
+int bsg_simple_destroy(bsg_simple* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

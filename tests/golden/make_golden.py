@@ -1,0 +1,183 @@
+"""Generate golden fixtures from the reference's own finite-volume sources.
+
+    python tests/golden/make_golden.py
+
+Requires oracle/_ref/babelsim-oracle (built by `make -C oracle/ref`, which
+compiles the reference sources in place).  For each case it writes a BabelSim
+case directory, runs the reference's unmodified SIMPLE loop for k = 1..K outer
+iterations (one run per k, so the state after every iteration is captured) and
+to convergence, and stores in tests/golden/<case>.npz:
+
+* the mesh (vertices, face rings, owner/neighbour/patch) and the geometry the
+  reference computed from it;
+* the assembled LDU systems of iteration K (momentum after relax/scale, each
+  pressure-correction system) as handed to the linear-solver backend;
+* U, p, phi after every iteration k <= K and at convergence.
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from babelsim_b200 import meshgen  # noqa: E402
+from oracle import refdata  # noqa: E402
+
+ORACLE = os.path.join(ROOT, "oracle", "_ref", "babelsim-oracle")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+BC_TEXT = {"fixedValue": "fixedValue", "zeroGradient": "zeroGradient", "symmetry": "symmetry",
+           "fixedGradient": "fixedGradient", "inletOutlet": "inletOutlet"}
+
+
+def vec(v):
+    return f"({v[0]!r} {v[1]!r} {v[2]!r})"
+
+
+def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics):
+    os.makedirs(os.path.join(path, "mesh"), exist_ok=True)
+    os.makedirs(os.path.join(path, "fields", "initial"), exist_ok=True)
+    os.makedirs(os.path.join(path, "numerics"), exist_ok=True)
+    os.makedirs(os.path.join(path, "physics"), exist_ok=True)
+    meshgen.write_mesh(os.path.join(path, "mesh", "case.mesh"), mesh)
+    with open(os.path.join(path, "case.bs"), "w") as f:
+        f.write("solver simple\nmesh mesh/case.mesh\nfields fields/initial\nphysics physics/simple.bs\n"
+                "methods numerics/methods.bs\nsolution numerics/solution.bs\ncontrol control.bs\noutput output.bs\n")
+    with open(os.path.join(path, "control.bs"), "w") as f:
+        f.write("startTime 0\nendTime 0\ndeltaT 1\n")
+    with open(os.path.join(path, "output.bs"), "w") as f:
+        f.write("directory results\ntimeName final\n")
+    with open(os.path.join(path, "physics", "simple.bs"), "w") as f:
+        f.write("".join(f"{k} {v!r}\n" for k, v in physics.items()))
+    with open(os.path.join(path, "numerics", "methods.bs"), "w") as f:
+        f.write("time steady\n")
+        for eq, opts in methods.items():
+            for k, v in opts.items():
+                f.write(f"equation.{eq}.{k} {v}\n")
+    with open(os.path.join(path, "numerics", "solution.bs"), "w") as f:
+        f.write("".join(f"{k} {v}\n" for k, v in solution.items()))
+
+    def field(name, kind, bcs):
+        lines = [f"field {name}", "{", f"    type {kind}", "    location cell",
+                 "    internal uniform " + ("(0 0 0)" if kind == "vector" else "(0)"), "    boundary", "    {"]
+        for patch, (t, v) in zip(mesh.patch_names, bcs):
+            if t in ("zeroGradient", "symmetry"):
+                lines.append(f"        {patch} {{ type {t} }}")
+            else:
+                val = vec(v) if kind == "vector" else f"({v!r})"
+                lines.append(f"        {patch} {{ type {t} value {val} }}")
+        lines += ["    }", "}"]
+        with open(os.path.join(path, "fields", "initial", f"{name}.field"), "w") as f:
+            f.write("\n".join(lines) + "\n")
+    field("U", "vector", U_bcs)
+    field("p", "scalar", p_bcs)
+
+
+def run(case_dir, iterations, dump=False):
+    sol = os.path.join(case_dir, "numerics", "solution.bs")
+    text = open(sol).read().splitlines()
+    text = [ln for ln in text if not ln.startswith("maxIterations ")] + [f"maxIterations {iterations}"]
+    open(sol, "w").write("\n".join(text) + "\n")
+    out = tempfile.mkdtemp(prefix="bsg_golden_")
+    env = dict(os.environ)
+    if dump:
+        os.makedirs(os.path.join(out, "dump"))
+        env["BABELSIM_ORACLE_DUMP"] = os.path.join(out, "dump")
+    res = subprocess.run([ORACLE, case_dir, out], env=env, capture_output=True, text=True)
+    if res.returncode not in (0, 2):
+        raise RuntimeError(res.stderr)
+    fields = refdata.read_records(os.path.join(out, "fields.bin"))
+    geo = refdata.read_records(os.path.join(out, "geometry.bin"))
+    info = json.load(open(os.path.join(out, "run.json")))
+    systems = refdata.read_systems(os.path.join(out, "dump")) if dump else []
+    shutil.rmtree(out)
+    return fields, geo, info, systems
+
+
+def make(name, mesh, U_bcs, p_bcs, methods, solution, physics, K, converge_iterations=None):
+    work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
+    write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics)
+    data = {}
+    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    data["mesh_vertices"] = mesh.vertices
+    data["mesh_offsets"] = offsets
+    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
+    for k in range(1, K + 1):
+        fields, geo, info, systems = run(work, k, dump=(k == K))
+        data[f"U_{k}"] = fields["U"].reshape(-1, 3)
+        data[f"p_{k}"] = fields["p"]
+        data[f"phi_{k}"] = fields["phi"]
+    for key, arr in geo.items():
+        data["geo_" + key] = arr
+    for j, s in enumerate(systems):
+        for key in ("diag", "upper", "lower", "source", "before", "after"):
+            data[f"sys{j}_{key}"] = s[key]
+        data[f"sys{j}_meta"] = np.array([s["status"], s["iterations"]])
+        data[f"sys{j}_identity"] = np.array(s["identity"])
+    data["n_systems_last"] = np.array(len(systems))
+    if converge_iterations:
+        fields, _, info, _ = run(work, converge_iterations)
+        data["U_conv"], data["p_conv"], data["phi_conv"] = fields["U"].reshape(-1, 3), fields["p"], fields["phi"]
+        data["conv_info"] = np.array([info["status"], info["reported_iteration_intervals"] + 1])
+    meta = dict(patch_names=mesh.patch_names, patch_kinds=mesh.patch_kinds, U_bcs=[(t, list(map(float, v)))
+                for t, v in U_bcs], p_bcs=[(t, float(v)) for t, v in p_bcs], methods=methods,
+                solution=solution, physics=physics, K=K)
+    data["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
+    shutil.rmtree(work)
+    print(name, "written", {k: v.shape for k, v in data.items() if k.startswith(("U_", "sys0_diag"))})
+
+
+def cavity_bcs(lid=(1.0, 0.0, 0.0)):
+    U = [("fixedValue", (0.0, 0.0, 0.0))] * 3 + [("fixedValue", lid), ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    p = [("zeroGradient", 0.0)] * 4 + [("symmetry", 0.0)] * 2
+    return U, p
+
+
+def config1_solution(p_rtol=1e-10):
+    return {"velocityRelaxation": 0.7, "pressureRelaxation": 0.3, "continuityTolerance": 1e-6,
+            "velocityTolerance": 1e-6, "momentumTolerance": 1e-6, "pressureCorrectionTolerance": 1e-6,
+            "nonOrthogonalCorrections": 2,
+            "equation.momentum.kspType": "bcgs", "equation.momentum.pcType": "bjacobi",
+            "equation.momentum.absoluteTolerance": 1e-15, "equation.momentum.relativeTolerance": 1e-12,
+            "equation.momentum.maxIterations": 2000,
+            "equation.pressureCorrection.kspType": "cg", "equation.pressureCorrection.pcType": "hypre",
+            "equation.pressureCorrection.absoluteTolerance": 1e-15,
+            "equation.pressureCorrection.relativeTolerance": p_rtol,
+            "equation.pressureCorrection.maxIterations": 20000}
+
+
+def methods(conv="upwind", grad="greenGauss", diff="orthogonal"):
+    o = dict(interpolation="linear", gradient=grad, convection=conv, diffusion=diff)
+    return {"momentum": o, "pressureCorrection": o}
+
+
+def main():
+    if not os.path.exists(ORACLE):
+        sys.exit(f"{ORACLE} missing: run `make -C oracle/ref` first")
+    U, p = cavity_bcs()
+    # config-1 settings on a 12x12x1 cavity (fast), 3 iterations + convergence
+    make("cavity12_upwind", meshgen.cavity_2d(12), U, p, methods(), config1_solution(1e-12),
+         {"density": 1.0, "dynamicViscosity": 0.01}, K=3, converge_iterations=2000)
+    # the reference's own 64x64x1 cavity mesh with config-1 settings, converged
+    ref_mesh = os.environ.get("BABELSIM_REFERENCE", "/root/reference") + "/cases/cavity/mesh/cavity.mesh"
+    make("cavity64_config1", meshgen.read_mesh(ref_mesh), U, p, methods(), config1_solution(1e-12),
+         {"density": 1.0, "dynamicViscosity": 0.01}, K=1, converge_iterations=5000)
+    # non-orthogonal 3D: warped 5^3 box, LS gradient, corrected diffusion, linearUpwind, 2 correctors
+    Uw = [("fixedValue", (0.0, 0.0, 0.0))] * 3 + [("fixedValue", (1.0, 0.0, 0.0))] + [("fixedValue", (0.0, 0.0, 0.0))] * 2
+    pw = [("zeroGradient", 0.0)] * 6
+    make("warped5_corrected", meshgen.warped_box(5), Uw, pw, methods("linearUpwind", "leastSquares", "corrected"),
+         config1_solution(1e-12), {"density": 1.0, "dynamicViscosity": 0.01}, K=3, converge_iterations=3000)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,93 @@
+"""Shared test helpers: golden fixtures, oracle set-up and the product's settings."""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from babelsim_b200 import meshgen  # noqa: E402
+from oracle import fvm, geometry, simple  # noqa: E402
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
+GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
+            "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",
+            "face_skewness", "cell_centres", "cell_volumes", "orthogonal_geometry"]
+
+
+class Golden:
+    def __init__(self, name):
+        self.name = name
+        self.d = np.load(os.path.join(GOLDEN, name + ".npz"))
+        self.meta = json.loads(str(self.d["meta"]))
+        off = self.d["mesh_offsets"]
+        ids = self.d["mesh_ids"]
+        faces = [ids[off[i]:off[i + 1]] for i in range(len(off) - 1)]
+        self.poly = meshgen.PolyMesh(self.d["mesh_vertices"], faces, self.d["mesh_owner"], self.d["mesh_neighbour"],
+                                     self.d["mesh_patch"], self.meta["patch_names"], self.meta["patch_kinds"])
+        self.K = self.meta["K"]
+
+    def __getitem__(self, k):
+        return self.d[k]
+
+    def ref_geometry(self):
+        return {k: self.d["geo_" + k] for k in GEO_KEYS}
+
+    def oracle_geometry(self):
+        p = self.poly
+        return geometry.compute_geometry(geometry.PolyMesh(p.vertices, p.faces, p.owner, p.neighbour, p.patch,
+                                                           p.patch_names, p.patch_kinds))
+
+    def U_bcs(self):
+        return [(fvm.BC_NAMES[t], np.array(v, float)) for t, v in self.meta["U_bcs"]]
+
+    def p_bcs(self):
+        return [(fvm.BC_NAMES[t], float(v)) for t, v in self.meta["p_bcs"]]
+
+    def systems(self):
+        n = int(self.d["n_systems_last"])
+        return [dict(identity=str(self.d[f"sys{j}_identity"]),
+                     **{k: self.d[f"sys{j}_{k}"] for k in ("diag", "upper", "lower", "source", "before", "after")})
+                for j in range(n)]
+
+    def settings(self, **over) -> simple.SimpleSettings:
+        sol = self.meta["solution"]
+        m = self.meta["methods"]
+        s = simple.SimpleSettings(rho=self.meta["physics"]["density"], mu=self.meta["physics"]["dynamicViscosity"],
+                                  alpha_u=sol["velocityRelaxation"], alpha_p=sol["pressureRelaxation"],
+                                  non_orthogonal_corrections=sol.get("nonOrthogonalCorrections", 1),
+                                  mass_tolerance=sol["continuityTolerance"], velocity_tolerance=sol["velocityTolerance"],
+                                  momentum_tolerance=sol["momentumTolerance"],
+                                  pressure_tolerance=sol["pressureCorrectionTolerance"],
+                                  momentum=dict(m["momentum"]), pressure=dict(m["pressureCorrection"]))
+        for k, v in over.items():
+            setattr(s, k, v)
+        return s
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def ref_system_groups(g: Golden):
+    """Split the dumped systems into per-iteration groups [momentum, pressure...]."""
+    groups, cur = [], None
+    for s in g.systems():
+        if s["identity"] == "momentum":
+            cur = dict(momentum=s, pressure=[])
+            groups.append(cur)
+        else:
+            cur["pressure"].append(s)
+    return groups

@@ -1,0 +1,97 @@
+"""The oracle restatement pinned against the reference's own sources (golden fixtures).
+
+The fixtures come from tests/golden/make_golden.py, which runs the reference's
+unmodified finite-volume sources and SIMPLE loop (compiled serially by
+oracle/ref).  Tolerances: assembled coefficients 1e-12 relative; fields after
+one iteration from the reference's own state 1e-9 (the reference's Krylov
+solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
+"""
+import numpy as np
+import pytest
+
+from helpers import CASES, Golden, ref_system_groups, rel, rel_l2
+from oracle import fvm, simple
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_geometry_matches_reference(name):
+    g = Golden(name)
+    geo = g.oracle_geometry()
+    ref = g.ref_geometry()
+    pairs = [("face_area_vectors", geo.Sf), ("face_centres", geo.xf), ("face_areas", geo.area),
+             ("face_normals", geo.normal), ("face_owner_weights", geo.weight),
+             ("face_orthogonal_coefficients", geo.dcoef), ("face_non_orthogonal", geo.kvec),
+             ("face_skewness", geo.skew), ("cell_centres", geo.xc), ("cell_volumes", geo.volume)]
+    for key, mine in pairs:
+        r = ref[key].reshape(mine.shape)
+        scale = max(np.max(np.abs(r)), 1e-300)
+        assert np.max(np.abs(mine - r)) <= 1e-12 * scale + 1e-15, key
+    assert geo.orthogonal == bool(ref["orthogonal_geometry"][0])
+
+
+def _state(g, k):
+    n = g.poly.n_cells
+    if k == 0:
+        return np.zeros((n, 3)), np.zeros(n), None
+    return g[f"U_{k}"], g[f"p_{k}"], g[f"phi_{k}"]
+
+
+@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"])
+def test_one_iteration_systems_and_fields(name):
+    g = Golden(name)
+    geo = g.oracle_geometry()
+    groups = ref_system_groups(g)
+    for k in range(1, g.K + 1):
+        U0, p0, phi0 = _state(g, k - 1)
+        cap = {}
+
+        def capture(it, d):
+            cap.update(d)
+        st = simple.run_simple(geo, g.U_bcs(), g.p_bcs(), g.settings(), U0=U0, p0=p0, phi0=phi0, iterations=1,
+                               capture=capture)
+        ref = groups[k - 1]
+        mom = cap["momentum_relaxed"]
+        for key in ("diag", "upper", "lower", "source"):
+            assert rel(getattr(mom, key), ref["momentum"][key].reshape(getattr(mom, key).shape)) < 1e-12, (k, key)
+        for j, (mine, theirs) in enumerate(zip(cap["pressure"], ref["pressure"])):
+            tol = 1e-12 if j == 0 else 1e-8
+            for key in ("diag", "upper", "lower"):
+                assert rel(getattr(mine, key), theirs[key]) < 1e-12, (k, j, key)
+            assert rel(mine.source, theirs["source"]) < tol, (k, j, "source")
+        assert rel_l2(st.U, g[f"U_{k}"]) < 1e-9
+        assert rel_l2(st.p, g[f"p_{k}"]) < 1e-9
+        assert rel_l2(st.phi, g[f"phi_{k}"]) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"])
+def test_converged_fields(name):
+    g = Golden(name)
+    st = simple.run_simple(g.oracle_geometry(), g.U_bcs(), g.p_bcs(), g.settings(), iterations=5000)
+    assert st.converged
+    assert abs(st.iterations - int(g["conv_info"][1])) <= 2
+    assert rel_l2(st.U, g["U_conv"]) < 1e-7
+    assert rel_l2(st.p, g["p_conv"]) < 1e-7
+
+
+def test_operators_known_answers():
+    """Analytic answers of the reference's tests/operators_test.cpp:71-104 on a 3x3x3 box."""
+    from babelsim_b200 import meshgen
+    from oracle import geometry
+    pm = meshgen.hex_box(3, 3, 3, (0, 0, 0), (3, 3, 3))
+    geo = geometry.compute_geometry(geometry.PolyMesh(pm.vertices, pm.faces, pm.owner, pm.neighbour, pm.patch,
+                                                      pm.patch_names, pm.patch_kinds))
+    lin = 2.0 * geo.xc[:, 0] - 3.0 * geo.xc[:, 1] + 0.5 * geo.xc[:, 2] + 1.0
+    centre = 1 + 3 * (1 + 3 * 1)
+    zg = [(fvm.ZERO_GRADIENT, 0.0)] * 6
+    f = fvm.Field(geo, lin, zg)
+    for method in ("greenGauss", "leastSquares"):
+        gr = fvm.gradient(f, method)
+        assert np.allclose(gr[centre], [2.0, -3.0, 0.5], atol=1e-12)
+    U = fvm.Field(geo, geo.xc.copy(), [(fvm.ZERO_GRADIENT, np.zeros(3))] * 6)
+    phi = fvm.flux(U, "linear", "greenGauss")
+    assert abs(fvm.divergence_flux(geo, phi)[centre] - 3.0) < 1e-12
+    quad = fvm.Field(geo, np.sum(geo.xc ** 2, axis=1), zg)
+    eq = fvm.LDU(geo, False)
+    fvm.add_diffusion(eq, np.ones(geo.n_faces), quad, None, "orthogonal")
+    lap = -(eq.apply(quad.v) - eq.source) / geo.volume   # -(A x - b) / V = laplacian
+    assert abs(lap[centre] - 6.0) < 1e-12
