@@ -267,6 +267,7 @@ def gradient_least_squares(field: Field):
         np.add.at(R, ob, wgt[:, None, None] * d[:, :, None] * diff[:, None, :])
         sol = np.linalg.solve(M, R)          # (N,3 rows of d, 3 components)
         return np.transpose(sol, (0, 2, 1))  # Tensor3 rows = component gradients
+    np.add.at(R, ob, wgt[:, None] * d * diff[:, None])
     return np.linalg.solve(M, R[:, :, None])[:, :, 0]
 
 

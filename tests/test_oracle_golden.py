@@ -87,6 +87,15 @@ def test_operators_known_answers():
     for method in ("greenGauss", "leastSquares"):
         gr = fvm.gradient(f, method)
         assert np.allclose(gr[centre], [2.0, -3.0, 0.5], atol=1e-12)
+    # Least squares is exact for a linear field whose constraints are consistent with
+    # it on every patch, boundary cells included (mirror points, operators.cpp:336-347).
+    from babelsim_b200 import meshgen as mg
+    wp = mg.warped_box(4)
+    wgeo = geometry.compute_geometry(geometry.PolyMesh(wp.vertices, wp.faces, wp.owner, wp.neighbour, wp.patch,
+                                                       wp.patch_names, wp.patch_kinds))
+    xf = fvm.Field(wgeo, wgeo.xc[:, 0].copy(), [(fvm.FIXED_VALUE, 0.0), (fvm.FIXED_VALUE, 1.0)] +
+                   [(fvm.ZERO_GRADIENT, 0.0)] * 4)
+    assert np.allclose(fvm.gradient(xf, "leastSquares"), [1.0, 0.0, 0.0], atol=1e-12)
     U = fvm.Field(geo, geo.xc.copy(), [(fvm.ZERO_GRADIENT, np.zeros(3))] * 6)
     phi = fvm.flux(U, "linear", "greenGauss")
     assert abs(fvm.divergence_flux(geo, phi)[centre] - 3.0) < 1e-12
