@@ -17,14 +17,16 @@ LIB_PATH = os.path.join(HERE, "libbabelsim_b200.so")
 # Entry points declared in include/babelsim_b200.h, in declaration order.
 EXPORTS = [
     "bsg_context_create", "bsg_context_destroy", "bsg_last_error", "bsg_global_error", "bsg_context_launches",
-    "bsg_context_synchronize", "bsg_mesh_create", "bsg_mesh_create_polyhedral", "bsg_mesh_destroy",
+    "bsg_context_synchronize", "bsg_context_profile", "bsg_context_profile_report", "bsg_context_event_record",
+    "bsg_context_event_elapsed", "bsg_mesh_create", "bsg_mesh_create_polyhedral", "bsg_mesh_destroy",
     "bsg_mesh_sizes", "bsg_mesh_export", "bsg_field_create", "bsg_field_destroy", "bsg_field_set_boundary",
     "bsg_field_upload", "bsg_field_download", "bsg_field_set_boundary_flux", "bsg_math_grad",
     "bsg_math_interpolate", "bsg_math_flux", "bsg_math_div_flux", "bsg_math_normal_gradient",
     "bsg_equation_create", "bsg_equation_destroy", "bsg_equ_reset", "bsg_equ_div", "bsg_equ_laplacian",
     "bsg_equ_source", "bsg_equ_relax", "bsg_equ_scale", "bsg_equ_reference_if_unanchored", "bsg_equ_face_flux",
     "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_simple_create",
-    "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_iterate", "bsg_simple_get_fields",
+    "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
+    "bsg_simple_iterate", "bsg_simple_get_fields",
     "bsg_simple_destroy",
 ]
 
@@ -91,6 +93,9 @@ def lib():
         sig = {
             "bsg_context_create": [i32, pp], "bsg_context_destroy": [vp], "bsg_last_error": [vp],
             "bsg_global_error": [], "bsg_context_launches": [vp, C.POINTER(i64)], "bsg_context_synchronize": [vp],
+            "bsg_context_profile": [vp, i32], "bsg_context_profile_report": [vp, C.c_char_p, i32],
+            "bsg_context_event_record": [vp, i32], "bsg_context_event_elapsed": [vp, i32, i32, C.POINTER(dbl)],
+            "bsg_simple_load_state": [vp, vp, vp, vp],
             "bsg_mesh_create": [vp, C.POINTER(MeshGeometry), pp],
             "bsg_mesh_create_polyhedral": [vp, i32, vp, i32, vp, vp, vp, vp, vp, i32, pp],
             "bsg_mesh_destroy": [vp], "bsg_mesh_sizes": [vp, vp], "bsg_mesh_export": [vp, C.c_char_p, vp],

@@ -49,6 +49,23 @@ class Context:
     def synchronize(self):
         check(lib().bsg_context_synchronize(self.h), self.h)
 
+    def profile(self, enable: bool):
+        check(lib().bsg_context_profile(self.h, int(enable)), self.h)
+
+    def profile_report(self) -> dict:
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        check(lib().bsg_context_profile_report(self.h, buf, len(buf)), self.h)
+        return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
+
+    def record(self, slot: int):
+        check(lib().bsg_context_event_record(self.h, slot), self.h)
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        v = C.c_double()
+        check(lib().bsg_context_event_elapsed(self.h, a, b, C.byref(v)), self.h)
+        return v.value
+
     def close(self):
         if self.h:
             lib().bsg_context_destroy(self.h)
@@ -291,6 +308,14 @@ class Simple:
 
     def set_flux(self, phi):
         check(lib().bsg_simple_set_flux(self.h, ptr(f64(phi))), self.mesh.ctx.h)
+
+    def load_state(self, U, p, phi):
+        """Copy host U, p, phi in between outer iterations (no restart)."""
+        check(lib().bsg_simple_load_state(self.h, ptr(U), ptr(p), ptr(phi)), self.mesh.ctx.h)
+
+    def fields_into(self, U, p, phi):
+        """Download U, p, phi into caller-provided (pinned) arrays."""
+        check(lib().bsg_simple_get_fields(self.h, ptr(U), ptr(p), ptr(phi)), self.mesh.ctx.h)
 
     def iterate(self, max_iterations: int) -> SimpleReport:
         r = SimpleReport()

@@ -359,56 +359,59 @@ void AmgPreconditioner::apply(Context& ctx, const double* r, double* z) {
     const int L = static_cast<int>(levels_.size());
     const int nu = std::max(1, cfg_.amg_smoothing_steps);
     cudaStream_t s = ctx.stream;
-    // Downward leg: level l solves A_l x_l = b_l approximately.
+    std::vector<double*> xs(L, nullptr);   // buffer holding each level's pre-smoothed iterate
+    // Downward leg: damped-Jacobi pre-smoothing from a zero guess, then the
+    // fused residual + aggregate restriction.
     for (int l = 0; l < L - 1; ++l) {
         Level* f = levels_[l];
         Level* c = levels_[l + 1];
         const double* b = l == 0 ? r : f->b.data();
-        double* x = f->x.data();
-        double* t = f->t.data();
+        double* cur = f->x.data();
+        double* other = f->t.data();
         const unsigned g = gridFor(f->n, kBlock);
-        kSmoothZero<<<g, kBlock, 0, s>>>(f->n, f->rdiag.data(), b, x);
+        BSG_PROFILE(ctx, l == 0 ? "amg_pre_smooth_restrict_l0" : "amg_coarse_levels");
+        kSmoothZero<<<g, kBlock, 0, s>>>(f->n, f->rdiag.data(), b, cur);
         ctx.launched();
-        for (int it = 1; it < nu; ++it) {
-            kSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), b, x, t);
-            kCopy<<<g, kBlock, 0, s>>>(f->n, t, x);
-            ctx.launches += 2;
-        }
-        kResidualRestrict<<<gridFor(c->n, kBlock), kBlock, 0, s>>>(c->n, f->agg_ptr.data(), f->agg_rows.data(), f->dptr,
-                                                                    f->dcol, f->ddiag, f->dval, b, x, c->b.data());
-        ctx.launched();
-    }
-    Level* last = levels_.back();
-    {
-        const double* b = L == 1 ? r : last->b.data();
-        double* x = L == 1 ? z : last->x.data();
-        kDenseSolve<<<gridFor(last->n, 128), 128, 0, s>>>(last->n, last->dense.data(), b, x);
-        ctx.launched();
-    }
-    // Upward leg: prolongate and post-smooth.
-    for (int l = L - 2; l >= 0; --l) {
-        Level* f = levels_[l];
-        Level* c = levels_[l + 1];
-        const double* b = l == 0 ? r : f->b.data();
-        double* x = f->x.data();
-        double* t = f->t.data();
-        double* out = l == 0 ? z : x;
-        const unsigned g = gridFor(f->n, kBlock);
-        // first post sweep fused with prolongation writes t, further sweeps ping-pong
-        kProlongSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), f->agg.data(),
-                                            c->x.data(), b, x, t);
-        ctx.launched();
-        double* cur = t;
-        double* other = x;
         for (int it = 1; it < nu; ++it) {
             kSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), b, cur, other);
             ctx.launched();
             std::swap(cur, other);
         }
-        if (cur != out) {
-            kCopy<<<g, kBlock, 0, s>>>(f->n, cur, out);
+        xs[l] = cur;
+        kResidualRestrict<<<gridFor(c->n, kBlock), kBlock, 0, s>>>(c->n, f->agg_ptr.data(), f->agg_rows.data(), f->dptr,
+                                                                    f->dcol, f->ddiag, f->dval, b, cur, c->b.data());
+        ctx.launched();
+    }
+    Level* last = levels_.back();
+    {
+        BSG_PROFILE(ctx, "amg_coarse_levels");
+        const double* b = L == 1 ? r : last->b.data();
+        double* x = L == 1 ? z : last->x.data();
+        kDenseSolve<<<gridFor(last->n, 128), 128, 0, s>>>(last->n, last->dense.data(), b, x);
+        ctx.launched();
+        xs[L - 1] = x;
+    }
+    // Upward leg: first post-smoothing sweep fused with the prolongation, then
+    // further sweeps ping-pong; level 0 ends in z.
+    for (int l = L - 2; l >= 0; --l) {
+        Level* f = levels_[l];
+        const double* b = l == 0 ? r : f->b.data();
+        double* x = xs[l];
+        double* other = x == f->x.data() ? f->t.data() : f->x.data();
+        const unsigned g = gridFor(f->n, kBlock);
+        BSG_PROFILE(ctx, l == 0 ? "amg_prolong_post_smooth_l0" : "amg_coarse_levels");
+        double* out = (l == 0 && nu == 1) ? z : other;
+        kProlongSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), f->agg.data(),
+                                            xs[l + 1], b, x, out);
+        ctx.launched();
+        double* cur = out;
+        for (int it = 1; it < nu; ++it) {
+            double* dst = (l == 0 && it == nu - 1) ? z : (cur == f->x.data() ? f->t.data() : f->x.data());
+            kSmooth<<<g, kBlock, 0, s>>>(f->n, f->dptr, f->dcol, f->ddiag, f->dval, f->rdiag.data(), b, cur, dst);
             ctx.launched();
+            cur = dst;
         }
+        xs[l] = cur;
     }
     BSG_CUDA(cudaGetLastError());
 }

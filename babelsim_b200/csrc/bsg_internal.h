@@ -93,8 +93,8 @@ private:
     std::size_t n_ = 0;
 };
 
-// One device, one stream, a launch counter and pinned scratch for scalars
-// read back by the host.
+// One device, one stream, a launch counter, pinned scratch for scalars read
+// back by the host, and optional per-kernel CUDA-event timing.
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -102,11 +102,42 @@ struct Context {
     long long launches = 0;
     std::string last_error;
     double* pinned = nullptr;            // 64 doubles of pinned host memory
+    // Per-kernel timing: while `profiling`, every instrumented launch is
+    // bracketed by two events on `stream`; profileReport() resolves them.
+    bool profiling = false;
+    struct Record { const char* name; cudaEvent_t start, stop; };
+    std::vector<Record> records;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<cudaEvent_t> user_events;  // bsg_context_event_record slots
     explicit Context(int dev);
     ~Context();
     void sync() { BSG_CUDA(cudaStreamSynchronize(stream)); }
     void launched() { ++launches; }
+    cudaEvent_t takeEvent();
+    std::string profileReport();         // JSON {"name": [launches, total_ms], ...}; clears records
 };
+
+// Brackets the launches issued in its scope with timing events when profiling.
+class ProfileScope {
+public:
+    ProfileScope(Context& ctx, const char* name) : ctx_(ctx) {
+        if (ctx.profiling) {
+            rec_ = {name, ctx.takeEvent(), ctx.takeEvent()};
+            checkCuda(cudaEventRecord(rec_.start, ctx.stream), "cudaEventRecord");
+        }
+    }
+    ~ProfileScope() {
+        if (ctx_.profiling && rec_.start) {
+            cudaEventRecord(rec_.stop, ctx_.stream);
+            ctx_.records.push_back(rec_);
+        }
+    }
+
+private:
+    Context& ctx_;
+    Context::Record rec_{nullptr, nullptr, nullptr};
+};
+#define BSG_PROFILE(ctx, name) ::bsg::ProfileScope bsg_profile_scope_((ctx), (name))
 
 // Per-patch boundary constraint as seen by the kernels.
 struct PatchBC {

@@ -6,6 +6,7 @@
 #include "linalg.h"
 #include "simple.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -53,8 +54,45 @@ Context::Context(int dev) : device(dev) {
 
 Context::~Context() {
     if (stream) cudaStreamSynchronize(stream);
+    for (auto& r : records) { event_pool.push_back(r.start); event_pool.push_back(r.stop); }
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : user_events) if (e) cudaEventDestroy(e);
     if (pinned) cudaFreeHost(pinned);
     if (stream) cudaStreamDestroy(stream);
+}
+
+cudaEvent_t Context::takeEvent() {
+    if (event_pool.empty()) {
+        cudaEvent_t e;
+        checkCuda(cudaEventCreate(&e), "cudaEventCreate");
+        return e;
+    }
+    cudaEvent_t e = event_pool.back();
+    event_pool.pop_back();
+    return e;
+}
+
+std::string Context::profileReport() {
+    sync();
+    std::vector<std::pair<std::string, std::pair<long long, double>>> acc;
+    for (auto& r : records) {
+        float ms = 0.0f;
+        checkCuda(cudaEventElapsedTime(&ms, r.start, r.stop), "cudaEventElapsedTime");
+        auto it = std::find_if(acc.begin(), acc.end(), [&](const auto& a) { return a.first == r.name; });
+        if (it == acc.end()) acc.push_back({r.name, {1, ms}});
+        else { it->second.first += 1; it->second.second += ms; }
+        event_pool.push_back(r.start);
+        event_pool.push_back(r.stop);
+    }
+    records.clear();
+    std::string out = "{";
+    for (std::size_t i = 0; i < acc.size(); ++i) {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s\"%s\": [%lld, %.6f]", i ? ", " : "", acc[i].first.c_str(),
+                      acc[i].second.first, acc[i].second.second);
+        out += buf;
+    }
+    return out + "}";
 }
 
 }  // namespace bsg
@@ -201,6 +239,45 @@ int bsg_context_launches(const bsg_context* ctx, int64_t* out) {
 
 int bsg_context_synchronize(bsg_context* ctx) {
     return guard(ctx, [&] { ctx->ctx->sync(); });
+}
+
+int bsg_context_profile(bsg_context* ctx, int32_t enable) {
+    return guard(ctx, [&] {
+        require(ctx != nullptr, "null context");
+        ctx->ctx->profiling = enable != 0;
+    });
+}
+
+int bsg_context_profile_report(bsg_context* ctx, char* buffer, int32_t capacity) {
+    return guard(ctx, [&] {
+        require(ctx && buffer && capacity > 0, "bad argument");
+        const std::string r = ctx->ctx->profileReport();
+        if (static_cast<int32_t>(r.size()) >= capacity) bsg::fail(bsg::kArgument, "profile report buffer too small");
+        std::memcpy(buffer, r.c_str(), r.size() + 1);
+    });
+}
+
+int bsg_context_event_record(bsg_context* ctx, int32_t slot) {
+    return guard(ctx, [&] {
+        require(ctx && slot >= 0 && slot < 64, "event slot must be in [0,64)");
+        auto& ev = ctx->ctx->user_events;
+        if (ev.size() <= static_cast<std::size_t>(slot)) ev.resize(slot + 1, nullptr);
+        if (!ev[slot]) BSG_CUDA(cudaEventCreate(&ev[slot]));
+        BSG_CUDA(cudaEventRecord(ev[slot], ctx->ctx->stream));
+    });
+}
+
+int bsg_context_event_elapsed(bsg_context* ctx, int32_t a, int32_t b, double* ms) {
+    return guard(ctx, [&] {
+        require(ctx && ms, "null argument");
+        auto& ev = ctx->ctx->user_events;
+        require(a >= 0 && b >= 0 && static_cast<std::size_t>(std::max(a, b)) < ev.size() && ev[a] && ev[b],
+                "event slot was never recorded");
+        BSG_CUDA(cudaEventSynchronize(ev[b]));
+        float f = 0.0f;
+        BSG_CUDA(cudaEventElapsedTime(&f, ev[a], ev[b]));
+        *ms = f;
+    });
 }
 
 int bsg_mesh_create(bsg_context* ctx, const bsg_mesh_geometry* g, bsg_mesh** out) {
@@ -616,6 +693,13 @@ int bsg_simple_set_flux(bsg_simple* s, const double* phi) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && phi, "null argument");
         s->solver->phi().uploadExternal(phi);
+    });
+}
+
+int bsg_simple_load_state(bsg_simple* s, const double* U, const double* p, const double* phi) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && U && p && phi, "null argument");
+        s->solver->loadState(U, p, phi);
     });
 }
 

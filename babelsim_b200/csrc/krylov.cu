@@ -571,10 +571,16 @@ SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig
         (void)solver;
         for (;;) {
             for (int it = 0; it < check_interval; ++it) {
-                kCgSpmv<<<g, kBlock, 0, ctx.stream>>>(A, m.p.data(), m.q.data(), m.partial.data(), m.sc.data());
+                {
+                    BSG_PROFILE(ctx, "cg_spmv_dot");
+                    kCgSpmv<<<g, kBlock, 0, ctx.stream>>>(A, m.p.data(), m.q.data(), m.partial.data(), m.sc.data());
+                }
                 kCgAlpha<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
-                kCgUpdate<<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.p.data(), m.q.data(), m.partial.data(),
-                                                         m.sc.data());
+                {
+                    BSG_PROFILE(ctx, "cg_update_norm");
+                    kCgUpdate<<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.p.data(), m.q.data(),
+                                                             m.partial.data(), m.sc.data());
+                }
                 kCgCheck<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 ctx.launches += 4;
                 if (jac) {
@@ -671,14 +677,20 @@ void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, 
             for (int it = 0; it < check_interval; ++it) {
                 kBiDirection<3><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.p.data(), m.v.data(),
                                                               m.ph.data(), m.sc.data());
-                kBiSpmvV<3><<<g, kBlock, 0, ctx.stream>>>(A, m.ph.data(), m.v.data(), m.r0.data(), m.partial.data(),
-                                                          m.sc.data());
+                {
+                    BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
+                    kBiSpmvV<3><<<g, kBlock, 0, ctx.stream>>>(A, m.ph.data(), m.v.data(), m.r0.data(),
+                                                              m.partial.data(), m.sc.data());
+                }
                 kBiAlpha<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 kBiS<3><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.v.data(), m.sh.data(), m.partial.data(),
                                                       m.sc.data());
                 kBiCheckS<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
-                kBiSpmvT<3><<<g, kBlock, 0, ctx.stream>>>(A, m.sh.data(), m.t.data(), m.r.data(), m.partial.data(),
-                                                          m.sc.data());
+                {
+                    BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
+                    kBiSpmvT<3><<<g, kBlock, 0, ctx.stream>>>(A, m.sh.data(), m.t.data(), m.r.data(),
+                                                              m.partial.data(), m.sc.data());
+                }
                 kBiOmega<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 kBiUpdate<3><<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.ph.data(), m.sh.data(), m.t.data(),
                                                            m.r0.data(), m.partial.data(), m.sc.data());

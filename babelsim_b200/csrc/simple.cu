@@ -85,6 +85,15 @@ void SimpleSolver::start() {
     ctx_.sync();
 }
 
+void SimpleSolver::loadState(const double* U, const double* p, const double* phi) {
+    if (!started_) fail(kState, "load_state requires a started SIMPLE solver (set_fields first)");
+    const std::size_t N = m_.n_cells;
+    U_.v.upload(U, 3 * N, ctx_.stream);
+    p_.v.upload(p, N, ctx_.stream);
+    // phi arrives in the caller's face numbering; the device keeps interior faces first.
+    phi_.uploadExternal(phi);
+}
+
 SimpleReport SimpleSolver::iterate(int max_iterations) {
     if (!started_) start();
     for (int k = 0; k < max_iterations; ++k) {
@@ -100,11 +109,14 @@ void SimpleSolver::outerIteration() {
     copyAsync(ctx_, Uprev_.data(), U_.v.data(), 3LL * N);
     // Momentum assembly (simple/main.cpp:51-56).
     DeviceEquation& mom = *mom_;
-    mom.reset();
-    addConvection(mom, phi_, cfg_.rho, cfg_.momentum);
-    addLaplacian(mom, &muEff_, 0.0, -1.0, cfg_.momentum);
-    gradient(p_, cfg_.pressure.gradient, gradP_);
-    addSource(mom, gradP_.data(), -1.0);
+    {
+        BSG_PROFILE(ctx_, "momentum_assembly");
+        mom.reset();
+        addConvection(mom, phi_, cfg_.rho, cfg_.momentum);
+        addLaplacian(mom, &muEff_, 0.0, -1.0, cfg_.momentum);
+        gradient(p_, cfg_.pressure.gradient, gradP_);
+        addSource(mom, gradP_.data(), -1.0);
+    }
     // rU before relaxation (simple/main.cpp:59-60).
     relativeResidualNorms(mom, U_.v.data(), red_);
     double diag_h[16];
@@ -134,11 +146,14 @@ void SimpleSolver::outerIteration() {
     report_.momentum_iterations = mom_iters;
     if (!mom_healthy) { report_.status = 2; return; }
     // Rhie-Chow face flux (simple/main.cpp:71-79); p is unchanged since assembly, so gradP is reused.
-    faceFlux(U_, cfg_.momentum.interpolation, cfg_.momentum.gradient, phiH_);
-    kRhieChow<<<gridFor(m_.n_interior, kBlock), kBlock, 0, ctx_.stream>>>(
-        mv, p_.bcView(), rAU_.v.data(), gradP_.data(), p_.v.data(), cfg_.pressure.diffusion, phiH_.v.data());
-    ctx_.launched();
-    divFlux(phiH_, divPhiH_);
+    {
+        BSG_PROFILE(ctx_, "rhie_chow_flux");
+        faceFlux(U_, cfg_.momentum.interpolation, cfg_.momentum.gradient, phiH_);
+        kRhieChow<<<gridFor(m_.n_interior, kBlock), kBlock, 0, ctx_.stream>>>(
+            mv, p_.bcView(), rAU_.v.data(), gradP_.data(), p_.v.data(), cfg_.pressure.diffusion, phiH_.v.data());
+        ctx_.launched();
+        divFlux(phiH_, divPhiH_);
+    }
     // Pressure correction (simple/main.cpp:81-93).
     BSG_CUDA(cudaMemsetAsync(pP_.v.data(), 0, sizeof(double) * N, ctx_.stream));
     const int pressure_solves = cfg_.pressure.diffusion == 0 ? 1 : cfg_.non_orthogonal_corrections + 1;
@@ -147,13 +162,19 @@ void SimpleSolver::outerIteration() {
     int p_iters = 0;
     double linP = 0.0;
     for (int corr = 0; corr < pressure_solves; ++corr) {
-        peq.reset();
-        addLaplacian(peq, &rAU_, 0.0, -1.0, cfg_.pressure);
-        addSource(peq, divPhiH_.data(), -1.0);
-        referenceIfUnanchored(peq, 0.0, flags_.data());
+        {
+            BSG_PROFILE(ctx_, "pressure_assembly");
+            peq.reset();
+            addLaplacian(peq, &rAU_, 0.0, -1.0, cfg_.pressure);
+            addSource(peq, divPhiH_.data(), -1.0);
+            referenceIfUnanchored(peq, 0.0, flags_.data());
+        }
         Dcsr<double> P{N, m_.cf_ptr.data(), m_.cf_col.data(), peq.diag.data(), peq.val.data(), 2LL * m_.n_interior};
         if (auto* jac = dynamic_cast<JacobiPreconditioner*>(ppc_.get())) { jac->diag = peq.diag.data(); jac->n = N; }
-        if (auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get())) amg->update(P, corr == 0);
+        if (auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get())) {
+            BSG_PROFILE(ctx_, "amg_numeric_setup");
+            amg->update(P, corr == 0);
+        }
         const SolveOutcome po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), pP_.v.data());
         if (po.status == 2 || !std::isfinite(po.final_)) { report_.status = 2; return; }
         p_ok = p_ok && po.status == 0;
@@ -164,6 +185,7 @@ void SimpleSolver::outerIteration() {
     report_.linP = linP;
     // Field updates (simple/main.cpp:95-98).
     axpyCell(ctx_, p_.v.data(), cfg_.alpha_p, pP_.v.data(), N);
+    BSG_PROFILE(ctx_, "field_updates_diagnostics");
     faceFluxEquation(peq, pP_.v.data(), pflux_);
     gradient(pP_, cfg_.pressure.gradient, gradPP_);
     subtractScaledGradient(m_, U_.v.data(), rAU_.v.data(), gradPP_.data());

@@ -38,6 +38,8 @@ public:
     void start();
     // Outer iterations until converged or `max_iterations` more are done.
     SimpleReport iterate(int max_iterations);
+    // Overwrite U, p, phi from host memory (caller numbering) keeping all other state.
+    void loadState(const double* U, const double* p, const double* phi);
     const SimpleReport& report() const { return report_; }
 
 private:

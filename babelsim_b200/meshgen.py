@@ -184,135 +184,9 @@ def warped_box(n: int, amplitude=0.08, seed=7) -> PolyMesh:
                    kinds=["wall"] * 6)
 
 
-def _circumcentres(p):
-    """Circumcentres of tetrahedra p (M,4,3); also |det| of the edge matrix."""
-    a = p[:, 0]
-    A = p[:, 1:] - a[:, None, :]
-    rhs = 0.5 * np.einsum("mij,mij->mi", A, A)
-    det = np.linalg.det(A)
-    safe = np.abs(det) > 0
-    c = np.zeros_like(a)
-    c[safe] = a[safe] + np.linalg.solve(A[safe], rhs[safe][:, :, None])[:, :, 0]
-    return c, np.abs(det)
 
 
 def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, kinds=None) -> PolyMesh:
-    """Voronoi tessellation of the unit cube from a jittered n^3 lattice of sites.
-
-    Site (i,j,k) = ((i,j,k) + 0.5 + U(-jitter, jitter)^3) / n, cell index
-    i + n*(j + n*k), seeded by ``seed``.  Sites within 2.5/n of a cube face are
-    mirrored across it; the bisector of a site and its own mirror is the cube
-    face, so every cell is exactly its Voronoi cell clipped to the cube.  The
-    tessellation is the dual of the Delaunay tetrahedralisation (scipy/qhull):
-    Voronoi vertices are tetrahedron circumcentres and the face between sites
-    i and j is the ring of circumcentres of the tetrahedra around edge (i,j).
-    Coincident circumcentres (cospherical site groups, which the mirror planes
-    create) are merged at 1e-9/n.  Patches: minus_x, plus_x, minus_y, plus_y,
-    minus_z, plus_z.
-    """
-    from scipy.spatial import Delaunay
-    rng = np.random.default_rng(seed)
-    h = 1.0 / n
-    ii, jj, kk = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
-    lattice = np.stack([ii.ravel(order="F"), jj.ravel(order="F"), kk.ravel(order="F")], axis=1).astype(float)
-    sites = (lattice + 0.5 + rng.uniform(-jitter, jitter, size=lattice.shape)) * h
-    N = len(sites)
-    layer = 2.5 * h
-    mirror_pts, mirror_of, mirror_patch = [], [], []
-    for axis in range(3):
-        for side in range(2):
-            sel = np.nonzero(sites[:, axis] < layer)[0] if side == 0 else np.nonzero(sites[:, axis] > 1 - layer)[0]
-            q = sites[sel].copy()
-            q[:, axis] = -q[:, axis] if side == 0 else 2.0 - q[:, axis]
-            mirror_pts.append(q)
-            mirror_of.append(sel)
-            mirror_patch.append(np.full(len(sel), 2 * axis + side))
-    pts = np.concatenate([sites] + mirror_pts)
-    of = np.concatenate([np.arange(N)] + mirror_of)          # original site of every point
-    ppatch = np.concatenate([np.full(N, -1)] + mirror_patch)  # patch of every mirror point
-    tri = Delaunay(pts)
-    tets = tri.simplices.astype(np.int64)
-    cc, det = _circumcentres(pts[tets])
-    good = det > 1e-12 * h ** 3
-    # edges of the tetrahedra that produce faces of original cells
-    pairs = np.array([(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)])
-    ea = tets[:, pairs[:, 0]].ravel()
-    eb = tets[:, pairs[:, 1]].ravel()
-    et = np.repeat(np.arange(len(tets)), 6)
-    lo, hi = np.minimum(ea, eb), np.maximum(ea, eb)
-    interior = (hi < N)
-    own_mirror = (lo < N) & (hi >= N) & (of[hi] == lo)
-    keep = (interior | own_mirror) & good[et]
-    lo, hi, et = lo[keep], hi[keep], et[keep]
-    key = lo * len(pts) + hi
-    # merge coincident circumcentres
-    q = np.round(cc / (1e-9 * h)).astype(np.int64)
-    _, vid = np.unique(q, axis=0, return_inverse=True)
-    vid = vid.ravel()
-    # angular order of the ring around each edge
-    e = pts[hi] - pts[lo]
-    e /= np.linalg.norm(e, axis=1)[:, None]
-    ref = np.where((np.abs(e[:, 0]) < 0.9)[:, None], np.array([1.0, 0, 0]), np.array([0, 1.0, 0]))
-    u = np.cross(e, ref)
-    u /= np.linalg.norm(u, axis=1)[:, None]
-    v = np.cross(e, u)
-    # The face is convex and lies in the bisector plane, but need not surround the
-    # Delaunay edge (non-Gabriel edges): order by angle about the ring's mean point.
-    _, grp = np.unique(key, return_inverse=True)
-    grp = grp.ravel()
-    cnt = np.bincount(grp)
-    mean = np.stack([np.bincount(grp, weights=cc[et][:, c]) / cnt for c in range(3)], axis=1)
-    r = cc[et] - mean[grp]
-    ang = np.arctan2(np.einsum("ij,ij->i", r, v), np.einsum("ij,ij->i", r, u))
-    order = np.lexsort((ang, key))
-    key, lo, hi, vv = key[order], lo[order], hi[order], vid[et[order]]
-    start = np.r_[True, key[1:] != key[:-1]]
-    # drop consecutive duplicates inside each ring, then the wrap-around duplicate
-    dup = np.r_[False, (vv[1:] == vv[:-1]) & ~start[1:]]
-    key, lo, hi, vv, start = key[~dup], lo[~dup], hi[~dup], vv[~dup], start[~dup]
-    gid = np.cumsum(start) - 1
-    first_pos = np.nonzero(start)[0]
-    last_pos = np.r_[first_pos[1:], len(vv)] - 1
-    wrap = (vv[last_pos] == vv[first_pos]) & (last_pos > first_pos)
-    drop = np.zeros(len(vv), bool)
-    drop[last_pos[wrap]] = True
-    key, lo, hi, vv, gid = key[~drop], lo[~drop], hi[~drop], vv[~drop], gid[~drop]
-    counts = np.bincount(gid, minlength=len(first_pos))
-    ok_face = counts >= 3
-    ok = ok_face[gid]
-    lo, hi, vv, gid = lo[ok], hi[ok], vv[ok], gid[ok]
-    fstart = np.r_[True, gid[1:] != gid[:-1]]
-    f_lo, f_hi = lo[fstart], hi[fstart]
-    sizes = np.diff(np.r_[np.nonzero(fstart)[0], len(vv)])
-    # compact vertex numbering
-    used, ids = np.unique(vv, return_inverse=True)
-    rep = np.zeros(used.max() + 1 if len(used) else 0, np.int64)
-    # representative coordinates: the circumcentre of one tetrahedron per merged vertex
-    first_tet = np.full(vid.max() + 1, -1, np.int64)
-    first_tet[vid[::-1]] = np.arange(len(vid))[::-1]
-    verts = cc[first_tet[used]]
-    del rep
-    is_int = f_hi < N
-    owner = f_lo.astype(np.int32)
-    neighbour = np.where(is_int, f_hi, -1).astype(np.int32)
-    patch = np.where(is_int, -1, ppatch[f_hi]).astype(np.int32)
-    # interior faces first, then boundary faces by patch (stable)
-    order = np.lexsort((np.arange(len(owner)), patch))
-    offsets = np.r_[0, np.cumsum(sizes)].astype(np.int64)
-    ring_ids = ids.astype(np.int32)
-    new_off = np.r_[0, np.cumsum(sizes[order])].astype(np.int32)
-    gather = np.concatenate([np.arange(offsets[f], offsets[f + 1]) for f in order]) if len(order) < 50000 else \
-        _ranges(offsets, order)
-    names = names or ["minus_x", "plus_x", "minus_y", "plus_y", "minus_z", "plus_z"]
-    kinds = kinds or ["wall"] * 6
-    return PolyMesh(verts, None, owner[order], neighbour[order], patch[order], list(names), list(kinds),
-                    offsets=new_off, ids=ring_ids[gather])
-
-
-def _ranges(offsets, order):
-    """Concatenation of arange(offsets[f], offsets[f+1]) for f in order, vectorised."""
-    sizes = (offsets[1:] - offsets[:-1])[order]
-    starts = offsets[:-1][order]
-    total = int(sizes.sum())
-    base = np.repeat(starts - np.r_[0, np.cumsum(sizes)[:-1]], sizes)
-    return base + np.arange(total)
+    """Jittered-lattice Voronoi tessellation of the unit cube (see babelsim_b200.voronoi)."""
+    from .voronoi import voronoi_cube as build
+    return build(n, jitter, seed, names, kinds)

@@ -1,0 +1,131 @@
+"""3D Voronoi tessellation of the unit cube from jittered lattice sites.
+
+Site (i,j,k) = ((i,j,k) + 0.5 + U(-jitter, jitter)^3) / n with a seeded
+generator; cell index i + n*(j + n*k).  Sites within 2.5/n of a cube face are
+mirrored across it; the bisector of a site and its own mirror is the cube
+face, so every cell is exactly its Voronoi cell clipped to the cube.  The
+tessellation is the dual of the Delaunay tetrahedralisation (scipy/qhull):
+Voronoi vertices are tetrahedron circumcentres and the face between sites i
+and j is the ring of circumcentres of the tetrahedra around edge (i,j), ordered
+by angle about the ring's mean point in the bisector plane.  Coincident
+circumcentres (cospherical site groups, which the mirror planes create) are
+merged at 1e-9/n.  Everything after the triangulation is vectorised numpy.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .meshgen import PolyMesh
+
+PATCHES = ["minus_x", "plus_x", "minus_y", "plus_y", "minus_z", "plus_z"]
+
+
+def sites(n: int, jitter: float = 0.3, seed: int = 20261007) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    ii, jj, kk = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    lattice = np.stack([ii.ravel(order="F"), jj.ravel(order="F"), kk.ravel(order="F")], axis=1).astype(float)
+    return (lattice + 0.5 + rng.uniform(-jitter, jitter, size=lattice.shape)) / n
+
+
+def _circumcentres(p):
+    a = p[:, 0]
+    A = p[:, 1:] - a[:, None, :]
+    rhs = 0.5 * np.einsum("mij,mij->mi", A, A)
+    det = np.linalg.det(A)
+    safe = np.abs(det) > 0
+    c = np.zeros_like(a)
+    c[safe] = a[safe] + np.linalg.solve(A[safe], rhs[safe][:, :, None])[:, :, 0]
+    return c, np.abs(det)
+
+
+def _merge_ids(c, tol):
+    """Ids that agree for points equal after quantisation at `tol` (64-bit hash of the cell)."""
+    q = np.round(c / tol).astype(np.int64).view(np.uint64)
+    h = (q[:, 0] * np.uint64(0x9E3779B97F4A7C15)) ^ (q[:, 1] * np.uint64(0xC2B2AE3D27D4EB4F)) ^ \
+        (q[:, 2] * np.uint64(0x165667B19E3779F9))
+    _, inv = np.unique(h, return_inverse=True)
+    return inv.ravel()
+
+
+def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, kinds=None) -> PolyMesh:
+    from scipy.spatial import Delaunay
+    h = 1.0 / n
+    S = sites(n, jitter, seed)
+    N = len(S)
+    layer = 2.5 * h
+    mp, mo, mpatch = [], [], []
+    for axis in range(3):
+        for side in range(2):
+            sel = np.nonzero(S[:, axis] < layer)[0] if side == 0 else np.nonzero(S[:, axis] > 1 - layer)[0]
+            q = S[sel].copy()
+            q[:, axis] = -q[:, axis] if side == 0 else 2.0 - q[:, axis]
+            mp.append(q)
+            mo.append(sel)
+            mpatch.append(np.full(len(sel), 2 * axis + side))
+    pts = np.concatenate([S] + mp)
+    of = np.concatenate([np.arange(N)] + mo)
+    ppatch = np.concatenate([np.full(N, -1)] + mpatch)
+    tets = Delaunay(pts).simplices.astype(np.int64)
+    cc, det = _circumcentres(pts[tets])
+    good = det > 1e-12 * h ** 3
+    vid_of_tet = _merge_ids(cc, 1e-9 * h)
+    pairs = np.array([(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)])
+    ea = tets[:, pairs[:, 0]].ravel()
+    eb = tets[:, pairs[:, 1]].ravel()
+    et = np.repeat(np.arange(len(tets)), 6)
+    lo, hi = np.minimum(ea, eb), np.maximum(ea, eb)
+    keep = ((hi < N) | ((lo < N) & (hi >= N) & (of[hi] == lo))) & good[et]
+    lo, hi, et = lo[keep], hi[keep], et[keep]
+    del ea, eb, keep
+    key = lo * len(pts) + hi
+    o1 = np.argsort(key, kind="stable")
+    key, lo, hi, et = key[o1], lo[o1], hi[o1], et[o1]
+    start = np.r_[True, key[1:] != key[:-1]]
+    sidx = np.nonzero(start)[0]
+    grp = np.cumsum(start) - 1
+    cnt = np.diff(np.r_[sidx, len(key)])
+    c = cc[et]
+    mean = np.add.reduceat(c, sidx, axis=0) / cnt[:, None]
+    e = pts[hi[sidx]] - pts[lo[sidx]]
+    e /= np.linalg.norm(e, axis=1)[:, None]
+    ref = np.where((np.abs(e[:, 0]) < 0.9)[:, None], np.array([1.0, 0, 0]), np.array([0, 1.0, 0]))
+    u = np.cross(e, ref)
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    v = np.cross(e, u)
+    r = c - mean[grp]
+    ang = np.arctan2(np.einsum("ij,ij->i", r, v[grp]), np.einsum("ij,ij->i", r, u[grp]))
+    o2 = np.argsort(grp + (ang + np.pi) * (0.999 / (2 * np.pi)), kind="stable")
+    grp, vv = grp[o2], vid_of_tet[et[o2]]
+    first = np.r_[True, grp[1:] != grp[:-1]]
+    dup = np.r_[False, (vv[1:] == vv[:-1]) & ~first[1:]]
+    grp, vv, et2 = grp[~dup], vv[~dup], et[o2][~dup]
+    first = np.r_[True, grp[1:] != grp[:-1]]
+    fpos = np.nonzero(first)[0]
+    lpos = np.r_[fpos[1:], len(vv)] - 1
+    wrap = (vv[lpos] == vv[fpos]) & (lpos > fpos)
+    drop = np.zeros(len(vv), bool)
+    drop[lpos[wrap]] = True
+    grp, vv, et2 = grp[~drop], vv[~drop], et2[~drop]
+    sizes_all = np.bincount(grp, minlength=len(sidx))
+    okf = sizes_all >= 3
+    ok = okf[grp]
+    grp, vv, et2 = grp[ok], vv[ok], et2[ok]
+    faces_g = np.nonzero(okf)[0]
+    f_lo, f_hi = lo[sidx[faces_g]], hi[sidx[faces_g]]
+    sizes = sizes_all[faces_g]
+    used, ids = np.unique(vv, return_inverse=True)
+    rep = np.empty(used.max() + 1, np.int64)
+    rep[vv] = et2
+    verts = cc[rep[used]]
+    is_int = f_hi < N
+    owner = f_lo.astype(np.int32)
+    neighbour = np.where(is_int, f_hi, -1).astype(np.int32)
+    patch = np.where(is_int, -1, ppatch[f_hi]).astype(np.int32)
+    order = np.argsort(patch, kind="stable")            # interior (-1) first, then by patch
+    offsets = np.r_[0, np.cumsum(sizes)].astype(np.int64)
+    sz = sizes[order]
+    starts = offsets[:-1][order]
+    gather = np.repeat(starts - np.r_[0, np.cumsum(sz)[:-1]], sz) + np.arange(int(sz.sum()))
+    return PolyMesh(verts, None, owner[order], neighbour[order], patch[order], list(names or PATCHES),
+                    list(kinds or ["wall"] * 6), offsets=np.r_[0, np.cumsum(sz)].astype(np.int32),
+                    ids=ids.ravel()[gather].astype(np.int32))

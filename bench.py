@@ -1,0 +1,328 @@
+"""Benchmark: steady SIMPLE outer iterations on the 1M-cell polyhedral cube cavity.
+
+Workload (the reference's 3D polyhedral cavity configuration): unit cube,
+100^3 = 1,000,000 Voronoi cells of a jittered lattice (jitter 0.3h, seed
+20261007, ~13.8 faces per cell), lid u = 1 on plus_y, other walls no-slip,
+rho = 1, mu = 1e-3, linearUpwind convection, least-squares gradients, corrected
+diffusion, 2 non-orthogonal correctors, relaxation U 0.7 / p 0.3, momentum
+BiCGStab + Jacobi and pressure CG + AMG, both to rtol 1e-10.  A step is one
+SIMPLE outer iteration (the unit of cell-iters/s); the first outer iterations
+are warm-up.  Synthetic mesh and initial state (fields at rest); the working
+set (~1.5 GB of geometry, matrices and fields) is far larger than L2, so no
+L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--cells 1000000]
+
+Under torchrun (N > 1) every rank solves its own copy of the case (independent
+requests: replicas, weak scaling); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-iters/s (steady SIMPLE outer iterations, 1M-cell polyhedral cube cavity)"
+SEED = 20261007
+
+
+def case_settings():
+    return dict(rho=1.0, mu=1e-3, alpha_u=0.7, alpha_p=0.3, non_orthogonal_corrections=2,
+                interpolation="linear", gradient="leastSquares", convection="linearUpwind", diffusion="corrected",
+                rtol=1e-10, atol=1e-14)
+
+
+def mesh_for(n: int):
+    """Generate (or reuse from /tmp) the jittered-Voronoi cube of n^3 cells."""
+    from babelsim_b200 import meshgen
+    path = os.path.join(tempfile.gettempdir(), f"bsg_voronoi_{n}_{SEED}.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        return meshgen.PolyMesh(d["vertices"], None, d["owner"], d["neighbour"], d["patch"],
+                                ["minus_x", "plus_x", "minus_y", "plus_y", "minus_z", "plus_z"], ["wall"] * 6,
+                                offsets=d["offsets"], ids=d["ids"])
+    pm = meshgen.voronoi_cube(n, 0.3, SEED)
+    np.savez(path, vertices=pm.vertices, owner=pm.owner, neighbour=pm.neighbour, patch=pm.patch,
+             offsets=pm.offsets, ids=pm.ids)
+    return pm
+
+
+def build_simple(bsg, mesh, s):
+    opts = bsg.options(s["interpolation"], s["gradient"], s["convection"], s["diffusion"])
+    sim = bsg.Simple(mesh, s["rho"], s["mu"], s["alpha_u"], s["alpha_p"], s["non_orthogonal_corrections"],
+                     1e-8, 1e-7, 1e-6, 1e-6, opts, opts,
+                     bsg.solver_config("bcgs", "bjacobi", s["atol"], s["rtol"], 1000),
+                     bsg.solver_config("cg", "hypre", s["atol"], s["rtol"], 1000))
+    for patch in range(6):
+        sim.set_boundary("U", patch, "fixedValue", (1.0, 0.0, 0.0) if patch == 3 else (0.0, 0.0, 0.0))
+        sim.set_boundary("p", patch, "zeroGradient")
+    n = mesh.n_cells
+    sim.set_fields(np.zeros((n, 3)), np.zeros(n))
+    return sim
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_bytes(name, N, nnz_off, amg_rows):
+    """Bytes each instrumented kernel must move (each array counted once; FP64 8 B, int32 4 B)."""
+    matrix = 8 * N + 4 * (N + 1) + 12 * nnz_off          # diag, row pointers, values + columns
+    if name == "cg_spmv_dot":
+        return matrix + 8 * N + 8 * N                     # read p, write q
+    if name == "bicgstab3_spmv_dot":
+        return matrix + 24 * N * 3                        # read x(3), write y(3), read r0(3) for the dot
+    if name == "cg_update_norm":
+        return 8 * N * 6                                  # x, r, p, q read; x, r write
+    if name == "amg_pre_smooth_restrict_l0":
+        # x = w b / d; x' = x + w (b - A x) / d; coarse b = sum over aggregate of (b - A x')
+        return (8 * 3 * N) + (matrix + 8 * 5 * N) + (matrix + 8 * 2 * N + 4 * N + 4 * amg_rows + 8 * amg_rows)
+    if name == "amg_prolong_post_smooth_l0":
+        return (matrix + 8 * 4 * N + 4 * N + 8 * amg_rows) + (matrix + 8 * 4 * N)
+    return None
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(seconds_budget=25.0):
+    """The reference's own sources (oracle/_ref) on a bounded sample of the workload, 1 core."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "babelsim-oracle")
+    if not os.path.exists(exe):
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import write_case  # noqa: E402  (case writer shared with the fixture generator)
+    from babelsim_b200 import meshgen
+    s = case_settings()
+    n = 24
+    pm = meshgen.voronoi_cube(n, 0.3, SEED)
+    work = tempfile.mkdtemp(prefix="bsg_cpu_baseline_")
+    U = [("fixedValue", (1.0, 0.0, 0.0) if p == 3 else (0.0, 0.0, 0.0)) for p in range(6)]
+    P = [("zeroGradient", 0.0)] * 6
+    methods = {"momentum": dict(interpolation="linear", gradient=s["gradient"], convection=s["convection"],
+                                diffusion=s["diffusion"])}
+    methods["pressureCorrection"] = dict(methods["momentum"])
+    iterations = 6
+    sol = {"maxIterations": iterations, "velocityRelaxation": s["alpha_u"], "pressureRelaxation": s["alpha_p"],
+           "nonOrthogonalCorrections": s["non_orthogonal_corrections"], "continuityTolerance": 1e-8,
+           "velocityTolerance": 1e-7, "momentumTolerance": 1e-6, "pressureCorrectionTolerance": 1e-6,
+           "equation.momentum.kspType": "bcgs", "equation.momentum.pcType": "bjacobi",
+           "equation.momentum.absoluteTolerance": s["atol"], "equation.momentum.relativeTolerance": s["rtol"],
+           "equation.momentum.maxIterations": 1000, "equation.pressureCorrection.kspType": "cg",
+           "equation.pressureCorrection.pcType": "hypre", "equation.pressureCorrection.absoluteTolerance": s["atol"],
+           "equation.pressureCorrection.relativeTolerance": s["rtol"],
+           "equation.pressureCorrection.maxIterations": 20000}
+    write_case(work, pm, U, P, methods, sol, {"density": s["rho"], "dynamicViscosity": s["mu"]})
+    out = os.path.join(work, "out")
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    res = subprocess.run([exe, work, out], env=env, capture_output=True, text=True,
+                         timeout=max(60.0, 10 * seconds_budget))
+    info = json.load(open(os.path.join(out, "run.json")))
+    intervals = max(int(info["reported_iteration_intervals"]), 1)
+    secs = float(info["iteration_compute_seconds"]) or float(info["solver_seconds"])
+    value = pm.n_cells * intervals / secs
+    return {"value": value, "unit": "cell-iters/s", "cores": 1, "kind": "reference",
+            "sample": f"reference finite-volume sources + CPU Krylov backend, {pm.n_cells}-cell Voronoi cube "
+                      f"(same generator and settings), {iterations} outer iterations, first excluded, "
+                      f"exit {res.returncode}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_baseline()
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/babelsim-oracle was not built here"}))
+        return
+    line = {"metric": METRIC, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "steady SIMPLE, jittered-Voronoi cube cavity (bounded CPU sample)"},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    import babelsim_b200 as bsg
+    n_side = max(2, round(args.cells ** (1.0 / 3.0)))
+    t0 = time.time()
+    poly = mesh_for(n_side)
+    t_mesh = time.time() - t0
+    ctx = bsg.Context(local)
+    mesh = bsg.Mesh.from_polyhedral(ctx, poly)
+    N, F, Fi = mesh.n_cells, mesh.n_faces, mesh.n_interior
+    s = case_settings()
+    sim = build_simple(bsg, mesh, s)
+    sim.iterate(max(args.warmup, 3))
+    ctx.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = ctx.launches()
+    with ClockSampler(local) as clocks:
+        ctx.record(0)
+        rep = sim.iterate(args.steps)
+        ctx.record(1)
+        ms = ctx.elapsed_ms(0, 1)
+    launches = ctx.launches() - launches0
+    if dist:
+        import torch
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_done = args.steps
+    value = world * N * steps_done / (ms / 1e3)
+    # Live per-kernel timing of one more outer iteration (CUDA events on the library's stream).
+    ctx.profile(True)
+    sim.iterate(1)
+    prof = ctx.profile_report()
+    ctx.profile(False)
+    amg_rows = int(N / 4)
+    candidates = {k: v for k, v in prof.items() if algorithmic_bytes(k, N, 2 * Fi, amg_rows)}
+    top = max(candidates, key=lambda k: candidates[k][1]) if candidates else None
+    peak, peak_kind = load_peaks()
+    roofline = None
+    if top:
+        cnt, tot = candidates[top]
+        avg_s = tot / cnt / 1e3
+        ab = algorithmic_bytes(top, N, 2 * Fi, amg_rows)
+        achieved = ab / avg_s / 1e9
+        roofline = {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 3),
+                    "traffic": None, "algorithmic_bytes_per_launch": ab, "avg_launch_us": round(avg_s * 1e6, 2),
+                    "launches_per_step": cnt}
+    # End to end through the C ABI with host buffers: every step copies U, p, phi in from
+    # pinned host memory, runs one outer iteration and copies them back out.
+    import torch
+    Uh = torch.zeros((N, 3), dtype=torch.float64).pin_memory().numpy()
+    ph = torch.zeros(N, dtype=torch.float64).pin_memory().numpy()
+    phih = torch.zeros(F, dtype=torch.float64).pin_memory().numpy()
+    sim.fields_into(Uh, ph, phih)
+    e2e_steps = max(2, min(args.steps, 5))
+    ctx.synchronize()
+    ctx.record(2)
+    for _ in range(e2e_steps):
+        sim.load_state(Uh, ph, phih)
+        sim.iterate(1)
+        sim.fields_into(Uh, ph, phih)
+    ctx.record(3)
+    e2e_ms = ctx.elapsed_ms(2, 3)
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    bytes_io = 8 * (3 * N + N + F)
+    e2e = {"value": world * N * e2e_steps / (e2e_ms / 1e3), "unit": "cell-iters/s", "h2d_bytes_per_step": bytes_io,
+           "d2h_bytes_per_step": bytes_io, "steps": e2e_steps}
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline()
+        except Exception as exc:  # the baseline is reported, never required for the GPU number
+            cb = {"value": None, "error": str(exc)[:200]}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": world, "steps": steps_done,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms / steps_done, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"steady SIMPLE, {N}-cell jittered-Voronoi cube cavity (n={n_side}^3)",
+                           "cells": N, "faces": F, "interior_faces": Fi, "nu": s["mu"], "lid": 1.0,
+                           "convection": s["convection"], "gradient": s["gradient"], "diffusion": s["diffusion"],
+                           "non_orthogonal_corrections": 2, "solver_rtol": s["rtol"],
+                           "momentum": "bcgs+jacobi", "pressure": "cg+amg", "precision": "fp64",
+                           "l2": "working set >> 126 MB L2, no flush", "parallelism": f"replicas x{world}",
+                           "mesh_seconds": round(t_mesh, 1)},
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
+                "last_report": {"momentum_iterations": rep.momentum_iterations,
+                                "pressure_iterations": rep.pressure_iterations, "rU": rep.rU, "dU": rep.dU,
+                                "mass": rep.mass}}
+        print(json.dumps(line))
+    sim.close()
+    mesh.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

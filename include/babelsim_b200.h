@@ -137,6 +137,15 @@ const char* bsg_global_error(void);
 int bsg_context_launches(const bsg_context* ctx, int64_t* out);
 /* Wait for all work of this context. */
 int bsg_context_synchronize(bsg_context* ctx);
+/* Per-kernel timing: while enabled, instrumented kernels are bracketed by CUDA
+ * events on the context's stream.  The report is JSON
+ * {"kernel": [launches, total_ms], ...} and clears the records. */
+int bsg_context_profile(bsg_context* ctx, int32_t enable);
+int bsg_context_profile_report(bsg_context* ctx, char* buffer, int32_t capacity);
+/* CUDA events on the context's stream, for timing a region of calls:
+ * record into numbered slots, then read the elapsed milliseconds between two. */
+int bsg_context_event_record(bsg_context* ctx, int32_t slot);
+int bsg_context_event_elapsed(bsg_context* ctx, int32_t start_slot, int32_t stop_slot, double* ms);
 
 /* ---- mesh --------------------------------------------------------------
  * bsg_mesh_create takes geometry already computed by the caller (the drop-in
@@ -242,6 +251,10 @@ int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int
 int bsg_simple_set_fields(bsg_simple* s, const double* U, const double* p);
 /* Resume from a saved face flux phi (n_faces) instead of flux(U). */
 int bsg_simple_set_flux(bsg_simple* s, const double* phi);
+/* Overwrite U, p and phi with host values between outer iterations, keeping
+ * every other piece of solver state (the drop-in path whose fields live in
+ * host memory copies them in and out around each iteration). */
+int bsg_simple_load_state(bsg_simple* s, const double* U, const double* p, const double* phi);
 /* Run outer iterations until converged or max_iterations more have been done. */
 int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report* report);
 int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi);
