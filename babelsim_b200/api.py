@@ -92,8 +92,9 @@ class Mesh:
     @classmethod
     def from_polyhedral(cls, ctx: Context, poly):
         """Geometry computed by the library from a polyhedral description (see meshgen.PolyMesh)."""
-        offsets = i32(np.concatenate([[0], np.cumsum([len(f) for f in poly.faces])]))
-        ids = i32(np.concatenate(poly.faces))
+        off, ids = poly.flat() if hasattr(poly, "flat") else (
+            np.concatenate([[0], np.cumsum([len(f) for f in poly.faces])]), np.concatenate(poly.faces))
+        offsets, ids = i32(off), i32(ids)
         verts = f64(poly.vertices)
         owner, nbr, patch = i32(poly.owner), i32(poly.neighbour), i32(poly.patch)
         h = C.c_void_p()

@@ -96,13 +96,160 @@ double trueResidual(const Csr& a, const std::vector<double>& b, const std::vecto
     return std::sqrt(dotv(r, r));
 }
 
-// Jacobi-preconditioned CG on the recursive residual; stops when the
-// recursive norm reaches `inner` or the budget is spent.
-int pcg(const Csr& a, const std::vector<double>& b, std::vector<double>& x, double inner, int budget) {
+// CPU aggregation AMG (stand-in for Hypre BoomerAMG behind pcType hypre|gamg):
+// pairwise matching of strongest negative couplings applied twice per level,
+// Galerkin coarse operators of piecewise-constant prolongation, V(2,2) cycle
+// with damped Jacobi (omega 2/3) and a dense LU solve on the coarsest level.
+struct CpuAmg {
+    struct Level {
+        Csr a;
+        std::vector<int> agg;  // to the next level
+        std::vector<double> x, b, t;
+    };
+    std::vector<Level> levels;
+    std::vector<double> lu;   // coarsest dense LU (row-major), partial pivoting
+    std::vector<int> piv;
+
+    static std::vector<int> pairwise(const Csr& a, int& nc) {
+        std::vector<int> agg(a.n, -1);
+        nc = 0;
+        for (int i = 0; i < a.n; ++i) {
+            if (agg[i] >= 0) continue;
+            int best = -1;
+            double bs = 0.0;
+            for (int k = a.row[i]; k < a.row[i + 1]; ++k) {
+                const int j = a.col[k];
+                if (j == i || agg[j] >= 0) continue;
+                if (-a.val[k] > bs) { bs = -a.val[k]; best = j; }
+            }
+            agg[i] = nc;
+            if (best >= 0) agg[best] = nc;
+            ++nc;
+        }
+        return agg;
+    }
+    static Csr galerkin(const Csr& a, const std::vector<int>& agg, int nc) {
+        std::vector<std::vector<std::pair<int, double>>> rows(nc);
+        for (int i = 0; i < a.n; ++i)
+            for (int k = a.row[i]; k < a.row[i + 1]; ++k) rows[agg[i]].push_back({agg[a.col[k]], a.val[k]});
+        Csr c;
+        c.n = nc;
+        c.row.assign(nc + 1, 0);
+        for (int I = 0; I < nc; ++I) {
+            auto& r = rows[I];
+            std::sort(r.begin(), r.end(), [](const auto& u, const auto& v) { return u.first < v.first; });
+            int diag_pos = -1;
+            for (std::size_t k = 0; k < r.size(); ++k) {
+                if (!c.col.empty() && static_cast<int>(c.col.size()) > c.row[I] && c.col.back() == r[k].first) {
+                    c.val.back() += r[k].second;
+                } else {
+                    c.col.push_back(r[k].first);
+                    c.val.push_back(r[k].second);
+                }
+                if (r[k].first == I) diag_pos = static_cast<int>(c.col.size()) - 1;
+            }
+            (void)diag_pos;
+            c.row[I + 1] = static_cast<int>(c.col.size());
+        }
+        c.inv_diag.assign(nc, 1.0);
+        for (int I = 0; I < nc; ++I)
+            for (int k = c.row[I]; k < c.row[I + 1]; ++k)
+                if (c.col[k] == I && c.val[k] != 0.0) c.inv_diag[I] = 1.0 / c.val[k];
+        return c;
+    }
+    explicit CpuAmg(const Csr& fine) {
+        levels.push_back({fine, {}, {}, {}, {}});
+        while (levels.back().a.n > 64 && levels.size() < 12) {
+            int n1 = 0, n2 = 0;
+            const Csr& a = levels.back().a;
+            const std::vector<int> a1 = pairwise(a, n1);
+            const Csr c1 = galerkin(a, a1, n1);
+            const std::vector<int> a2 = pairwise(c1, n2);
+            if (n2 >= a.n) break;
+            std::vector<int> agg(a.n);
+            for (int i = 0; i < a.n; ++i) agg[i] = a2[a1[i]];
+            Csr c = galerkin(a, agg, n2);
+            levels.back().agg = std::move(agg);
+            levels.push_back({std::move(c), {}, {}, {}, {}});
+        }
+        for (auto& l : levels) { l.x.resize(l.a.n); l.b.resize(l.a.n); l.t.resize(l.a.n); }
+        const Csr& c = levels.back().a;
+        const int n = c.n;
+        lu.assign(static_cast<std::size_t>(n) * n, 0.0);
+        for (int i = 0; i < n; ++i)
+            for (int k = c.row[i]; k < c.row[i + 1]; ++k) lu[static_cast<std::size_t>(i) * n + c.col[k]] += c.val[k];
+        piv.resize(n);
+        for (int k = 0; k < n; ++k) {
+            int p = k;
+            for (int i = k + 1; i < n; ++i)
+                if (std::fabs(lu[static_cast<std::size_t>(i) * n + k]) > std::fabs(lu[static_cast<std::size_t>(p) * n + k])) p = i;
+            piv[k] = p;
+            if (p != k)
+                for (int j = 0; j < n; ++j) std::swap(lu[static_cast<std::size_t>(k) * n + j], lu[static_cast<std::size_t>(p) * n + j]);
+            const double d = lu[static_cast<std::size_t>(k) * n + k];
+            for (int i = k + 1; i < n; ++i) {
+                const double f = (lu[static_cast<std::size_t>(i) * n + k] /= d);
+                for (int j = k + 1; j < n; ++j) lu[static_cast<std::size_t>(i) * n + j] -= f * lu[static_cast<std::size_t>(k) * n + j];
+            }
+        }
+    }
+    void smooth(const Csr& a, const std::vector<double>& b, std::vector<double>& x, std::vector<double>& t) {
+        for (int i = 0; i < a.n; ++i) {
+            double ax = 0.0;
+            for (int k = a.row[i]; k < a.row[i + 1]; ++k) ax += a.val[k] * x[a.col[k]];
+            t[i] = x[i] + (2.0 / 3.0) * a.inv_diag[i] * (b[i] - ax);
+        }
+        x.swap(t);
+    }
+    void cycle(std::size_t l) {
+        Level& L = levels[l];
+        if (l + 1 == levels.size()) {
+            const int n = L.a.n;
+            std::vector<double> y(L.b);
+            for (int k = 0; k < n; ++k) std::swap(y[k], y[piv[k]]);
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < i; ++j) y[i] -= lu[static_cast<std::size_t>(i) * n + j] * y[j];
+            for (int i = n - 1; i >= 0; --i) {
+                for (int j = i + 1; j < n; ++j) y[i] -= lu[static_cast<std::size_t>(i) * n + j] * y[j];
+                y[i] /= lu[static_cast<std::size_t>(i) * n + i];
+            }
+            L.x = y;
+            return;
+        }
+        std::fill(L.x.begin(), L.x.end(), 0.0);
+        smooth(L.a, L.b, L.x, L.t);
+        smooth(L.a, L.b, L.x, L.t);
+        Level& C = levels[l + 1];
+        std::fill(C.b.begin(), C.b.end(), 0.0);
+        for (int i = 0; i < L.a.n; ++i) {
+            double ax = 0.0;
+            for (int k = L.a.row[i]; k < L.a.row[i + 1]; ++k) ax += L.a.val[k] * L.x[L.a.col[k]];
+            C.b[L.agg[i]] += L.b[i] - ax;
+        }
+        cycle(l + 1);
+        for (int i = 0; i < L.a.n; ++i) L.x[i] += C.x[L.agg[i]];
+        smooth(L.a, L.b, L.x, L.t);
+        smooth(L.a, L.b, L.x, L.t);
+    }
+    void apply(const std::vector<double>& r, std::vector<double>& z) {
+        levels[0].b = r;
+        cycle(0);
+        z = levels[0].x;
+    }
+};
+
+// Preconditioned CG on the recursive residual (Jacobi, or the CPU AMG when
+// given); stops when the recursive norm reaches `inner` or the budget is spent.
+int pcg(const Csr& a, const std::vector<double>& b, std::vector<double>& x, double inner, int budget,
+        CpuAmg* amg = nullptr) {
     const int n = a.n;
     std::vector<double> r(n), z(n), p(n), q(n);
     trueResidual(a, b, x, r);
-    for (int i = 0; i < n; ++i) z[i] = a.inv_diag[i] * r[i];
+    auto precondition = [&]() {
+        if (amg) amg->apply(r, z);
+        else for (int i = 0; i < n; ++i) z[i] = a.inv_diag[i] * r[i];
+    };
+    precondition();
     p = z;
     double rz = dotv(r, z);
     int it = 0;
@@ -112,7 +259,7 @@ int pcg(const Csr& a, const std::vector<double>& b, std::vector<double>& x, doub
         if (!(std::fabs(pq) > 0.0) || !std::isfinite(pq)) break;
         const double alpha = rz / pq;
         for (int i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
-        for (int i = 0; i < n; ++i) z[i] = a.inv_diag[i] * r[i];
+        precondition();
         const double rz_new = dotv(r, z);
         const double beta = rz_new / rz;
         rz = rz_new;
@@ -173,9 +320,13 @@ SolveResult acceptanceSolve(const Csr& a, const LinearSolverConfig& config, cons
     double inner = target;
     int used = 0;
     double final_residual = r0;
+    std::unique_ptr<CpuAmg> amg;
+    if (config.solver == LinearSolverType::ConjugateGradient &&
+        (config.preconditioner == PreconditionerType::Hypre || config.preconditioner == PreconditionerType::GAMG))
+        amg = std::make_unique<CpuAmg>(a);
     for (int restart = 0; restart < 3 && used < config.max_iterations; ++restart) {
         const int budget = config.max_iterations - used;
-        used += config.solver == LinearSolverType::ConjugateGradient ? pcg(a, b, x, inner, budget)
+        used += config.solver == LinearSolverType::ConjugateGradient ? pcg(a, b, x, inner, budget, amg.get())
                                                                       : bicgstab(a, b, x, inner, budget);
         final_residual = trueResidual(a, b, x, r);
         if (residualConverged(final_residual, target) || !std::isfinite(final_residual)) break;
