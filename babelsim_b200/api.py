@@ -78,6 +78,19 @@ class Context:
             pass
 
 
+def validate_polyhedral(poly):
+    """Run the library's host geometry on a polyhedral mesh (no device); returns (n_cells, orthogonal)."""
+    off, ids = poly.flat() if hasattr(poly, "flat") else (
+        np.concatenate([[0], np.cumsum([len(f) for f in poly.faces])]), np.concatenate(poly.faces))
+    verts, off, ids = f64(poly.vertices), i32(off), i32(ids)
+    owner, nbr, patch = i32(poly.owner), i32(poly.neighbour), i32(poly.patch)
+    nc, orth = C.c_int32(), C.c_int32()
+    check(lib().bsg_mesh_validate_polyhedral(len(verts), ptr(verts), len(owner), ptr(off), ptr(ids), ptr(owner),
+                                             ptr(nbr), ptr(patch), len(poly.patch_names), C.byref(nc),
+                                             C.byref(orth)))
+    return nc.value, bool(orth.value)
+
+
 class Mesh:
     """A device-resident mesh (bsg_mesh)."""
 

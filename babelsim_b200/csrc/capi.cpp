@@ -337,6 +337,19 @@ int bsg_mesh_destroy(bsg_mesh* mesh) {
     return bsg::kOk;
 }
 
+int bsg_mesh_validate_polyhedral(int32_t n_vertices, const double* vertices, int32_t n_faces, const int32_t* offsets,
+                                 const int32_t* ids, const int32_t* owner, const int32_t* neighbour,
+                                 const int32_t* patch, int32_t n_patches, int32_t* n_cells_out,
+                                 int32_t* orthogonal_out) {
+    return guard(nullptr, [&] {
+        require(vertices && offsets && ids && owner && neighbour && patch, "null argument");
+        const bsg::HostGeometry h = bsg::computePolyhedralGeometry(n_vertices, vertices, n_faces, offsets, ids, owner,
+                                                                    neighbour, patch, n_patches);
+        if (n_cells_out) *n_cells_out = h.n_cells;
+        if (orthogonal_out) *orthogonal_out = h.orthogonal ? 1 : 0;
+    });
+}
+
 int bsg_mesh_sizes(const bsg_mesh* mesh, int64_t out[5]) {
     if (!mesh || !out) return bsg::kArgument;
     const bsg::DeviceMesh& m = *mesh->mesh;

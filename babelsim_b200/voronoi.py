@@ -121,6 +121,24 @@ def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, 
     owner = f_lo.astype(np.int32)
     neighbour = np.where(is_int, f_hi, -1).astype(np.int32)
     patch = np.where(is_int, -1, ppatch[f_hi]).astype(np.int32)
+    # Drop slivers: faces whose area is below max(1e-9 h^2, 1e-12) (near-cospherical
+    # site groups).  Both cells lose the face, so the mesh stays consistent; the
+    # closure error is the sliver's area.  The reference rejects faces whose
+    # projected area is below 1e-13 (src/core/mesh.cpp:89-104).
+    offsets0 = np.r_[0, np.cumsum(sizes)].astype(np.int64)
+    face_of = np.repeat(np.arange(len(sizes)), sizes)
+    p = verts[ids.ravel()]
+    p0 = p[offsets0[:-1]][face_of]
+    nxt = np.r_[np.arange(1, len(p)), 0]
+    nxt[offsets0[1:] - 1] = offsets0[:-1]
+    tri = np.cross(p - p0, p[nxt] - p0)
+    area = 0.5 * np.linalg.norm(np.add.reduceat(tri, offsets0[:-1], axis=0), axis=1)
+    big = area > max(1e-9 * h * h, 1e-12)
+    if not np.all(big):
+        keep_el = big[face_of]
+        ids = ids.ravel()[keep_el]
+        sizes = sizes[big]
+        owner, neighbour, patch = owner[big], neighbour[big], patch[big]
     order = np.argsort(patch, kind="stable")            # interior (-1) first, then by patch
     offsets = np.r_[0, np.cumsum(sizes)].astype(np.int64)
     sz = sizes[order]

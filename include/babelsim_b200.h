@@ -160,6 +160,14 @@ int bsg_mesh_create_polyhedral(bsg_context* ctx, int32_t n_vertices, const doubl
                                const int32_t* neighbour, const int32_t* patch, int32_t n_patches,
                                bsg_mesh** out);
 int bsg_mesh_destroy(bsg_mesh* mesh);
+/* Host-only check of a polyhedral description: computes the geometry exactly as
+ * bsg_mesh_create_polyhedral does (no device needed) and reports the first
+ * problem the reference's Mesh::polyhedral would reject.  Outputs: cell count
+ * and the orthogonal-geometry flag. */
+int bsg_mesh_validate_polyhedral(int32_t n_vertices, const double* vertices, int32_t n_faces,
+                                 const int32_t* face_point_offsets, const int32_t* face_point_ids,
+                                 const int32_t* owner, const int32_t* neighbour, const int32_t* patch,
+                                 int32_t n_patches, int32_t* n_cells_out, int32_t* orthogonal_out);
 /* n_cells, n_faces, n_interior_faces, n_patches, orthogonal flag. */
 int bsg_mesh_sizes(const bsg_mesh* mesh, int64_t out[5]);
 /* Copy one geometry array (a bsg_mesh_geometry member name, e.g.

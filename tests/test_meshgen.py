@@ -1,0 +1,65 @@
+"""Mesh generators and the library's host geometry (no GPU needed)."""
+import numpy as np
+import pytest
+
+from babelsim_b200 import meshgen
+from babelsim_b200.api import validate_polyhedral
+from oracle import geometry
+
+
+def _oracle_geo(pm):
+    return geometry.compute_geometry(geometry.PolyMesh(pm.vertices, pm.rings(), pm.owner, pm.neighbour, pm.patch,
+                                                       pm.patch_names, pm.patch_kinds))
+
+
+@pytest.mark.parametrize("n", [6, 12])
+def test_voronoi_cube_is_a_closed_tessellation(n):
+    pm = meshgen.voronoi_cube(n)
+    geo = _oracle_geo(pm)
+    assert geo.n_cells == n ** 3
+    assert abs(geo.volume.sum() - 1.0) < 1e-12
+    closure = np.zeros((geo.n_cells, 3))
+    np.add.at(closure, geo.owner, geo.Sf)
+    inn = geo.neighbour >= 0
+    np.add.at(closure, geo.neighbour[inn], -geo.Sf[inn])
+    assert np.abs(closure).max() < 1e-12 / n ** 2 * 100
+    faces_per_cell = np.bincount(geo.owner, minlength=geo.n_cells) + np.bincount(geo.neighbour[inn],
+                                                                                  minlength=geo.n_cells)
+    assert 12.0 < faces_per_cell.mean() < 16.0
+    assert not geo.orthogonal
+    # the library's host geometry accepts it (the reference's Mesh::polyhedral checks)
+    assert validate_polyhedral(pm) == (n ** 3, False)
+
+
+def test_voronoi_cube_is_seeded():
+    a, b = meshgen.voronoi_cube(5, seed=1), meshgen.voronoi_cube(5, seed=1)
+    c = meshgen.voronoi_cube(5, seed=2)
+    assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.ids, b.ids)
+    assert not np.array_equal(a.vertices, c.vertices)
+
+
+def test_voronoi_boundary_faces_lie_on_the_cube():
+    pm = meshgen.voronoi_cube(8)
+    geo = _oracle_geo(pm)
+    bf = geo.neighbour < 0
+    for patch, (axis, value) in enumerate([(0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (2, 1)]):
+        m = bf & (geo.patch == patch)
+        assert np.allclose(geo.xf[m, axis], value, atol=1e-12)
+
+
+def test_mesh_file_round_trip(tmp_path):
+    pm = meshgen.voronoi_cube(4)
+    meshgen.write_mesh(tmp_path / "v.mesh", pm)
+    back = meshgen.read_mesh(tmp_path / "v.mesh")
+    assert np.array_equal(back.owner, pm.owner) and np.array_equal(back.neighbour, pm.neighbour)
+    assert np.array_equal(np.concatenate(back.faces), pm.ids)
+    assert np.allclose(back.vertices, pm.vertices, rtol=0, atol=0)
+
+
+def test_library_geometry_rejects_what_the_reference_rejects():
+    pm = meshgen.cavity_2d(3)
+    pm.vertices = pm.vertices.copy()
+    ring = pm.faces[0]
+    pm.vertices[ring[1]] = pm.vertices[ring[0]]   # collapse an edge of one face: zero-area triangle
+    with pytest.raises(Exception):
+        validate_polyhedral(pm)
