@@ -328,6 +328,14 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
     Level* last = levels_.back();
     last->dense.resize(2 * static_cast<std::size_t>(last->n) * last->n);
     built_ = true;
+    if (std::getenv("BSG_AMG_VERBOSE")) {
+        long long total = 0;
+        for (Level* l : levels_) total += l->nnz + l->n;
+        for (std::size_t i = 0; i < levels_.size(); ++i)
+            std::fprintf(stderr, "amg level %zu: rows %d, off-diagonal nnz %lld (%.1f per row)\n", i, levels_[i]->n,
+                         levels_[i]->nnz, levels_[i]->n ? double(levels_[i]->nnz) / levels_[i]->n : 0.0);
+        std::fprintf(stderr, "amg operator complexity %.3f\n", double(total) / double(levels_[0]->nnz + levels_[0]->n));
+    }
 }
 
 void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {

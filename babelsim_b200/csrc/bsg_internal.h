@@ -167,6 +167,8 @@ struct DeviceMesh {
     // the two matrix slots of each interior face: owner row (upper) and neighbour row (lower)
     std::vector<int> h_slot_own, h_slot_nbr;
     DeviceArray<int> slot_own, slot_nbr;
+    // scratch for the first Green-Gauss pass (3*9*n_cells doubles at most)
+    DeviceArray<double> ws_grad_pass1;
     // external geometry copy for bsg_mesh_export (host)
     std::vector<double> ext_Sf, ext_xf, ext_area, ext_n, ext_w, ext_dcoef, ext_k, ext_skew, ext_xc, ext_V;
     std::vector<int> ext_owner, ext_nbr, ext_patch;

@@ -753,8 +753,25 @@ void DeviceEquation::reset() {
     diag.zero(s);
     val.zero(s);
     src.zero(s);
+    for (auto& d : diffusion) spare.push_back(std::move(d));
     diffusion.clear();
     boundary_flux = nullptr;
+    grad_method = -1;
+}
+
+std::unique_ptr<DiffusionSnapshot> DeviceEquation::takeSnapshot() {
+    if (spare.empty()) return std::make_unique<DiffusionSnapshot>();
+    auto s = std::move(spare.back());
+    spare.pop_back();
+    return s;
+}
+
+const double* DeviceEquation::unknownGradient(int method) {
+    if (grad_method != method) {
+        gradient(*x, method, grad_ws);
+        grad_method = method;
+    }
+    return grad_ws.data();
 }
 
 void Reducer::ensure(int blocks, int nv) {
@@ -783,7 +800,8 @@ void gradient(DeviceField& x, int method, DeviceArray<double>& out) {
         else launch(ctx, kGradGauss<3, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, out.data());
         return;
     }
-    DeviceArray<double> first(out.size());
+    DeviceArray<double>& first = m.ws_grad_pass1;  // persistent scratch: no allocation per call
+    if (first.size() < out.size()) first.resize(out.size());
     if (C == 1) {
         launch(ctx, kGradGauss<1, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, first.data());
         launch(ctx, kGradGauss<1, true>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)first.data(), out.data());
@@ -791,7 +809,6 @@ void gradient(DeviceField& x, int method, DeviceArray<double>& out) {
         launch(ctx, kGradGauss<3, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, first.data());
         launch(ctx, kGradGauss<3, true>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)first.data(), out.data());
     }
-    ctx.sync();  // `first` is released on return
 }
 
 void gradientTrace(DeviceField& x, const double* g, DeviceArray<double>& trace_out) {
@@ -867,17 +884,16 @@ void addConvection(DeviceEquation& eq, DeviceField& phi, double scale, const Opt
     if (o.interpolation != 0 && o.interpolation != 1) fail(kArgument, "unsupported convection interpolation method");
     eq.boundary_flux = &phi;
     x.setFluxContext(phi);
-    DeviceArray<double> g;
+    eq.grad_method = -1;  // the flux context feeds inletOutlet traces of the gradient
     const bool need_grad = o.convection == 1 || (o.convection == 2 && o.interpolation == 1);
-    if (need_grad) gradient(x, o.gradient, g);
+    const double* g = need_grad ? eq.unknownGradient(o.gradient) : nullptr;
     const BcView b = x.bcView();
     if (x.comps == 1)
-        launch(ctx, kAddConvection<1>, m.n_cells, view(m), b, (const double*)x.v.data(), (const double*)g.data(),
+        launch(ctx, kAddConvection<1>, m.n_cells, view(m), b, (const double*)x.v.data(), g,
                (const double*)phi.v.data(), o.convection, scale, eq.diag.data(), eq.val.data(), eq.src.data());
     else
-        launch(ctx, kAddConvection<3>, m.n_cells, view(m), b, (const double*)x.v.data(), (const double*)g.data(),
+        launch(ctx, kAddConvection<3>, m.n_cells, view(m), b, (const double*)x.v.data(), g,
                (const double*)phi.v.data(), o.convection, scale, eq.diag.data(), eq.val.data(), eq.src.data());
-    if (need_grad) ctx.sync();
 }
 
 void addLaplacian(DeviceEquation& eq, DeviceField* coef, double k, double factor, const Options& o) {
@@ -885,14 +901,14 @@ void addLaplacian(DeviceEquation& eq, DeviceField* coef, double k, double factor
     DeviceMesh& m = *x.mesh;
     Context& ctx = *m.ctx;
     if (!std::isfinite(factor) || (!coef && !std::isfinite(k))) fail(kArgument, "nonfinite equ coefficient");
-    auto snap = std::make_unique<DiffusionSnapshot>();
+    auto snap = eq.takeSnapshot();
     snap->kf.resize(m.n_faces);
     if (coef) {
         if (coef->mesh != &m || coef->comps != 1) fail(kArgument, "equ diffusivity must be a compatible cell or face field");
         if (coef->location == 0) {
-            DeviceArray<double> gws;
-            interpolate(*coef, o.coefInterp(), o.coefGrad(), snap->kf, &gws);
-            ctx.sync();
+            // corrected coefficient interpolation needs the coefficient's own gradient
+            if (o.coefInterp() != 0) interpolate(*coef, o.coefInterp(), o.coefGrad(), snap->kf, &snap->correction);
+            else interpolate(*coef, 0, 0, snap->kf);
         } else {
             BSG_CUDA(cudaMemcpyAsync(snap->kf.data(), coef->v.data(), sizeof(double) * m.n_faces,
                                      cudaMemcpyDeviceToDevice, ctx.stream));
@@ -902,29 +918,35 @@ void addLaplacian(DeviceEquation& eq, DeviceField* coef, double k, double factor
         std::vector<double> h(m.n_faces, k);
         snap->kf.upload(h, ctx.stream);
     }
-    DeviceArray<double> g;
-    if (o.diffusion != 0) gradient(x, o.gradient, g);
+    const double* g = o.diffusion != 0 ? eq.unknownGradient(o.gradient) : nullptr;
     const BcView b = x.bcView();
     const double mult = -factor;
     if (x.comps == 1)
-        launch(ctx, kAddDiffusion<1>, m.n_cells, view(m), b, (const double*)x.v.data(), (const double*)g.data(),
+        launch(ctx, kAddDiffusion<1>, m.n_cells, view(m), b, (const double*)x.v.data(), g,
                (const double*)snap->kf.data(), 0.0, o.diffusion, mult, eq.diag.data(), eq.val.data(), eq.src.data());
     else
-        launch(ctx, kAddDiffusion<3>, m.n_cells, view(m), b, (const double*)x.v.data(), (const double*)g.data(),
+        launch(ctx, kAddDiffusion<3>, m.n_cells, view(m), b, (const double*)x.v.data(), g,
                (const double*)snap->kf.data(), 0.0, o.diffusion, mult, eq.diag.data(), eq.val.data(), eq.src.data());
     if (x.comps == 1) {
         snap->correction.resize(m.n_faces);
         if (o.diffusion != 0)
-            launch(ctx, kDiffusionCorrection, m.n_faces, view(m), b, (const double*)x.v.data(), (const double*)g.data(),
+            launch(ctx, kDiffusionCorrection, m.n_faces, view(m), b, (const double*)x.v.data(), g,
                    (const double*)snap->kf.data(), o.diffusion, snap->correction.data());
         else
             snap->correction.zero(ctx.stream);
-        snap->bcs = x.bcs;
-        snap->d_bcs.upload(snap->bcs, ctx.stream);
+        bool same = snap->bcs.size() == x.bcs.size();
+        for (std::size_t i = 0; same && i < x.bcs.size(); ++i)
+            same = snap->bcs[i].type == x.bcs[i].type && snap->bcs[i].value[0] == x.bcs[i].value[0] &&
+                   snap->bcs[i].value[1] == x.bcs[i].value[1] && snap->bcs[i].value[2] == x.bcs[i].value[2];
+        if (!same || snap->d_bcs.size() != x.bcs.size()) {
+            snap->bcs = x.bcs;
+            snap->d_bcs.upload(snap->bcs, ctx.stream);
+        }
         snap->factor = factor;
         eq.diffusion.push_back(std::move(snap));
+    } else {
+        eq.spare.push_back(std::move(snap));
     }
-    ctx.sync();
 }
 
 void addSource(DeviceEquation& eq, const double* values, double factor) {

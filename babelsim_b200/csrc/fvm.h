@@ -53,14 +53,22 @@ struct DiffusionSnapshot {
 };
 
 // DiscreteEquation<T> + equ::Equation state (procedural_equation.cpp:15-34).
+// Snapshot buffers and the gradient workspace persist across reset(), so an
+// outer iteration allocates no device memory.
 struct DeviceEquation {
     DeviceField* x = nullptr;
     Options options;
     DeviceArray<double> diag, val, src;
-    std::vector<std::unique_ptr<DiffusionSnapshot>> diffusion;
+    std::vector<std::unique_ptr<DiffusionSnapshot>> diffusion;  // active contributions
+    std::vector<std::unique_ptr<DiffusionSnapshot>> spare;      // recycled buffers
     const DeviceField* boundary_flux = nullptr;
+    DeviceArray<double> grad_ws;     // gradient of the unknown, valid for grad_method while assembling
+    int grad_method = -1;
     DeviceEquation(DeviceField& unknown, const Options& o);
     void reset();
+    std::unique_ptr<DiffusionSnapshot> takeSnapshot();
+    // Gradient of the unknown for this assembly (computed once per method).
+    const double* unknownGradient(int method);
 };
 
 // Reduction workspace: per-block partials + final results in device memory.

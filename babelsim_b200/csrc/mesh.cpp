@@ -146,6 +146,7 @@ HostGeometry computePolyhedralGeometry(int n_vertices, const double* verts, int 
     for (int c = 0; c < n_cells; ++c) ref[c] = mul(1.0 / std::max(1.0, pcnt[c]), psum[c]);
     g.Sf.resize(3 * n_faces); g.xf.resize(3 * n_faces); g.area.resize(n_faces); g.normal.resize(3 * n_faces);
     std::vector<std::vector<Tri>> tris(n_faces);
+    std::vector<int> oriented(ids, ids + offsets[n_faces]);  // rings after outward orientation
     std::vector<int> ring;
     for (int f = 0; f < n_faces; ++f) {
         ring.assign(ids + offsets[f], ids + offsets[f + 1]);
@@ -190,6 +191,55 @@ HostGeometry computePolyhedralGeometry(int n_vertices, const double* verts, int 
             g.normal[3 * f + k] = a[k] / total;
         }
         g.area[f] = total;
+        std::copy(ring.begin(), ring.end(), oriented.begin() + offsets[f]);
+    }
+    // Every cell must be a closed, consistently oriented surface: vector areas
+    // close and each edge of the outward-oriented rings appears exactly twice
+    // with opposite directions (Mesh::validate, src/core/mesh.cpp:709-756).
+    {
+        std::vector<int> cptr(n_cells + 1, 0);
+        for (int f = 0; f < n_faces; ++f) {
+            ++cptr[owner[f] + 1];
+            if (neighbour[f] >= 0) ++cptr[neighbour[f] + 1];
+        }
+        for (int c = 0; c < n_cells; ++c) cptr[c + 1] += cptr[c];
+        std::vector<int> cface(cptr[n_cells]), fill(cptr.begin(), cptr.end() - 1);
+        for (int f = 0; f < n_faces; ++f) {
+            cface[fill[owner[f]]++] = f;
+            if (neighbour[f] >= 0) cface[fill[neighbour[f]]++] = -f - 1;
+        }
+        std::vector<std::pair<long long, int>> edges;
+        for (int c = 0; c < n_cells; ++c) {
+            double cx = 0, cy = 0, cz = 0, total = 0;
+            edges.clear();
+            for (int k = cptr[c]; k < cptr[c + 1]; ++k) {
+                const int f = cface[k] >= 0 ? cface[k] : -cface[k] - 1;
+                const double s = cface[k] >= 0 ? 1.0 : -1.0;
+                cx += s * g.Sf[3 * f]; cy += s * g.Sf[3 * f + 1]; cz += s * g.Sf[3 * f + 2];
+                total += g.area[f];
+                const int* ring = oriented.data() + offsets[f];
+                const std::size_t m = static_cast<std::size_t>(offsets[f + 1] - offsets[f]);
+                for (std::size_t e = 0; e < m; ++e) {
+                    int from = ring[e], to = ring[(e + 1) % m];
+                    if (s < 0) std::swap(from, to);
+                    const int a = std::min(from, to), b = std::max(from, to);
+                    edges.push_back({static_cast<long long>(a) * n_vertices + b, from == a ? 1 : -1});
+                }
+            }
+            if (!(std::isfinite(total) && std::sqrt(cx * cx + cy * cy + cz * cz) <= 1e-9 * std::max(total, 1.0)))
+                fail(kArgument, "polyhedral cell face area vectors do not close (cell " + std::to_string(c) + ")");
+            std::sort(edges.begin(), edges.end());
+            for (std::size_t e = 0; e < edges.size();) {
+                std::size_t j = e;
+                int orient = 0;
+                while (j < edges.size() && edges[j].first == edges[e].first) orient += edges[j++].second;
+                if (j - e != 2 || orient != 0)
+                    fail(kArgument, "polyhedral cell surface has a non-manifold or inconsistently oriented edge " +
+                                        std::to_string(edges[e].first / n_vertices) + "-" +
+                                        std::to_string(edges[e].first % n_vertices));
+                e = j;
+            }
+        }
     }
     // Cell volume and centroid (mesh.cpp:486-519).
     g.V.assign(n_cells, 0.0);

@@ -118,14 +118,9 @@ void SimpleSolver::outerIteration() {
         addSource(mom, gradP_.data(), -1.0);
     }
     // rU before relaxation (simple/main.cpp:59-60).
+    // The norms stay on the device and are read with the other diagnostics: a
+    // non-finite rU still ends the run as a numerical failure, one sync later.
     relativeResidualNorms(mom, U_.v.data(), red_);
-    double diag_h[16];
-    BSG_CUDA(cudaMemcpyAsync(ctx_.pinned, red_.result.data(), 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
-    ctx_.sync();
-    std::memcpy(diag_h, ctx_.pinned, 3 * sizeof(double));
-    const double rU = std::sqrt(diag_h[0]) / std::max(std::sqrt(diag_h[1]) + std::sqrt(diag_h[2]), 1e-30);
-    report_.rU = rU;
-    if (!std::isfinite(rU)) { report_.status = 2; return; }
     relax(mom, Uprev_.data(), cfg_.alpha_u);
     scale(mom, cfg_.alpha_u);
     ratioVolume(m_, mom.diag.data(), rAU_.v.data());
@@ -191,22 +186,23 @@ void SimpleSolver::outerIteration() {
     subtractScaledGradient(m_, U_.v.data(), rAU_.v.data(), gradPP_.data());
     addArrays(ctx_, phi_.v.data(), phiH_.v.data(), pflux_.data(), m_.n_faces);
     // Convergence diagnostics (simple/main.cpp:112-126).
-    relativeChangeNorms(ctx_, U_.v.data(), Uprev_.data(), 3LL * N, red_);
-    BSG_CUDA(cudaMemcpyAsync(ctx_.pinned, red_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    relativeChangeNorms(ctx_, U_.v.data(), Uprev_.data(), 3LL * N, redU_);
+    relativeChangeNorms(ctx_, pP_.v.data(), nullptr, N, redPP_);
+    relativeChangeNorms(ctx_, p_.v.data(), nullptr, N, redP_);
+    fluxBalance(m_, phi_.v.data(), redM_);
+    double* h = ctx_.pinned;
+    BSG_CUDA(cudaMemcpyAsync(h + 0, red_.result.data(), 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(h + 4, redU_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(h + 6, redPP_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(h + 8, redP_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(h + 10, redM_.result.data(), 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
     ctx_.sync();
-    const double dU = std::sqrt(ctx_.pinned[0]) / std::max(std::sqrt(ctx_.pinned[1]), 1e-30);
-    relativeChangeNorms(ctx_, pP_.v.data(), nullptr, N, red_);
-    BSG_CUDA(cudaMemcpyAsync(ctx_.pinned, red_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
-    ctx_.sync();
-    const double pp2 = ctx_.pinned[0];
-    relativeChangeNorms(ctx_, p_.v.data(), nullptr, N, red_);
-    BSG_CUDA(cudaMemcpyAsync(ctx_.pinned, red_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
-    ctx_.sync();
-    const double dP = std::sqrt(pp2) / std::max(std::sqrt(ctx_.pinned[1]), 1e-30);
-    fluxBalance(m_, phi_.v.data(), red_);
-    BSG_CUDA(cudaMemcpyAsync(ctx_.pinned, red_.result.data(), 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
-    ctx_.sync();
-    const double mass = ctx_.pinned[0] / std::max(ctx_.pinned[2], 1e-30);
+    const double rU = std::sqrt(h[0]) / std::max(std::sqrt(h[1]) + std::sqrt(h[2]), 1e-30);
+    const double dU = std::sqrt(h[4]) / std::max(std::sqrt(h[5]), 1e-30);
+    const double dP = std::sqrt(h[6]) / std::max(std::sqrt(h[9]), 1e-30);
+    const double mass = h[10] / std::max(h[12], 1e-30);
+    report_.rU = rU;
+    if (!std::isfinite(rU)) { report_.status = 2; return; }
     report_.dU = dU;
     report_.dP = dP;
     report_.mass = mass;

@@ -51,7 +51,7 @@ private:
     std::unique_ptr<DeviceEquation> mom_, peq_;
     KrylovSolver krylov_;
     std::unique_ptr<Preconditioner> ppc_;
-    Reducer red_;
+    Reducer red_, redU_, redPP_, redP_, redM_;  // one per diagnostic, read back together
     DeviceArray<double> Uprev_, gradP_, gradPP_, divPhiH_, pflux_, diag_ws_;
     DeviceArray<int> flags_;
     SimpleReport report_;

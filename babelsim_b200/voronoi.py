@@ -47,6 +47,89 @@ def _merge_ids(c, tol):
     return inv.ravel()
 
 
+def _face_areas(ids, sizes, verts):
+    off = np.r_[0, np.cumsum(sizes)].astype(np.int64)
+    face_of = np.repeat(np.arange(len(sizes)), sizes)
+    p = verts[ids]
+    p0 = p[off[:-1]][face_of]
+    nxt = np.r_[np.arange(1, len(p)), 0]
+    nxt[off[1:] - 1] = off[:-1]
+    tri = np.cross(p - p0, p[nxt] - p0)
+    return 0.5 * np.linalg.norm(np.add.reduceat(tri, off[:-1], axis=0), axis=1)
+
+
+def _collapse_slivers(ids, sizes, verts, min_area):
+    """Collapse faces smaller than `min_area` (near-cospherical site groups) to a point.
+
+    All vertices of a sliver are merged into their mean, every ring is
+    re-deduplicated, and rings left with fewer than three vertices disappear.
+    Merging keeps every cell a closed, consistently oriented surface (each
+    edge still bounds exactly two faces of the cell), which the reference's
+    Mesh::validate requires (src/core/mesh.cpp:709-756); the reference also
+    rejects faces whose projected area is below 1e-13 (mesh.cpp:89-104).
+    Returns (ids, sizes, vertices, kept-face mask over the input faces).
+    """
+    keep = np.ones(len(sizes), bool)
+    verts = verts.copy()
+    for _ in range(8):
+        area = _face_areas(ids, sizes, verts)
+        small = np.nonzero(area <= min_area)[0]
+        if len(small) == 0:
+            break
+        parent = np.arange(len(verts))
+
+        def find(a):
+            while parent[a] != a:
+                parent[a] = parent[parent[a]]
+                a = parent[a]
+            return a
+        off = np.r_[0, np.cumsum(sizes)]
+        for f in small:
+            ring = ids[off[f]:off[f + 1]]
+            r0 = find(ring[0])
+            for v in ring[1:]:
+                rv = find(v)
+                if rv != r0:
+                    parent[rv] = r0
+        roots = _roots(parent)
+        sums = np.zeros_like(verts)
+        np.add.at(sums, roots, verts)
+        cnt = np.bincount(roots, minlength=len(verts)).astype(float)
+        hit = cnt > 1
+        verts[hit] = sums[hit] / cnt[hit][:, None]   # merged vertex at the mean of its members
+        ids = roots[ids]
+        # de-duplicate consecutive repeats inside rings (and the wrap-around)
+        face_of = np.repeat(np.arange(len(sizes)), sizes)
+        first = np.r_[True, face_of[1:] != face_of[:-1]]
+        dup = np.r_[False, (ids[1:] == ids[:-1]) & ~first[1:]]
+        ids, face_of = ids[~dup], face_of[~dup]
+        sizes = np.bincount(face_of, minlength=len(sizes))
+        off = np.r_[0, np.cumsum(sizes)]
+        lastpos = off[1:] - 1
+        has = sizes > 1
+        wrap = np.zeros(len(ids), bool)
+        wrap[lastpos[has]] = ids[lastpos[has]] == ids[off[:-1][has]]
+        ids, face_of = ids[~wrap], face_of[~wrap]
+        sizes = np.bincount(face_of, minlength=len(sizes))
+        alive = sizes >= 3
+        if not np.all(alive):
+            el = alive[face_of]
+            ids = ids[el]
+            sizes = sizes[alive]
+            idx = np.nonzero(keep)[0]
+            keep[idx[~alive]] = False
+    return ids, sizes, verts, keep
+
+
+def _roots(parent):
+    r = parent.copy()
+    while True:
+        nr = r[r]
+        if np.array_equal(nr, r):
+            return r
+        r = nr
+
+
 def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, kinds=None) -> PolyMesh:
     from scipy.spatial import Delaunay
     h = 1.0 / n
@@ -121,24 +204,8 @@ def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, 
     owner = f_lo.astype(np.int32)
     neighbour = np.where(is_int, f_hi, -1).astype(np.int32)
     patch = np.where(is_int, -1, ppatch[f_hi]).astype(np.int32)
-    # Drop slivers: faces whose area is below max(1e-9 h^2, 1e-12) (near-cospherical
-    # site groups).  Both cells lose the face, so the mesh stays consistent; the
-    # closure error is the sliver's area.  The reference rejects faces whose
-    # projected area is below 1e-13 (src/core/mesh.cpp:89-104).
-    offsets0 = np.r_[0, np.cumsum(sizes)].astype(np.int64)
-    face_of = np.repeat(np.arange(len(sizes)), sizes)
-    p = verts[ids.ravel()]
-    p0 = p[offsets0[:-1]][face_of]
-    nxt = np.r_[np.arange(1, len(p)), 0]
-    nxt[offsets0[1:] - 1] = offsets0[:-1]
-    tri = np.cross(p - p0, p[nxt] - p0)
-    area = 0.5 * np.linalg.norm(np.add.reduceat(tri, offsets0[:-1], axis=0), axis=1)
-    big = area > max(1e-9 * h * h, 1e-12)
-    if not np.all(big):
-        keep_el = big[face_of]
-        ids = ids.ravel()[keep_el]
-        sizes = sizes[big]
-        owner, neighbour, patch = owner[big], neighbour[big], patch[big]
+    ids, sizes, verts, keep = _collapse_slivers(ids.ravel(), sizes, verts, max(1e-9 * h * h, 1e-12))
+    owner, neighbour, patch = owner[keep], neighbour[keep], patch[keep]
     order = np.argsort(patch, kind="stable")            # interior (-1) first, then by patch
     offsets = np.r_[0, np.cumsum(sizes)].astype(np.int64)
     sz = sizes[order]

@@ -174,6 +174,8 @@ def cpu_baseline(seconds_budget=25.0):
     env = dict(os.environ, OMP_NUM_THREADS="1")
     res = subprocess.run([exe, work, out], env=env, capture_output=True, text=True,
                          timeout=max(60.0, 10 * seconds_budget))
+    if not os.path.exists(os.path.join(out, "run.json")):
+        raise RuntimeError(f"reference run failed (exit {res.returncode}): {res.stderr[-300:]}")
     info = json.load(open(os.path.join(out, "run.json")))
     intervals = max(int(info["reported_iteration_intervals"]), 1)
     secs = float(info["iteration_compute_seconds"]) or float(info["solver_seconds"])
