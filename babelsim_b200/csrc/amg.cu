@@ -343,7 +343,10 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
     fine_ = A;
     Level* l0 = levels_[0];
     l0->dptr = A.ptr; l0->dcol = A.col; l0->ddiag = A.diag; l0->dval = A.val;
-    if (!numeric) return;
+    if (!numeric) {
+        uploadViews();
+        return;
+    }
     for (std::size_t l = 0; l + 1 < levels_.size(); ++l) {
         Level* f = levels_[l];
         Level* c = levels_[l + 1];
@@ -361,6 +364,32 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
                                               last->dense.data());
     ctx_.launched();
     BSG_CUDA(cudaGetLastError());
+    uploadViews();
+}
+
+void AmgPreconditioner::uploadViews() {
+    // level views for the persistent solver (level 0 borrows the caller's matrix arrays)
+    std::vector<AmgLevelView<double>> views(levels_.size());
+    for (std::size_t l = 0; l < levels_.size(); ++l) {
+        Level* lv = levels_[l];
+        const bool coarser = l + 1 < levels_.size();
+        views[l] = AmgLevelView<double>{lv->n, lv->dptr, lv->dcol, lv->ddiag, lv->dval, lv->rdiag.data(),
+                                        coarser ? lv->agg.data() : nullptr, coarser ? lv->agg_ptr.data() : nullptr,
+                                        coarser ? lv->agg_rows.data() : nullptr, lv->x.data(), lv->b.data(),
+                                        lv->t.data()};
+    }
+    d_views_.upload(views, ctx_.stream);
+}
+
+AmgView<double> AmgPreconditioner::deviceView() const {
+    AmgView<double> v;
+    v.levels = static_cast<int>(levels_.size());
+    v.nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
+    v.lv = d_views_.data();
+    const Level* last = levels_.back();
+    v.dense_inv = last->dense.data() + last->n;
+    v.dense_ld = 2 * last->n;
+    return v;
 }
 
 void AmgPreconditioner::apply(Context& ctx, const double* r, double* z) {

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "linalg.h"
+#include "pcg_persistent.cuh"
 
 #include <vector>
 
@@ -27,17 +28,29 @@ public:
     void apply(Context& ctx, const double* r, double* z) override;
     int levels() const;
     long long coarseRows(int level) const;
+    // Device-side description of the hierarchy for the persistent PCG kernel
+    // (valid after update()).
+    AmgView<double> deviceView() const;
 
     struct Level;
 
 private:
     void buildStructure(const Dcsr<double>& A);
+    void uploadViews();
     DeviceMesh& mesh_;
     Context& ctx_;
     SolverConfig cfg_;
     std::vector<Level*> levels_;
     bool built_ = false;
     Dcsr<double> fine_{};
+    DeviceArray<AmgLevelView<double>> d_views_;
 };
+
+// Launch the persistent PCG (pcg_persistent.cu); `jac` is the Jacobi diagonal
+// when amg.levels == 0 (nullptr: no preconditioner).
+void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<double>& amg, const double* jac,
+                         const double* b, double* x, double* r, double* z, double* p0, double* p1, double* q,
+                         double* partial, PcgState* st);
+int persistentGrid(Context& ctx);
 
 }  // namespace bsg

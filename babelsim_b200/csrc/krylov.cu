@@ -6,6 +6,7 @@
 // finishing kernel, so an iteration needs no host round trip.  The host only
 // reads a convergence word every `check_interval` iterations; kernels of
 // iterations issued after convergence return immediately.
+#include "amg.h"
 #include "bsg_device.cuh"
 #include "linalg.h"
 
@@ -458,6 +459,7 @@ struct KrylovSolver::Impl {
     Context& ctx;
     DeviceArray<double> r, z, p, q, r0, v, ph, sh, t, partial, tmp;
     DeviceArray<Scalars> sc;
+    DeviceArray<PcgState> pst;
     explicit Impl(Context& c) : ctx(c) { sc.resize(1); }
     int grid(int n) const {
         const long long g = (static_cast<long long>(n) + kBlock - 1) / kBlock;
@@ -531,11 +533,68 @@ inline double residualScale(double initial, double rhs) {
 }
 }  // namespace
 
+SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg,
+                                           const double* jacobi_diag, const double* b, double* x) {
+    Impl& m = *impl_;
+    Context& ctx = m.ctx;
+    const int n = A.n;
+    m.ensure(n);
+    if (m.pst.size() < 1) m.pst.resize(1);
+    const AmgView<double> view = amg ? amg->deviceView() : AmgView<double>{};
+    PcgState h{};
+    h.target2 = -1.0;
+    h.warm = cfg.warm_start ? 1 : 0;
+    h.max_iterations = cfg.max_iterations;
+    h.atol = cfg.atol;
+    h.rtol = cfg.rtol;
+    SolveOutcome out;
+    double scale = 1.0, target = 0.0, fin = 0.0;
+    int used = 0;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        BSG_CUDA(cudaMemcpyAsync(m.pst.data(), &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
+        launchPersistentPcg(ctx, A, view, jacobi_diag, b, x, m.r.data(), m.z.data(), m.p.data(), m.v.data(),
+                            m.q.data(), m.partial.data(), m.pst.data());
+        BSG_CUDA(cudaMemcpyAsync(ctx.pinned, m.pst.data(), sizeof(PcgState), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        PcgState r;
+        std::memcpy(&r, ctx.pinned, sizeof(r));
+        if (attempt == 0) {
+            out.initial = std::sqrt(r.rr0);
+            scale = residualScale(std::sqrt(r.rr0), std::sqrt(r.bb));
+            target = std::max(cfg.atol, cfg.rtol * scale);
+            if (r.iterations == 0 && r.status == 0) {
+                // r0 already meets the target (petsc_linear_system.cpp:386-398)
+                out.status = 0;
+                out.final_ = out.initial;
+                out.relative = out.initial / scale;
+                return out;
+            }
+        }
+        used += r.iterations;
+        fin = trueResidualNorm(ctx, A, b, x, m.r.data());
+        if (!std::isfinite(fin) || fin <= target || r.status == 2 || used >= cfg.max_iterations) break;
+        // true-residual restart from this x with a halved internal target (petsc_linear_system.cpp:412-439)
+        h.target2 = 0.25 * r.target2;
+        h.warm = 1;
+        h.max_iterations = cfg.max_iterations - used;
+    }
+    out.iterations = used;
+    out.final_ = fin;
+    out.relative = fin / scale;
+    out.status = (std::isfinite(fin) && fin <= target) ? 0 : (std::isfinite(fin) ? 1 : 2);
+    return out;
+}
+
 SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc,
                                        const double* b, double* x) {
     Impl& m = *impl_;
     Context& ctx = m.ctx;
     const int n = A.n;
+    if (persistent && cfg.solver == 0) {
+        auto* amg = dynamic_cast<AmgPreconditioner*>(pc);
+        auto* jac = dynamic_cast<JacobiPreconditioner*>(pc);
+        if (amg || jac || !pc) return solvePersistent(A, cfg, amg, jac ? jac->diag : nullptr, b, x);
+    }
     m.ensure(n);
     const int g = m.grid(n);
     SolveOutcome out;

@@ -40,7 +40,7 @@ struct SolveOutcome {
     double initial = 0.0, final_ = 0.0, relative = 0.0;
 };
 
-class AmgHierarchy;
+class AmgPreconditioner;
 
 // Preconditioner application z = M^-1 r for a single right-hand side.
 struct Preconditioner {
@@ -64,8 +64,13 @@ public:
     void solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                       SolveOutcome out[3]);
     int check_interval = 8;  // iterations between host convergence checks
+    // CG with AMG, Jacobi or no preconditioner runs as one persistent cooperative
+    // kernel per attempt (pcg_persistent.cu); set false to use per-kernel launches.
+    bool persistent = true;
 
 private:
+    SolveOutcome solvePersistent(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg,
+                                 const double* jacobi_diag, const double* b, double* x);
     struct Impl;
     std::unique_ptr<Impl> impl_;
 };

@@ -1,0 +1,348 @@
+// Persistent cooperative PCG + AMG V-cycle (see pcg_persistent.cuh).
+#include <cooperative_groups.h>
+
+#include "linalg.h"
+#include "pcg_persistent.cuh"
+
+#include <cmath>
+#include <cstring>
+
+namespace cg = cooperative_groups;
+
+namespace bsg {
+namespace {
+
+constexpr int PB = 256;   // threads per block
+constexpr int LPR = 4;    // lanes per row
+constexpr int NVMAX = 2;  // values per grid reduction
+
+struct Cursor {
+    int group, ngroups, lane;
+    unsigned mask;
+};
+
+__device__ __forceinline__ Cursor cursor() {
+    Cursor c;
+    const int gt = blockIdx.x * PB + threadIdx.x;
+    c.group = gt / LPR;
+    c.ngroups = gridDim.x * PB / LPR;
+    c.lane = threadIdx.x & (LPR - 1);
+    c.mask = 0xFu << (threadIdx.x & 28);
+    return c;
+}
+
+__device__ __forceinline__ double groupSum(double v, unsigned mask) {
+    v += __shfl_xor_sync(mask, v, 1);
+    v += __shfl_xor_sync(mask, v, 2);
+    return v;
+}
+
+// Deterministic grid reduction of NV values; every block returns the same totals.
+// `buf` alternates between two halves of `partial` so a fast block's next write
+// never overtakes a slow block's read.
+template <int NV>
+__device__ void gridReduce(cg::grid_group& g, double v[NV], double* partial, int& buf) {
+    __shared__ double sh[NVMAX][PB / 32];
+    __shared__ double tot[NVMAX];
+    double* part = partial + static_cast<long long>(buf) * gridDim.x * NVMAX;
+    buf ^= 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = v[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[j][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double s = 0.0;
+            for (int w = 0; w < PB / 32; ++w) s += sh[j][w];
+            part[blockIdx.x * NVMAX + j] = s;
+        }
+    }
+    g.sync();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += PB) x += part[b * NVMAX + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[j][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double s = 0.0;
+            for (int w = 0; w < PB / 32; ++w) s += sh[j][w];
+            tot[j] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = tot[j];
+    __syncthreads();
+}
+
+// (A y)_row for one row by a 4-lane group, y given by a functor of the column.
+template <class Y>
+__device__ __forceinline__ double rowApply(const int* __restrict__ ptr, const int* __restrict__ col,
+                                           const double* __restrict__ val, int row, const Cursor& c, Y y) {
+    double s = 0.0;
+    const int e = ptr[row + 1];
+    for (int k = ptr[row] + c.lane; k < e; k += LPR) s += val[k] * y(col[k]);
+    return groupSum(s, c.mask);
+}
+
+// One V-cycle: z = M r.  Returns this thread's partial of r.z (lane 0 of each row group).
+__device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const double* __restrict__ r,
+                         double* __restrict__ z) {
+    const Cursor c = cursor();
+    const int L = a.levels;
+    // ---- down: smoothing from a zero guess, then residual + aggregate restriction
+    for (int l = 0; l < L - 1; ++l) {
+        const AmgLevelView<double> f = a.lv[l];
+        const double* b = l == 0 ? r : f.b;
+        for (int i = c.group; i < f.n; i += c.ngroups) {
+            double xi;
+            if (a.nu <= 1) {
+                xi = f.rd[i] * b[i];
+            } else {
+                // two damped-Jacobi sweeps from x = 0 in one pass: x1 = rd.b is formed on the fly
+                const double x1i = f.rd[i] * b[i];
+                const double ax = rowApply(f.ptr, f.col, f.val, i, c, [&](int j) { return f.rd[j] * b[j]; });
+                xi = x1i + f.rd[i] * (b[i] - (f.diag[i] * x1i + ax));
+            }
+            if (c.lane == 0) f.x[i] = xi;
+        }
+        g.sync();
+        const AmgLevelView<double> cl = a.lv[l + 1];
+        for (int I = c.group; I < cl.n; I += c.ngroups) {
+            double s = 0.0;
+            for (int m = f.agg_ptr[I] + c.lane; m < f.agg_ptr[I + 1]; m += LPR) {
+                const int i = f.agg_rows[m];
+                double ax = f.diag[i] * f.x[i];
+                for (int k = f.ptr[i]; k < f.ptr[i + 1]; ++k) ax += f.val[k] * f.x[f.col[k]];
+                s += b[i] - ax;
+            }
+            s = groupSum(s, c.mask);
+            if (c.lane == 0) cl.b[I] = s;
+        }
+        g.sync();
+    }
+    // ---- coarsest: dense inverse times the right-hand side
+    {
+        const AmgLevelView<double> cl = a.lv[L - 1];
+        const double* b = L == 1 ? r : cl.b;
+        double* x = L == 1 ? z : cl.x;
+        for (int i = c.group; i < cl.n; i += c.ngroups) {
+            double s = 0.0;
+            const double* row = a.dense_inv + static_cast<long long>(i) * a.dense_ld;
+            for (int j = c.lane; j < cl.n; j += LPR) s += row[j] * b[j];
+            s = groupSum(s, c.mask);
+            if (c.lane == 0) x[i] = s;
+        }
+        g.sync();
+    }
+    // ---- up: prolongation fused into the first post-smoothing sweep
+    double rz = 0.0;
+    for (int l = L - 2; l >= 0; --l) {
+        const AmgLevelView<double> f = a.lv[l];
+        const double* xc = a.lv[l + 1].x;
+        const double* b = l == 0 ? r : f.b;
+        const bool last = a.nu <= 1;
+        double* out = last ? (l == 0 ? z : f.t) : f.t;
+        for (int i = c.group; i < f.n; i += c.ngroups) {
+            const double yi = f.x[i] + xc[f.agg[i]];
+            const double ay = rowApply(f.ptr, f.col, f.val, i, c, [&](int j) { return f.x[j] + xc[f.agg[j]]; });
+            const double v = yi + f.rd[i] * (b[i] - (f.diag[i] * yi + ay));
+            if (c.lane == 0) {
+                out[i] = v;
+                if (last && l == 0) rz += r[i] * v;
+            }
+        }
+        g.sync();
+        if (!last) {
+            double* fin = l == 0 ? z : f.x;
+            for (int i = c.group; i < f.n; i += c.ngroups) {
+                const double ti = f.t[i];
+                const double at = rowApply(f.ptr, f.col, f.val, i, c, [&](int j) { return f.t[j]; });
+                const double v = ti + f.rd[i] * (b[i] - (f.diag[i] * ti + at));
+                if (c.lane == 0) {
+                    fin[i] = v;
+                    if (l == 0) rz += r[i] * v;
+                }
+            }
+            if (l > 0) g.sync();
+        } else if (l > 0) {
+            // the iterate of this level lives in t; copy back so the next finer level reads x
+            for (int i = c.group * LPR + c.lane; i < f.n; i += c.ngroups * LPR) f.x[i] = f.t[i];
+            g.sync();
+        }
+    }
+    if (L == 1) {
+        // z was written by the dense solve
+        for (int i = c.group; i < a.lv[0].n; i += c.ngroups)
+            if (c.lane == 0) rz += r[i] * z[i];
+    }
+    return rz;
+}
+
+struct PcgArgs {
+    Dcsr<double> A;
+    AmgView<double> amg;        // levels == 0: Jacobi on the diagonal `jac`, or none when jac == nullptr
+    const double* jac;
+    const double* b;
+    double* x;
+    double* r;
+    double* z;
+    double* p0;
+    double* p1;
+    double* q;
+    double* partial;
+    PcgState* st;
+};
+
+// z = M r and the partial of r.z
+__device__ double precondition(cg::grid_group& g, const PcgArgs& a) {
+    if (a.amg.levels > 0) return vcycle(g, a.amg, a.r, a.z);
+    const Cursor c = cursor();
+    double rz = 0.0;
+    for (int i = c.group * LPR + c.lane; i < a.A.n; i += c.ngroups * LPR) {
+        const double zi = a.jac ? a.r[i] / a.jac[i] : a.r[i];
+        a.z[i] = zi;
+        rz += a.r[i] * zi;
+    }
+    return rz;
+}
+
+__global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
+    cg::grid_group g = cg::this_grid();
+    const Cursor c = cursor();
+    const int n = a.A.n;
+    int buf = 0;
+    PcgState& st = *a.st;
+    // inputs are read before block 0 writes any result into the same struct
+    const int warm = st.warm;
+    const int max_iterations = st.max_iterations;
+    const double target2_in = st.target2, atol = st.atol, rtol = st.rtol;
+    // r = b - A x (x = 0 unless warm), with ||r0||^2 and ||b||^2
+    double v[2] = {0.0, 0.0};
+    for (int i = c.group; i < n; i += c.ngroups) {
+        double ri;
+        if (warm) {
+            const double ax = rowApply(a.A.ptr, a.A.col, a.A.val, i, c, [&](int j) { return a.x[j]; });
+            ri = a.b[i] - (a.A.diag[i] * a.x[i] + ax);
+        } else {
+            ri = a.b[i];
+        }
+        if (c.lane == 0) {
+            if (!warm) a.x[i] = 0.0;
+            a.r[i] = ri;
+            v[0] += ri * ri;
+            v[1] += a.b[i] * a.b[i];
+        }
+    }
+    gridReduce<2>(g, v, a.partial, buf);
+    double target2 = target2_in;
+    if (target2 < 0.0) {
+        // the reference's contract: max(atol, rtol * max(||r0||, ||b||)) (solver_control.h:199-210)
+        double scale = fmax(sqrt(v[0]), sqrt(v[1]));
+        if (!(scale > 0.0)) scale = 1.0;
+        const double t = fmax(atol, rtol * scale);
+        target2 = t * t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st.rr0 = v[0];
+        st.bb = v[1];
+        st.target2 = target2;
+        st.rr = v[0];
+        st.iterations = 0;
+        st.status = 1;
+    }
+    if (isfinite(v[0]) && v[0] <= target2) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st.status = 0;
+        return;
+    }
+    double w[1] = {precondition(g, a)};
+    gridReduce<1>(g, w, a.partial, buf);
+    double rz = w[0];
+    double beta = 0.0;
+    double* pold = a.p0;
+    double* pnew = a.p1;
+    int it = 0;
+    int status = 1;
+    double rr = v[0];
+    while (it < max_iterations) {
+        if (!isfinite(rz) || rz == 0.0) { status = 2; break; }
+        // p_new = z + beta p_old and q = A p_new in one pass (neighbours' p_new formed on the fly)
+        double pq[1] = {0.0};
+        for (int i = c.group; i < n; i += c.ngroups) {
+            const double pi = beta == 0.0 ? a.z[i] : a.z[i] + beta * pold[i];
+            const double ap = rowApply(a.A.ptr, a.A.col, a.A.val, i, c, [&](int j) {
+                return beta == 0.0 ? a.z[j] : a.z[j] + beta * pold[j];
+            });
+            const double qi = a.A.diag[i] * pi + ap;
+            if (c.lane == 0) {
+                pnew[i] = pi;
+                a.q[i] = qi;
+                pq[0] += pi * qi;
+            }
+        }
+        gridReduce<1>(g, pq, a.partial, buf);
+        if (!(fabs(pq[0]) > 0.0) || !isfinite(pq[0])) { status = 2; break; }
+        const double alpha = rz / pq[0];
+        double nr[1] = {0.0};
+        for (int i = c.group * LPR + c.lane; i < n; i += c.ngroups * LPR) {
+            a.x[i] += alpha * pnew[i];
+            const double ri = a.r[i] - alpha * a.q[i];
+            a.r[i] = ri;
+            nr[0] += ri * ri;
+        }
+        gridReduce<1>(g, nr, a.partial, buf);
+        rr = nr[0];
+        ++it;
+        if (!isfinite(rr)) { status = 2; break; }
+        if (rr <= target2) { status = 0; break; }
+        if (it >= max_iterations) break;
+        double zr[1] = {precondition(g, a)};
+        gridReduce<1>(g, zr, a.partial, buf);
+        beta = zr[0] / rz;
+        rz = zr[0];
+        double* tmp = pold;
+        pold = pnew;
+        pnew = tmp;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st.rr = rr;
+        st.iterations = it;
+        st.status = status;
+    }
+}
+
+}  // namespace
+
+int persistentGrid(Context& ctx) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kPcgPersistent, PB, 0));
+        if (per_sm <= 0) fail(kCuda, "persistent PCG kernel cannot be resident");
+    }
+    return ctx.sm_count * std::min(per_sm, 4);
+}
+
+void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<double>& amg, const double* jac,
+                         const double* b, double* x, double* r, double* z, double* p0, double* p1, double* q,
+                         double* partial, PcgState* st) {
+    PcgArgs args{A, amg, jac, b, x, r, z, p0, p1, q, partial, st};
+    void* params[] = {&args};
+    const int grid = persistentGrid(ctx);
+    BSG_PROFILE(ctx, "pcg_amg_persistent");
+    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgPersistent), grid, PB, params, 0, ctx.stream));
+    ctx.launched();
+}
+
+}  // namespace bsg
