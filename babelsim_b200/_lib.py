@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libbabelsim_b200.so")
 # Entry points declared in include/babelsim_b200.h, in declaration order.
 EXPORTS = [
     "bsg_context_create", "bsg_context_destroy", "bsg_last_error", "bsg_global_error", "bsg_context_launches",
-    "bsg_context_synchronize", "bsg_context_profile", "bsg_context_profile_report", "bsg_context_event_record",
+    "bsg_context_synchronize", "bsg_context_profile", "bsg_context_profile_report", "bsg_context_phase_log",
+    "bsg_context_phase_log_read", "bsg_context_event_record",
     "bsg_context_event_elapsed", "bsg_mesh_create", "bsg_mesh_create_polyhedral", "bsg_mesh_destroy",
     "bsg_mesh_validate_polyhedral",
     "bsg_mesh_sizes", "bsg_mesh_export", "bsg_field_create", "bsg_field_destroy", "bsg_field_set_boundary",
@@ -95,6 +96,7 @@ def lib():
             "bsg_context_create": [i32, pp], "bsg_context_destroy": [vp], "bsg_last_error": [vp],
             "bsg_global_error": [], "bsg_context_launches": [vp, C.POINTER(i64)], "bsg_context_synchronize": [vp],
             "bsg_context_profile": [vp, i32], "bsg_context_profile_report": [vp, C.c_char_p, i32],
+            "bsg_context_phase_log": [vp, i32], "bsg_context_phase_log_read": [vp, vp, i32, C.POINTER(i32)],
             "bsg_context_event_record": [vp, i32], "bsg_context_event_elapsed": [vp, i32, i32, C.POINTER(dbl)],
             "bsg_simple_load_state": [vp, vp, vp, vp],
             "bsg_mesh_create": [vp, C.POINTER(MeshGeometry), pp],

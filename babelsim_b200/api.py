@@ -58,6 +58,17 @@ class Context:
         check(lib().bsg_context_profile_report(self.h, buf, len(buf)), self.h)
         return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
 
+    def phase_log(self, capacity: int):
+        """Enable (capacity > 0) or disable the persistent-kernel phase timeline."""
+        check(lib().bsg_context_phase_log(self.h, capacity), self.h)
+
+    def phase_log_read(self, capacity: int = 1 << 20):
+        """[(phase id, ns)] recorded since the last read (device globaltimer)."""
+        buf = np.zeros(2 * capacity, np.int64)
+        n = C.c_int32()
+        check(lib().bsg_context_phase_log_read(self.h, ptr(buf), capacity, C.byref(n)), self.h)
+        return buf[:2 * n.value].reshape(-1, 2)
+
     def record(self, slot: int):
         check(lib().bsg_context_event_record(self.h, slot), self.h)
 

@@ -100,9 +100,9 @@ HostCsr coarsen(const HostCsr& a, const std::vector<int>& agg, int nc, std::vect
     return c;
 }
 
-__global__ void kRdiag(int n, const double* __restrict__ d, double* __restrict__ rd) {
+__global__ void kRdiag(int n, double omega, const double* __restrict__ d, double* __restrict__ rd) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) rd[i] = kOmega / d[i];
+    if (i < n) rd[i] = omega / d[i];
 }
 
 // Coarse Galerkin values: fixed-order gathers over precomputed fine contributions.
@@ -228,7 +228,13 @@ __global__ void kCopy(int n, const double* __restrict__ a, double* __restrict__ 
 }  // namespace
 
 AmgPreconditioner::AmgPreconditioner(DeviceMesh& mesh, const SolverConfig& cfg)
-    : mesh_(mesh), ctx_(*mesh.ctx), cfg_(cfg) {}
+    : mesh_(mesh), ctx_(*mesh.ctx), cfg_(cfg) {
+    // Tuning overrides for experiments: Jacobi weight and coarse-correction scale.
+    if (const char* w = std::getenv("BSG_AMG_OMEGA")) omega_ = std::atof(w);
+    if (const char* g = std::getenv("BSG_AMG_GAMMA")) gamma_ = std::atof(g);
+    if (!(omega_ > 0.0 && omega_ <= 1.0) || !(gamma_ > 0.0 && gamma_ <= 3.0))
+        fail(kArgument, "AMG Jacobi weight must be in (0,1] and the correction scale in (0,3]");
+}
 
 AmgPreconditioner::~AmgPreconditioner() {
     for (Level* l : levels_) delete l;
@@ -356,7 +362,7 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
         ctx_.launched();
     }
     for (Level* l : levels_) {
-        kRdiag<<<gridFor(l->n, kBlock), kBlock, 0, ctx_.stream>>>(l->n, l->ddiag, l->rdiag.data());
+        kRdiag<<<gridFor(l->n, kBlock), kBlock, 0, ctx_.stream>>>(l->n, omega_, l->ddiag, l->rdiag.data());
         ctx_.launched();
     }
     Level* last = levels_.back();
@@ -385,6 +391,7 @@ AmgView<double> AmgPreconditioner::deviceView() const {
     AmgView<double> v;
     v.levels = static_cast<int>(levels_.size());
     v.nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
+    v.gamma = gamma_;
     v.lv = d_views_.data();
     const Level* last = levels_.back();
     v.dense_inv = last->dense.data() + last->n;

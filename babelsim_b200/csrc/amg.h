@@ -44,6 +44,8 @@ private:
     bool built_ = false;
     Dcsr<double> fine_{};
     DeviceArray<AmgLevelView<double>> d_views_;
+    double omega_ = 2.0 / 3.0;  // damped-Jacobi weight
+    double gamma_ = 1.0;        // coarse-correction scale
 };
 
 // Launch the persistent PCG (pcg_persistent.cu); `jac` is the Jacobi diagonal

@@ -109,6 +109,10 @@ struct Context {
     std::vector<Record> records;
     std::vector<cudaEvent_t> event_pool;
     std::vector<cudaEvent_t> user_events;  // bsg_context_event_record slots
+    // Phase timeline of persistent kernels (device memory, enabled on request).
+    long long* phase_entries = nullptr;
+    int* phase_count = nullptr;
+    int phase_capacity = 0;
     explicit Context(int dev);
     ~Context();
     void sync() { BSG_CUDA(cudaStreamSynchronize(stream)); }

@@ -57,6 +57,8 @@ Context::~Context() {
     for (auto& r : records) { event_pool.push_back(r.start); event_pool.push_back(r.stop); }
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : user_events) if (e) cudaEventDestroy(e);
+    if (phase_entries) cudaFree(phase_entries);
+    if (phase_count) cudaFree(phase_count);
     if (pinned) cudaFreeHost(pinned);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -254,6 +256,38 @@ int bsg_context_profile_report(bsg_context* ctx, char* buffer, int32_t capacity)
         const std::string r = ctx->ctx->profileReport();
         if (static_cast<int32_t>(r.size()) >= capacity) bsg::fail(bsg::kArgument, "profile report buffer too small");
         std::memcpy(buffer, r.c_str(), r.size() + 1);
+    });
+}
+
+int bsg_context_phase_log(bsg_context* ctx, int32_t capacity) {
+    return guard(ctx, [&] {
+        require(ctx && capacity >= 0, "bad argument");
+        bsg::Context& c = *ctx->ctx;
+        c.sync();
+        if (c.phase_entries) { cudaFree(c.phase_entries); c.phase_entries = nullptr; }
+        if (c.phase_count) { cudaFree(c.phase_count); c.phase_count = nullptr; }
+        c.phase_capacity = 0;
+        if (capacity > 0) {
+            BSG_CUDA(cudaMalloc(&c.phase_entries, sizeof(long long) * 2 * static_cast<std::size_t>(capacity)));
+            BSG_CUDA(cudaMalloc(&c.phase_count, sizeof(int)));
+            BSG_CUDA(cudaMemset(c.phase_count, 0, sizeof(int)));
+            c.phase_capacity = capacity;
+        }
+    });
+}
+
+int bsg_context_phase_log_read(bsg_context* ctx, int64_t* pairs, int32_t capacity, int32_t* count) {
+    return guard(ctx, [&] {
+        require(ctx && pairs && count, "null argument");
+        bsg::Context& c = *ctx->ctx;
+        require(c.phase_capacity > 0, "phase log is not enabled");
+        c.sync();
+        int n = 0;
+        BSG_CUDA(cudaMemcpy(&n, c.phase_count, sizeof(int), cudaMemcpyDeviceToHost));
+        n = std::min(n, std::min(capacity, c.phase_capacity));
+        if (n) BSG_CUDA(cudaMemcpy(pairs, c.phase_entries, sizeof(long long) * 2 * n, cudaMemcpyDeviceToHost));
+        BSG_CUDA(cudaMemset(c.phase_count, 0, sizeof(int)));
+        *count = n;
     });
 }
 

@@ -87,6 +87,20 @@ __device__ void gridReduce(cg::grid_group& g, double v[NV], double* partial, int
     __syncthreads();
 }
 
+// Appends (id, globaltimer) to the phase log; called by every thread right after a barrier.
+__device__ __forceinline__ void mark(const PhaseLog& log, int id) {
+    if (log.entries && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int k = *log.count;
+        if (k < log.capacity) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            log.entries[2 * k] = id;
+            log.entries[2 * k + 1] = static_cast<long long>(t);
+            *log.count = k + 1;
+        }
+    }
+}
+
 // (A y)_row for one row by a 4-lane group, y given by a functor of the column.
 template <class Y>
 __device__ __forceinline__ double rowApply(const int* __restrict__ ptr, const int* __restrict__ col,
@@ -99,9 +113,10 @@ __device__ __forceinline__ double rowApply(const int* __restrict__ ptr, const in
 
 // One V-cycle: z = M r.  Returns this thread's partial of r.z (lane 0 of each row group).
 __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const double* __restrict__ r,
-                         double* __restrict__ z) {
+                         double* __restrict__ z, const PhaseLog& log) {
     const Cursor c = cursor();
     const int L = a.levels;
+    const double gamma = a.gamma;
     // ---- down: smoothing from a zero guess, then residual + aggregate restriction
     for (int l = 0; l < L - 1; ++l) {
         const AmgLevelView<double> f = a.lv[l];
@@ -119,6 +134,7 @@ __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const doub
             if (c.lane == 0) f.x[i] = xi;
         }
         g.sync();
+        mark(log, 10 + l);
         const AmgLevelView<double> cl = a.lv[l + 1];
         for (int I = c.group; I < cl.n; I += c.ngroups) {
             double s = 0.0;
@@ -132,6 +148,7 @@ __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const doub
             if (c.lane == 0) cl.b[I] = s;
         }
         g.sync();
+        mark(log, 30 + l);
     }
     // ---- coarsest: dense inverse times the right-hand side
     {
@@ -146,6 +163,7 @@ __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const doub
             if (c.lane == 0) x[i] = s;
         }
         g.sync();
+        mark(log, 50);
     }
     // ---- up: prolongation fused into the first post-smoothing sweep
     double rz = 0.0;
@@ -156,8 +174,9 @@ __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const doub
         const bool last = a.nu <= 1;
         double* out = last ? (l == 0 ? z : f.t) : f.t;
         for (int i = c.group; i < f.n; i += c.ngroups) {
-            const double yi = f.x[i] + xc[f.agg[i]];
-            const double ay = rowApply(f.ptr, f.col, f.val, i, c, [&](int j) { return f.x[j] + xc[f.agg[j]]; });
+            const double yi = f.x[i] + gamma * xc[f.agg[i]];
+            const double ay =
+                rowApply(f.ptr, f.col, f.val, i, c, [&](int j) { return f.x[j] + gamma * xc[f.agg[j]]; });
             const double v = yi + f.rd[i] * (b[i] - (f.diag[i] * yi + ay));
             if (c.lane == 0) {
                 out[i] = v;
@@ -165,6 +184,7 @@ __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const doub
             }
         }
         g.sync();
+        mark(log, 60 + l);
         if (!last) {
             double* fin = l == 0 ? z : f.x;
             for (int i = c.group; i < f.n; i += c.ngroups) {
@@ -176,7 +196,10 @@ __device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const doub
                     if (l == 0) rz += r[i] * v;
                 }
             }
-            if (l > 0) g.sync();
+            if (l > 0) {
+                g.sync();
+                mark(log, 80 + l);
+            }
         } else if (l > 0) {
             // the iterate of this level lives in t; copy back so the next finer level reads x
             for (int i = c.group * LPR + c.lane; i < f.n; i += c.ngroups * LPR) f.x[i] = f.t[i];
@@ -204,11 +227,12 @@ struct PcgArgs {
     double* q;
     double* partial;
     PcgState* st;
+    PhaseLog log;
 };
 
 // z = M r and the partial of r.z
 __device__ double precondition(cg::grid_group& g, const PcgArgs& a) {
-    if (a.amg.levels > 0) return vcycle(g, a.amg, a.r, a.z);
+    if (a.amg.levels > 0) return vcycle(g, a.amg, a.r, a.z, a.log);
     const Cursor c = cursor();
     double rz = 0.0;
     for (int i = c.group * LPR + c.lane; i < a.A.n; i += c.ngroups * LPR) {
@@ -247,6 +271,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
         }
     }
     gridReduce<2>(g, v, a.partial, buf);
+    mark(a.log, 1);
     double target2 = target2_in;
     if (target2 < 0.0) {
         // the reference's contract: max(atol, rtol * max(||r0||, ||b||)) (solver_control.h:199-210)
@@ -293,6 +318,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
             }
         }
         gridReduce<1>(g, pq, a.partial, buf);
+        mark(a.log, 2);
         if (!(fabs(pq[0]) > 0.0) || !isfinite(pq[0])) { status = 2; break; }
         const double alpha = rz / pq[0];
         double nr[1] = {0.0};
@@ -303,6 +329,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
             nr[0] += ri * ri;
         }
         gridReduce<1>(g, nr, a.partial, buf);
+        mark(a.log, 3);
         rr = nr[0];
         ++it;
         if (!isfinite(rr)) { status = 2; break; }
@@ -310,6 +337,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
         if (it >= max_iterations) break;
         double zr[1] = {precondition(g, a)};
         gridReduce<1>(g, zr, a.partial, buf);
+        mark(a.log, 4);
         beta = zr[0] / rz;
         rz = zr[0];
         double* tmp = pold;
@@ -337,7 +365,8 @@ int persistentGrid(Context& ctx) {
 void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<double>& amg, const double* jac,
                          const double* b, double* x, double* r, double* z, double* p0, double* p1, double* q,
                          double* partial, PcgState* st) {
-    PcgArgs args{A, amg, jac, b, x, r, z, p0, p1, q, partial, st};
+    const PhaseLog log{ctx.phase_entries, ctx.phase_capacity, ctx.phase_count};
+    PcgArgs args{A, amg, jac, b, x, r, z, p0, p1, q, partial, st, log};
     void* params[] = {&args};
     const int grid = persistentGrid(ctx);
     BSG_PROFILE(ctx, "pcg_amg_persistent");

@@ -40,6 +40,15 @@ struct AmgView {
     const AmgLevelView<T>* lv = nullptr;  // device array of `levels` views
     const T* dense_inv = nullptr;         // coarsest inverse, row i at dense_inv + i*dense_ld
     int dense_ld = 0;
+    double gamma = 1.0;                   // coarse-correction scale: x += gamma * P x_c
+};
+
+// Optional phase timeline of a persistent solve: block 0 / thread 0 appends
+// (phase id, %globaltimer ns) after every grid barrier, up to `capacity` entries.
+struct PhaseLog {
+    long long* entries = nullptr;  // 2 * capacity
+    int capacity = 0;
+    int* count = nullptr;
 };
 
 // Scalars of one persistent solve (host-visible results at the end).

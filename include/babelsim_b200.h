@@ -142,6 +142,14 @@ int bsg_context_synchronize(bsg_context* ctx);
  * {"kernel": [launches, total_ms], ...} and clears the records. */
 int bsg_context_profile(bsg_context* ctx, int32_t enable);
 int bsg_context_profile_report(bsg_context* ctx, char* buffer, int32_t capacity);
+/* Phase timeline of the persistent solver kernels: with capacity > 0, each grid
+ * barrier appends (phase id, device nanoseconds) until `capacity` entries;
+ * capacity 0 turns it off.  Reading returns the entries and clears the log.
+ * Phase ids: 1 initial residual, 2 SpMV+dot, 3 update+norm, 4 r.z, 10+l
+ * pre-smoothing of level l, 30+l restriction from level l, 50 coarsest solve,
+ * 60+l prolongation + first post sweep, 80+l second post sweep. */
+int bsg_context_phase_log(bsg_context* ctx, int32_t capacity);
+int bsg_context_phase_log_read(bsg_context* ctx, int64_t* pairs, int32_t capacity, int32_t* count);
 /* CUDA events on the context's stream, for timing a region of calls:
  * record into numbered slots, then read the elapsed milliseconds between two. */
 int bsg_context_event_record(bsg_context* ctx, int32_t slot);
