@@ -26,7 +26,8 @@ EXPORTS = [
     "bsg_math_interpolate", "bsg_math_flux", "bsg_math_div_flux", "bsg_math_normal_gradient",
     "bsg_equation_create", "bsg_equation_destroy", "bsg_equ_reset", "bsg_equ_div", "bsg_equ_laplacian",
     "bsg_equ_source", "bsg_equ_relax", "bsg_equ_scale", "bsg_equ_reference_if_unanchored", "bsg_equ_face_flux",
-    "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_simple_create",
+    "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_pcg_jacobi_static",
+    "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
     "bsg_simple_iterate", "bsg_simple_get_fields",
     "bsg_simple_destroy",
@@ -118,6 +119,7 @@ def lib():
             "bsg_equ_solve": [vp, C.POINTER(SolverConfig), C.POINTER(SolveResult)],
             "bsg_equ_download": [vp, vp, vp, vp, vp],
             "bsg_solve_ldu": [vp, C.POINTER(SolverConfig), i32, vp, vp, vp, vp, vp, C.POINTER(SolveResult)],
+            "bsg_pcg_jacobi_static": [i32, vp, vp, vp, vp, vp, vp, dbl, dbl, i32, C.POINTER(SolveResult)],
             "bsg_simple_create": [vp, C.POINTER(SimpleConfig), pp],
             "bsg_simple_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_simple_set_fields": [vp, vp, vp],
             "bsg_simple_set_flux": [vp, vp],

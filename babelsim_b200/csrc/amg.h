@@ -55,4 +55,9 @@ void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<doub
                          double* partial, PcgState* st);
 int persistentGrid(Context& ctx);
 
+// Jacobi PCG on caller-provided device arrays with the library's file-scope
+// static scratch: allocates nothing (pcg_persistent.cu).
+SolveOutcome staticJacobiPcg(int n, const int* row_ptr, const int* cols, const double* diag, const double* vals,
+                             const double* b, double* x, double atol, double rtol, int max_iterations);
+
 }  // namespace bsg

@@ -686,6 +686,17 @@ int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t compo
     });
 }
 
+int bsg_pcg_jacobi_static(int32_t n, const int32_t* row_ptr, const int32_t* cols, const double* diag,
+                          const double* vals, const double* b, double* x, double absolute_tolerance,
+                          double relative_tolerance, int32_t max_iterations, bsg_solve_result* result) {
+    return guard(nullptr, [&] {
+        require(result != nullptr, "null result");
+        const bsg::SolveOutcome o = bsg::staticJacobiPcg(n, row_ptr, cols, diag, vals, b, x, absolute_tolerance,
+                                                          relative_tolerance, max_iterations);
+        toResult(o, result);
+    });
+}
+
 int bsg_simple_create(bsg_mesh* mesh, const bsg_simple_config* c, bsg_simple** out) {
     return guard(ctxOf(mesh), [&] {
         require(mesh && c && out, "null argument");

@@ -4,8 +4,11 @@
 #include "linalg.h"
 #include "pcg_persistent.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 namespace cg = cooperative_groups;
 
@@ -360,6 +363,133 @@ int persistentGrid(Context& ctx) {
         if (per_sm <= 0) fail(kCuda, "persistent PCG kernel cannot be resident");
     }
     return ctx.sm_count * std::min(per_sm, 4);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (bsg_pcg_jacobi_static in include/babelsim_b200.h).
+//
+// Some callers cannot allocate device memory once they are running: solvers
+// embedded in an application that owns a fixed device-memory budget or pool,
+// real-time loops that must not pay cudaMalloc's implicit device
+// synchronisation, or hosts whose allocation calls are forbidden after start-up.
+// For them this variant of the persistent PCG (Jacobi preconditioner) keeps its
+// scratch in the file-scope arrays below, which every GPU that loads the
+// library holds until the process exits (about 5.4 MB).  The caller passes the
+// matrix, right-hand side and solution in its own device memory.
+//
+// Host code must not hand the symbol itself to a kernel: in host code it is a
+// host-side stand-in, not a device address.  The device address is looked up
+// once per device, with that device current, by cudaGetSymbolAddress; the first
+// call on a device does that set-up, so make the first call before any stream
+// capture.  Nothing in the scratch has to start at zero: the solver state is
+// written from the host before every launch, and each launch writes every
+// vector entry and reduction partial before it reads it (x is zeroed by the
+// kernel for the zero initial guess).  Every call shares the same scratch and
+// it keeps the last call's contents, so calls that overlap on the GPU race:
+// issue them one at a time.
+constexpr int kStaticMaxRows = 131072;
+constexpr int kStaticMaxBlocks = 4096;
+static __device__ __align__(256) double g_static_scratch[5 * kStaticMaxRows + 2 * NVMAX * kStaticMaxBlocks];
+static __device__ __align__(256) PcgState g_static_state;
+
+namespace {
+struct StaticScratch {
+    double* base = nullptr;
+    PcgState* state = nullptr;
+};
+StaticScratch g_static_by_device[64];
+std::mutex g_static_mutex;
+
+StaticScratch staticScratch() {
+    int dev = 0;
+    checkCuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) fail(kArgument, "device index out of range for the static scratch table");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    StaticScratch& s = g_static_by_device[dev];
+    if (!s.base) {
+        void* p = nullptr;
+        checkCuda(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(scratch)");
+        void* q = nullptr;
+        checkCuda(cudaGetSymbolAddress(&q, g_static_state), "cudaGetSymbolAddress(state)");
+        s.base = static_cast<double*>(p);
+        s.state = static_cast<PcgState*>(q);
+    }
+    return s;
+}
+}  // namespace
+
+SolveOutcome staticJacobiPcg(int n, const int* row_ptr, const int* cols, const double* diag, const double* vals,
+                             const double* b, double* x, double atol, double rtol, int max_iterations) {
+    if (n <= 0 || n > kStaticMaxRows)
+        fail(kArgument, "the allocation-free PCG accepts 1.." + std::to_string(kStaticMaxRows) + " rows, got " +
+                            std::to_string(n));
+    if (!row_ptr || !cols || !diag || !vals || !b || !x) fail(kArgument, "null argument");
+    if (!(atol > 0.0) || !(rtol > 0.0) || !std::isfinite(atol) || !std::isfinite(rtol) || max_iterations <= 0)
+        fail(kArgument, "linear solver tolerances or iteration limit are invalid");
+    const StaticScratch s = staticScratch();
+    int dev = 0, sms = 0, per_sm = 0;
+    checkCuda(cudaGetDevice(&dev), "cudaGetDevice");
+    checkCuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    checkCuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kPcgPersistent, PB, 0), "occupancy");
+    const int grid = std::min(sms * std::min(per_sm, 4), kStaticMaxBlocks);
+    if (grid <= 0) fail(kCuda, "persistent PCG kernel cannot be resident");
+    double* r = s.base;
+    double* z = r + kStaticMaxRows;
+    double* p0 = z + kStaticMaxRows;
+    double* p1 = p0 + kStaticMaxRows;
+    double* q = p1 + kStaticMaxRows;
+    double* partial = q + kStaticMaxRows;
+    Dcsr<double> A{n, row_ptr, cols, diag, vals, 0};
+    PcgState h{};
+    h.target2 = -1.0;
+    h.warm = 0;
+    h.max_iterations = max_iterations;
+    h.atol = atol;
+    h.rtol = rtol;
+    SolveOutcome out;
+    double scale = 1.0, target = 0.0;
+    int used = 0;
+    auto run = [&](PcgState in) {
+        checkCuda(cudaMemcpy(s.state, &in, sizeof(in), cudaMemcpyHostToDevice), "cudaMemcpy(state)");
+        PcgArgs args{A, AmgView<double>{}, diag, b, x, r, z, p0, p1, q, partial, s.state, PhaseLog{}};
+        void* params[] = {&args};
+        checkCuda(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgPersistent), grid, PB, params, 0, 0),
+                  "cudaLaunchCooperativeKernel");
+        PcgState res;
+        checkCuda(cudaMemcpy(&res, s.state, sizeof(res), cudaMemcpyDeviceToHost), "cudaMemcpy(result)");
+        return res;
+    };
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        const PcgState res = run(h);
+        if (attempt == 0) {
+            out.initial = std::sqrt(res.rr0);
+            scale = std::max(std::sqrt(res.rr0), std::sqrt(res.bb));
+            if (!(scale > 0.0)) scale = 1.0;
+            target = std::max(atol, rtol * scale);
+            if (res.iterations == 0 && res.status == 0) {
+                out.status = 0;
+                out.final_ = out.initial;
+                out.relative = out.initial / scale;
+                return out;
+            }
+        }
+        used += res.iterations;
+        // true residual of the returned x: the same kernel from x with no iterations
+        PcgState check = h;
+        check.warm = 1;
+        check.max_iterations = 0;
+        check.target2 = target * target;
+        const PcgState tr = run(check);
+        out.final_ = std::sqrt(tr.rr0);
+        if (!std::isfinite(out.final_) || out.final_ <= target || res.status == 2 || used >= max_iterations) break;
+        h.target2 = 0.25 * res.target2;
+        h.warm = 1;
+        h.max_iterations = max_iterations - used;
+    }
+    out.iterations = used;
+    out.relative = out.final_ / scale;
+    out.status = (std::isfinite(out.final_) && out.final_ <= target) ? 0 : (std::isfinite(out.final_) ? 1 : 2);
+    return out;
 }
 
 void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<double>& amg, const double* jac,

@@ -231,6 +231,28 @@ int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t compo
                   const double* diagonal, const double* upper, const double* lower,
                   const double* source, double* x, bsg_solve_result* results);
 
+/* ---- allocation-free solve ---------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while running (an application that owns a fixed device-memory budget
+ * or pool, a real-time loop that must not take cudaMalloc's implicit device
+ * synchronisation, a host that forbids allocation after start-up): Jacobi-
+ * preconditioned CG on a matrix, right-hand side and solution that live in the
+ * caller's device memory, with all scratch in a fixed array compiled into the
+ * library (each GPU that loads the library holds about 5.4 MB until exit).
+ * It calls no cudaMalloc, cudaFree or allocating library routine.
+ *
+ * Matrix: n rows, diagonal `diag[n]` plus the off-diagonal entries in CSR
+ * (`row_ptr[n+1]`, `cols`, `vals`), all device pointers; n <= 131072, larger
+ * systems are rejected with BSG_ERR_ARGUMENT.  x (device, n) receives the
+ * solution from a zero initial guess; the acceptance contract is the same as
+ * bsg_solve_ldu.  Runs on the default stream of the current device and returns
+ * when the result is in `result`.  The first call on a device looks up the
+ * scratch's device address (make it before any stream capture).  All calls
+ * share the scratch: calls that overlap on the GPU race, so issue one at a time. */
+int bsg_pcg_jacobi_static(int32_t n, const int32_t* row_ptr, const int32_t* cols, const double* diag,
+                          const double* vals, const double* b, double* x, double absolute_tolerance,
+                          double relative_tolerance, int32_t max_iterations, bsg_solve_result* result);
+
 /* ---- steady SIMPLE (src/physics/simple/main.cpp:11-131) ----------------- */
 typedef struct {
     double density;

@@ -34,3 +34,16 @@ def test_errors_are_reported_without_a_device():
     code = _lib.lib().bsg_context_create(10_000, C.byref(h))
     assert code != 0
     assert _lib.lib().bsg_global_error()
+
+
+def test_static_pcg_rejects_oversized_systems_without_a_device():
+    """The allocation-free PCG checks its size limit before touching the device."""
+    import ctypes as C
+    from babelsim_b200 import _lib
+    res = _lib.SolveResult()
+    L = _lib.lib()
+    code = L.bsg_pcg_jacobi_static(131073, None, None, None, None, None, None, 1e-30, 1e-12, 10, C.byref(res))
+    assert code == 1   # BSG_ERR_ARGUMENT
+    assert b"131072" in L.bsg_global_error()
+    code = L.bsg_pcg_jacobi_static(0, None, None, None, None, None, None, 1e-30, 1e-12, 10, C.byref(res))
+    assert code == 1
