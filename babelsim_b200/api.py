@@ -56,7 +56,8 @@ class Context:
         import json
         buf = C.create_string_buffer(1 << 16)
         check(lib().bsg_context_profile_report(self.h, buf, len(buf)), self.h)
-        return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
+        # name -> (launches, total ms, algorithmic bytes, work units such as Krylov iterations)
+        return {k: (int(v[0]), float(v[1]), float(v[2]), float(v[3])) for k, v in json.loads(buf.value.decode()).items()}
 
     def phase_log(self, capacity: int):
         """Enable (capacity > 0) or disable the persistent-kernel phase timeline."""

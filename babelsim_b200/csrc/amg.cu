@@ -399,6 +399,27 @@ AmgView<double> AmgPreconditioner::deviceView() const {
     return v;
 }
 
+double AmgPreconditioner::vcycleBytes() const {
+    const int L = static_cast<int>(levels_.size());
+    const int nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
+    double bytes = 0.0;
+    for (int l = 0; l + 1 < L; ++l) {
+        const double n = levels_[l]->n, nc = levels_[l + 1]->n;
+        const double matrix = 8.0 * n + 4.0 * (n + 1) + 12.0 * static_cast<double>(levels_[l]->nnz);
+        // pre-smoothing: nu == 2 reads the matrix once (first sweep formed on the fly)
+        bytes += nu == 2 ? matrix + 24.0 * n : 24.0 * n;
+        // residual + restriction: aggregate lists, matrix, x, b; coarse b written
+        bytes += 4.0 * (nc + 1) + 4.0 * n + matrix + 16.0 * n + 8.0 * nc;
+        // prolongation + first post sweep: matrix, x, agg, rd, b, coarse x; t (or z) written
+        bytes += matrix + 36.0 * n + 8.0 * nc;
+        if (nu == 2) bytes += matrix + 32.0 * n + (l == 0 ? 8.0 * n : 0.0);  // second sweep (+ r for r.z)
+        else bytes += l == 0 ? 8.0 * n : 16.0 * n;                           // r.z, or the t -> x copy
+    }
+    const double nc = levels_.back()->n;
+    bytes += 8.0 * nc * nc + 16.0 * nc;  // dense coarsest solve
+    return bytes;
+}
+
 void AmgPreconditioner::apply(Context& ctx, const double* r, double* z) {
     const int L = static_cast<int>(levels_.size());
     const int nu = std::max(1, cfg_.amg_smoothing_steps);

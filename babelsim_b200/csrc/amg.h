@@ -31,6 +31,9 @@ public:
     // Device-side description of the hierarchy for the persistent PCG kernel
     // (valid after update()).
     AmgView<double> deviceView() const;
+    // Algorithmic bytes of one V-cycle as the persistent kernel runs it (every
+    // array a phase reads or writes counted once; FP64 8 B, int32 4 B).
+    double vcycleBytes() const;
 
     struct Level;
 

@@ -109,6 +109,13 @@ struct Context {
     std::vector<Record> records;
     std::vector<cudaEvent_t> event_pool;
     std::vector<cudaEvent_t> user_events;  // bsg_context_event_record slots
+    // Algorithmic bytes and work units (e.g. Krylov iterations) that instrumented
+    // launches declare while profiling; reported beside their timings.
+    struct Note { const char* name; double bytes, units; };
+    std::vector<Note> notes;
+    void profileNote(const char* name, double bytes, double units) {
+        if (profiling) notes.push_back({name, bytes, units});
+    }
     // Phase timeline of persistent kernels (device memory, enabled on request).
     long long* phase_entries = nullptr;
     int* phase_count = nullptr;
@@ -118,7 +125,8 @@ struct Context {
     void sync() { BSG_CUDA(cudaStreamSynchronize(stream)); }
     void launched() { ++launches; }
     cudaEvent_t takeEvent();
-    std::string profileReport();         // JSON {"name": [launches, total_ms], ...}; clears records
+    // JSON {"name": [launches, total_ms, algorithmic_bytes, units], ...}; clears the records
+    std::string profileReport();
 };
 
 // Brackets the launches issued in its scope with timing events when profiling.

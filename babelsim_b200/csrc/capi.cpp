@@ -76,22 +76,35 @@ cudaEvent_t Context::takeEvent() {
 
 std::string Context::profileReport() {
     sync();
-    std::vector<std::pair<std::string, std::pair<long long, double>>> acc;
+    struct Acc { std::string name; long long launches = 0; double ms = 0.0, bytes = 0.0, units = 0.0; };
+    std::vector<Acc> acc;
+    auto slot = [&](const char* name) -> Acc& {
+        auto it = std::find_if(acc.begin(), acc.end(), [&](const Acc& a) { return a.name == name; });
+        if (it != acc.end()) return *it;
+        acc.push_back(Acc{name});
+        return acc.back();
+    };
     for (auto& r : records) {
         float ms = 0.0f;
         checkCuda(cudaEventElapsedTime(&ms, r.start, r.stop), "cudaEventElapsedTime");
-        auto it = std::find_if(acc.begin(), acc.end(), [&](const auto& a) { return a.first == r.name; });
-        if (it == acc.end()) acc.push_back({r.name, {1, ms}});
-        else { it->second.first += 1; it->second.second += ms; }
+        Acc& a = slot(r.name);
+        a.launches += 1;
+        a.ms += ms;
         event_pool.push_back(r.start);
         event_pool.push_back(r.stop);
     }
     records.clear();
+    for (const Note& n : notes) {
+        Acc& a = slot(n.name);
+        a.bytes += n.bytes;
+        a.units += n.units;
+    }
+    notes.clear();
     std::string out = "{";
     for (std::size_t i = 0; i < acc.size(); ++i) {
-        char buf[256];
-        std::snprintf(buf, sizeof(buf), "%s\"%s\": [%lld, %.6f]", i ? ", " : "", acc[i].first.c_str(),
-                      acc[i].second.first, acc[i].second.second);
+        char buf[320];
+        std::snprintf(buf, sizeof(buf), "%s\"%s\": [%lld, %.6f, %.17g, %.17g]", i ? ", " : "", acc[i].name.c_str(),
+                      acc[i].launches, acc[i].ms, acc[i].bytes, acc[i].units);
         out += buf;
     }
     return out + "}";
@@ -563,6 +576,73 @@ int bsg_equ_source(bsg_equation* e, const bsg_field* value, double factor) {
         require(e && value && value->field->location == 0 && value->field->comps == e->eq->x->comps,
                 "equ::source requires a compatible cell field");
         bsg::addSource(*e->eq, value->field->v.data(), factor);
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_ddt(bsg_equation* e, const bsg_field* capacity, double c, const bsg_field* previous,
+                const bsg_field* older, double dt, double older_dt, int32_t method) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && previous, "null argument");
+        const int C = e->eq->x->comps;
+        auto cellOf = [&](const bsg_field* f, int comps) {
+            return f && f->mesh == e->unknown->mesh && f->field->location == 0 && f->field->comps == comps;
+        };
+        require(cellOf(previous, C), "equ::ddt previous level must be a compatible cell field");
+        require(!older || cellOf(older, C), "equ::ddt older level must be a compatible cell field");
+        require(!capacity || cellOf(capacity, 1), "equ::ddt capacity must be a cell scalar field");
+        const bsg::TimeWeights t = bsg::timeWeights(method, dt, older_dt, older != nullptr);
+        if (!t.active) return;
+        bsg::Context& ctx = *e->eq->x->mesh->ctx;
+        if (capacity) {
+            int bad[2];
+            bsg::checkValues(ctx, capacity->field->v.data(), e->eq->x->mesh->n_cells, e->flags.data(), bad);
+            if (bad[0]) bsg::fail(bsg::kArgument, "time capacity must be positive and finite");
+        }
+        bsg::addTimeTerm(*e->eq, capacity ? capacity->field->v.data() : nullptr, c, previous->field->v.data(),
+                         older ? older->field->v.data() : nullptr, t);
+        ctx.sync();
+    });
+}
+
+int bsg_equ_reaction(bsg_equation* e, const bsg_field* coefficient, double c, double factor) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e != nullptr, "null equation");
+        bsg::Context& ctx = *e->eq->x->mesh->ctx;
+        if (coefficient) {
+            require(coefficient->mesh == e->unknown->mesh && coefficient->field->location == 0 &&
+                        coefficient->field->comps == 1,
+                    "equ::reaction coefficient must be a cell scalar field");
+            int bad[2];
+            bsg::checkValues(ctx, coefficient->field->v.data(), e->eq->x->mesh->n_cells, e->flags.data(), bad);
+            if (bad[1]) bsg::fail(bsg::kArgument, "nonfinite equ coefficient");
+        }
+        bsg::addReaction(*e->eq, coefficient ? coefficient->field->v.data() : nullptr, c, factor);
+        ctx.sync();
+    });
+}
+
+int bsg_equ_apply(const bsg_equation* e, const bsg_field* x, bsg_field* out) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && x && out, "null argument");
+        const int C = e->eq->x->comps;
+        require(x->field->location == 0 && x->field->comps == C && out->field->location == 0 &&
+                    out->field->comps == C && x->mesh == e->unknown->mesh && out->mesh == e->unknown->mesh,
+                "equ::apply requires compatible cell fields");
+        bsg::applyEquation(*e->eq, x->field->v.data(), out->field->v.data());
+        e->eq->x->mesh->ctx->sync();
+    });
+}
+
+int bsg_equ_residual(const bsg_equation* e, const bsg_field* x, bsg_field* out) {
+    return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
+        require(e && x && out, "null argument");
+        const int C = e->eq->x->comps;
+        require(x->field->location == 0 && x->field->comps == C && out->field->location == 0 &&
+                    out->field->comps == C && x->mesh == e->unknown->mesh && out->mesh == e->unknown->mesh,
+                "equ::residual requires compatible cell fields");
+        require(x->field.get() != out->field.get(), "equ::residual output must differ from its input");
+        bsg::residualEquation(*e->eq, x->field->v.data(), out->field->v.data());
         e->eq->x->mesh->ctx->sync();
     });
 }

@@ -507,6 +507,43 @@ __global__ void kRelax(int n, double alpha, const double* __restrict__ prev, dou
     for (int c = 0; c < C; ++c) src[C * i + c] += extra * prev[C * i + c];
 }
 
+// Transient term (procedural_equation.cpp:198-223): with w = capacity * V,
+// diag += w a0 and b += w a1 x_prev (+ w a2 x_older for variable-step BDF2).
+template <int C>
+__global__ void kTimeTerm(int n, const double* __restrict__ V, const double* __restrict__ cap, double c, double a0,
+                          double a1, double a2, const double* __restrict__ prev, const double* __restrict__ older,
+                          double* __restrict__ diag, double* __restrict__ src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double w = (cap ? cap[i] : c) * V[i];
+    diag[i] += w * a0;
+    const double w1 = w * a1, w2 = w * a2;
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        double s = src[C * i + k];
+        s += w1 * prev[C * i + k];
+        if (a2 != 0.0) s += w2 * older[C * i + k];
+        src[C * i + k] = s;
+    }
+}
+
+// Implicit reaction (procedural_equation.cpp:177-187): diag += factor c_i V_i.
+__global__ void kReaction(int n, const double* __restrict__ V, const double* __restrict__ coef, double c,
+                          double factor, double* __restrict__ diag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    diag[i] += coef ? factor * coef[i] * V[i] : c * V[i];
+}
+
+// flag[0] = 1 when any value is not positive and finite (flag[1]: any non-finite).
+__global__ void kCheckValues(int n, const double* __restrict__ a, int* __restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = a[i];
+    if (!(v > 0.0) || !isfinite(v)) flag[0] = 1;
+    if (!isfinite(v)) flag[1] = 1;
+}
+
 __global__ void kScaleArray(long long n, double f, double* __restrict__ a) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i < n) a[i] *= f;
@@ -646,6 +683,11 @@ __global__ void kAxpy(long long n, double* __restrict__ y, double a, const doubl
 __global__ void kAdd(long long n, double* __restrict__ out, const double* __restrict__ a, const double* __restrict__ b) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i < n) out[i] = a[i] + b[i];
+}
+// out = b - out (residual after out = A x)
+__global__ void kResidualFrom(long long n, const double* __restrict__ b, double* __restrict__ out) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i < n) out[i] = b[i] - out[i];
 }
 __global__ void kSubScaledGrad(int n, double* __restrict__ U, const double* __restrict__ r, const double* __restrict__ g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -963,6 +1005,52 @@ void relax(DeviceEquation& eq, const double* previous, double alpha) {
     else launch(*m.ctx, kRelax<3>, m.n_cells, m.n_cells, alpha, previous, eq.diag.data(), eq.src.data());
 }
 
+TimeWeights timeWeights(int method, double dt, double older_dt, bool have_older) {
+    TimeWeights t;
+    if (method == 0) return t;
+    if (method != 1 && method != 2) fail(kArgument, "unsupported time method");
+    if (!(dt > 0.0) || !std::isfinite(dt)) fail(kArgument, "equ::ddt requires positive finite dt");
+    t.a0 = 1.0 / dt;
+    t.a1 = 1.0 / dt;
+    if (method == 2) {
+        if (!have_older) fail(kArgument, "BDF2 requires explicit older field; use Euler to start");
+        if (older_dt == 0.0) older_dt = dt;
+        if (!(older_dt > 0.0) || !std::isfinite(older_dt)) fail(kArgument, "invalid previous dt");
+        const double r = dt / older_dt;
+        t.a0 = (1 + 2 * r) / ((1 + r) * dt);
+        t.a1 = (1 + r) / dt;
+        t.a2 = -r * r / ((1 + r) * dt);
+    }
+    t.active = true;
+    return t;
+}
+
+void addTimeTerm(DeviceEquation& eq, const double* capacity, double c, const double* previous, const double* older,
+                 const TimeWeights& t) {
+    if (!t.active) return;
+    if (!capacity && !(c > 0.0 && std::isfinite(c))) fail(kArgument, "time capacity must be positive and finite");
+    DeviceMesh& m = *eq.x->mesh;
+    if (eq.x->comps == 1)
+        launch(*m.ctx, kTimeTerm<1>, m.n_cells, m.n_cells, (const double*)m.V.data(), capacity, c, t.a0, t.a1, t.a2,
+               previous, older, eq.diag.data(), eq.src.data());
+    else
+        launch(*m.ctx, kTimeTerm<3>, m.n_cells, m.n_cells, (const double*)m.V.data(), capacity, c, t.a0, t.a1, t.a2,
+               previous, older, eq.diag.data(), eq.src.data());
+}
+
+void addReaction(DeviceEquation& eq, const double* coefficient, double c, double factor) {
+    if (!std::isfinite(c) || !std::isfinite(factor)) fail(kArgument, "nonfinite equ coefficient");
+    DeviceMesh& m = *eq.x->mesh;
+    launch(*m.ctx, kReaction, m.n_cells, m.n_cells, (const double*)m.V.data(), coefficient, c, factor, eq.diag.data());
+}
+
+void checkValues(Context& ctx, const double* a, long long n, int* flags_dev, int out[2]) {
+    BSG_CUDA(cudaMemsetAsync(flags_dev, 0, 2 * sizeof(int), ctx.stream));
+    if (n > 0) launch(ctx, kCheckValues, n, static_cast<int>(n), a, flags_dev);
+    BSG_CUDA(cudaMemcpyAsync(out, flags_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+}
+
 void scale(DeviceEquation& eq, double f) {
     if (!std::isfinite(f)) fail(kArgument, "nonfinite equ coefficient");
     Context& ctx = *eq.x->mesh->ctx;
@@ -995,6 +1083,12 @@ void applyEquation(const DeviceEquation& eq, const double* x, double* y) {
     else
         launch(*m.ctx, kApply<3>, m.n_cells, m.n_cells, (const int*)m.cf_ptr.data(), (const int*)m.cf_col.data(),
                eq.diag.data(), eq.val.data(), x, y);
+}
+
+void residualEquation(const DeviceEquation& eq, const double* x, double* y) {
+    applyEquation(eq, x, y);
+    const long long n = static_cast<long long>(eq.x->mesh->n_cells) * eq.x->comps;
+    launch(*eq.x->mesh->ctx, kResidualFrom, n, n, (const double*)eq.src.data(), y);
 }
 
 void faceFluxEquation(DeviceEquation& eq, const double* solution, DeviceArray<double>& out) {

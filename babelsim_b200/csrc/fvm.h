@@ -92,10 +92,26 @@ void addConvection(DeviceEquation& eq, DeviceField& phi, double scale, const Opt
 void addLaplacian(DeviceEquation& eq, DeviceField* coef, double k, double factor, const Options& o);
 void addSource(DeviceEquation& eq, const double* values, double factor);
 void relax(DeviceEquation& eq, const double* previous, double alpha);
+// Time-derivative weights of equ::ddt (procedural_equation.cpp:198-223); method
+// follows TimeMethod (0 steady, 1 Euler, 2 BDF2 with variable step).
+struct TimeWeights {
+    bool active = false;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+};
+TimeWeights timeWeights(int method, double dt, double older_dt, bool have_older);
+// capacity: per-cell values (checked by the caller) or nullptr for the constant c.
+void addTimeTerm(DeviceEquation& eq, const double* capacity, double c, const double* previous, const double* older,
+                 const TimeWeights& t);
+// diag += factor * coefficient_i * V_i, or c * V_i when coefficient is nullptr.
+void addReaction(DeviceEquation& eq, const double* coefficient, double c, double factor);
+// out[0] = any value not positive-finite, out[1] = any value non-finite (synchronises).
+void checkValues(Context& ctx, const double* a, long long n, int* flags_dev, int out[2]);
 void scale(DeviceEquation& eq, double f);
 // Returns through *flag_dev (device int) whether the gauge was applied; host reads if asked.
 void referenceIfUnanchored(DeviceEquation& eq, double value, int* flag_dev);
 void applyEquation(const DeviceEquation& eq, const double* x, double* y);
+// y = b - A x (procedural_equation.cpp:291-296)
+void residualEquation(const DeviceEquation& eq, const double* x, double* y);
 void faceFluxEquation(DeviceEquation& eq, const double* solution, DeviceArray<double>& out_face);
 // ||b-Ax||, ||Ax||, ||b|| into red.result[0..2]
 void relativeResidualNorms(const DeviceEquation& eq, const double* x, Reducer& red);

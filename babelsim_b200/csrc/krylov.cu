@@ -11,6 +11,8 @@
 #include "linalg.h"
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace bsg {
@@ -527,6 +529,13 @@ double hostNorm(Context& ctx, const double* x, int n, DeviceArray<double>& parti
     return std::sqrt(ctx.pinned[0]);
 }
 
+// BSG_TRACE_SOLVES=1 prints one line per persistent solve launch to stderr
+// (iterations and algorithmic bytes), to pair a profiler capture with its work.
+bool trace_solves() {
+    static const bool on = std::getenv("BSG_TRACE_SOLVES") != nullptr;
+    return on;
+}
+
 inline double residualScale(double initial, double rhs) {
     const double v = std::max(initial, rhs);
     return v > 0.0 ? v : 1.0;
@@ -558,6 +567,20 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
         ctx.sync();
         PcgState r;
         std::memcpy(&r, ctx.pinned, sizeof(r));
+        if (ctx.profiling || trace_solves()) {
+            // algorithmic bytes of this launch: initial residual, preconditioner
+            // applications and per-iteration SpMV + vector updates
+            const double N = n, M0 = 8.0 * N + 4.0 * (N + 1) + 12.0 * static_cast<double>(A.nnz_off);
+            const double init = h.warm ? M0 + 32.0 * N : 24.0 * N;
+            const double pre = amg ? amg->vcycleBytes() : (jacobi_diag ? 32.0 * N : 24.0 * N);
+            const double it = r.iterations;
+            const double applications = (r.iterations == 0 && r.status == 0) ? 0.0 : std::max(1.0, it);
+            const double bytes = init + applications * pre + it * (M0 + 80.0 * N);
+            ctx.profileNote("pcg_amg_persistent", bytes, it);
+            if (trace_solves())
+                std::fprintf(stderr, "bsg persistent pcg: rows %d iterations %d status %d algorithmic_bytes %.0f\n", n,
+                             r.iterations, r.status, bytes);
+        }
         if (attempt == 0) {
             out.initial = std::sqrt(r.rr0);
             scale = residualScale(std::sqrt(r.rr0), std::sqrt(r.bb));

@@ -134,6 +134,11 @@ def algorithmic_bytes(name, N, nnz_off, amg_rows):
     return None
 
 
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte,
+# measured by one capture of the kernel on this workload (profiles/ summaries).
+DRAM_PER_ALGORITHMIC_BYTE = {}
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -259,19 +264,29 @@ def main():
     prof = ctx.profile_report()
     ctx.profile(False)
     amg_rows = int(N / 4)
-    candidates = {k: v for k, v in prof.items() if algorithmic_bytes(k, N, 2 * Fi, amg_rows)}
+
+    def launch_bytes(name, rec):
+        if rec[2] > 0:  # algorithmic bytes the library declared for these launches
+            return rec[2] / rec[0]
+        return algorithmic_bytes(name, N, 2 * Fi, amg_rows)
+
+    candidates = {k: v for k, v in prof.items() if launch_bytes(k, v)}
     top = max(candidates, key=lambda k: candidates[k][1]) if candidates else None
     peak, peak_kind = load_peaks()
     roofline = None
     if top:
-        cnt, tot = candidates[top]
+        cnt, tot = candidates[top][0], candidates[top][1]
         avg_s = tot / cnt / 1e3
-        ab = algorithmic_bytes(top, N, 2 * Fi, amg_rows)
+        ab = launch_bytes(top, candidates[top])
         achieved = ab / avg_s / 1e9
+        ratio = DRAM_PER_ALGORITHMIC_BYTE.get(top)
         roofline = {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 3),
-                    "traffic": None, "algorithmic_bytes_per_launch": ab, "avg_launch_us": round(avg_s * 1e6, 2),
-                    "launches_per_step": cnt}
+                    "traffic": round(ratio * ab) if ratio else None, "algorithmic_bytes_per_launch": round(ab),
+                    "avg_launch_us": round(avg_s * 1e6, 2), "launches_per_step": cnt,
+                    "share_of_step": round(tot / sum(v[1] for v in prof.values()), 3)}
+        if candidates[top][3] > 0:
+            roofline["units_per_launch"] = round(candidates[top][3] / cnt, 1)
     # End to end through the C ABI with host buffers: every step copies U, p, phi in from
     # pinned host memory, runs one outer iteration and copies them back out.
     import torch
@@ -314,6 +329,8 @@ def main():
                            "mesh_seconds": round(t_mesh, 1)},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
+                "pressure_iterations_per_solve": round(prof["pcg_amg_persistent"][3] / prof["pcg_amg_persistent"][0], 1)
+                if "pcg_amg_persistent" in prof else None,
                 "last_report": {"momentum_iterations": rep.momentum_iterations,
                                 "pressure_iterations": rep.pressure_iterations, "rU": rep.rU, "dU": rep.dU,
                                 "mass": rep.mass}}

@@ -50,6 +50,8 @@ enum { BSG_INTERP_LINEAR = 0, BSG_INTERP_CORRECTED = 1 };
 enum { BSG_GRAD_GREEN_GAUSS = 0, BSG_GRAD_LEAST_SQUARES = 1 };
 enum { BSG_CONV_UPWIND = 0, BSG_CONV_LINEAR_UPWIND = 1, BSG_CONV_CENTRAL = 2 };
 enum { BSG_DIFF_ORTHOGONAL = 0, BSG_DIFF_CORRECTED = 1, BSG_DIFF_LIMITED_CORRECTED = 2 };
+/* TimeMethod, include/babelsim/methods.h:33-37 */
+enum { BSG_TIME_STEADY = 0, BSG_TIME_EULER = 1, BSG_TIME_BDF2 = 2 };
 /* LinearSolverType / PreconditionerType / SolveStatus,
  * include/babelsim/solver_control.h:12-36 */
 enum { BSG_KSP_CG = 0, BSG_KSP_BICGSTAB = 1, BSG_KSP_GMRES = 2, BSG_KSP_FGMRES = 3 };
@@ -211,6 +213,20 @@ int bsg_equ_div(bsg_equation* eq, const bsg_field* flux, double scale, const bsg
 int bsg_equ_laplacian(bsg_equation* eq, const bsg_field* coefficient, double k, double factor,
                       const bsg_options* term);
 int bsg_equ_source(bsg_equation* eq, const bsg_field* value, double factor);
+/* equ::ddt with explicit time levels (include/babelsim/equ.h:63-70,
+ * src/discretization/procedural_equation.cpp:198-223): capacity is a cell scalar
+ * field or NULL for the constant c; older may be NULL for Euler; older_dt 0
+ * means dt (variable-step BDF2 weights from r = dt/older_dt).  A steady method
+ * adds nothing. */
+int bsg_equ_ddt(bsg_equation* eq, const bsg_field* capacity, double c, const bsg_field* previous,
+                const bsg_field* older, double dt, double older_dt, int32_t method);
+/* equ::reaction (equ.h:56-57, procedural_equation.cpp:177-187): diagonal +=
+ * factor*coefficient*V, or c*V when coefficient is NULL. */
+int bsg_equ_reaction(bsg_equation* eq, const bsg_field* coefficient, double c, double factor);
+/* equ::apply / equ::residual (equ.h:79-80, procedural_equation.cpp:281-297):
+ * out = A x, or out = b - A x; x and out are cell fields shaped like the unknown. */
+int bsg_equ_apply(const bsg_equation* eq, const bsg_field* x, bsg_field* out);
+int bsg_equ_residual(const bsg_equation* eq, const bsg_field* x, bsg_field* out);
 int bsg_equ_relax(bsg_equation* eq, const bsg_field* previous, double alpha);
 int bsg_equ_scale(bsg_equation* eq, double factor);
 int bsg_equ_reference_if_unanchored(bsg_equation* eq, double value, int32_t* anchored_out);
