@@ -25,7 +25,7 @@ EXPORTS = [
     "bsg_field_upload", "bsg_field_download", "bsg_field_set_boundary_flux", "bsg_math_grad",
     "bsg_math_interpolate", "bsg_math_flux", "bsg_math_div_flux", "bsg_math_normal_gradient",
     "bsg_equation_create", "bsg_equation_destroy", "bsg_equ_reset", "bsg_equ_div", "bsg_equ_laplacian",
-    "bsg_equ_source", "bsg_equ_relax", "bsg_equ_scale", "bsg_equ_reference_if_unanchored", "bsg_equ_face_flux",
+    "bsg_equ_source", "bsg_equ_ddt", "bsg_equ_reaction", "bsg_equ_apply", "bsg_equ_residual", "bsg_equ_relax", "bsg_equ_scale", "bsg_equ_reference_if_unanchored", "bsg_equ_face_flux",
     "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_pcg_jacobi_static",
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
@@ -113,6 +113,8 @@ def lib():
             "bsg_equation_create": [vp, C.POINTER(Options), pp], "bsg_equation_destroy": [vp],
             "bsg_equ_reset": [vp], "bsg_equ_div": [vp, vp, dbl, C.POINTER(Options)],
             "bsg_equ_laplacian": [vp, vp, dbl, dbl, C.POINTER(Options)], "bsg_equ_source": [vp, vp, dbl],
+            "bsg_equ_ddt": [vp, vp, dbl, vp, vp, dbl, dbl, i32], "bsg_equ_reaction": [vp, vp, dbl, dbl],
+            "bsg_equ_apply": [vp, vp, vp], "bsg_equ_residual": [vp, vp, vp],
             "bsg_equ_relax": [vp, vp, dbl], "bsg_equ_scale": [vp, dbl],
             "bsg_equ_reference_if_unanchored": [vp, dbl, C.POINTER(i32)], "bsg_equ_face_flux": [vp, vp, vp],
             "bsg_equ_relative_residual": [vp, vp, C.POINTER(dbl)],

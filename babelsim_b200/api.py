@@ -258,6 +258,31 @@ class Equation:
     def source(self, value: Field, factor=1.0):
         self._c(lib().bsg_equ_source(self.h, value.h, factor))
 
+    def ddt(self, capacity, previous: Field, dt: float, method="euler", older: Field | None = None,
+            older_dt: float = 0.0):
+        """equ::ddt with explicit levels; capacity is a cell Field or a number."""
+        m = {"steady": 0, "euler": 1, "bdf2": 2}[method.lower()]
+        cap = capacity.h if isinstance(capacity, Field) else None
+        c = 0.0 if isinstance(capacity, Field) else float(capacity)
+        self._c(lib().bsg_equ_ddt(self.h, cap, c, previous.h, older.h if older else None, dt, older_dt, m))
+
+    def reaction(self, coefficient, factor=1.0):
+        """equ::reaction: diagonal += factor*coefficient*V (coefficient: cell Field or number)."""
+        if isinstance(coefficient, Field):
+            self._c(lib().bsg_equ_reaction(self.h, coefficient.h, 0.0, factor))
+        else:
+            self._c(lib().bsg_equ_reaction(self.h, None, float(coefficient), 1.0))
+
+    def apply(self, x: Field) -> Field:
+        out = Field(self.x.mesh, "cell", self.x.components)
+        self._c(lib().bsg_equ_apply(self.h, x.h, out.h))
+        return out
+
+    def residual(self, x: Field) -> Field:
+        out = Field(self.x.mesh, "cell", self.x.components)
+        self._c(lib().bsg_equ_residual(self.h, x.h, out.h))
+        return out
+
     def relax(self, previous: Field, alpha):
         self._c(lib().bsg_equ_relax(self.h, previous.h, alpha))
 
