@@ -2,6 +2,7 @@
 // matrix version, device V-cycle.  See amg.h for the design.
 #include "amg.h"
 #include "bsg_device.cuh"
+#include "pcg_sell.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -28,6 +29,22 @@ struct AmgPreconditioner::Level {
     DeviceArray<double> x, b, t;
     // coarsest level
     DeviceArray<double> dense;           // n x 2n augmented matrix, inverse in the right half
+    // SELL-32 copies for the persistent solver (pcg_sell.cuh)
+    int nslices = 0;
+    long long sell_entries = 0;
+    DeviceArray<int> s_ptr, s_col;
+    DeviceArray<double> s_val;           // FP64 values (FP64 V-cycle; on level 0 also the Krylov matrix)
+    DeviceArray<double> w;               // first Jacobi sweep (FP64 V-cycle)
+    DeviceArray<float> s_val32, diag32, rd32, x32, b32, w32, t32;
+    void buildSell(const int* hptr, const int* hcol, cudaStream_t s) {
+        SellPattern pat;
+        pat.build(n, hptr, hcol);
+        nslices = pat.nslices;
+        sell_entries = pat.entries;
+        s_ptr.upload(pat.sptr, s);
+        if (pat.col.empty()) pat.col.push_back(0);
+        s_col.upload(pat.col, s);
+    }
 };
 
 namespace {
@@ -164,6 +181,15 @@ __global__ void kDenseSolve(int n, const double* __restrict__ M, const double* _
     }
 }
 
+// Compact n x n copy (row-major, converted to T) of the inverse half of the augmented [A | A^-1].
+template <class T>
+__global__ void kDenseCompact(int n, const double* __restrict__ M, T* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * n) return;
+    const int i = e / n, j = e % n;
+    out[e] = static_cast<T>(M[static_cast<long long>(i) * 2 * n + n + j]);
+}
+
 // x = omega D^-1 b (first Jacobi sweep from a zero guess)
 __global__ void kSmoothZero(int n, const double* __restrict__ rd, const double* __restrict__ b, double* __restrict__ x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -234,6 +260,8 @@ AmgPreconditioner::AmgPreconditioner(DeviceMesh& mesh, const SolverConfig& cfg)
     if (const char* g = std::getenv("BSG_AMG_GAMMA")) gamma_ = std::atof(g);
     if (!(omega_ > 0.0 && omega_ <= 1.0) || !(gamma_ > 0.0 && gamma_ <= 3.0))
         fail(kArgument, "AMG Jacobi weight must be in (0,1] and the correction scale in (0,3]");
+    // FP32 V-cycle data on the mixed-precision path (FP64 Krylov vectors and true residual stay FP64)
+    fp32_ = cfg.precision == 1 || std::getenv("BSG_AMG_FP32") != nullptr;
 }
 
 AmgPreconditioner::~AmgPreconditioner() {
@@ -260,6 +288,7 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
     auto* l0 = new Level();
     l0->n = A.n;
     l0->nnz = A.nnz_off;
+    l0->buildSell(cur.ptr.data(), cur.col.data(), ctx_.stream);
     levels_.push_back(l0);
     while (cur.n > coarse_target && static_cast<int>(levels_.size()) < max_levels) {
         int n1 = 0, n2 = 0;
@@ -268,7 +297,9 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
         const std::vector<int> a2 = pairwise(c1, n2);
         std::vector<int> agg(cur.n);
         for (int i = 0; i < cur.n; ++i) agg[i] = a2[a1[i]];
-        if (n2 >= cur.n) break;  // no coarsening possible
+        // stop when coarsening stalls (< 1.5x fewer rows): such levels cost a
+        // V-cycle their barriers and gathers without shrinking the problem
+        if (3 * static_cast<long long>(n2) > 2 * static_cast<long long>(cur.n)) break;
         std::vector<int> target;
         HostCsr next = coarsen(cur, agg, n2, &target);
         Level* fine = levels_.back();
@@ -321,6 +352,7 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
         lv->dcol = lv->col.data();
         lv->ddiag = lv->diag.data();
         lv->dval = lv->val.data();
+        lv->buildSell(next.ptr.data(), next.col.data(), s);
         levels_.push_back(lv);
         ctx_.sync();
         cur = std::move(next);
@@ -330,9 +362,24 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
         l->b.resize(l->n);
         l->t.resize(l->n);
         l->rdiag.resize(l->n);
+        const std::size_t e = std::max<long long>(l->sell_entries, 1);
+        if (fp32_) {
+            for (DeviceArray<float>* a : {&l->diag32, &l->rd32, &l->x32, &l->b32, &l->w32, &l->t32}) a->resize(l->n);
+            l->s_val32.resize(e);
+            l->s_val32.zero(ctx_.stream);  // padding entries stay zero
+        } else {
+            l->w.resize(l->n);
+        }
+        if (!fp32_ || l == levels_.front()) {  // FP64 V-cycle values, and the level-0 Krylov matrix
+            l->s_val.resize(e);
+            l->s_val.zero(ctx_.stream);
+        }
     }
     Level* last = levels_.back();
     last->dense.resize(2 * static_cast<std::size_t>(last->n) * last->n);
+    const std::size_t nn = static_cast<std::size_t>(last->n) * last->n;
+    if (fp32_) dense32_.resize(nn);
+    else dense64_.resize(nn);
     built_ = true;
     if (std::getenv("BSG_AMG_VERBOSE")) {
         long long total = 0;
@@ -350,6 +397,11 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
     Level* l0 = levels_[0];
     l0->dptr = A.ptr; l0->dcol = A.col; l0->ddiag = A.diag; l0->dval = A.val;
     if (!numeric) {
+        // hierarchy kept; the level-0 Krylov matrix always follows the matrix being solved
+        kCsrToSell<double><<<gridFor(l0->n, kBlock), kBlock, 0, ctx_.stream>>>(
+            l0->n, l0->dptr, l0->dval, l0->ddiag, l0->s_ptr.data(), omega_, l0->s_val.data(), nullptr, nullptr);
+        ctx_.launched();
+        BSG_CUDA(cudaGetLastError());
         uploadViews();
         return;
     }
@@ -370,6 +422,23 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
                                               last->dense.data());
     ctx_.launched();
     BSG_CUDA(cudaGetLastError());
+    // SELL-32 values for the persistent solver
+    const int nn = last->n * last->n;
+    if (fp32_) kDenseCompact<float><<<gridFor(nn, kBlock), kBlock, 0, ctx_.stream>>>(last->n, last->dense.data(), dense32_.data());
+    else kDenseCompact<double><<<gridFor(nn, kBlock), kBlock, 0, ctx_.stream>>>(last->n, last->dense.data(), dense64_.data());
+    ctx_.launched();
+    for (std::size_t li = 0; li < levels_.size(); ++li) {
+        Level* l = levels_[li];
+        const unsigned g = gridFor(l->n, kBlock);
+        if (fp32_)
+            kCsrToSell<float><<<g, kBlock, 0, ctx_.stream>>>(l->n, l->dptr, l->dval, l->ddiag, l->s_ptr.data(), omega_,
+                                                              l->s_val32.data(), l->diag32.data(), l->rd32.data());
+        if (!fp32_ || li == 0)
+            kCsrToSell<double><<<g, kBlock, 0, ctx_.stream>>>(l->n, l->dptr, l->dval, l->ddiag, l->s_ptr.data(), omega_,
+                                                               l->s_val.data(), nullptr, nullptr);
+        ctx_.launches += (fp32_ && li == 0) ? 2 : 1;
+    }
+    BSG_CUDA(cudaGetLastError());
     uploadViews();
 }
 
@@ -385,6 +454,89 @@ void AmgPreconditioner::uploadViews() {
                                         lv->t.data()};
     }
     d_views_.upload(views, ctx_.stream);
+    const int L = static_cast<int>(levels_.size());
+    if (fp32_) {
+        std::vector<VLevel<float>> v(L);
+        for (int l = 0; l < L; ++l) {
+            Level* lv = levels_[l];
+            const bool coarser = l + 1 < L;
+            v[l].A = SellMat<float>{lv->n, lv->nslices, lv->s_ptr.data(), lv->s_col.data(), lv->s_val32.data(),
+                                    lv->diag32.data()};
+            v[l].rd = lv->rd32.data();
+            v[l].agg_ptr = coarser ? lv->agg_ptr.data() : nullptr;
+            v[l].agg_rows = coarser ? lv->agg_rows.data() : nullptr;
+            v[l].b = lv->b32.data();
+            v[l].w = lv->w32.data();
+            v[l].x = lv->x32.data();
+            v[l].t = lv->t32.data();
+        }
+        d_vl32_.upload(v, ctx_.stream);
+    } else {
+        std::vector<VLevel<double>> v(L);
+        for (int l = 0; l < L; ++l) {
+            Level* lv = levels_[l];
+            const bool coarser = l + 1 < L;
+            v[l].A = SellMat<double>{lv->n, lv->nslices, lv->s_ptr.data(), lv->s_col.data(), lv->s_val.data(),
+                                     lv->ddiag};
+            v[l].rd = lv->rdiag.data();
+            v[l].agg_ptr = coarser ? lv->agg_ptr.data() : nullptr;
+            v[l].agg_rows = coarser ? lv->agg_rows.data() : nullptr;
+            v[l].b = lv->b.data();
+            v[l].w = lv->w.data();
+            v[l].x = lv->x.data();
+            v[l].t = lv->t.data();
+        }
+        d_vl64_.upload(v, ctx_.stream);
+    }
+}
+
+SellMat<double> AmgPreconditioner::krylovMatrix() const {
+    const Level* l = levels_.front();
+    return SellMat<double>{l->n, l->nslices, l->s_ptr.data(), l->s_col.data(), l->s_val.data(), l->ddiag};
+}
+
+long long AmgPreconditioner::krylovEntries() const { return levels_.front()->sell_entries; }
+
+VCycleView<double> AmgPreconditioner::sellView64() const {
+    VCycleView<double> v;
+    v.levels = static_cast<int>(levels_.size());
+    v.nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
+    v.gamma = gamma_;
+    v.lv = d_vl64_.data();
+    v.dense_inv = dense64_.data();
+    return v;
+}
+
+VCycleView<float> AmgPreconditioner::sellView32() const {
+    VCycleView<float> v;
+    v.levels = static_cast<int>(levels_.size());
+    v.nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
+    v.gamma = static_cast<float>(gamma_);
+    v.lv = d_vl32_.data();
+    v.dense_inv = dense32_.data();
+    return v;
+}
+
+double AmgPreconditioner::sellVcycleBytes() const {
+    // One V-cycle of the SELL persistent kernel, every array a phase touches counted once.
+    const int L = static_cast<int>(levels_.size());
+    const int nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
+    const double s = fp32_ ? 4.0 : 8.0;  // V-cycle value size
+    double bytes = 0.0;
+    for (int l = 0; l + 1 < L; ++l) {
+        const Level* f = levels_[l];
+        const double n = f->n, nc = levels_[l + 1]->n;
+        const double sweep = (4.0 + s) * static_cast<double>(f->sell_entries) + 4.0 * (f->nslices + 1) + s * n;  // matrix + diag
+        if (nu >= 2) bytes += sweep + 4.0 * s * n;                   // D1: w (gathered), rd, b read; x written
+        bytes += sweep + 3.0 * s * n;                                // D2: x, b read; t written
+        bytes += 4.0 * (nc + 1) + 4.0 * n + s * n + 3.0 * s * nc;    // D3: lists, t read; b_c, w_c written, rd_c read
+        bytes += sweep + 4.0 * s * n;                                // U1: y, rd, b read; t (or output) written
+        if (nu >= 2) bytes += sweep + 4.0 * s * n;                   // U2: t, rd, b read; output written
+        bytes += 4.0 * n + 4.0 * (nc + 1) + 2.0 * s * n;             // pushes into the finer iterate (l > 0) / z
+    }
+    const double nc = levels_.back()->n;
+    bytes += s * nc * nc + 2.0 * s * nc + 12.0 * (L > 1 ? levels_[L - 2]->n : 0);  // dense solve + push
+    return bytes;
 }
 
 AmgView<double> AmgPreconditioner::deviceView() const {

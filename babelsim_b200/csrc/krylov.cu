@@ -7,6 +7,7 @@
 // reads a convergence word every `check_interval` iterations; kernels of
 // iterations issued after convergence return immediately.
 #include "amg.h"
+#include "pcg_sell.cuh"
 #include "bsg_device.cuh"
 #include "linalg.h"
 
@@ -561,8 +562,20 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
     int used = 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
         BSG_CUDA(cudaMemcpyAsync(m.pst.data(), &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
-        launchPersistentPcg(ctx, A, view, jacobi_diag, b, x, m.r.data(), m.z.data(), m.p.data(), m.v.data(),
-                            m.q.data(), m.partial.data(), m.pst.data());
+        if (amg && amg->fp32VCycle()) {
+            SellPcgArgs<double, float> args{amg->krylovMatrix(), amg->sellView32(), b, x, m.r.data(), m.z.data(),
+                                            m.p.data(), m.v.data(), m.q.data(), m.partial.data(), m.pst.data(),
+                                            PhaseLog{}};
+            launchSellPcg(ctx, args);
+        } else if (amg) {
+            SellPcgArgs<double, double> args{amg->krylovMatrix(), amg->sellView64(), b, x, m.r.data(), m.z.data(),
+                                             m.p.data(), m.v.data(), m.q.data(), m.partial.data(), m.pst.data(),
+                                             PhaseLog{}};
+            launchSellPcg(ctx, args);
+        } else {
+            launchPersistentPcg(ctx, A, view, jacobi_diag, b, x, m.r.data(), m.z.data(), m.p.data(), m.v.data(),
+                                m.q.data(), m.partial.data(), m.pst.data());
+        }
         BSG_CUDA(cudaMemcpyAsync(ctx.pinned, m.pst.data(), sizeof(PcgState), cudaMemcpyDeviceToHost, ctx.stream));
         ctx.sync();
         PcgState r;
@@ -570,9 +583,14 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
         if (ctx.profiling || trace_solves()) {
             // algorithmic bytes of this launch: initial residual, preconditioner
             // applications and per-iteration SpMV + vector updates
-            const double N = n, M0 = 8.0 * N + 4.0 * (N + 1) + 12.0 * static_cast<double>(A.nnz_off);
+            const double N = n;
+            // the SELL solver streams the padded level-0 slices; the CSR solver the CSR arrays
+            const double M0 = amg ? 8.0 * N + 4.0 * (amg->krylovMatrix().nslices + 1) +
+                                        12.0 * static_cast<double>(amg->krylovEntries())
+                                  : 8.0 * N + 4.0 * (N + 1) + 12.0 * static_cast<double>(A.nnz_off);
             const double init = h.warm ? M0 + 32.0 * N : 24.0 * N;
-            const double pre = amg ? amg->vcycleBytes() : (jacobi_diag ? 32.0 * N : 24.0 * N);
+            const double pre = amg ? amg->sellVcycleBytes() + (amg->fp32VCycle() ? 8.0 : 16.0) * N
+                                   : (jacobi_diag ? 32.0 * N : 24.0 * N);
             const double it = r.iterations;
             const double applications = (r.iterations == 0 && r.status == 0) ? 0.0 : std::max(1.0, it);
             const double bytes = init + applications * pre + it * (M0 + 80.0 * N);

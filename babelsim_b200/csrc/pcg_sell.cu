@@ -1,0 +1,373 @@
+// Persistent cooperative PCG + AMG V-cycle on SELL-32 levels (see pcg_sell.cuh).
+#include <cooperative_groups.h>
+
+#include "pcg_sell.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace cg = cooperative_groups;
+
+namespace bsg {
+namespace {
+
+constexpr int SB = 256;  // threads per block
+
+struct Lanes {
+    int lane, gwarp, nwarps, gthread, nthreads;
+};
+
+__device__ __forceinline__ Lanes lanes() {
+    Lanes c;
+    c.gthread = blockIdx.x * SB + threadIdx.x;
+    c.nthreads = gridDim.x * SB;
+    c.lane = threadIdx.x & 31;
+    c.gwarp = c.gthread >> 5;
+    c.nwarps = c.nthreads >> 5;
+    return c;
+}
+
+// Deterministic grid sum of NV values (FP64); every block returns the same
+// totals.  `buf` alternates between two halves of `partial` so a fast block's
+// next write never overtakes a slow block's read of the previous sum.
+template <int NV>
+__device__ void gridSum(cg::grid_group& g, double v[NV], double* partial, int& buf) {
+    __shared__ double sh[NV][SB / 32];
+    __shared__ double tot[NV];
+    double* part = partial + static_cast<long long>(buf) * gridDim.x * NV;
+    buf ^= 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = v[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[j][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double s = 0.0;
+            for (int w = 0; w < SB / 32; ++w) s += sh[j][w];
+            part[blockIdx.x * NV + j] = s;
+        }
+    }
+    g.sync();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += SB) x += part[b * NV + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[j][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double s = 0.0;
+            for (int w = 0; w < SB / 32; ++w) s += sh[j][w];
+            tot[j] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = tot[j];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void mark(const PhaseLog& log, int id) {
+    if (log.entries && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int k = *log.count;
+        if (k < log.capacity) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            log.entries[2 * k] = id;
+            log.entries[2 * k + 1] = static_cast<long long>(t);
+            *log.count = k + 1;
+        }
+    }
+}
+
+// Final value v of row i on level l: level 0 writes z and returns r_i z_i;
+// coarser levels push gamma v into their members' iterate on the finer level
+// `fin` (level l - 1).
+template <class TK, class TV>
+__device__ __forceinline__ double emitRow(const VCycleView<TV>& V, const VLevel<TV>& fin, int l, int i, TV v,
+                                          const TK* r, TK* z) {
+    if (l == 0) {
+        const TK zi = static_cast<TK>(v);
+        z[i] = zi;
+        return static_cast<double>(r[i]) * static_cast<double>(zi);
+    }
+    const TV* from = V.nu >= 2 ? fin.x : fin.w;
+    const TV add = V.gamma * v;
+    for (int m = fin.agg_ptr[i]; m < fin.agg_ptr[i + 1]; ++m) {
+        const int ii = fin.agg_rows[m];
+        fin.x[ii] = from[ii] + add;
+    }
+    return 0.0;
+}
+
+// z = M r with M the V-cycle; returns this thread's share of r.z.  Level 0's b
+// and w were written by the phase that produced r.
+template <class TK, class TV>
+__device__ double vcycle(cg::grid_group& g, const VCycleView<TV>& V, const TK* r, TK* z, const PhaseLog& log) {
+    const Lanes c = lanes();
+    const int L = V.levels;
+    // ---- down
+    for (int l = 0; l < L - 1; ++l) {
+        const VLevel<TV> f = V.lv[l];
+        if (V.nu >= 2) {
+            for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+                const int i = 32 * s + c.lane;
+                const TV* w = f.w;
+                const TV aw = sellRow(f.A, s, c.lane, [&](int j) { return w[j]; });
+                if (i < f.A.n) {
+                    const TV wi = w[i];
+                    f.x[i] = wi + f.rd[i] * (f.b[i] - (f.A.diag[i] * wi + aw));
+                }
+            }
+            g.sync();
+            mark(log, 10 + l);
+        }
+        const TV* xs = V.nu >= 2 ? f.x : f.w;
+        for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+            const int i = 32 * s + c.lane;
+            const TV ax = sellRow(f.A, s, c.lane, [&](int j) { return xs[j]; });
+            if (i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
+        }
+        g.sync();
+        mark(log, 30 + l);
+        const VLevel<TV> cl = V.lv[l + 1];
+        for (int I = c.gthread; I < cl.A.n; I += c.nthreads) {
+            TV s = TV(0);
+            for (int m = f.agg_ptr[I]; m < f.agg_ptr[I + 1]; ++m) s += f.t[f.agg_rows[m]];
+            cl.b[I] = s;
+            cl.w[I] = cl.rd[I] * s;
+        }
+        g.sync();
+        mark(log, 100 + l);
+    }
+    // ---- coarsest: dense inverse, one warp per row, pushed into the finer level
+    double rz = 0.0;
+    {
+        const VLevel<TV> cl = V.lv[L - 1];
+        const int n = cl.A.n;
+        const TV* b = cl.b;
+        for (int I = c.gwarp; I < n; I += c.nwarps) {
+            const TV* row = V.dense_inv + static_cast<long long>(I) * n;
+            TV s = TV(0);
+            for (int J = c.lane; J < n; J += 32) s += row[J] * b[J];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (L == 1) {
+                if (c.lane == 0) rz += emitRow<TK, TV>(V, cl, 0, I, s, r, z);
+            } else {
+                const VLevel<TV> f = V.lv[L - 2];
+                const TV* from = V.nu >= 2 ? f.x : f.w;
+                const TV add = V.gamma * s;
+                for (int m = f.agg_ptr[I] + c.lane; m < f.agg_ptr[I + 1]; m += 32) {
+                    const int ii = f.agg_rows[m];
+                    f.x[ii] = from[ii] + add;
+                }
+            }
+        }
+        if (L > 1) {
+            g.sync();
+            mark(log, 50);
+        }
+    }
+    // ---- up
+    for (int l = L - 2; l >= 0; --l) {
+        const VLevel<TV> f = V.lv[l];
+        const VLevel<TV> fin = l > 0 ? V.lv[l - 1] : f;
+        const bool single = V.nu < 2;
+        const TV* y = f.x;
+        for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+            const int i = 32 * s + c.lane;
+            const TV ay = sellRow(f.A, s, c.lane, [&](int j) { return y[j]; });
+            if (i < f.A.n) {
+                const TV yi = y[i];
+                const TV v = yi + f.rd[i] * (f.b[i] - (f.A.diag[i] * yi + ay));
+                if (single) rz += emitRow<TK, TV>(V, fin, l, i, v, r, z);
+                else f.t[i] = v;
+            }
+        }
+        if (!single) {
+            g.sync();
+            mark(log, 60 + l);
+            const TV* t = f.t;
+            for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+                const int i = 32 * s + c.lane;
+                const TV at = sellRow(f.A, s, c.lane, [&](int j) { return t[j]; });
+                if (i < f.A.n) {
+                    const TV ti = t[i];
+                    rz += emitRow<TK, TV>(V, fin, l, i, ti + f.rd[i] * (f.b[i] - (f.A.diag[i] * ti + at)), r, z);
+                }
+            }
+        }
+        if (l > 0) {
+            g.sync();
+            mark(log, 80 + l);
+        }
+    }
+    return rz;
+}
+
+// Level-0 V-cycle inputs from the current residual value of row i.
+template <class TK, class TV>
+__device__ __forceinline__ void seedLevel0(const VLevel<TV>& f0, int i, TK ri) {
+    const TV rv = static_cast<TV>(ri);
+    f0.b[i] = rv;
+    f0.w[i] = f0.rd[i] * rv;
+}
+
+template <class TK, class TV>
+__global__ void __launch_bounds__(SB, 4) kPcgSell(SellPcgArgs<TK, TV> a) {
+    cg::grid_group g = cg::this_grid();
+    const Lanes c = lanes();
+    const SellMat<TK>& A = a.A;
+    const int n = A.n;
+    int buf = 0;
+    PcgState& st = *a.st;
+    const int warm = st.warm;
+    const int max_iterations = st.max_iterations;
+    const double target2_in = st.target2, atol = st.atol, rtol = st.rtol;
+    const VLevel<TV> f0 = a.V.lv[0];
+    // r = b - A x (x = 0 unless warm), ||r0||^2, ||b||^2, level-0 V-cycle inputs
+    double v[2] = {0.0, 0.0};
+    for (int s = c.gwarp; s < A.nslices; s += c.nwarps) {
+        const int i = 32 * s + c.lane;
+        TK ri = TK(0);
+        if (warm) {
+            const TK* x = a.x;
+            const TK ax = sellRow(A, s, c.lane, [&](int j) { return x[j]; });
+            if (i < n) ri = a.b[i] - (A.diag[i] * x[i] + ax);
+        } else if (i < n) {
+            ri = a.b[i];
+            a.x[i] = TK(0);
+        }
+        if (i < n) {
+            a.r[i] = ri;
+            seedLevel0<TK, TV>(f0, i, ri);
+            v[0] += static_cast<double>(ri) * static_cast<double>(ri);
+            v[1] += static_cast<double>(a.b[i]) * static_cast<double>(a.b[i]);
+        }
+    }
+    gridSum<2>(g, v, a.partial, buf);
+    mark(a.log, 1);
+    double target2 = target2_in;
+    if (target2 < 0.0) {
+        // the reference's contract: max(atol, rtol * max(||r0||, ||b||)) (solver_control.h:199-210)
+        double scale = fmax(sqrt(v[0]), sqrt(v[1]));
+        if (!(scale > 0.0)) scale = 1.0;
+        const double t = fmax(atol, rtol * scale);
+        target2 = t * t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st.rr0 = v[0];
+        st.bb = v[1];
+        st.target2 = target2;
+        st.rr = v[0];
+        st.iterations = 0;
+        st.status = 1;
+    }
+    if (isfinite(v[0]) && v[0] <= target2) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st.status = 0;
+        return;
+    }
+    double w[1] = {vcycle<TK, TV>(g, a.V, a.r, a.z, a.log)};
+    gridSum<1>(g, w, a.partial, buf);
+    mark(a.log, 4);
+    double rz = w[0];
+    double beta = 0.0;
+    TK* pold = a.p0;
+    TK* pnew = a.p1;
+    int it = 0;
+    int status = 1;
+    double rr = v[0];
+    while (it < max_iterations) {
+        if (!isfinite(rz) || rz == 0.0) { status = 2; break; }
+        // p_new = z + beta p_old and q = A p_new in one sweep (neighbours' p_new formed on the fly)
+        const TK bk = static_cast<TK>(beta);
+        const TK* zz = a.z;
+        const TK* po = pold;
+        double pq[1] = {0.0};
+        for (int s = c.gwarp; s < A.nslices; s += c.nwarps) {
+            const int i = 32 * s + c.lane;
+            const TK ap = beta == 0.0 ? sellRow(A, s, c.lane, [&](int j) { return zz[j]; })
+                                      : sellRow(A, s, c.lane, [&](int j) { return zz[j] + bk * po[j]; });
+            if (i < n) {
+                const TK pi = beta == 0.0 ? zz[i] : zz[i] + bk * po[i];
+                const TK qi = A.diag[i] * pi + ap;
+                pnew[i] = pi;
+                a.q[i] = qi;
+                pq[0] += static_cast<double>(pi) * static_cast<double>(qi);
+            }
+        }
+        gridSum<1>(g, pq, a.partial, buf);
+        mark(a.log, 2);
+        if (!(fabs(pq[0]) > 0.0) || !isfinite(pq[0])) { status = 2; break; }
+        const double alpha = rz / pq[0];
+        const TK ak = static_cast<TK>(alpha);
+        double nr[1] = {0.0};
+        for (int i = c.gthread; i < n; i += c.nthreads) {
+            a.x[i] += ak * pnew[i];
+            const TK ri = a.r[i] - ak * a.q[i];
+            a.r[i] = ri;
+            seedLevel0<TK, TV>(f0, i, ri);
+            nr[0] += static_cast<double>(ri) * static_cast<double>(ri);
+        }
+        gridSum<1>(g, nr, a.partial, buf);
+        mark(a.log, 3);
+        rr = nr[0];
+        ++it;
+        if (!isfinite(rr)) { status = 2; break; }
+        if (rr <= target2) { status = 0; break; }
+        if (it >= max_iterations) break;
+        double zr[1] = {vcycle<TK, TV>(g, a.V, a.r, a.z, a.log)};
+        gridSum<1>(g, zr, a.partial, buf);
+        mark(a.log, 4);
+        beta = zr[0] / rz;
+        rz = zr[0];
+        TK* tmp = pold;
+        pold = pnew;
+        pnew = tmp;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st.rr = rr;
+        st.iterations = it;
+        st.status = status;
+    }
+}
+
+template <class TK, class TV>
+int sellGrid(Context& ctx) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kPcgSell<TK, TV>, SB, 0));
+        if (per_sm <= 0) fail(kCuda, "persistent SELL PCG kernel cannot be resident");
+    }
+    return ctx.sm_count * std::min(per_sm, 8);
+}
+
+}  // namespace
+
+template <class TK, class TV>
+void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& in) {
+    SellPcgArgs<TK, TV> args = in;
+    args.log = PhaseLog{ctx.phase_entries, ctx.phase_capacity, ctx.phase_count};
+    void* params[] = {&args};
+    const int grid = sellGrid<TK, TV>(ctx);
+    BSG_PROFILE(ctx, "pcg_amg_persistent");
+    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgSell<TK, TV>), grid, SB, params, 0, ctx.stream));
+    ctx.launched();
+}
+
+template void launchSellPcg<double, double>(Context&, const SellPcgArgs<double, double>&);
+template void launchSellPcg<double, float>(Context&, const SellPcgArgs<double, float>&);
+template void launchSellPcg<float, float>(Context&, const SellPcgArgs<float, float>&);
+
+}  // namespace bsg
