@@ -28,7 +28,7 @@ struct AmgPreconditioner::Level {
     // work vectors
     DeviceArray<double> x, b, t;
     // coarsest level
-    DeviceArray<double> dense;           // n x 2n augmented matrix, inverse in the right half
+    DeviceArray<double> dense;           // coarsest level: n x n inverse, row-major
     // SELL-32 copies for the persistent solver (pcg_sell.cuh)
     int nslices = 0;
     long long sell_entries = 0;
@@ -141,53 +141,52 @@ __global__ void kGalerkin(int nc, const int* __restrict__ agg_ptr, const int* __
     }
 }
 
-// Dense [A | I] of the coarsest level, then in-place Gauss-Jordan (one block).
-__global__ void kDenseInvert(int n, const int* __restrict__ ptr, const int* __restrict__ col,
-                             const double* __restrict__ diag, const double* __restrict__ val, double* __restrict__ M) {
-    const int w = 2 * n;
-    for (int e = threadIdx.x; e < n * w; e += blockDim.x) M[e] = 0.0;
+// In-place Gauss-Jordan inverse of the coarsest matrix (SPD, so no pivoting),
+// one block; each step stages the pivot row and column in shared memory and
+// every thread updates its share of the n x n entries.
+__global__ void kDenseInverse(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+                              const double* __restrict__ diag, const double* __restrict__ val, double* __restrict__ M) {
+    extern __shared__ double sh[];
+    double* prow = sh;
+    double* pcol = sh + n;
+    const int nn = n * n;
+    for (int e = threadIdx.x; e < nn; e += blockDim.x) M[e] = 0.0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        M[i * w + i] = diag[i];
-        M[i * w + n + i] = 1.0;
-        for (int k = ptr[i]; k < ptr[i + 1]; ++k) M[i * w + col[k]] += val[k];
+        M[static_cast<long long>(i) * n + i] = diag[i];
+        for (int k = ptr[i]; k < ptr[i + 1]; ++k) M[static_cast<long long>(i) * n + col[k]] += val[k];
     }
     __syncthreads();
-    __shared__ double piv;
     for (int k = 0; k < n; ++k) {
-        if (threadIdx.x == 0) piv = 1.0 / M[k * w + k];
-        __syncthreads();
-        for (int j = threadIdx.x; j < w; j += blockDim.x) M[k * w + j] *= piv;
-        __syncthreads();
-        for (int e = threadIdx.x; e < n * w; e += blockDim.x) {
-            const int i = e / w, j = e % w;
-            if (i == k) continue;
-            const double f = M[i * w + k];
-            if (j != k && f != 0.0) M[e] -= f * M[k * w + j];
+        const double p = 1.0 / M[static_cast<long long>(k) * n + k];
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            prow[j] = M[static_cast<long long>(k) * n + j];
+            pcol[j] = M[static_cast<long long>(j) * n + k];
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
-            if (i != k) M[i * w + k] = 0.0;
+        for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+            const int i = e / n, j = e - i * n;
+            double v;
+            if (i == k) v = j == k ? p : prow[j] * p;
+            else if (j == k) v = -pcol[i] * p;
+            else v = M[e] - pcol[i] * prow[j] * p;
+            M[e] = v;
+        }
         __syncthreads();
     }
 }
 
-__global__ void kDenseSolve(int n, const double* __restrict__ M, const double* __restrict__ b, double* __restrict__ x) {
-    const int w = 2 * n;
+__global__ void kDenseSolve(int n, const double* __restrict__ Minv, const double* __restrict__ b, double* __restrict__ x) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = 0.0;
-        for (int j = 0; j < n; ++j) s += M[i * w + n + j] * b[j];
+        for (int j = 0; j < n; ++j) s += Minv[static_cast<long long>(i) * n + j] * b[j];
         x[i] = s;
     }
 }
 
-// Compact n x n copy (row-major, converted to T) of the inverse half of the augmented [A | A^-1].
-template <class T>
-__global__ void kDenseCompact(int n, const double* __restrict__ M, T* __restrict__ out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n * n) return;
-    const int i = e / n, j = e % n;
-    out[e] = static_cast<T>(M[static_cast<long long>(i) * 2 * n + n + j]);
+__global__ void kToFloat(long long n, const double* __restrict__ a, float* __restrict__ out) {
+    const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (e < n) out[e] = static_cast<float>(a[e]);
 }
 
 // x = omega D^-1 b (first Jacobi sweep from a zero guess)
@@ -299,7 +298,8 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
         for (int i = 0; i < cur.n; ++i) agg[i] = a2[a1[i]];
         // stop when coarsening stalls (< 1.5x fewer rows): such levels cost a
         // V-cycle their barriers and gathers without shrinking the problem
-        if (3 * static_cast<long long>(n2) > 2 * static_cast<long long>(cur.n)) break;
+        if (3 * static_cast<long long>(n2) > 2 * static_cast<long long>(cur.n) && cur.n <= 1024) break;
+        if (n2 >= cur.n) break;  // no coarsening possible
         std::vector<int> target;
         HostCsr next = coarsen(cur, agg, n2, &target);
         Level* fine = levels_.back();
@@ -376,10 +376,12 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
         }
     }
     Level* last = levels_.back();
-    last->dense.resize(2 * static_cast<std::size_t>(last->n) * last->n);
+    if (last->n > 2048)
+        fail(kState, "AMG coarsening stalled at " + std::to_string(last->n) +
+                         " rows, too many for the dense coarsest solve");
     const std::size_t nn = static_cast<std::size_t>(last->n) * last->n;
+    last->dense.resize(nn);
     if (fp32_) dense32_.resize(nn);
-    else dense64_.resize(nn);
     built_ = true;
     if (std::getenv("BSG_AMG_VERBOSE")) {
         long long total = 0;
@@ -418,15 +420,16 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
         ctx_.launched();
     }
     Level* last = levels_.back();
-    kDenseInvert<<<1, 1024, 0, ctx_.stream>>>(last->n, last->dptr, last->dcol, last->ddiag, last->dval,
-                                              last->dense.data());
+    kDenseInverse<<<1, 1024, 2 * sizeof(double) * last->n, ctx_.stream>>>(last->n, last->dptr, last->dcol, last->ddiag,
+                                                                         last->dval, last->dense.data());
     ctx_.launched();
     BSG_CUDA(cudaGetLastError());
     // SELL-32 values for the persistent solver
     const int nn = last->n * last->n;
-    if (fp32_) kDenseCompact<float><<<gridFor(nn, kBlock), kBlock, 0, ctx_.stream>>>(last->n, last->dense.data(), dense32_.data());
-    else kDenseCompact<double><<<gridFor(nn, kBlock), kBlock, 0, ctx_.stream>>>(last->n, last->dense.data(), dense64_.data());
-    ctx_.launched();
+    if (fp32_) {
+        kToFloat<<<gridFor(nn, kBlock), kBlock, 0, ctx_.stream>>>(nn, last->dense.data(), dense32_.data());
+        ctx_.launched();
+    }
     for (std::size_t li = 0; li < levels_.size(); ++li) {
         Level* l = levels_[li];
         const unsigned g = gridFor(l->n, kBlock);
@@ -503,7 +506,7 @@ VCycleView<double> AmgPreconditioner::sellView64() const {
     v.nu = std::max(1, std::min(2, cfg_.amg_smoothing_steps));
     v.gamma = gamma_;
     v.lv = d_vl64_.data();
-    v.dense_inv = dense64_.data();
+    v.dense_inv = levels_.back()->dense.data();
     return v;
 }
 
@@ -546,8 +549,8 @@ AmgView<double> AmgPreconditioner::deviceView() const {
     v.gamma = gamma_;
     v.lv = d_views_.data();
     const Level* last = levels_.back();
-    v.dense_inv = last->dense.data() + last->n;
-    v.dense_ld = 2 * last->n;
+    v.dense_inv = last->dense.data();
+    v.dense_ld = last->n;
     return v;
 }
 

@@ -59,7 +59,6 @@ private:
     bool fp32_ = false;
     DeviceArray<VLevel<double>> d_vl64_;
     DeviceArray<VLevel<float>> d_vl32_;
-    DeviceArray<double> dense64_;
     DeviceArray<float> dense32_;
     // Damped-Jacobi weight and coarse-correction scale.  Piecewise-constant
     // aggregation under-corrects smooth error; scaling the coarse correction by

@@ -166,6 +166,8 @@ struct DeviceMesh {
     std::vector<int> face_kind;          // per external face: 0 interior, 1 boundary
     std::vector<int> face_slot;          // per external face: index in interior or boundary list
     std::vector<int> interior_ext, boundary_ext;
+    DeviceArray<int> face_perm;          // caller face -> internal position (interior faces first)
+    DeviceArray<double> face_stage;      // staging for face fields crossing the ABI
     // host copies kept for setup work (AMG aggregation, exports)
     std::vector<int> h_own, h_nbr, h_cf_ptr, h_cf_col, h_cf_face, h_bown, h_cb_ptr;
     std::vector<double> h_dcoef;

@@ -684,6 +684,19 @@ __global__ void kAdd(long long n, double* __restrict__ out, const double* __rest
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i < n) out[i] = a[i] + b[i];
 }
+// Face reordering between the caller's numbering and the internal one:
+// to_internal: out[perm[f]] = in[f]; otherwise out[f] = in[perm[f]] (C values per face).
+__global__ void kPermuteFaces(int nf, int C, const int* __restrict__ perm, const double* __restrict__ in,
+                              double* __restrict__ out, int to_internal) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const long long t = perm[f];
+    for (int c = 0; c < C; ++c) {
+        if (to_internal) out[C * t + c] = in[static_cast<long long>(C) * f + c];
+        else out[static_cast<long long>(C) * f + c] = in[C * t + c];
+    }
+}
+
 // out = b - out (residual after out = A x)
 __global__ void kResidualFrom(long long n, const double* __restrict__ b, double* __restrict__ out) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
@@ -739,34 +752,35 @@ BcView DeviceField::bcView() {
 
 void DeviceField::uploadExternal(const double* host) {
     const int C = comps;
+    Context& ctx = *mesh->ctx;
     if (location == 0) {
-        v.upload(host, static_cast<std::size_t>(mesh->n_cells) * C, mesh->ctx->stream);
-        mesh->ctx->sync();
+        v.upload(host, static_cast<std::size_t>(mesh->n_cells) * C, ctx.stream);
+        ctx.sync();
         return;
     }
-    std::vector<double> tmp(static_cast<std::size_t>(mesh->n_faces) * C);
-    for (int f = 0; f < mesh->n_faces; ++f) {
-        const int t = mesh->face_kind[f] == 0 ? mesh->face_slot[f] : mesh->n_interior + mesh->face_slot[f];
-        for (int c = 0; c < C; ++c) tmp[static_cast<std::size_t>(C) * t + c] = host[static_cast<std::size_t>(C) * f + c];
-    }
-    v.upload(tmp, mesh->ctx->stream);
-    mesh->ctx->sync();
+    // copy in caller order, then scatter to the internal face order on the device
+    const std::size_t n = static_cast<std::size_t>(mesh->n_faces) * C;
+    if (mesh->face_stage.size() < n) mesh->face_stage.resize(n);
+    if (n) BSG_CUDA(cudaMemcpyAsync(mesh->face_stage.data(), host, n * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+    launch(ctx, kPermuteFaces, mesh->n_faces, mesh->n_faces, C, (const int*)mesh->face_perm.data(),
+           (const double*)mesh->face_stage.data(), v.data(), 1);
+    ctx.sync();
 }
 
 void DeviceField::downloadExternal(double* host) const {
     const int C = comps;
+    Context& ctx = *mesh->ctx;
     if (location == 0) {
-        v.download(host, mesh->ctx->stream);
-        mesh->ctx->sync();
+        v.download(host, ctx.stream);
+        ctx.sync();
         return;
     }
-    std::vector<double> tmp(static_cast<std::size_t>(mesh->n_faces) * C);
-    v.download(tmp.data(), mesh->ctx->stream);
-    mesh->ctx->sync();
-    for (int f = 0; f < mesh->n_faces; ++f) {
-        const int t = mesh->face_kind[f] == 0 ? mesh->face_slot[f] : mesh->n_interior + mesh->face_slot[f];
-        for (int c = 0; c < C; ++c) host[static_cast<std::size_t>(C) * f + c] = tmp[static_cast<std::size_t>(C) * t + c];
-    }
+    const std::size_t n = static_cast<std::size_t>(mesh->n_faces) * C;
+    if (mesh->face_stage.size() < n) mesh->face_stage.resize(n);
+    launch(ctx, kPermuteFaces, mesh->n_faces, mesh->n_faces, C, (const int*)mesh->face_perm.data(),
+           (const double*)v.data(), mesh->face_stage.data(), 0);
+    if (n) BSG_CUDA(cudaMemcpyAsync(host, mesh->face_stage.data(), n * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
 }
 
 void DeviceField::setFluxContext(const DeviceField& face_flux) {

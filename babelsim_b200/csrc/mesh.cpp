@@ -329,6 +329,12 @@ std::unique_ptr<DeviceMesh> buildDeviceMesh(Context& ctx, const HostGeometry& g)
     m->face_slot.assign(F, 0);
     for (int i = 0; i < Fi; ++i) { m->face_kind[m->interior_ext[i]] = 0; m->face_slot[m->interior_ext[i]] = i; }
     for (int i = 0; i < Fb; ++i) { m->face_kind[m->boundary_ext[i]] = 1; m->face_slot[m->boundary_ext[i]] = i; }
+    {
+        // caller face -> internal face position (interior first), for device-side reordering
+        std::vector<int> perm(F);
+        for (int f = 0; f < F; ++f) perm[f] = m->face_kind[f] == 0 ? m->face_slot[f] : Fi + m->face_slot[f];
+        m->face_perm.upload(perm, ctx.stream);
+    }
 
     auto gather1 = [](const std::vector<double>& a, const std::vector<int>& idx) {
         std::vector<double> o(idx.size());

@@ -136,7 +136,10 @@ def algorithmic_bytes(name, N, nnz_off, amg_rows):
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte,
 # measured by one capture of the kernel on this workload (profiles/ summaries).
-DRAM_PER_ALGORITHMIC_BYTE = {}
+# kPcgSell, first pressure solve of the 1M-cell Voronoi cavity (33 CG iterations):
+# 35.69 GB of DRAM traffic for 37.34 GB of algorithmic bytes
+# (profiles/kPcgSell_simple_1M_voronoi.md).
+DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.956}
 
 
 def load_peaks():
