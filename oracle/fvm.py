@@ -566,10 +566,10 @@ def eq_div(eq: Equation, phi, factor=1.0, term=None):
 
 
 def eq_laplacian(eq: Equation, k, factor, term=None):
-    """equ::laplacian with a cell or face coefficient (procedural_equation.cpp:149-176).
+    """equ::laplacian with a cell or face coefficient (procedural_equation.cpp:130-176).
 
     ``k`` is a Field (cell coefficient, interpolated with the coefficient
-    options) or a float (constant coefficient).
+    options), an array of face values (used as given) or a float (constant).
     """
     m = eq.opts(term)
     x = eq.x
@@ -577,6 +577,8 @@ def eq_laplacian(eq: Equation, k, factor, term=None):
     if isinstance(k, Field):
         kf = interpolate(k, m.get("coefficientInterpolation") or m["interpolation"],
                          m.get("coefficientGradient") or m["gradient"])
+    elif isinstance(k, np.ndarray):
+        kf = np.array(k, dtype=np.float64)   # a face coefficient is used as given
     else:
         kf = np.full(geo.n_faces, float(k))
     contrib = LDU(geo, x.vector)

@@ -42,23 +42,24 @@ def vec(v):
     return f"({v[0]!r} {v[1]!r} {v[2]!r})"
 
 
-def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics):
+def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics, solver="simple", time="steady",
+               control=(0.0, 0.0, 1.0)):
     os.makedirs(os.path.join(path, "mesh"), exist_ok=True)
     os.makedirs(os.path.join(path, "fields", "initial"), exist_ok=True)
     os.makedirs(os.path.join(path, "numerics"), exist_ok=True)
     os.makedirs(os.path.join(path, "physics"), exist_ok=True)
     meshgen.write_mesh(os.path.join(path, "mesh", "case.mesh"), mesh)
     with open(os.path.join(path, "case.bs"), "w") as f:
-        f.write("solver simple\nmesh mesh/case.mesh\nfields fields/initial\nphysics physics/simple.bs\n"
+        f.write(f"solver {solver}\nmesh mesh/case.mesh\nfields fields/initial\nphysics physics/simple.bs\n"
                 "methods numerics/methods.bs\nsolution numerics/solution.bs\ncontrol control.bs\noutput output.bs\n")
     with open(os.path.join(path, "control.bs"), "w") as f:
-        f.write("startTime 0\nendTime 0\ndeltaT 1\n")
+        f.write("startTime %r\nendTime %r\ndeltaT %r\n" % tuple(control))
     with open(os.path.join(path, "output.bs"), "w") as f:
         f.write("directory results\ntimeName final\n")
     with open(os.path.join(path, "physics", "simple.bs"), "w") as f:
         f.write("".join(f"{k} {v!r}\n" for k, v in physics.items()))
     with open(os.path.join(path, "numerics", "methods.bs"), "w") as f:
-        f.write("time steady\n")
+        f.write(f"time {time}\n")
         for eq, opts in methods.items():
             for k, v in opts.items():
                 f.write(f"equation.{eq}.{k} {v}\n")
@@ -161,6 +162,61 @@ def methods(conv="upwind", grad="greenGauss", diff="orthogonal"):
     return {"momentum": o, "pressureCorrection": o}
 
 
+def make_piso(name, mesh, U_bcs, p_bcs, methods, solution, physics, time, start, dt, ends):
+    """Transient fixture: the reference's runPiso to each end time in `ends` (one run per step)."""
+    work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
+    data = {}
+    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    data["mesh_vertices"] = mesh.vertices
+    data["mesh_offsets"] = offsets
+    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
+    for k, end in enumerate(ends, start=1):
+        write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics, solver="piso", time=time,
+                   control=(start, end, dt))
+        fields, geo, info, _ = run(work, solution.get("maxIterations", 1))
+        if info["status"] != 0:
+            raise RuntimeError(f"{name}: reference PISO did not complete step {k}: {info}")
+        data[f"U_{k}"] = fields["U"].reshape(-1, 3)
+        data[f"p_{k}"] = fields["p"]
+        data[f"phi_{k}"] = fields["phi"]
+    for key, arr in geo.items():
+        data["geo_" + key] = arr
+    meta = dict(patch_names=mesh.patch_names, patch_kinds=mesh.patch_kinds, U_bcs=[(t, list(map(float, v)))
+                for t, v in U_bcs], p_bcs=[(t, float(v)) for t, v in p_bcs], methods=methods,
+                solution=solution, physics=physics, K=len(ends), time=time, start=start, dt=dt, ends=list(ends))
+    data["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
+    shutil.rmtree(work)
+    print(name, "written", len(ends), "steps")
+
+
+def piso_solution(n_correctors=2, non_orth=1, p_rtol=1e-12):
+    return {"maxIterations": 1, "nCorrectors": n_correctors, "nonOrthogonalCorrections": non_orth,
+            "velocityRelaxation": 1.0, "continuityTolerance": 1e-7, "velocityTolerance": 1e-7,
+            "momentumTolerance": 1e-6, "pressureCorrectionTolerance": 1e-7,
+            "equation.momentum.kspType": "bcgs", "equation.momentum.pcType": "bjacobi",
+            "equation.momentum.absoluteTolerance": 1e-15, "equation.momentum.relativeTolerance": 1e-12,
+            "equation.momentum.maxIterations": 2000,
+            "equation.pressureCorrection.kspType": "cg", "equation.pressureCorrection.pcType": "hypre",
+            "equation.pressureCorrection.absoluteTolerance": 1e-15,
+            "equation.pressureCorrection.relativeTolerance": p_rtol,
+            "equation.pressureCorrection.maxIterations": 20000}
+
+
+def main_piso():
+    U, p = cavity_bcs()
+    # BDF2 lid cavity, 6 steps, the last one shortened (variable-step BDF2 weights)
+    make_piso("piso_cavity12_bdf2", meshgen.cavity_2d(12), U, p, methods("linearUpwind"), piso_solution(2, 1),
+              {"density": 1.0, "dynamicViscosity": 0.01}, "bdf2", 0.0, 0.05, [0.05, 0.1, 0.15, 0.2, 0.25, 0.27])
+    # warped box, least squares + corrected diffusion, Euler, 3 correctors
+    Uw = [("fixedValue", (0.0, 0.0, 0.0))] * 3 + [("fixedValue", (1.0, 0.0, 0.0))] + [("fixedValue", (0.0, 0.0, 0.0))] * 2
+    pw = [("zeroGradient", 0.0)] * 6
+    make_piso("piso_warped5_euler", meshgen.warped_box(5), Uw, pw, methods("linearUpwind", "leastSquares", "corrected"),
+              piso_solution(3, 2), {"density": 1.0, "dynamicViscosity": 0.01}, "euler", 0.0, 0.02,
+              [0.02, 0.04, 0.06, 0.08])
+
+
 def main():
     if not os.path.exists(ORACLE):
         sys.exit(f"{ORACLE} missing: run `make -C oracle/ref` first")
@@ -180,4 +236,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "piso":
+        main_piso()
+    else:
+        main()
+        main_piso()

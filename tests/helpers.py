@@ -12,10 +12,11 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 from babelsim_b200 import meshgen  # noqa: E402
-from oracle import fvm, geometry, simple  # noqa: E402
+from oracle import fvm, geometry, piso, simple  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
+PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler"]
 GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
             "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",
             "face_skewness", "cell_centres", "cell_volumes", "orthogonal_geometry"]
@@ -91,3 +92,17 @@ def ref_system_groups(g: Golden):
         else:
             cur["pressure"].append(s)
     return groups
+
+
+def piso_settings(g: "Golden", end_time=None) -> piso.PisoSettings:
+    """PisoSettings of a transient fixture (the case written by tests/golden/make_golden.py)."""
+    sol, m, phys = g.meta["solution"], g.meta["methods"], g.meta["physics"]
+    return piso.PisoSettings(rho=phys["density"], mu=phys["dynamicViscosity"], alpha_u=sol["velocityRelaxation"],
+                             max_iterations=sol["maxIterations"], correctors=sol["nCorrectors"],
+                             non_orthogonal_corrections=sol["nonOrthogonalCorrections"],
+                             mass_tolerance=sol["continuityTolerance"], velocity_tolerance=sol["velocityTolerance"],
+                             momentum_tolerance=sol["momentumTolerance"],
+                             pressure_tolerance=sol["pressureCorrectionTolerance"], time=g.meta["time"],
+                             start_time=g.meta["start"], delta_t=g.meta["dt"],
+                             end_time=g.meta["ends"][-1] if end_time is None else end_time,
+                             momentum=m["momentum"], pressure=m["pressureCorrection"])

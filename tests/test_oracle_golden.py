@@ -9,7 +9,7 @@ solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
 import numpy as np
 import pytest
 
-from helpers import CASES, Golden, ref_system_groups, rel, rel_l2
+from helpers import CASES, PISO_CASES, Golden, piso_settings, ref_system_groups, rel, rel_l2
 from oracle import fvm, simple
 
 
@@ -104,3 +104,35 @@ def test_operators_known_answers():
     fvm.add_diffusion(eq, np.ones(geo.n_faces), quad, None, "orthogonal")
     lap = -(eq.apply(quad.v) - eq.source) / geo.volume   # -(A x - b) / V = laplacian
     assert abs(lap[centre] - 6.0) < 1e-12
+
+
+@pytest.mark.parametrize("name", PISO_CASES)
+def test_piso_steps_match_reference(name):
+    """The PISO restatement reproduces the reference's runPiso after every time step
+    (BDF2 with a shortened last step, and Euler with non-orthogonal correctors)."""
+    from oracle import piso
+    g = Golden(name)
+    geo = g.oracle_geometry()
+    st = piso.run_piso(geo, g.U_bcs(), g.p_bcs(), piso_settings(g), steps=1)
+    assert st.steps == 1
+    for k in range(1, g.K + 1):
+        st = piso.run_piso(geo, g.U_bcs(), g.p_bcs(), piso_settings(g, g.meta["ends"][k - 1]))
+        assert st.status == "completed" and st.steps == k
+        assert rel_l2(st.U, g[f"U_{k}"]) <= 1e-10, k
+        assert rel_l2(st.p, g[f"p_{k}"]) <= 1e-10, k
+        assert rel_l2(st.phi, g[f"phi_{k}"]) <= 1e-10, k
+
+
+def test_bdf2_weights_variable_step():
+    """Variable-step BDF2 weights (procedural_equation.cpp:205-214) reduce to the constant-step
+    1.5/2/-0.5 form and integrate a quadratic exactly."""
+    from oracle import piso
+    dt = 0.1
+    a0, a1, a2 = piso.time_weights("bdf2", dt, dt)
+    assert np.allclose([a0 * dt, a1 * dt, a2 * dt], [1.5, 2.0, -0.5])
+    # exactness on y(t) = t^2 with steps h1 (older) and h0 (current)
+    h1, h0 = 0.3, 0.12
+    a0, a1, a2 = piso.time_weights("bdf2", h0, h1)
+    t0 = 1.0
+    y = lambda t: t * t
+    assert abs(a0 * y(t0) - a1 * y(t0 - h0) - a2 * y(t0 - h0 - h1) - 2 * t0) < 1e-12
