@@ -30,7 +30,8 @@ EXPORTS = [
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
     "bsg_simple_iterate", "bsg_simple_get_fields",
-    "bsg_simple_destroy",
+    "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
+    "bsg_piso_get_fields", "bsg_piso_destroy",
 ]
 
 
@@ -81,6 +82,24 @@ class SimpleReport(C.Structure):
                 ("pressure_iterations", C.c_int32)]
 
 
+class PisoConfig(C.Structure):
+    _fields_ = [("density", C.c_double), ("viscosity", C.c_double), ("velocity_relaxation", C.c_double),
+                ("max_iterations", C.c_int32), ("correctors", C.c_int32), ("max_correctors", C.c_int32),
+                ("coupling_tolerance", C.c_double), ("non_orthogonal_corrections", C.c_int32),
+                ("continuity_tolerance", C.c_double), ("velocity_tolerance", C.c_double),
+                ("momentum_tolerance", C.c_double), ("pressure_correction_tolerance", C.c_double),
+                ("time_method", C.c_int32), ("start_time", C.c_double), ("end_time", C.c_double),
+                ("delta_t", C.c_double), ("momentum", Options), ("pressure", Options),
+                ("momentum_solver", SolverConfig), ("pressure_solver", SolverConfig)]
+
+
+class PisoReport(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("time", C.c_double), ("status", C.c_int32), ("accepted", C.c_int32),
+                ("mass", C.c_double), ("dU", C.c_double), ("rU", C.c_double), ("dP", C.c_double),
+                ("coupling", C.c_double), ("courant_max", C.c_double), ("courant_mean", C.c_double),
+                ("correctors", C.c_int32), ("momentum_iterations", C.c_int32), ("pressure_iterations", C.c_int32)]
+
+
 _lib = None
 
 
@@ -127,6 +146,10 @@ def lib():
             "bsg_simple_set_flux": [vp, vp],
             "bsg_simple_iterate": [vp, i32, C.POINTER(SimpleReport)], "bsg_simple_get_fields": [vp, vp, vp, vp],
             "bsg_simple_destroy": [vp],
+            "bsg_piso_create": [vp, C.POINTER(PisoConfig), pp],
+            "bsg_piso_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_piso_set_fields": [vp, vp, vp],
+            "bsg_piso_advance": [vp, i32, C.POINTER(PisoReport)], "bsg_piso_get_fields": [vp, vp, vp, vp],
+            "bsg_piso_destroy": [vp],
         }
         for name in EXPORTS:
             fn = getattr(L, name)

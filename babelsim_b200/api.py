@@ -10,8 +10,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (MeshGeometry, Options, SimpleConfig, SimpleReport, SolveResult, SolverConfig, check, f64, i32,
-                   lib, ptr)
+from ._lib import (MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
+                   check, f64, i32, lib, ptr)
 
 BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
 INTERP = {"linear": 0, "corrected": 1}
@@ -382,4 +382,49 @@ class Simple:
     def close(self):
         if self.h:
             lib().bsg_simple_destroy(self.h)
+            self.h = None
+
+
+class Piso:
+    """Transient PISO on the device (bsg_piso), piso/main.cpp:60-301."""
+
+    def __init__(self, mesh: Mesh, rho=1.0, mu=0.01, alpha_u=1.0, max_iterations=1, correctors=2,
+                 max_correctors=None, coupling_tolerance=None, non_orthogonal_corrections=1,
+                 continuity_tolerance=1e-8, velocity_tolerance=1e-7, momentum_tolerance=1e-6, pressure_tolerance=1e-6,
+                 time="bdf2", start_time=0.0, end_time=1.0, delta_t=1e-3, momentum=None, pressure=None,
+                 momentum_solver=None, pressure_solver=None):
+        self.mesh = mesh
+        cfg = PisoConfig(rho, mu, alpha_u, max_iterations, correctors, max_correctors or correctors,
+                         coupling_tolerance or 0.0, non_orthogonal_corrections, continuity_tolerance,
+                         velocity_tolerance, momentum_tolerance, pressure_tolerance,
+                         {"steady": 0, "euler": 1, "bdf2": 2}[time.lower()], start_time, end_time, delta_t,
+                         momentum or options(), pressure or options(),
+                         momentum_solver or solver_config("bcgs", "bjacobi", 1e-14, 1e-10),
+                         pressure_solver or solver_config("cg", "hypre", 1e-14, 1e-10, 5000))
+        h = C.c_void_p()
+        check(lib().bsg_piso_create(mesh.h, C.byref(cfg), C.byref(h)), mesh.ctx.h)
+        self.h = h
+
+    def set_boundary(self, field: str, patch: int, kind: str, value=0.0):
+        v = f64(np.broadcast_to(np.asarray(value, np.float64), (3,)) if np.ndim(value) == 0 else
+                np.pad(np.asarray(value, np.float64), (0, 3 - len(value))))
+        check(lib().bsg_piso_set_boundary(self.h, field.encode(), patch, BC[kind], ptr(v)), self.mesh.ctx.h)
+
+    def set_fields(self, U, p):
+        check(lib().bsg_piso_set_fields(self.h, ptr(f64(U)), ptr(f64(p))), self.mesh.ctx.h)
+
+    def advance(self, steps: int) -> PisoReport:
+        r = PisoReport()
+        check(lib().bsg_piso_advance(self.h, steps, C.byref(r)), self.mesh.ctx.h)
+        return r
+
+    def fields(self):
+        m = self.mesh
+        U, p, phi = np.zeros((m.n_cells, 3)), np.zeros(m.n_cells), np.zeros(m.n_faces)
+        check(lib().bsg_piso_get_fields(self.h, ptr(U), ptr(p), ptr(phi)), m.ctx.h)
+        return U, p, phi
+
+    def close(self):
+        if self.h:
+            lib().bsg_piso_destroy(self.h)
             self.h = None

@@ -4,6 +4,7 @@
 #include "amg.h"
 #include "fvm.h"
 #include "linalg.h"
+#include "piso.h"
 #include "simple.h"
 
 #include <algorithm>
@@ -34,6 +35,10 @@ struct bsg_equation {
 struct bsg_simple {
     bsg_mesh* mesh;
     std::unique_ptr<bsg::SimpleSolver> solver;
+};
+struct bsg_piso {
+    bsg_mesh* mesh;
+    std::unique_ptr<bsg::PisoSolver> solver;
 };
 
 namespace bsg {
@@ -870,6 +875,97 @@ int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi
 }
 
 int bsg_simple_destroy(bsg_simple* s) {
+    delete s;
+    return bsg::kOk;
+}
+
+int bsg_piso_create(bsg_mesh* mesh, const bsg_piso_config* c, bsg_piso** out) {
+    return guard(ctxOf(mesh), [&] {
+        require(mesh && c && out, "null argument");
+        bsg::PisoConfig cfg;
+        cfg.rho = c->density;
+        cfg.mu = c->viscosity;
+        cfg.alpha_u = c->velocity_relaxation;
+        cfg.max_iterations = c->max_iterations;
+        cfg.correctors = c->correctors;
+        cfg.max_correctors = c->max_correctors > 0 ? c->max_correctors : c->correctors;
+        cfg.coupling_tolerance = c->coupling_tolerance > 0 ? c->coupling_tolerance : 1.7976931348623157e308;
+        cfg.non_orthogonal_corrections = c->non_orthogonal_corrections;
+        cfg.mass_tolerance = c->continuity_tolerance;
+        cfg.velocity_tolerance = c->velocity_tolerance;
+        cfg.momentum_tolerance = c->momentum_tolerance;
+        cfg.pressure_tolerance = c->pressure_correction_tolerance;
+        cfg.time_method = c->time_method;
+        cfg.start_time = c->start_time;
+        cfg.end_time = c->end_time;
+        cfg.delta_t = c->delta_t;
+        cfg.momentum = options(&c->momentum);
+        cfg.pressure = options(&c->pressure);
+        cfg.momentum_solver = solverConfig(&c->momentum_solver);
+        cfg.pressure_solver = solverConfig(&c->pressure_solver);
+        auto* s = new bsg_piso{mesh, nullptr};
+        try {
+            s->solver = std::make_unique<bsg::PisoSolver>(*mesh->mesh, cfg);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int bsg_piso_set_boundary(bsg_piso* s, const char* field, int32_t patch, int32_t type, const double* value) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && field, "null argument");
+        const std::string n(field);
+        if (n == "U") s->solver->U().setBoundary(patch, type, value);
+        else if (n == "p") s->solver->p().setBoundary(patch, type, value);
+        else bsg::fail(bsg::kArgument, "PISO boundary field must be U or p");
+    });
+}
+
+int bsg_piso_set_fields(bsg_piso* s, const double* U, const double* p) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && U && p, "null argument");
+        s->solver->U().uploadExternal(U);
+        s->solver->p().uploadExternal(p);
+        s->solver->start();
+    });
+}
+
+int bsg_piso_advance(bsg_piso* s, int32_t steps, bsg_piso_report* report) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && steps >= 0, "bad argument");
+        const bsg::PisoReport r = s->solver->advance(steps);
+        if (report) {
+            report->steps = r.steps;
+            report->time = r.time;
+            report->status = r.status;
+            report->accepted = r.accepted;
+            report->mass = r.mass;
+            report->dU = r.dU;
+            report->rU = r.rU;
+            report->dP = r.dP;
+            report->coupling = r.coupling;
+            report->courant_max = r.courant_max;
+            report->courant_mean = r.courant_mean;
+            report->correctors = r.correctors;
+            report->momentum_iterations = r.momentum_iterations;
+            report->pressure_iterations = r.pressure_iterations;
+        }
+    });
+}
+
+int bsg_piso_get_fields(const bsg_piso* s, double* U, double* p, double* phi) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s != nullptr, "null argument");
+        if (U) s->solver->U().downloadExternal(U);
+        if (p) s->solver->p().downloadExternal(p);
+        if (phi) s->solver->phi().downloadExternal(phi);
+    });
+}
+
+int bsg_piso_destroy(bsg_piso* s) {
     delete s;
     return bsg::kOk;
 }

@@ -663,17 +663,24 @@ __global__ void kRelChange(long long n, const double* __restrict__ a, const doub
 }
 
 // Sums per-block partials of NV quantities (max for entries flagged in max_mask).
+// Second stage of a reduction: warp j combines value j of every block's partial
+// (lanes stride over blocks, then a fixed shuffle tree), sum or max per max_mask.
 __global__ void kFinishReduce(int blocks, int nv, unsigned max_mask, const double* __restrict__ partial,
                               double* __restrict__ result) {
-    const int j = threadIdx.x;
+    const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (j >= nv) return;
     const bool is_max = (max_mask >> j) & 1u;
     double r = 0.0;
-    for (int bidx = 0; bidx < blocks; ++bidx) {
+    for (int bidx = lane; bidx < blocks; bidx += 32) {
         const double p = partial[nv * bidx + j];
         r = is_max ? fmax(r, p) : r + p;
     }
-    result[j] = r;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double q = __shfl_down_sync(0xffffffffu, r, o);
+        r = is_max ? fmax(r, q) : r + q;
+    }
+    if (lane == 0) result[j] = r;
 }
 
 __global__ void kAxpy(long long n, double* __restrict__ y, double a, const double* __restrict__ x) {
@@ -1130,7 +1137,7 @@ void relativeResidualNorms(const DeviceEquation& eq, const double* x, Reducer& r
     else
         launch(ctx, kResidualNorms<3>, m.n_cells, m.n_cells, (const int*)m.cf_ptr.data(), (const int*)m.cf_col.data(),
                eq.diag.data(), eq.val.data(), eq.src.data(), x, red.partial.data());
-    kFinishReduce<<<1, 32, 0, ctx.stream>>>(blocks, 3, 0u, red.partial.data(), red.result.data());
+    kFinishReduce<<<1, 32 * 3, 0, ctx.stream>>>(blocks, 3, 0u, red.partial.data(), red.result.data());
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
 }
@@ -1140,7 +1147,7 @@ void fluxBalance(DeviceMesh& m, const double* phi, Reducer& red) {
     const int blocks = static_cast<int>(gridFor(m.n_cells, kBlock));
     red.ensure(blocks, 4);
     launch(ctx, kFluxBalance, m.n_cells, view(m), phi, red.partial.data());
-    kFinishReduce<<<1, 32, 0, ctx.stream>>>(blocks, 4, 0x8u, red.partial.data(), red.result.data());
+    kFinishReduce<<<1, 32 * 4, 0, ctx.stream>>>(blocks, 4, 0x8u, red.partial.data(), red.result.data());
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
 }
@@ -1151,7 +1158,7 @@ void relativeChangeNorms(Context& ctx, const double* a, const double* b, long lo
     kRelChange<<<blocks, kBlock, 0, ctx.stream>>>(n, a, b, red.partial.data());
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
-    kFinishReduce<<<1, 32, 0, ctx.stream>>>(blocks, 2, 0u, red.partial.data(), red.result.data());
+    kFinishReduce<<<1, 32 * 2, 0, ctx.stream>>>(blocks, 2, 0u, red.partial.data(), red.result.data());
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
 }

@@ -314,6 +314,55 @@ int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report*
 int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi);
 int bsg_simple_destroy(bsg_simple* s);
 
+/* ---- transient PISO (src/physics/piso/main.cpp:60-301) -------------------
+ * Time control follows TimeStepper (src/io/case.cpp:391-403): level k is at
+ * start_time + k*delta_t, the last step shortened to end at end_time. */
+typedef struct bsg_piso bsg_piso;
+
+typedef struct {
+    double density;
+    double viscosity;                   /* dynamic viscosity */
+    double velocity_relaxation;         /* momentum predictor relaxation (1: none) */
+    int32_t max_iterations;             /* predictor-corrector passes per time step */
+    int32_t correctors;                 /* nCorrectors */
+    int32_t max_correctors;             /* maxCorrectors (>= correctors) */
+    double coupling_tolerance;          /* DBL_MAX when unset */
+    int32_t non_orthogonal_corrections;
+    double continuity_tolerance;
+    double velocity_tolerance;
+    double momentum_tolerance;
+    double pressure_correction_tolerance;
+    int32_t time_method;                /* BSG_TIME_EULER or BSG_TIME_BDF2 */
+    double start_time;
+    double end_time;
+    double delta_t;
+    bsg_options momentum;
+    bsg_options pressure;
+    bsg_solver_config momentum_solver;
+    bsg_solver_config pressure_solver;
+} bsg_piso_config;
+
+typedef struct {
+    int32_t steps;                      /* time steps done so far */
+    double time;
+    int32_t status;                     /* 0 end time reached, 1 running or a step rejected, 2 numerical failure */
+    int32_t accepted;                   /* the last step met the continuity and coupling tolerances */
+    double mass, dU, rU, dP, coupling;
+    double courant_max, courant_mean;
+    int32_t correctors;
+    int32_t momentum_iterations;
+    int32_t pressure_iterations;
+} bsg_piso_report;
+
+int bsg_piso_create(bsg_mesh* mesh, const bsg_piso_config* config, bsg_piso** out);
+int bsg_piso_set_boundary(bsg_piso* s, const char* field, int32_t patch, int32_t type, const double* value);
+/* Initial U (3*n_cells) and p (n_cells); phi becomes flux(U) with the pressure options. */
+int bsg_piso_set_fields(bsg_piso* s, const double* U, const double* p);
+/* Advance up to `steps` time steps (fewer at end_time or when a step is rejected). */
+int bsg_piso_advance(bsg_piso* s, int32_t steps, bsg_piso_report* report);
+int bsg_piso_get_fields(const bsg_piso* s, double* U, double* p, double* phi);
+int bsg_piso_destroy(bsg_piso* s);
+
 #ifdef __cplusplus
 }
 #endif
