@@ -403,6 +403,12 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
         kCsrToSell<double><<<gridFor(l0->n, kBlock), kBlock, 0, ctx_.stream>>>(
             l0->n, l0->dptr, l0->dval, l0->ddiag, l0->s_ptr.data(), omega_, l0->s_val.data(), nullptr, nullptr);
         ctx_.launched();
+        if (fp32_) {
+            kCsrToSell<float><<<gridFor(l0->n, kBlock), kBlock, 0, ctx_.stream>>>(
+                l0->n, l0->dptr, l0->dval, l0->ddiag, l0->s_ptr.data(), omega_, l0->s_val32.data(), l0->diag32.data(),
+                l0->rd32.data());
+            ctx_.launched();
+        }
         BSG_CUDA(cudaGetLastError());
         uploadViews();
         return;
@@ -496,6 +502,11 @@ void AmgPreconditioner::uploadViews() {
 SellMat<double> AmgPreconditioner::krylovMatrix() const {
     const Level* l = levels_.front();
     return SellMat<double>{l->n, l->nslices, l->s_ptr.data(), l->s_col.data(), l->s_val.data(), l->ddiag};
+}
+
+SellMat<float> AmgPreconditioner::krylovMatrix32() const {
+    const Level* l = levels_.front();
+    return SellMat<float>{l->n, l->nslices, l->s_ptr.data(), l->s_col.data(), l->s_val32.data(), l->diag32.data()};
 }
 
 long long AmgPreconditioner::krylovEntries() const { return levels_.front()->sell_entries; }

@@ -39,6 +39,7 @@ public:
     // matrix in FP64 for the Krylov products, and the V-cycle in FP64 or FP32.
     bool fp32VCycle() const { return fp32_; }
     SellMat<double> krylovMatrix() const;
+    SellMat<float> krylovMatrix32() const;  // level 0 in FP32 (mixed-precision path)
     VCycleView<double> sellView64() const;
     VCycleView<float> sellView32() const;
     double sellVcycleBytes() const;

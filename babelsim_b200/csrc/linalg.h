@@ -67,8 +67,14 @@ public:
     // CG with AMG, Jacobi or no preconditioner runs as one persistent cooperative
     // kernel per attempt (pcg_persistent.cu); set false to use per-kernel launches.
     bool persistent = true;
+    // FP32-inner iterative refinement (precision 1): each pass asks the FP32 solve
+    // for this reduction of the current FP64 residual.
+    double refine_inner_rtol = 1e-5;
+    int max_refinements = 12;
 
 private:
+    SolveOutcome solveRefined(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg, const double* b,
+                              double* x);
     SolveOutcome solvePersistent(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg,
                                  const double* jacobi_diag, const double* b, double* x);
     struct Impl;

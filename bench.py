@@ -58,12 +58,12 @@ def mesh_for(n: int):
     return pm
 
 
-def build_simple(bsg, mesh, s):
+def build_simple(bsg, mesh, s, precision=0):
     opts = bsg.options(s["interpolation"], s["gradient"], s["convection"], s["diffusion"])
     sim = bsg.Simple(mesh, s["rho"], s["mu"], s["alpha_u"], s["alpha_p"], s["non_orthogonal_corrections"],
                      1e-8, 1e-7, 1e-6, 1e-6, opts, opts,
                      bsg.solver_config("bcgs", "bjacobi", s["atol"], s["rtol"], 1000),
-                     bsg.solver_config("cg", "hypre", s["atol"], s["rtol"], 1000))
+                     bsg.solver_config("cg", "hypre", s["atol"], s["rtol"], 1000, precision=precision))
     for patch in range(6):
         sim.set_boundary("U", patch, "fixedValue", (1.0, 0.0, 0.0) if patch == 3 else (0.0, 0.0, 0.0))
         sim.set_boundary("p", patch, "zeroGradient")
@@ -219,6 +219,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison run")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -313,6 +314,33 @@ def main():
     bytes_io = 8 * (3 * N + N + F)
     e2e = {"value": world * N * e2e_steps / (e2e_ms / 1e3), "unit": "cell-iters/s", "h2d_bytes_per_step": bytes_io,
            "d2h_bytes_per_step": bytes_io, "steps": e2e_steps}
+    # Mixed precision (FP32 inner PCG + FP32 V-cycle inside FP64 iterative refinement, pressure
+    # solves) from the same initial state and for the same number of outer iterations; its
+    # fields are compared with the FP64 run's.
+    mixed = None
+    if not args.no_mixed:
+        U64, p64, _ = sim.fields()
+        steps64 = max(args.warmup, 3) + steps_done + 1 + e2e_steps
+        sim.close()
+        sim = build_simple(bsg, mesh, s, precision=1)
+        sim.iterate(max(args.warmup, 3))
+        ctx.synchronize()
+        ctx.record(4)
+        sim.iterate(steps_done)
+        ctx.record(5)
+        mms = ctx.elapsed_ms(4, 5)
+        if dist:
+            t = torch.tensor([mms], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mms = float(t.item())
+        sim.iterate(steps64 - max(args.warmup, 3) - steps_done)
+        U32, p32, _ = sim.fields()
+        mixed = {"value": world * N * steps_done / (mms / 1e3), "unit": "cell-iters/s",
+                 "ms_per_step": mms / steps_done, "precision": "fp32 inner PCG + fp32 AMG V-cycle, fp64 refinement",
+                 "vs_fp64_value": round(mms and (ms / mms), 3),
+                 "rel_l2_vs_fp64_after_%d_iterations" % steps64: {
+                     "U": float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)),
+                     "p": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}}
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -330,7 +358,8 @@ def main():
                            "momentum": "bcgs+jacobi", "pressure": "cg+amg", "precision": "fp64",
                            "l2": "working set >> 126 MB L2, no flush", "parallelism": f"replicas x{world}",
                            "mesh_seconds": round(t_mesh, 1)},
-                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "mixed_precision": mixed,
+                "gpu_launches": launches,
                 "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
                 "pressure_iterations_per_solve": round(prof["pcg_amg_persistent"][3] / prof["pcg_amg_persistent"][0], 1)
                 if "pcg_amg_persistent" in prof else None,
