@@ -1,0 +1,196 @@
+"""Wilcox-1988m k-omega, restated from src/physics/RANS/k_omega.cpp and model.cpp.  TEST INFRASTRUCTURE ONLY.
+
+Derived fields carry boundary traces exactly as the reference's calculated
+fields do (include/babelsim/field.h:262-320, math.h:184-258): every pointwise
+expression is applied to the cell values and to the boundary traces of its
+operands, the traces of a field with boundary conditions being
+Field::boundaryTrace (field.h:302-313).  The traces matter where the derived
+fields meet faces: the viscosity and diffusivities in equ::laplacian and the
+deviatoric stress in math::div(TensorField).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import fvm
+from .simple import _solve
+
+
+@dataclass
+class KOmegaConstants:
+    """Model constants and bounds (k_omega.cpp:31-41)."""
+    beta_star: float = 0.09
+    beta: float = 3.0 / 40.0
+    gamma: float = 5.0 / 9.0
+    sigma_k: float = 0.5
+    sigma_omega: float = 0.5
+    k_min: float = 1e-12
+    omega_min: float = 1e-12
+    viscosity_ratio_max: float = 1e5
+    relaxation: float = 0.7
+    tolerance: float = 1e-6
+
+
+def strain_squared(G):
+    """2 dev(symm(grad U)):dev(symm(grad U)) (k_omega.cpp:11-23); G rows = component gradients."""
+    div = G[:, 0, 0] + G[:, 1, 1] + G[:, 2, 2]
+    S = 0.5 * (G + np.transpose(G, (0, 2, 1)))
+    for i in range(3):
+        S[:, i, i] -= div / 3.0
+    return 2.0 * np.sum(S * S, axis=(1, 2))
+
+
+def _symmetric_tensor(G, n):
+    """symmetricBoundaryValue(Tensor3) (include/babelsim/vector.h:107-116): 0.5 (G + R G R), R = I - 2 n n^T."""
+    R = np.eye(3)[None] - 2.0 * n[:, :, None] * n[:, None, :]
+    return 0.5 * (G + R @ G @ R)
+
+
+def vector_gradient_trace(U: fvm.Field, G):
+    """Boundary traces of a computed vector gradient (fvm_execution.cpp:240-262)."""
+    geo = U.geo
+    trace = np.zeros((geo.n_faces, 3, 3))
+    bf = np.nonzero(geo.neighbour < 0)[0]
+    o = geo.owner[bf]
+    n = geo.normal[bf]
+    d = geo.xf[bf] - geo.xc[o]
+    dn = np.einsum("ij,ij->i", d, n)
+    tang = d - dn[:, None] * n
+    g = G[o].copy()
+    types, values = fvm.face_condition(U, bf)
+    sym = types == fvm.SYMMETRY
+    if np.any(sym):
+        g[sym] = _symmetric_tensor(g[sym], n[sym])
+    rest = ~sym
+    for c in range(3):
+        gc = g[:, c, :]
+        sn = np.where(types == fvm.FIXED_VALUE,
+                      (values[:, c] - U.v[o, c] - np.einsum("ij,ij->i", gc, tang)) / np.where(dn != 0, dn, 1.0),
+                      np.where(types == fvm.FIXED_GRADIENT, values[:, c], 0.0))
+        upd = gc + (sn - np.einsum("ij,ij->i", gc, n))[:, None] * n
+        g[rest, c, :] = upd[rest]
+    trace[bf] = g
+    return trace
+
+
+def tensor_divergence(geo, T, T_trace, interpolation="linear"):
+    """divergence(TensorField) (operators.cpp:1568-1591): each row reconstructed like a vector field."""
+    if interpolation != "linear":
+        raise NotImplementedError("the restatement covers linear reconstruction of the stress rows")
+    out = np.zeros((geo.n_cells, 3))
+    inn = np.nonzero(geo.neighbour >= 0)[0]
+    bf = np.nonzero(geo.neighbour < 0)[0]
+    w = geo.weight[inn]
+    o, n = geo.owner[inn], geo.neighbour[inn]
+    for c in range(3):
+        fv = np.zeros((geo.n_faces, 3))
+        fv[inn] = w[:, None] * T[o, c, :] + (1.0 - w)[:, None] * T[n, c, :]
+        fv[bf] = T_trace[bf, c, :]
+        contrib = np.einsum("ij,ij->i", fv, geo.Sf)
+        col = np.zeros(geo.n_cells)
+        np.add.at(col, geo.owner, contrib / geo.volume[geo.owner])
+        np.add.at(col, geo.neighbour[inn], -contrib[inn] / geo.volume[geo.neighbour[inn]])
+        out[:, c] = col
+    return out
+
+
+class KOmega:
+    """KOmega (k_omega.cpp:25-160) on oracle fields."""
+
+    def __init__(self, geo, k: fvm.Field, omega: fvm.Field, rho, mu, c: KOmegaConstants, k_opts, omega_opts,
+                 momentum_opts, phi0):
+        self.geo, self.k, self.omega, self.rho, self.mu, self.c = geo, k, omega, rho, mu, c
+        self.k_opts, self.omega_opts, self.mom_opts = k_opts, omega_opts, momentum_opts
+        self.bf = np.nonzero(geo.neighbour < 0)[0]
+        nf = geo.n_faces
+        # mut created as 0 then calculated: traces 0; muEffective created as mu then calculated (model.cpp:56-62)
+        self.mut_v = np.zeros(geo.n_cells)
+        self.mut_tr = np.zeros(nf)
+        self.mueff_v = np.full(geo.n_cells, mu)
+        self.mueff_tr = np.full(nf, mu)
+        self.bound_transport_fields(phi0)
+        self.update_viscosity()
+
+    def _trace(self, f: fvm.Field):
+        out = np.zeros(self.geo.n_faces)
+        out[self.bf] = fvm.boundary_trace(f, self.bf)
+        return out
+
+    def bound_omega(self):
+        k, w = self.k.v, self.omega.v
+        lim = np.maximum(self.c.omega_min, self.rho * k / (self.c.viscosity_ratio_max * self.mu))
+        self.omega.v = np.maximum(w, lim)
+
+    def bound_transport_fields(self, phi):
+        self.k.flux = np.array(phi, dtype=np.float64)
+        self.omega.flux = np.array(phi, dtype=np.float64)
+        self.k.v = np.maximum(self.k.v, self.c.k_min)
+        self.bound_omega()
+
+    def update_viscosity(self):
+        """mut = rho k / max(omega, omegaMin); muEff = mu + mut (k_omega.cpp:153-156)."""
+        wmin = self.c.omega_min
+        self.mut_v = (self.rho * self.k.v) / np.maximum(self.omega.v, wmin)
+        kt, wt = self._trace(self.k), self._trace(self.omega)
+        self.mut_tr = np.zeros(self.geo.n_faces)
+        self.mut_tr[self.bf] = (self.rho * kt[self.bf]) / np.maximum(wt[self.bf], wmin)
+        self.mueff_v = self.mut_v + self.mu
+        self.mueff_tr = self.mut_tr + self.mu
+
+    def effective_viscosity(self):
+        return fvm.Field(self.geo, self.mueff_v.copy(), None, trace=self.mueff_tr.copy())
+
+    def stress_remainder_divergence(self, U: fvm.Field):
+        """math::div(muEff (grad(U)^T - 2/3 tr(grad U) I)) (model.cpp:65-69, operators.cpp:1568-1591)."""
+        G = fvm.gradient(U, self.mom_opts["gradient"])
+        Gt = vector_gradient_trace(U, G)
+
+        def remainder(g, m):
+            tr = g[:, 0, 0] + g[:, 1, 1] + g[:, 2, 2]
+            iso = np.zeros_like(g)
+            for i in range(3):
+                iso[:, i, i] = tr
+            return m[:, None, None] * (np.transpose(g, (0, 2, 1)) - (2.0 / 3.0) * iso)
+
+        T = remainder(G, self.mueff_v)
+        Tt = np.zeros_like(Gt)
+        Tt[self.bf] = remainder(Gt[self.bf], self.mueff_tr[self.bf])
+        return tensor_divergence(self.geo, T, Tt, self.mom_opts["interpolation"])
+
+    def solve_transport(self, U: fvm.Field, phi):
+        """KOmega::solveTransport (k_omega.cpp:65-125), steady (no time term)."""
+        geo, c, rho, mu = self.geo, self.c, self.rho, self.mu
+        prev_k, prev_w = self.k.v.copy(), self.omega.v.copy()
+        U.flux = np.array(phi, dtype=np.float64)
+        self.update_viscosity()
+        G = fvm.gradient(U, self.mom_opts["gradient"])
+        production = self.mut_v * strain_squared(G)
+        k_diff = fvm.Field(geo, c.sigma_k * self.mut_v + mu, None, trace=c.sigma_k * self.mut_tr + mu)
+        w_diff = fvm.Field(geo, c.sigma_omega * self.mut_v + mu, None, trace=c.sigma_omega * self.mut_tr + mu)
+        w_destruction = (c.beta * rho) * self.omega.v
+        w_production = ((c.gamma * production) * self.omega.v) / np.maximum(self.k.v, c.k_min)
+        # omega first
+        weq = fvm.Equation(self.omega, self.omega_opts, {})
+        fvm.eq_div(weq, phi, rho)
+        fvm.eq_laplacian(weq, w_diff, -1.0)
+        weq.ldu.diag = weq.ldu.diag + (1.0 * w_destruction) * geo.volume
+        fvm.eq_source(weq, w_production)
+        r_w = fvm.relative_residual(weq.ldu, self.omega.v)
+        fvm.eq_relax(weq, prev_w, c.relaxation)
+        self.omega.v = _solve(weq.ldu.matrix(), weq.ldu.source)
+        self.bound_omega()
+        # then k, with the new omega in its sink
+        keq = fvm.Equation(self.k, self.k_opts, {})
+        fvm.eq_div(keq, phi, rho)
+        fvm.eq_laplacian(keq, k_diff, -1.0)
+        keq.ldu.diag = keq.ldu.diag + (1.0 * ((c.beta_star * rho) * self.omega.v)) * geo.volume
+        fvm.eq_source(keq, production)
+        r_k = fvm.relative_residual(keq.ldu, self.k.v)
+        fvm.eq_relax(keq, prev_k, c.relaxation)
+        self.k.v = _solve(keq.ldu.matrix(), keq.ldu.source)
+        self.bound_transport_fields(phi)
+        self.update_viscosity()
+        return dict(d=max(fvm.relative_change(self.omega.v, prev_w), fvm.relative_change(self.k.v, prev_k)),
+                    r=max(r_w, r_k))

@@ -95,6 +95,13 @@ int main(int argc, char** argv) {
         writeVector(f, "U", detail::fieldValues(problem.existingVectorField("U")));
         writeVector(f, "p", detail::fieldValues(problem.existingScalarField("p")));
         writeVector(f, "phi", detail::fieldValues(problem.existingFaceField("phi")));
+        // turbulence fields, when the case has a model
+        for (const char* name : {"k", "omega", "mut", "muEffective"}) {
+            try {
+                writeVector(f, name, detail::fieldValues(problem.existingScalarField(name)));
+            } catch (const std::exception&) {
+            }
+        }
         std::fclose(f);
         const PerformanceCounters perf = problem.localPerformance();
         std::ofstream json(out_dir / "run.json");

@@ -51,17 +51,21 @@ def _solve(A, b):
 
 
 def run_simple(geo, U_bcs, p_bcs, settings: SimpleSettings, U0=None, p0=None, iterations=None,
-               capture=None, phi0=None) -> SimpleState:
+               capture=None, phi0=None, turbulence=None) -> SimpleState:
     """runSimple (simple/main.cpp:11-131).  ``capture(iter, dict)`` receives the
     assembled systems of each iteration (momentum after assembly and after
     relax/scale; pressure systems as solved) for parity checks.  ``phi0``
-    resumes from a saved face flux instead of flux(U0)."""
+    resumes from a saved face flux instead of flux(U0).  ``turbulence(geo, phi)``
+    builds an eddy-viscosity model (oracle.rans.KOmega) before the initial flux,
+    as rans::load does (simple/main.cpp:33); its effective viscosity, stress
+    remainder and transport solve enter where simple/main.cpp:53-56, 102-110 put them."""
     nc = geo.n_cells
     U = fvm.Field(geo, np.zeros((nc, 3)) if U0 is None else U0, U_bcs)
     p = fvm.Field(geo, np.zeros(nc) if p0 is None else p0, p_bcs)
     mom_opts = dict(settings.momentum)
     p_opts = dict(settings.pressure)
     pressure_solves = 1 if p_opts["diffusion"] == "orthogonal" else settings.non_orthogonal_corrections + 1
+    model = turbulence(geo, np.zeros(geo.n_faces)) if turbulence is not None else None
     phi = fvm.flux(U, mom_opts["interpolation"], mom_opts["gradient"])
     if phi0 is not None:
         phi = np.array(phi0, dtype=np.float64)
@@ -73,9 +77,11 @@ def run_simple(geo, U_bcs, p_bcs, settings: SimpleSettings, U0=None, p0=None, it
         U_prev = U.v.copy()
         mom = fvm.Equation(U, mom_opts, {})
         fvm.eq_div(mom, phi, settings.rho)
-        fvm.eq_laplacian(mom, mu_field, -1.0)
+        fvm.eq_laplacian(mom, model.effective_viscosity() if model else mu_field, -1.0)
         grad_p = fvm.gradient(p, p_opts["gradient"])
         fvm.eq_source(mom, -grad_p)
+        if model:
+            fvm.eq_source(mom, model.stress_remainder_divergence(U))
         if capture is not None:
             capture(it, dict(momentum=mom.ldu.copy()))
         rU = fvm.relative_residual(mom.ldu, U.v)
@@ -120,13 +126,19 @@ def run_simple(geo, U_bcs, p_bcs, settings: SimpleSettings, U0=None, p0=None, it
         pflux = fvm.eq_face_flux(peq, pP.v)
         U.v = U.v - rAU_v[:, None] * fvm.gradient(pP, p_opts["gradient"])
         phi = phiH + pflux
+        turbulence_ok = True
+        if model:
+            t = model.solve_transport(U, phi)
+            turbulence_ok = t["d"] <= model.c.tolerance and t["r"] <= model.c.tolerance
         dU = fvm.relative_change(U.v, U_prev)
         dP = fvm.relative_magnitude(pP.v, p.v)
         mass = fvm.flux_balance(geo, phi)
-        conv = (rU <= settings.momentum_tolerance and dU <= settings.velocity_tolerance
+        conv = (turbulence_ok and rU <= settings.momentum_tolerance and dU <= settings.velocity_tolerance
                 and dP <= settings.pressure_tolerance and mass["relative"] <= settings.mass_tolerance)
         state.history.append(dict(rU=rU, dU=dU, dP=dP, mass=mass["relative"]))
         state.U, state.p, state.phi, state.iterations = U.v, p.v, phi, it + 1
+        if model:
+            state.k, state.omega, state.mut = model.k.v, model.omega.v, model.mut_v
         if conv:
             state.converged = True
             break

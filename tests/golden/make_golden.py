@@ -43,7 +43,7 @@ def vec(v):
 
 
 def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics, solver="simple", time="steady",
-               control=(0.0, 0.0, 1.0)):
+               control=(0.0, 0.0, 1.0), extra_fields=()):
     os.makedirs(os.path.join(path, "mesh"), exist_ok=True)
     os.makedirs(os.path.join(path, "fields", "initial"), exist_ok=True)
     os.makedirs(os.path.join(path, "numerics"), exist_ok=True)
@@ -66,9 +66,10 @@ def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics, solver="sim
     with open(os.path.join(path, "numerics", "solution.bs"), "w") as f:
         f.write("".join(f"{k} {v}\n" for k, v in solution.items()))
 
-    def field(name, kind, bcs):
+    def field(name, kind, bcs, internal=0.0):
         lines = [f"field {name}", "{", f"    type {kind}", "    location cell",
-                 "    internal uniform " + ("(0 0 0)" if kind == "vector" else "(0)"), "    boundary", "    {"]
+                 "    internal uniform " + ("(0 0 0)" if kind == "vector" else f"({internal!r})"), "    boundary",
+                 "    {"]
         for patch, (t, v) in zip(mesh.patch_names, bcs):
             if t in ("zeroGradient", "symmetry"):
                 lines.append(f"        {patch} {{ type {t} }}")
@@ -80,6 +81,8 @@ def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics, solver="sim
             f.write("\n".join(lines) + "\n")
     field("U", "vector", U_bcs)
     field("p", "scalar", p_bcs)
+    for name, internal, bcs in extra_fields:
+        field(name, "scalar", bcs, internal)
 
 
 def run(case_dir, iterations, dump=False):
@@ -191,6 +194,78 @@ def make_piso(name, mesh, U_bcs, p_bcs, methods, solution, physics, time, start,
     print(name, "written", len(ends), "steps")
 
 
+def make_rans(name, mesh, U_bcs, p_bcs, k_field, w_field, methods, solution, physics, K):
+    """Steady SIMPLE with the reference's k-omega model: U, p, phi, k, omega after iterations 1..K."""
+    work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
+    write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics,
+               extra_fields=[("k",) + tuple(k_field), ("omega",) + tuple(w_field)])
+    data = {}
+    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    data["mesh_vertices"] = mesh.vertices
+    data["mesh_offsets"] = offsets
+    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
+    for k in range(1, K + 1):
+        fields, geo, info, _ = run(work, k)
+        data[f"U_{k}"] = fields["U"].reshape(-1, 3)
+        for key in ("p", "phi", "k", "omega", "mut", "muEffective"):
+            data[f"{key}_{k}"] = fields[key]
+    for key, arr in geo.items():
+        data["geo_" + key] = arr
+    meta = dict(patch_names=mesh.patch_names, patch_kinds=mesh.patch_kinds,
+                U_bcs=[(t, list(map(float, v))) for t, v in U_bcs], p_bcs=[(t, float(v)) for t, v in p_bcs],
+                k_internal=k_field[0], k_bcs=[(t, float(v)) for t, v in k_field[1]],
+                omega_internal=w_field[0], omega_bcs=[(t, float(v)) for t, v in w_field[1]],
+                methods=methods, solution=solution, physics=physics, K=K)
+    data["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
+    shutil.rmtree(work)
+    print(name, "written", K, "iterations")
+
+
+def rans_methods(conv="upwind", grad="greenGauss", diff="orthogonal", turb_conv="upwind"):
+    o = dict(interpolation="linear", gradient=grad, convection=conv, diffusion=diff)
+    t = dict(o, convection=turb_conv)
+    return {"momentum": o, "pressureCorrection": o, "kTransport": t, "omegaTransport": t}
+
+
+def rans_solution():
+    sol = config1_solution(1e-12)
+    sol.update({"turbulenceRelaxation": 0.7, "turbulenceTolerance": 1e-6})
+    for eq in ("kTransport", "omegaTransport"):
+        sol.update({f"equation.{eq}.kspType": "bcgs", f"equation.{eq}.pcType": "bjacobi",
+                    f"equation.{eq}.absoluteTolerance": 1e-18, f"equation.{eq}.relativeTolerance": 1e-12,
+                    f"equation.{eq}.maxIterations": 2000})
+    return sol
+
+
+def main_rans():
+    komega = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "kOmega", "kOmegaBetaStar": 0.09,
+              "kOmegaBeta": 0.075, "kOmegaGamma": 5.0 / 9.0, "kOmegaSigmaK": 0.5, "kOmegaSigmaOmega": 0.5,
+              "kMin": 1e-12, "omegaMin": 1e-10, "maxTurbulentViscosityRatio": 1e5}
+    # channel: inlet / outlet / two walls, one cell thick
+    ch = meshgen.hex_box(16, 8, 1, hi=(4.0, 1.0, 0.25),
+                         names=["inlet", "outlet", "lower", "upper", "front", "back"],
+                         kinds=["inlet", "outlet", "wall", "wall", "symmetry", "symmetry"])
+    U = [("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0)), ("fixedValue", (0.0, 0.0, 0.0)),
+         ("fixedValue", (0.0, 0.0, 0.0)), ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    p = [("zeroGradient", 0.0), ("fixedValue", 0.0), ("zeroGradient", 0.0), ("zeroGradient", 0.0),
+         ("symmetry", 0.0), ("symmetry", 0.0)]
+    kb = [("fixedValue", 3.75e-3), ("zeroGradient", 0.0), ("fixedValue", 1e-12), ("fixedValue", 1e-12),
+          ("symmetry", 0.0), ("symmetry", 0.0)]
+    wb = [("fixedValue", 2.0), ("zeroGradient", 0.0), ("fixedValue", 800.0), ("fixedValue", 800.0),
+          ("symmetry", 0.0), ("symmetry", 0.0)]
+    make_rans("komega_channel", ch, U, p, (3.75e-3, kb), (2.0, wb), rans_methods("linearUpwind"), rans_solution(),
+              komega, K=4)
+    # warped box: lid, least squares, corrected diffusion, 2 non-orthogonal correctors
+    Uw = [("fixedValue", (0.0, 0.0, 0.0))] * 3 + [("fixedValue", (1.0, 0.0, 0.0))] + [("fixedValue", (0.0, 0.0, 0.0))] * 2
+    pw = [("zeroGradient", 0.0)] * 6
+    kw = [("fixedValue", 1e-12)] * 6
+    ww = [("fixedValue", 500.0)] * 6
+    make_rans("komega_warped5", meshgen.warped_box(5), Uw, pw, (1e-3, kw), (5.0, ww),
+              rans_methods("linearUpwind", "leastSquares", "corrected"), rans_solution(), komega, K=3)
+
+
 def piso_solution(n_correctors=2, non_orth=1, p_rtol=1e-12):
     return {"maxIterations": 1, "nCorrectors": n_correctors, "nonOrthogonalCorrections": non_orth,
             "velocityRelaxation": 1.0, "continuityTolerance": 1e-7, "velocityTolerance": 1e-7,
@@ -238,6 +313,9 @@ def main():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "piso":
         main_piso()
+    elif len(sys.argv) > 1 and sys.argv[1] == "rans":
+        main_rans()
     else:
         main()
         main_piso()
+        main_rans()

@@ -12,11 +12,12 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 from babelsim_b200 import meshgen  # noqa: E402
-from oracle import fvm, geometry, piso, simple  # noqa: E402
+from oracle import fvm, geometry, piso, rans, simple  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
 PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler"]
+RANS_CASES = ["komega_channel", "komega_warped5"]
 GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
             "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",
             "face_skewness", "cell_centres", "cell_volumes", "orthogonal_geometry"]
@@ -106,3 +107,24 @@ def piso_settings(g: "Golden", end_time=None) -> piso.PisoSettings:
                              start_time=g.meta["start"], delta_t=g.meta["dt"],
                              end_time=g.meta["ends"][-1] if end_time is None else end_time,
                              momentum=m["momentum"], pressure=m["pressureCorrection"])
+
+
+def komega_constants(g: "Golden") -> rans.KOmegaConstants:
+    ph, sol = g.meta["physics"], g.meta["solution"]
+    return rans.KOmegaConstants(ph["kOmegaBetaStar"], ph["kOmegaBeta"], ph["kOmegaGamma"], ph["kOmegaSigmaK"],
+                                ph["kOmegaSigmaOmega"], ph["kMin"], ph["omegaMin"], ph["maxTurbulentViscosityRatio"],
+                                sol["turbulenceRelaxation"], sol["turbulenceTolerance"])
+
+
+def komega_factory(g: "Golden"):
+    """Model factory for oracle.simple.run_simple(turbulence=...) from a k-omega fixture."""
+    ph, m = g.meta["physics"], g.meta["methods"]
+    kb = [(fvm.BC_NAMES[t], v) for t, v in g.meta["k_bcs"]]
+    wb = [(fvm.BC_NAMES[t], v) for t, v in g.meta["omega_bcs"]]
+
+    def make(geo, phi0):
+        k = fvm.Field(geo, np.full(geo.n_cells, g.meta["k_internal"]), kb)
+        w = fvm.Field(geo, np.full(geo.n_cells, g.meta["omega_internal"]), wb)
+        return rans.KOmega(geo, k, w, ph["density"], ph["dynamicViscosity"], komega_constants(g),
+                           m["kTransport"], m["omegaTransport"], m["momentum"], phi0)
+    return make
