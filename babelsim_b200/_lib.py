@@ -29,7 +29,8 @@ EXPORTS = [
     "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_pcg_jacobi_static",
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
-    "bsg_simple_iterate", "bsg_simple_get_fields",
+    "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_set_turbulence_fields",
+    "bsg_simple_get_turbulence_fields", "bsg_simple_get_fields",
     "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
     "bsg_piso_get_fields", "bsg_piso_destroy",
 ]
@@ -79,7 +80,16 @@ class SimpleReport(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("status", C.c_int32), ("mass", C.c_double),
                 ("dU", C.c_double), ("rU", C.c_double), ("dP", C.c_double),
                 ("linear_pressure_residual", C.c_double), ("momentum_iterations", C.c_int32),
-                ("pressure_iterations", C.c_int32)]
+                ("pressure_iterations", C.c_int32), ("turbulence_change", C.c_double),
+                ("turbulence_residual", C.c_double)]
+
+
+class KOmegaConfig(C.Structure):
+    _fields_ = [("beta_star", C.c_double), ("beta", C.c_double), ("gamma", C.c_double), ("sigma_k", C.c_double),
+                ("sigma_omega", C.c_double), ("k_min", C.c_double), ("omega_min", C.c_double),
+                ("max_viscosity_ratio", C.c_double), ("relaxation", C.c_double), ("tolerance", C.c_double),
+                ("k_transport", Options), ("omega_transport", Options), ("k_solver", SolverConfig),
+                ("omega_solver", SolverConfig)]
 
 
 class PisoConfig(C.Structure):
@@ -144,7 +154,9 @@ def lib():
             "bsg_simple_create": [vp, C.POINTER(SimpleConfig), pp],
             "bsg_simple_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_simple_set_fields": [vp, vp, vp],
             "bsg_simple_set_flux": [vp, vp],
-            "bsg_simple_iterate": [vp, i32, C.POINTER(SimpleReport)], "bsg_simple_get_fields": [vp, vp, vp, vp],
+            "bsg_simple_iterate": [vp, i32, C.POINTER(SimpleReport)],
+            "bsg_simple_enable_komega": [vp, C.POINTER(KOmegaConfig)],
+            "bsg_simple_set_turbulence_fields": [vp, vp, vp], "bsg_simple_get_turbulence_fields": [vp, vp, vp, vp], "bsg_simple_get_fields": [vp, vp, vp, vp],
             "bsg_simple_destroy": [vp],
             "bsg_piso_create": [vp, C.POINTER(PisoConfig), pp],
             "bsg_piso_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_piso_set_fields": [vp, vp, vp],

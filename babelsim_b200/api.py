@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
+from ._lib import (KOmegaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
                    check, f64, i32, lib, ptr)
 
 BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
@@ -372,6 +372,25 @@ class Simple:
         r = SimpleReport()
         check(lib().bsg_simple_iterate(self.h, max_iterations, C.byref(r)), self.mesh.ctx.h)
         return r
+
+    def enable_komega(self, beta_star=0.09, beta=0.075, gamma=5.0 / 9.0, sigma_k=0.5, sigma_omega=0.5, k_min=1e-12,
+                      omega_min=1e-12, max_viscosity_ratio=1e5, relaxation=0.7, tolerance=1e-6, k_transport=None,
+                      omega_transport=None, k_solver=None, omega_solver=None):
+        """turbulenceModel kOmega (before set_fields); k and omega then take boundary conditions."""
+        cfg = KOmegaConfig(beta_star, beta, gamma, sigma_k, sigma_omega, k_min, omega_min, max_viscosity_ratio,
+                           relaxation, tolerance, k_transport or options(), omega_transport or options(),
+                           k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
+                           omega_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
+        check(lib().bsg_simple_enable_komega(self.h, C.byref(cfg)), self.mesh.ctx.h)
+
+    def set_turbulence_fields(self, k, omega):
+        check(lib().bsg_simple_set_turbulence_fields(self.h, ptr(f64(k)), ptr(f64(omega))), self.mesh.ctx.h)
+
+    def turbulence_fields(self):
+        n = self.mesh.n_cells
+        k, w, mut = np.zeros(n), np.zeros(n), np.zeros(n)
+        check(lib().bsg_simple_get_turbulence_fields(self.h, ptr(k), ptr(w), ptr(mut)), self.mesh.ctx.h)
+        return k, w, mut
 
     def fields(self):
         m = self.mesh

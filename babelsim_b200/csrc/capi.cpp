@@ -207,6 +207,11 @@ void solveEquation(bsg_equation* e, const bsg::SolverConfig& cfg, bsg_solve_resu
         for (int c = 0; c < 3; ++c) toResult(o[c], results + c);
         return;
     }
+    if (cfg.solver != 0) {
+        // BiCGStab (and the GMRES types): Jacobi-preconditioned lockstep BiCGStab on one right-hand side
+        toResult(e->krylov->solveBicgstab(A, cfg, eq.src.data(), eq.x->v.data()), results);
+        return;
+    }
     std::unique_ptr<bsg::Preconditioner> jac;
     bsg::Preconditioner* pc = nullptr;
     if (cfg.preconditioner == 2 || cfg.preconditioner == 3) {
@@ -817,9 +822,12 @@ int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && field, "null argument");
         const std::string n(field);
+        bsg::KOmegaModel* t = s->solver->turbulence();
         if (n == "U") s->solver->U().setBoundary(patch, type, value);
         else if (n == "p") s->solver->p().setBoundary(patch, type, value);
-        else bsg::fail(bsg::kArgument, "SIMPLE boundary field must be U or p");
+        else if (n == "k" && t) t->k().setBoundary(patch, type, value);
+        else if (n == "omega" && t) t->omega().setBoundary(patch, type, value);
+        else bsg::fail(bsg::kArgument, "SIMPLE boundary field must be U or p (k, omega with a k-omega model)");
     });
 }
 
@@ -861,7 +869,52 @@ int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report*
             report->linear_pressure_residual = r.linP;
             report->momentum_iterations = r.momentum_iterations;
             report->pressure_iterations = r.pressure_iterations;
+            report->turbulence_change = r.turbulence_change;
+            report->turbulence_residual = r.turbulence_residual;
         }
+    });
+}
+
+int bsg_simple_enable_komega(bsg_simple* s, const bsg_komega_config* c) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && c, "null argument");
+        bsg::KOmegaConfig k;
+        k.beta_star = c->beta_star;
+        k.beta = c->beta;
+        k.gamma = c->gamma;
+        k.sigma_k = c->sigma_k;
+        k.sigma_omega = c->sigma_omega;
+        k.k_min = c->k_min;
+        k.omega_min = c->omega_min;
+        k.viscosity_ratio_max = c->max_viscosity_ratio;
+        k.relaxation = c->relaxation;
+        k.tolerance = c->tolerance;
+        k.k_options = options(&c->k_transport);
+        k.omega_options = options(&c->omega_transport);
+        k.k_solver = solverConfig(&c->k_solver);
+        k.omega_solver = solverConfig(&c->omega_solver);
+        s->solver->enableKOmega(k);
+    });
+}
+
+int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* omega) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && k && omega, "null argument");
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        t->k().uploadExternal(k);
+        t->omega().uploadExternal(omega);
+    });
+}
+
+int bsg_simple_get_turbulence_fields(const bsg_simple* s, double* k, double* omega, double* mut) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s != nullptr, "null argument");
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        if (k) t->k().downloadExternal(k);
+        if (omega) t->omega().downloadExternal(omega);
+        if (mut) t->turbulentViscosity().downloadExternal(mut);
     });
 }
 

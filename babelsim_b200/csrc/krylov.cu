@@ -432,27 +432,31 @@ __global__ void kBiInit(int blocks, const double* __restrict__ partial, Scalars*
     }
 }
 
-// r = b - A x for 3 interleaved components, partials of |r_c|^2 and |b_c|^2.
-__global__ void kResidual3(Dcsr<double> A, const double* __restrict__ b, const double* __restrict__ x,
+// r = b - A x for C interleaved components, partials of |r_c|^2 and |b_c|^2.
+template <int C>
+__global__ void kResidualC(Dcsr<double> A, const double* __restrict__ b, const double* __restrict__ x,
                            double* __restrict__ r, double* __restrict__ partial) {
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
-        double acc[3];
-        rowProduct<3>(A, i, x, acc);
+    double v[2 * C];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const double bi = b[3 * i + c], ri = bi - acc[c];
-            r[3 * i + c] = ri;
+    for (int j = 0; j < 2 * C; ++j) v[j] = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
+        double acc[C];
+        rowProduct<C>(A, i, x, acc);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const double bi = b[C * i + c], ri = bi - acc[c];
+            r[C * i + c] = ri;
             v[c] += ri * ri;
-            v[3 + c] += bi * bi;
+            v[C + c] += bi * bi;
         }
     }
-    writePartial<6>(v, partial);
+    writePartial<2 * C>(v, partial);
 }
-__global__ void kFinish6(int blocks, const double* __restrict__ partial, double* __restrict__ out) {
-    double s[6];
-    finishSums<6>(blocks, partial, s);
-    if (threadIdx.x == 0) for (int j = 0; j < 6; ++j) out[j] = s[j];
+template <int NV>
+__global__ void kFinishN(int blocks, const double* __restrict__ partial, double* __restrict__ out) {
+    double s[NV];
+    finishSums<NV>(blocks, partial, s);
+    if (threadIdx.x == 0) for (int j = 0; j < NV; ++j) out[j] = s[j];
 }
 
 }  // namespace
@@ -798,33 +802,34 @@ SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig
     return out;
 }
 
-void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
-                                SolveOutcome out[3]) {
+template <int C>
+void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                                    SolveOutcome out[]) {
     Impl& m = *impl_;
     Context& ctx = m.ctx;
     const int n = A.n;
-    m.ensure(3 * static_cast<std::size_t>(n));
+    m.ensure(C * static_cast<std::size_t>(n));
     const int g = m.grid(n);
-    if (!cfg.warm_start) BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * 3 * n, ctx.stream));
+    if (!cfg.warm_start) BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * C * n, ctx.stream));
     double* result = m.partial.data() + 8 * 4096 - 8;
     // r = b - A x with per-component squared norms; also ||b|| per component.
-    auto residual3 = [&](double res[3], double bres[3]) {
-        kResidual3<<<g, kBlock, 0, ctx.stream>>>(A, b, x, m.r.data(), m.partial.data());
-        kFinish6<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), result);
+    auto residual3 = [&](double res[], double bres[]) {
+        kResidualC<C><<<g, kBlock, 0, ctx.stream>>>(A, b, x, m.r.data(), m.partial.data());
+        kFinishN<2 * C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), result);
         ctx.launches += 2;
         BSG_CUDA(cudaGetLastError());
-        BSG_CUDA(cudaMemcpyAsync(ctx.pinned, result, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+        BSG_CUDA(cudaMemcpyAsync(ctx.pinned, result, 2 * C * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
         ctx.sync();
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < C; ++c) {
             res[c] = std::sqrt(ctx.pinned[c]);
-            if (bres) bres[c] = std::sqrt(ctx.pinned[3 + c]);
+            if (bres) bres[c] = std::sqrt(ctx.pinned[C + c]);
         }
     };
-    double bn[3], r0n[3], scale[3], target[3], inner[3], fin[3];
-    int used[3] = {0, 0, 0};
-    bool finished[3] = {false, false, false};
+    double bn[C], r0n[C], scale[C], target[C], inner[C], fin[C];
+    int used[C] = {};
+    bool finished[C] = {};
     residual3(r0n, bn);
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < C; ++c) {
         if (!cfg.warm_start) r0n[c] = bn[c];
         scale[c] = residualScale(r0n[c], bn[c]);
         target[c] = std::max(cfg.atol, cfg.rtol * scale[c]);
@@ -836,43 +841,43 @@ void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, 
     }
     for (int restart = 0; restart < 3; ++restart) {
         bool any = false;
-        for (int c = 0; c < 3; ++c) any = any || (!finished[c] && used[c] < cfg.max_iterations);
+        for (int c = 0; c < C; ++c) any = any || (!finished[c] && used[c] < cfg.max_iterations);
         if (!any) break;
-        if (restart > 0) { double dummy[3]; residual3(dummy, nullptr); }
+        if (restart > 0) { double dummy[C]; residual3(dummy, nullptr); }
         Scalars s{};
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < C; ++c) {
             s.target2[c] = inner[c] * inner[c];
             s.done[c] = (finished[c] || used[c] >= cfg.max_iterations) ? 1 : 0;
             s.iters[c] = used[c];
         }
         s.max_iters = cfg.max_iterations;
         BSG_CUDA(cudaMemcpyAsync(m.sc.data(), &s, sizeof(s), cudaMemcpyHostToDevice, ctx.stream));
-        kBiStart<3><<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.r0.data(), m.p.data(), m.v.data(), m.partial.data());
-        kBiInit<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+        kBiStart<C><<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.r0.data(), m.p.data(), m.v.data(), m.partial.data());
+        kBiInit<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
         ctx.launches += 2;
         Scalars h{};
         for (;;) {
             for (int it = 0; it < check_interval; ++it) {
-                kBiDirection<3><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.p.data(), m.v.data(),
+                kBiDirection<C><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.p.data(), m.v.data(),
                                                               m.ph.data(), m.sc.data());
                 {
                     BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
-                    kBiSpmvV<3><<<g, kBlock, 0, ctx.stream>>>(A, m.ph.data(), m.v.data(), m.r0.data(),
+                    kBiSpmvV<C><<<g, kBlock, 0, ctx.stream>>>(A, m.ph.data(), m.v.data(), m.r0.data(),
                                                               m.partial.data(), m.sc.data());
                 }
-                kBiAlpha<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
-                kBiS<3><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.v.data(), m.sh.data(), m.partial.data(),
+                kBiAlpha<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiS<C><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.v.data(), m.sh.data(), m.partial.data(),
                                                       m.sc.data());
-                kBiCheckS<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiCheckS<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 {
                     BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
-                    kBiSpmvT<3><<<g, kBlock, 0, ctx.stream>>>(A, m.sh.data(), m.t.data(), m.r.data(),
+                    kBiSpmvT<C><<<g, kBlock, 0, ctx.stream>>>(A, m.sh.data(), m.t.data(), m.r.data(),
                                                               m.partial.data(), m.sc.data());
                 }
-                kBiOmega<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
-                kBiUpdate<3><<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.ph.data(), m.sh.data(), m.t.data(),
+                kBiOmega<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiUpdate<C><<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.ph.data(), m.sh.data(), m.t.data(),
                                                            m.r0.data(), m.partial.data(), m.sc.data());
-                kBiCheck<3><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                kBiCheck<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 ctx.launches += 9;
             }
             BSG_CUDA(cudaGetLastError());
@@ -881,9 +886,9 @@ void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, 
             std::memcpy(&h, ctx.pinned, sizeof(h));
             if (h.all_done) break;
         }
-        double res[3];
+        double res[C];
         residual3(res, nullptr);
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < C; ++c) {
             if (finished[c]) continue;
             used[c] = h.iters[c];
             fin[c] = res[c];
@@ -891,12 +896,23 @@ void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, 
             else inner[c] *= 0.5;
         }
     }
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < C; ++c) {
         out[c].iterations = used[c];
         out[c].final_ = fin[c];
         out[c].relative = fin[c] / scale[c];
         out[c].status = (std::isfinite(fin[c]) && fin[c] <= target[c]) ? 0 : (std::isfinite(fin[c]) ? 1 : 2);
     }
+}
+
+void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                                SolveOutcome out[3]) {
+    lockstepBicgstab<3>(A, cfg, b, x, out);
+}
+
+SolveOutcome KrylovSolver::solveBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x) {
+    SolveOutcome out[1];
+    lockstepBicgstab<1>(A, cfg, b, x, out);
+    return out[0];
 }
 
 }  // namespace bsg

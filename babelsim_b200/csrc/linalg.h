@@ -63,6 +63,9 @@ public:
     // BiCGStab in lockstep, one matrix read per product for all three.
     void solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                       SolveOutcome out[3]);
+    // One right-hand side, Jacobi-preconditioned BiCGStab (non-symmetric scalar systems:
+    // transported turbulence quantities, and any scalar equation configured with kspType bcgs).
+    SolveOutcome solveBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x);
     int check_interval = 8;  // iterations between host convergence checks
     // CG with AMG, Jacobi or no preconditioner runs as one persistent cooperative
     // kernel per attempt (pcg_persistent.cu); set false to use per-kernel launches.
@@ -75,6 +78,9 @@ public:
 private:
     SolveOutcome solveRefined(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg, const double* b,
                               double* x);
+    template <int C>
+    void lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                          SolveOutcome out[]);
     SolveOutcome solvePersistent(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg,
                                  const double* jacobi_diag, const double* b, double* x);
     struct Impl;

@@ -1,0 +1,337 @@
+// Wilcox-1988m k-omega transport on the device (see rans.h).
+#include "bsg_device.cuh"
+#include "rans.h"
+
+#include <cmath>
+
+namespace bsg {
+namespace {
+constexpr int kBlock = 256;
+
+template <class K, class... A>
+void launch(Context& ctx, K kernel, long long n, A... args) {
+    kernel<<<gridFor(n, kBlock), kBlock, 0, ctx.stream>>>(args...);
+    BSG_CUDA(cudaGetLastError());
+    ctx.launched();
+}
+
+__global__ void kBoundK(int n, double k_min, double* __restrict__ k) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) k[i] = fmax(k[i], k_min);
+}
+
+// omega = max(omega, omegaMin, rho k / (ratioMax mu)) (k_omega.cpp:140-150)
+__global__ void kBoundOmega(int n, double omega_min, double rho, double ratio_mu, const double* __restrict__ k,
+                            double* __restrict__ w) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) w[i] = fmax(w[i], fmax(omega_min, rho * k[i] / ratio_mu));
+}
+
+// mut = rho k / max(omega, omegaMin), muEff = mu + mut on cells (k_omega.cpp:153-156)
+__global__ void kViscosity(int n, double rho, double mu, double omega_min, const double* __restrict__ k,
+                           const double* __restrict__ w, double* __restrict__ mut, double* __restrict__ mueff) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = (rho * k[i]) / fmax(w[i], omega_min);
+    mut[i] = v;
+    mueff[i] = v + mu;
+}
+
+// the same expressions on the boundary traces of k and omega (field.h:302-320)
+__global__ void kViscosityTrace(MeshView m, BcView bk, BcView bw, const double* __restrict__ k,
+                                const double* __restrict__ w, double rho, double mu, double omega_min,
+                                double* __restrict__ mut_tr, double* __restrict__ mueff_tr) {
+    const int fb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fb >= m.n_boundary) return;
+    double kt[1], wt[1];
+    boundaryTrace<1>(m, bk, k, fb, NAN, kt);
+    boundaryTrace<1>(m, bw, w, fb, NAN, wt);
+    const double v = (rho * kt[0]) / fmax(wt[0], omega_min);
+    mut_tr[fb] = v;
+    mueff_tr[fb] = v + mu;
+}
+
+// 2 dev(symm G) : dev(symm G) (k_omega.cpp:11-23); G row c = gradient of component c
+__device__ __forceinline__ double strainSquared(const double* G) {
+    const double div = G[0] + G[4] + G[8];
+    double sum = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double s = 0.5 * (G[3 * i + j] + G[3 * j + i]) - (i == j ? div / 3.0 : 0.0);
+            sum += s * s;
+        }
+    return 2.0 * sum;
+}
+
+// Frozen transport coefficients of one solveTransport (k_omega.cpp:75-81).
+__global__ void kTransportCoefficients(int n, double rho, double mu, double beta, double gamma, double sigma_k,
+                                       double sigma_w, double k_min, const double* __restrict__ G,
+                                       const double* __restrict__ mut, const double* __restrict__ k,
+                                       const double* __restrict__ w, double* __restrict__ production,
+                                       double* __restrict__ kdiff, double* __restrict__ wdiff,
+                                       double* __restrict__ wdestruction, double* __restrict__ wproduction) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double p = mut[i] * strainSquared(G + 9 * i);
+    production[i] = p;
+    kdiff[i] = sigma_k * mut[i] + mu;
+    wdiff[i] = sigma_w * mut[i] + mu;
+    wdestruction[i] = (beta * rho) * w[i];
+    wproduction[i] = ((gamma * p) * w[i]) / fmax(k[i], k_min);
+}
+
+__global__ void kDiffusivityTrace(int nb, double mu, double sigma_k, double sigma_w, const double* __restrict__ mut_tr,
+                                  double* __restrict__ kdiff_tr, double* __restrict__ wdiff_tr) {
+    const int fb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fb >= nb) return;
+    kdiff_tr[fb] = sigma_k * mut_tr[fb] + mu;
+    wdiff_tr[fb] = sigma_w * mut_tr[fb] + mu;
+}
+
+__global__ void kScaled(int n, double a, const double* __restrict__ x, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a * x[i];
+}
+
+// Boundary traces of grad(U) (fvm_execution.cpp:240-262): symmetry reflects the
+// tensor, otherwise each component's normal derivative takes its constraint.
+__global__ void kVectorGradientTrace(MeshView m, BcView bu, const double* __restrict__ U,
+                                     const double* __restrict__ G, double* __restrict__ Gtr) {
+    const int fb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fb >= m.n_boundary) return;
+    const int o = m.bown[fb];
+    const double n[3] = {m.bn[3 * fb], m.bn[3 * fb + 1], m.bn[3 * fb + 2]};
+    const double d[3] = {m.bxf[3 * fb] - m.xc[3 * o], m.bxf[3 * fb + 1] - m.xc[3 * o + 1],
+                         m.bxf[3 * fb + 2] - m.xc[3 * o + 2]};
+    double g[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) g[e] = G[9 * o + e];
+    double val[3];
+    const int t = faceCondition<3>(m, bu, fb, NAN, val);
+    if (t == SY) {
+        // 0.5 (g + R g R), R = I - 2 n n^T (include/babelsim/vector.h:107-116)
+        double R[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) R[3 * i + j] = (i == j ? 1.0 : 0.0) - 2 * n[i] * n[j];
+        double r[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double s = 0.0;
+                for (int kk = 0; kk < 3; ++kk)
+                    for (int l = 0; l < 3; ++l) s += R[3 * i + kk] * g[3 * kk + l] * R[3 * l + j];
+                r[3 * i + j] = s;
+            }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) g[e] = 0.5 * (g[e] + r[e]);
+    } else {
+        const double dn = d[0] * n[0] + d[1] * n[1] + d[2] * n[2];
+        const double tg[3] = {d[0] - dn * n[0], d[1] - dn * n[1], d[2] - dn * n[2]};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double* gc = g + 3 * c;
+            double sn = 0.0;
+            if (t == FV) sn = (val[c] - U[3 * o + c] - (gc[0] * tg[0] + gc[1] * tg[1] + gc[2] * tg[2])) / dn;
+            else if (t == FG) sn = val[c];
+            const double k = sn - (gc[0] * n[0] + gc[1] * n[1] + gc[2] * n[2]);
+            gc[0] += k * n[0];
+            gc[1] += k * n[1];
+            gc[2] += k * n[2];
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) Gtr[9 * fb + e] = g[e];
+}
+
+// muEff (G^T - 2/3 tr(G) I) (model.cpp:65-69); `count` tensors, one mu each.
+__global__ void kStressRemainder(int count, const double* __restrict__ G, const double* __restrict__ mueff,
+                                 double* __restrict__ T) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double* g = G + 9 * i;
+    const double tr = g[0] + g[4] + g[8];
+    const double m = mueff[i];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) T[9 * i + 3 * c + d] = m * (g[3 * d + c] - (c == d ? (2.0 / 3.0) * tr : 0.0));
+}
+
+// divergence(TensorField) with linear row reconstruction (operators.cpp:1568-1591), gathered per cell.
+__global__ void kTensorDivergence(MeshView m, const double* __restrict__ T, const double* __restrict__ Ttr,
+                                  double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n_cells) return;
+    const double V = m.V[i];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int s = m.cf_ptr[i]; s < m.cf_ptr[i + 1]; ++s) {
+        const int f = m.cf_face[s];
+        const int o = m.own[f], nb = m.nbr[f];
+        const double w = m.w[f];
+        const double* S = m.Sf + 3 * f;
+        const bool owner = o == i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double fv[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) fv[d] = w * T[9 * o + 3 * c + d] + (1.0 - w) * T[9 * nb + 3 * c + d];
+            const double q = (fv[0] * S[0] + fv[1] * S[1] + fv[2] * S[2]) / V;
+            acc[c] = owner ? acc[c] + q : acc[c] - q;
+        }
+    }
+    for (int fb = m.cb_ptr[i]; fb < m.cb_ptr[i + 1]; ++fb) {
+        const double* S = m.bSf + 3 * fb;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double* t = Ttr + 9 * fb + 3 * c;
+            acc[c] += (t[0] * S[0] + t[1] * S[1] + t[2] * S[2]) / V;
+        }
+    }
+    out[3 * i] = acc[0];
+    out[3 * i + 1] = acc[1];
+    out[3 * i + 2] = acc[2];
+}
+
+void makeCalculated(DeviceField& f, int n_boundary) {
+    f.calculated = true;
+    f.trace.resize(static_cast<std::size_t>(n_boundary) * f.comps);
+}
+
+}  // namespace
+
+KOmegaModel::KOmegaModel(DeviceMesh& mesh, const KOmegaConfig& cfg)
+    : m_(mesh), ctx_(*mesh.ctx), cfg_(cfg), k_(mesh, 0, 1), omega_(mesh, 0, 1), mut_(mesh, 0, 1), muEff_(mesh, 0, 1),
+      kDiff_(mesh, 0, 1), wDiff_(mesh, 0, 1), krylov_(*mesh.ctx) {
+    if (!(cfg.rho > 0) || !(cfg.mu > 0)) fail(kArgument, "density and dynamicViscosity must be positive");
+    for (double v : {cfg.beta_star, cfg.beta, cfg.gamma, cfg.sigma_k, cfg.sigma_omega, cfg.k_min, cfg.omega_min,
+                     cfg.viscosity_ratio_max, cfg.tolerance})
+        if (!(v > 0) || !std::isfinite(v)) fail(kArgument, "k-omega constants and bounds must be positive and finite");
+    if (!(cfg.relaxation > 0 && cfg.relaxation <= 1)) fail(kArgument, "turbulenceRelaxation must be in (0,1]");
+    if (cfg.momentum_options.interpolation != 0)
+        fail(kArgument, "the device stress-remainder divergence reconstructs the tensor rows linearly");
+    const int nb = mesh.n_boundary;
+    for (DeviceField* f : {&mut_, &muEff_, &kDiff_, &wDiff_}) makeCalculated(*f, nb);
+    const std::size_t N = mesh.n_cells;
+    G_.resize(9 * N);
+    T_.resize(9 * N);
+    Gtr_.resize(9 * static_cast<std::size_t>(std::max(nb, 1)));
+    Ttr_.resize(9 * static_cast<std::size_t>(std::max(nb, 1)));
+    for (DeviceArray<double>* a : {&production_, &wDestruction_, &wProduction_, &kSink_, &prevK_, &prevW_}) a->resize(N);
+    keq_ = std::make_unique<DeviceEquation>(k_, cfg.k_options);
+    weq_ = std::make_unique<DeviceEquation>(omega_, cfg.omega_options);
+}
+
+KOmegaModel::~KOmegaModel() = default;
+
+void KOmegaModel::boundOmega() {
+    const int N = m_.n_cells;
+    launch(ctx_, kBoundOmega, N, N, cfg_.omega_min, cfg_.rho, cfg_.viscosity_ratio_max * cfg_.mu,
+           (const double*)k_.v.data(), omega_.v.data());
+}
+
+void KOmegaModel::updateViscosity() {
+    const int N = m_.n_cells;
+    launch(ctx_, kViscosity, N, N, cfg_.rho, cfg_.mu, cfg_.omega_min, (const double*)k_.v.data(),
+           (const double*)omega_.v.data(), mut_.v.data(), muEff_.v.data());
+    if (m_.n_boundary)
+        launch(ctx_, kViscosityTrace, m_.n_boundary, view(m_), k_.bcView(), omega_.bcView(),
+               (const double*)k_.v.data(), (const double*)omega_.v.data(), cfg_.rho, cfg_.mu, cfg_.omega_min,
+               mut_.trace.data(), muEff_.trace.data());
+}
+
+void KOmegaModel::start(const DeviceField& phi) {
+    // boundTransportFields() then updateViscosity() (k_omega.cpp:51-56, 130-136)
+    k_.setFluxContext(phi);
+    omega_.setFluxContext(phi);
+    launch(ctx_, kBoundK, m_.n_cells, m_.n_cells, cfg_.k_min, k_.v.data());
+    boundOmega();
+    updateViscosity();
+}
+
+void KOmegaModel::gradientWithTraces(DeviceField& U) {
+    gradient(U, cfg_.momentum_options.gradient, G_);
+    if (m_.n_boundary)
+        launch(ctx_, kVectorGradientTrace, m_.n_boundary, view(m_), U.bcView(), (const double*)U.v.data(),
+               (const double*)G_.data(), Gtr_.data());
+}
+
+void KOmegaModel::stressRemainderDivergence(DeviceField& U, double* out) {
+    gradientWithTraces(U);
+    const int N = m_.n_cells, nb = m_.n_boundary;
+    launch(ctx_, kStressRemainder, N, N, (const double*)G_.data(), (const double*)muEff_.v.data(), T_.data());
+    if (nb) launch(ctx_, kStressRemainder, nb, nb, (const double*)Gtr_.data(), (const double*)muEff_.trace.data(), Ttr_.data());
+    launch(ctx_, kTensorDivergence, N, view(m_), (const double*)T_.data(), (const double*)Ttr_.data(), out);
+}
+
+TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
+    BSG_PROFILE(ctx_, "komega_transport");
+    const int N = m_.n_cells, nb = m_.n_boundary;
+    TransportResult res;
+    copyAsync(ctx_, prevK_.data(), k_.v.data(), N);
+    copyAsync(ctx_, prevW_.data(), omega_.v.data(), N);
+    U.setFluxContext(phi);
+    updateViscosity();
+    gradient(U, cfg_.momentum_options.gradient, G_);
+    launch(ctx_, kTransportCoefficients, N, N, cfg_.rho, cfg_.mu, cfg_.beta, cfg_.gamma, cfg_.sigma_k, cfg_.sigma_omega,
+           cfg_.k_min, (const double*)G_.data(), (const double*)mut_.v.data(), (const double*)k_.v.data(),
+           (const double*)omega_.v.data(), production_.data(), kDiff_.v.data(), wDiff_.v.data(),
+           wDestruction_.data(), wProduction_.data());
+    if (nb) launch(ctx_, kDiffusivityTrace, nb, nb, cfg_.mu, cfg_.sigma_k, cfg_.sigma_omega,
+                   (const double*)mut_.trace.data(), kDiff_.trace.data(), wDiff_.trace.data());
+    double* h = ctx_.pinned;
+    auto solveOne = [&](DeviceEquation& eq, DeviceField& x, DeviceField& diff, const double* sink, const double* src,
+                        const double* previous, const SolverConfig& scfg, Reducer& red, double& r0) {
+        eq.reset();
+        addConvection(eq, phi, cfg_.rho, eq.options);
+        addLaplacian(eq, &diff, 0.0, -1.0, eq.options);
+        addReaction(eq, sink, 0.0, 1.0);
+        addSource(eq, src, 1.0);
+        relativeResidualNorms(eq, x.v.data(), red);
+        BSG_CUDA(cudaMemcpyAsync(h, red.result.data(), 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+        ctx_.sync();
+        r0 = std::sqrt(h[0]) / std::max(std::sqrt(h[1]) + std::sqrt(h[2]), 1e-30);
+        relax(eq, previous, cfg_.relaxation);
+        Dcsr<double> A{N, m_.cf_ptr.data(), m_.cf_col.data(), eq.diag.data(), eq.val.data(), 2LL * m_.n_interior};
+        JacobiPreconditioner jac;
+        jac.diag = eq.diag.data();
+        jac.n = N;
+        const SolveOutcome o = scfg.solver == 0 ? krylov_.solveScalar(A, scfg, &jac, eq.src.data(), x.v.data())
+                                                : krylov_.solveBicgstab(A, scfg, eq.src.data(), x.v.data());
+        res.iterations += o.iterations;
+        res.linear_converged = res.linear_converged && o.status == 0;
+        res.healthy = res.healthy && o.status != 2 && std::isfinite(o.final_) && std::isfinite(r0);
+    };
+    // omega first, then k with the new omega in its sink (k_omega.cpp:83-110)
+    double rW = 0.0, rK = 0.0;
+    solveOne(*weq_, omega_, wDiff_, wDestruction_.data(), wProduction_.data(), prevW_.data(), cfg_.omega_solver, redW_,
+             rW);
+    if (!res.healthy) return res;
+    boundOmega();
+    launch(ctx_, kScaled, N, N, cfg_.beta_star * cfg_.rho, (const double*)omega_.v.data(), kSink_.data());
+    solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK);
+    if (!res.healthy) return res;
+    // boundTransportFields(); updateViscosity() (k_omega.cpp:114-116)
+    k_.setFluxContext(phi);
+    omega_.setFluxContext(phi);
+    launch(ctx_, kBoundK, N, N, cfg_.k_min, k_.v.data());
+    boundOmega();
+    updateViscosity();
+    relativeChangeNorms(ctx_, omega_.v.data(), prevW_.data(), N, redDW_);
+    relativeChangeNorms(ctx_, k_.v.data(), prevK_.data(), N, redDK_);
+    BSG_CUDA(cudaMemcpyAsync(h, redDW_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    BSG_CUDA(cudaMemcpyAsync(h + 2, redDK_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    ctx_.sync();
+    const double dW = std::sqrt(h[0]) / std::max(std::sqrt(h[1]), 1e-30);
+    const double dK = std::sqrt(h[2]) / std::max(std::sqrt(h[3]), 1e-30);
+    res.change = std::max(dW, dK);
+    res.residual = std::max(rW, rK);
+    res.healthy = res.healthy && std::isfinite(res.change);
+    return res;
+}
+
+}  // namespace bsg

@@ -69,12 +69,27 @@ SimpleSolver::SimpleSolver(DeviceMesh& mesh, const SimpleConfig& cfg)
 
 SimpleSolver::~SimpleSolver() = default;
 
+void SimpleSolver::enableKOmega(const KOmegaConfig& cfg) {
+    if (started_) fail(kState, "the turbulence model must be chosen before the fields are set");
+    KOmegaConfig c = cfg;
+    c.rho = cfg_.rho;
+    c.mu = cfg_.mu;
+    c.momentum_options = cfg_.momentum;
+    turb_ = std::make_unique<KOmegaModel>(m_, c);
+    divStress_.resize(3 * static_cast<std::size_t>(m_.n_cells));
+}
+
 void SimpleSolver::start() {
     // pPrime = homogeneousLike(p) (field.h:380-420)
     for (int patch = 0; patch < m_.n_patches; ++patch) {
         const int t = p_.bcs[patch].type;
         const double zero[3] = {0, 0, 0};
         pP_.setBoundary(patch, t == 0 ? 0 : (t == 4 ? 4 : 2), zero);
+    }
+    if (turb_) {
+        // rans::load runs before phi = flux(U) (simple/main.cpp:33-40): the model sees phi = 0
+        phi_.v.zero(ctx_.stream);
+        turb_->start(phi_);
     }
     faceFlux(U_, cfg_.momentum.interpolation, cfg_.momentum.gradient, phi_);
     const int pcType = cfg_.pressure_solver.preconditioner;
@@ -113,9 +128,14 @@ void SimpleSolver::outerIteration() {
         BSG_PROFILE(ctx_, "momentum_assembly");
         mom.reset();
         addConvection(mom, phi_, cfg_.rho, cfg_.momentum);
-        addLaplacian(mom, &muEff_, 0.0, -1.0, cfg_.momentum);
+        addLaplacian(mom, turb_ ? &turb_->effectiveViscosity() : &muEff_, 0.0, -1.0, cfg_.momentum);
         gradient(p_, cfg_.pressure.gradient, gradP_);
         addSource(mom, gradP_.data(), -1.0);
+        if (turb_) {
+            // explicit remainder of the eddy-viscosity stress (simple/main.cpp:54-56)
+            turb_->stressRemainderDivergence(U_, divStress_.data());
+            addSource(mom, divStress_.data(), 1.0);
+        }
     }
     // rU before relaxation (simple/main.cpp:59-60).
     // The norms stay on the device and are read with the other diagnostics: a
@@ -185,6 +205,16 @@ void SimpleSolver::outerIteration() {
     gradient(pP_, cfg_.pressure.gradient, gradPP_);
     subtractScaledGradient(m_, U_.v.data(), rAU_.v.data(), gradPP_.data());
     addArrays(ctx_, phi_.v.data(), phiH_.v.data(), pflux_.data(), m_.n_faces);
+    // turbulence transport after the flow update (simple/main.cpp:102-110)
+    TransportResult tr;
+    if (turb_) {
+        tr = turb_->solveTransport(U_, phi_);
+        report_.turbulence_change = tr.change;
+        report_.turbulence_residual = tr.residual;
+        if (!tr.healthy) { report_.status = 2; return; }
+    }
+    const bool turbulence_ok = !turb_ || (tr.linear_converged && tr.change <= turb_->config().tolerance &&
+                                          tr.residual <= turb_->config().tolerance);
     // Convergence diagnostics (simple/main.cpp:112-126).
     relativeChangeNorms(ctx_, U_.v.data(), Uprev_.data(), 3LL * N, redU_);
     relativeChangeNorms(ctx_, pP_.v.data(), nullptr, N, redPP_);
@@ -209,7 +239,7 @@ void SimpleSolver::outerIteration() {
     report_.iterations += 1;
     if (!(std::isfinite(dU) && std::isfinite(dP) && std::isfinite(mass))) { report_.status = 2; return; }
     const bool linear_ok = mom_ok && p_ok;
-    report_.converged = linear_ok && rU <= cfg_.momentum_tolerance && dU <= cfg_.velocity_tolerance &&
+    report_.converged = linear_ok && turbulence_ok && rU <= cfg_.momentum_tolerance && dU <= cfg_.velocity_tolerance &&
                         dP <= cfg_.pressure_tolerance && mass <= cfg_.mass_tolerance;
     report_.status = report_.converged ? 0 : 1;
 }

@@ -3,6 +3,7 @@
 
 #include "fvm.h"
 #include "linalg.h"
+#include "rans.h"
 
 #include <memory>
 
@@ -25,6 +26,7 @@ struct SimpleReport {
     int status = 1;
     double mass = 0, dU = 0, rU = 0, dP = 0, linP = 0;
     int momentum_iterations = 0, pressure_iterations = 0;
+    double turbulence_change = 0, turbulence_residual = 0;
 };
 
 class SimpleSolver {
@@ -40,6 +42,9 @@ public:
     SimpleReport iterate(int max_iterations);
     // Overwrite U, p, phi from host memory (caller numbering) keeping all other state.
     void loadState(const double* U, const double* p, const double* phi);
+    // Wilcox-1988m k-omega eddy viscosity (rans::load with turbulenceModel kOmega); call before start().
+    void enableKOmega(const KOmegaConfig& cfg);
+    KOmegaModel* turbulence() { return turb_.get(); }
     const SimpleReport& report() const { return report_; }
 
 private:
@@ -49,6 +54,8 @@ private:
     SimpleConfig cfg_;
     DeviceField U_, p_, phi_, pP_, muEff_, rAU_, phiH_;
     std::unique_ptr<DeviceEquation> mom_, peq_;
+    std::unique_ptr<KOmegaModel> turb_;
+    DeviceArray<double> divStress_;
     KrylovSolver krylov_;
     std::unique_ptr<Preconditioner> ppc_;
     Reducer red_, redU_, redPP_, redP_, redM_;  // one per diagnostic, read back together

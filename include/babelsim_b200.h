@@ -295,7 +295,24 @@ typedef struct {
     double linear_pressure_residual;
     int32_t momentum_iterations;        /* Krylov iterations in the last outer iteration */
     int32_t pressure_iterations;
+    double turbulence_change;           /* max relative change of the transported turbulence fields */
+    double turbulence_residual;         /* max initial normalised residual of their equations */
 } bsg_simple_report;
+
+/* Wilcox-1988m k-omega (src/physics/RANS/k_omega.cpp:25-160): physics keys
+ * kOmegaBetaStar/Beta/Gamma/SigmaK/SigmaOmega, kMin, omegaMin,
+ * maxTurbulentViscosityRatio; solution keys turbulenceRelaxation and
+ * turbulenceTolerance; equation controls kTransport and omegaTransport. */
+typedef struct {
+    double beta_star, beta, gamma, sigma_k, sigma_omega;
+    double k_min, omega_min, max_viscosity_ratio;
+    double relaxation;
+    double tolerance;
+    bsg_options k_transport;
+    bsg_options omega_transport;
+    bsg_solver_config k_solver;
+    bsg_solver_config omega_solver;
+} bsg_komega_config;
 
 int bsg_simple_create(bsg_mesh* mesh, const bsg_simple_config* config, bsg_simple** out);
 /* Boundary constraint of "U" or "p" on one patch (the case's fields/initial). */
@@ -311,6 +328,13 @@ int bsg_simple_set_flux(bsg_simple* s, const double* phi);
 int bsg_simple_load_state(bsg_simple* s, const double* U, const double* p, const double* phi);
 /* Run outer iterations until converged or max_iterations more have been done. */
 int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report* report);
+/* turbulenceModel kOmega (src/physics/RANS/model.cpp:24-53): call after create and
+ * before set_fields; then "k" and "omega" take boundary conditions through
+ * bsg_simple_set_boundary and initial values through set_turbulence_fields. */
+int bsg_simple_enable_komega(bsg_simple* s, const bsg_komega_config* config);
+int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* omega);
+/* k, omega and the turbulent viscosity mut (n_cells each; NULL skips). */
+int bsg_simple_get_turbulence_fields(const bsg_simple* s, double* k, double* omega, double* mut);
 int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi);
 int bsg_simple_destroy(bsg_simple* s);
 
