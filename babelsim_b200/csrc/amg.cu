@@ -260,7 +260,9 @@ AmgPreconditioner::AmgPreconditioner(DeviceMesh& mesh, const SolverConfig& cfg)
     if (!(omega_ > 0.0 && omega_ <= 1.0) || !(gamma_ > 0.0 && gamma_ <= 3.0))
         fail(kArgument, "AMG Jacobi weight must be in (0,1] and the correction scale in (0,3]");
     // FP32 V-cycle data on the mixed-precision path (FP64 Krylov vectors and true residual stay FP64)
-    fp32_ = cfg.precision == 1 || std::getenv("BSG_AMG_FP32") != nullptr;
+    fp32_ = cfg.precision == 1 || cfg.precision == 2 || std::getenv("BSG_AMG_FP32") != nullptr;
+    if (const char* p = std::getenv("BSG_AMG_PASSES0")) passes0_ = std::max(1, std::min(4, std::atoi(p)));
+    if (const char* p = std::getenv("BSG_AMG_PASSES")) passes_ = std::max(1, std::min(4, std::atoi(p)));
 }
 
 AmgPreconditioner::~AmgPreconditioner() {
@@ -290,12 +292,19 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
     l0->buildSell(cur.ptr.data(), cur.col.data(), ctx_.stream);
     levels_.push_back(l0);
     while (cur.n > coarse_target && static_cast<int>(levels_.size()) < max_levels) {
-        int n1 = 0, n2 = 0;
-        const std::vector<int> a1 = pairwise(cur, n1);
-        const HostCsr c1 = coarsen(cur, a1, n1, nullptr);
-        const std::vector<int> a2 = pairwise(c1, n2);
+        // aggregates from `passes` rounds of pairwise matching (2 by default: up to 4 rows)
+        const int passes = levels_.size() == 1 ? passes0_ : passes_;
+        int n2 = cur.n;
         std::vector<int> agg(cur.n);
-        for (int i = 0; i < cur.n; ++i) agg[i] = a2[a1[i]];
+        for (int i = 0; i < cur.n; ++i) agg[i] = i;
+        HostCsr work = cur;
+        for (int pass = 0; pass < passes; ++pass) {
+            int nn = 0;
+            const std::vector<int> a = pairwise(pass == 0 ? cur : work, nn);
+            if (pass + 1 < passes) work = coarsen(pass == 0 ? cur : work, a, nn, nullptr);
+            for (int i = 0; i < cur.n; ++i) agg[i] = a[agg[i]];
+            n2 = nn;
+        }
         // stop when coarsening stalls (< 1.5x fewer rows): such levels cost a
         // V-cycle their barriers and gathers without shrinking the problem
         if (3 * static_cast<long long>(n2) > 2 * static_cast<long long>(cur.n) && cur.n <= 1024) break;

@@ -58,6 +58,7 @@ private:
     Dcsr<double> fine_{};
     DeviceArray<AmgLevelView<double>> d_views_;
     bool fp32_ = false;
+    int passes0_ = 2, passes_ = 2;  // pairwise-matching rounds per level (level 0, coarser levels)
     DeviceArray<VLevel<double>> d_vl64_;
     DeviceArray<VLevel<float>> d_vl32_;
     DeviceArray<float> dense32_;

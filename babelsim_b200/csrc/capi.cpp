@@ -181,6 +181,7 @@ bsg::SolverConfig solverConfig(const bsg_solver_config* c) {
             "linear solver tolerances or iteration limit are invalid");
     require(r.solver >= 0 && r.solver <= 3, "unknown linear solver type");
     require(r.preconditioner >= 0 && r.preconditioner <= 6, "unknown preconditioner type");
+    require(r.precision >= 0 && r.precision <= 2, "unknown precision mode");
     return r;
 }
 

@@ -645,9 +645,10 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
     for (int attempt = 0; attempt < 3; ++attempt) {
         BSG_CUDA(cudaMemcpyAsync(m.pst.data(), &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
         if (amg && amg->fp32VCycle()) {
+            // FP64 Krylov vectors and products, FP32 V-cycle, flexible beta
             SellPcgArgs<double, float> args{amg->krylovMatrix(), amg->sellView32(), b, x, m.r.data(), m.z.data(),
                                             m.p.data(), m.v.data(), m.q.data(), m.partial.data(), m.pst.data(),
-                                            PhaseLog{}};
+                                            PhaseLog{}, 1};
             launchSellPcg(ctx, args);
         } else if (amg) {
             SellPcgArgs<double, double> args{amg->krylovMatrix(), amg->sellView64(), b, x, m.r.data(), m.z.data(),

@@ -12,6 +12,11 @@ namespace bsg {
 namespace {
 
 constexpr int SB = 256;  // threads per block
+// Minimum resident blocks per SM the register budget must allow: 3 (80 registers)
+// measured faster than 4 (64) on the 1M-cell pressure solves, 2 (128) slower.
+#ifndef BSG_SELL_MIN_BLOCKS
+#define BSG_SELL_MIN_BLOCKS 3
+#endif
 
 struct Lanes {
     int lane, gwarp, nwarps, gthread, nthreads;
@@ -225,7 +230,7 @@ __device__ __forceinline__ void seedLevel0(const VLevel<TV>& f0, int i, TK ri) {
 }
 
 template <class TK, class TV>
-__global__ void __launch_bounds__(SB, 4) kPcgSell(SellPcgArgs<TK, TV> a) {
+__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<TK, TV> a) {
     cg::grid_group g = cg::this_grid();
     const Lanes c = lanes();
     const SellMat<TK>& A = a.A;
@@ -312,17 +317,19 @@ __global__ void __launch_bounds__(SB, 4) kPcgSell(SellPcgArgs<TK, TV> a) {
         if (!(fabs(pq[0]) > 0.0) || !isfinite(pq[0])) { status = 2; break; }
         const double alpha = rz / pq[0];
         const TK ak = static_cast<TK>(alpha);
-        double nr[1] = {0.0};
+        double nr[2] = {0.0, 0.0};
         for (int i = c.gthread; i < n; i += c.nthreads) {
             a.x[i] += ak * pnew[i];
             const TK ri = a.r[i] - ak * a.q[i];
             a.r[i] = ri;
             seedLevel0<TK, TV>(f0, i, ri);
             nr[0] += static_cast<double>(ri) * static_cast<double>(ri);
+            if (a.flexible) nr[1] += static_cast<double>(ri) * static_cast<double>(a.z[i]);  // r_new . z_old
         }
-        gridSum<1>(g, nr, a.partial, buf);
+        gridSum<2>(g, nr, a.partial, buf);
         mark(a.log, 3);
         rr = nr[0];
+        const double rz_old_new = nr[1];
         ++it;
         if (!isfinite(rr)) { status = 2; break; }
         if (rr <= target2) { status = 0; break; }
@@ -330,7 +337,7 @@ __global__ void __launch_bounds__(SB, 4) kPcgSell(SellPcgArgs<TK, TV> a) {
         double zr[1] = {vcycle<TK, TV>(g, a.V, a.r, a.z, a.log)};
         gridSum<1>(g, zr, a.partial, buf);
         mark(a.log, 4);
-        beta = zr[0] / rz;
+        beta = a.flexible ? (zr[0] - rz_old_new) / rz : zr[0] / rz;
         rz = zr[0];
         TK* tmp = pold;
         pold = pnew;

@@ -65,6 +65,10 @@ struct SellPcgArgs {
     double* partial;
     PcgState* st;
     PhaseLog log;
+    // 1: flexible (Polak-Ribiere) beta = r_new.(z_new - z_old) / r_old.z_old, for a
+    // preconditioner that is not exactly the same linear operator every iteration
+    // (an FP32 V-cycle); 0: beta = r_new.z_new / r_old.z_old.
+    int flexible = 0;
 };
 
 // Launch (pcg_sell.cu); the grid is sized for co-residency.

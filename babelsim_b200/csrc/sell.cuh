@@ -18,6 +18,11 @@
 namespace bsg {
 
 constexpr int kSellC = 32;
+// Entries each thread loads before it gathers (memory-level parallelism of a row sweep).
+#ifndef BSG_SELL_BATCH
+#define BSG_SELL_BATCH 4
+#endif
+constexpr int kSellBatch = BSG_SELL_BATCH;
 
 template <class T>
 struct SellMat {
@@ -72,16 +77,23 @@ __device__ __forceinline__ T sellRow(const SellMat<T>& A, int s, int lane, Y y) 
     const T* __restrict__ v = A.val + beg + lane;
     T a0 = T(0), a1 = T(0);
     int k = 0;
-    for (; k + 4 <= w; k += 4) {
-        const int c0 = __ldg(c + 32 * k), c1 = __ldg(c + 32 * (k + 1));
-        const int c2 = __ldg(c + 32 * (k + 2)), c3 = __ldg(c + 32 * (k + 3));
-        const T v0 = __ldg(v + 32 * k), v1 = __ldg(v + 32 * (k + 1));
-        const T v2 = __ldg(v + 32 * (k + 2)), v3 = __ldg(v + 32 * (k + 3));
-        const T y0 = y(c0), y1 = y(c1), y2 = y(c2), y3 = y(c3);
-        a0 += v0 * y0;
-        a1 += v1 * y1;
-        a0 += v2 * y2;
-        a1 += v3 * y3;
+    // batches of SELL_BATCH entries: all index and value loads first, then all gathers
+    for (; k + kSellBatch <= w; k += kSellBatch) {
+        int cc[kSellBatch];
+        T vv[kSellBatch];
+#pragma unroll
+        for (int u = 0; u < kSellBatch; ++u) {
+            cc[u] = __ldg(c + 32 * (k + u));
+            vv[u] = __ldg(v + 32 * (k + u));
+        }
+        T yy[kSellBatch];
+#pragma unroll
+        for (int u = 0; u < kSellBatch; ++u) yy[u] = y(cc[u]);
+#pragma unroll
+        for (int u = 0; u < kSellBatch; u += 2) {
+            a0 += vv[u] * yy[u];
+            if (u + 1 < kSellBatch) a1 += vv[u + 1] * yy[u + 1];
+        }
     }
     for (; k < w; ++k) a0 += __ldg(v + 32 * k) * y(__ldg(c + 32 * k));
     return a0 + a1;

@@ -58,8 +58,10 @@ enum { BSG_KSP_CG = 0, BSG_KSP_BICGSTAB = 1, BSG_KSP_GMRES = 2, BSG_KSP_FGMRES =
 enum { BSG_PC_NONE = 0, BSG_PC_ICC = 1, BSG_PC_HYPRE = 2, BSG_PC_GAMG = 3,
        BSG_PC_BJACOBI = 4, BSG_PC_ASM = 5, BSG_PC_JACOBI = 6 };
 enum { BSG_CONVERGED = 0, BSG_MAX_ITERATIONS = 1, BSG_NUMERICAL_FAILURE = 2 };
-/* Precision of the inner Krylov/AMG iterations (north-star form (c)). */
-enum { BSG_PRECISION_FP64 = 0, BSG_PRECISION_FP32_REFINED = 1 };
+/* Precision of the inner Krylov/AMG iterations: all FP64; FP32 CG and FP32
+ * V-cycles inside FP64 iterative refinement; or FP64 (flexible) CG with FP32
+ * V-cycles.  The acceptance test is the FP64 true residual in every case. */
+enum { BSG_PRECISION_FP64 = 0, BSG_PRECISION_FP32_REFINED = 1, BSG_PRECISION_FP32_PRECONDITIONER = 2 };
 /* Field locations, include/babelsim/field.h:17-21 */
 enum { BSG_CELL = 0, BSG_FACE = 1 };
 
@@ -147,9 +149,11 @@ int bsg_context_profile_report(bsg_context* ctx, char* buffer, int32_t capacity)
 /* Phase timeline of the persistent solver kernels: with capacity > 0, each grid
  * barrier appends (phase id, device nanoseconds) until `capacity` entries;
  * capacity 0 turns it off.  Reading returns the entries and clears the log.
- * Phase ids: 1 initial residual, 2 SpMV+dot, 3 update+norm, 4 r.z, 10+l
- * pre-smoothing of level l, 30+l restriction from level l, 50 coarsest solve,
- * 60+l prolongation + first post sweep, 80+l second post sweep. */
+ * Phase ids: 1 initial residual, 2 SpMV+dot, 3 update+norm, 4 r.z (and the
+ * level-0 post sweep before it), 10+l pre-smoothing of level l, 30+l residual
+ * of level l, 100+l restriction to level l+1, 50 coarsest solve, 60+l first
+ * post sweep (when a second follows), 80+l last post sweep of level l > 0 with
+ * its prolongation into level l-1. */
 int bsg_context_phase_log(bsg_context* ctx, int32_t capacity);
 int bsg_context_phase_log_read(bsg_context* ctx, int64_t* pairs, int32_t capacity, int32_t* count);
 /* CUDA events on the context's stream, for timing a region of calls:

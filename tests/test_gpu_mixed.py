@@ -1,5 +1,6 @@
-"""Mixed precision (FP32 inner PCG and FP32 AMG V-cycles inside FP64 iterative
-refinement) against the FP64 path, the direct solve and the reference.
+"""Mixed precision against the FP64 path, the direct solve and the reference: FP32
+inner PCG and FP32 AMG V-cycles inside FP64 iterative refinement (precision 1),
+and FP64 flexible PCG with FP32 V-cycles (precision 2).
 
 Tolerances: the refined solve meets the same FP64 true-residual contract as
 the FP64 path, so solutions agree with a direct solve to 1e-8 (rtol 1e-12) and
@@ -23,8 +24,9 @@ def ctx():
     c.close()
 
 
+@pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("rtol", [1e-12, 1e-8])
-def test_refined_pressure_solve(ctx, rtol):
+def test_refined_pressure_solve(ctx, rtol, precision):
     import babelsim_b200 as bsg
     import scipy.sparse.linalg as spla
     g = Golden("cavity64_config1")
@@ -34,7 +36,7 @@ def test_refined_pressure_solve(ctx, rtol):
     ldu = fvm.LDU(geo, False)
     ldu.diag, ldu.upper, ldu.lower, ldu.source = sysp["diag"], sysp["upper"], sysp["lower"], sysp["source"]
     exact = spla.spsolve(ldu.matrix().tocsc(), ldu.source)
-    cfg = bsg.solver_config("cg", "hypre", 1e-30, rtol, 20000, precision=1)
+    cfg = bsg.solver_config("cg", "hypre", 1e-30, rtol, 20000, precision=precision)
     x, res = bsg.solve_ldu(m, cfg, sysp["diag"], sysp["upper"], sysp["lower"], sysp["source"])
     assert res[0].status == 0
     # FP64 true residual contract, whatever the inner precision
@@ -44,8 +46,9 @@ def test_refined_pressure_solve(ctx, rtol):
     m.close()
 
 
+@pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("name", ["warped5_corrected", "cavity64_config1"])
-def test_mixed_simple_converges_to_reference(ctx, name):
+def test_mixed_simple_converges_to_reference(ctx, name, precision):
     import babelsim_b200 as bsg
     g = Golden(name)
     m = bsg.Mesh.from_polyhedral(ctx, g.poly)
@@ -57,7 +60,8 @@ def test_mixed_simple_converges_to_reference(ctx, name):
                      bsg.solver_config("bcgs", "bjacobi", sol["equation.momentum.absoluteTolerance"],
                                        sol["equation.momentum.relativeTolerance"], 2000),
                      bsg.solver_config("cg", "hypre", sol["equation.pressureCorrection.absoluteTolerance"],
-                                       sol["equation.pressureCorrection.relativeTolerance"], 20000, precision=1))
+                                       sol["equation.pressureCorrection.relativeTolerance"], 20000,
+                                       precision=precision))
     for p, (t, v) in enumerate(g.meta["U_bcs"]):
         sim.set_boundary("U", p, t, v)
     for p, (t, v) in enumerate(g.meta["p_bcs"]):
