@@ -89,11 +89,13 @@ def write_mesh(path, mesh: PolyMesh):
         fh.write("\n".join(lines) + "\n")
 
 
-def hex_box(nx, ny, nz, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), names=None, kinds=None, warp=None) -> PolyMesh:
+def hex_box(nx, ny, nz, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), names=None, kinds=None, warp=None,
+            flat=False) -> PolyMesh:
     """Structured hexahedra; cell (a,b,c) has index a + nx*(b + ny*c).
 
     Patches, in order: minus_x, plus_x, minus_y, plus_y, minus_z, plus_z (or
-    ``names``).  ``warp(points)`` may move the vertices.
+    ``names``).  ``warp(points)`` may move the vertices.  ``flat`` stores the face
+    rings as offsets/ids arrays (large meshes) instead of a list.
     """
     lo, hi = np.asarray(lo, float), np.asarray(hi, float)
     a, b, c = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
@@ -156,7 +158,24 @@ def hex_box(nx, ny, nz, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), names=None, kind
     patch = np.concatenate([np.full(len(own_i), -1), pat_b]).astype(np.int32)
     names = names or ["minus_x", "plus_x", "minus_y", "plus_y", "minus_z", "plus_z"]
     kinds = kinds or ["generic"] * 6
+    if flat:
+        offsets = (4 * np.arange(len(rings) + 1)).astype(np.int32)
+        return PolyMesh(verts, None, owner, neighbour, patch, list(names), list(kinds), offsets=offsets,
+                        ids=rings.astype(np.int32).ravel())
     return PolyMesh(verts, list(rings), owner, neighbour, patch, list(names), list(kinds))
+
+
+def channel(nx: int, ny: int, nz: int, length=2 * np.pi, height=2.0, width=np.pi, stretch=2.0, flat=True) -> PolyMesh:
+    """Plane channel of hexahedra, wall-normal (y) spacing clustered at both walls by
+    tanh stretching.  Patches: inlet, outlet, lower, upper (walls), front, back."""
+    def warp(p):
+        q = p.copy()
+        eta = p[:, 1] / height * 2.0 - 1.0                    # [-1, 1]
+        q[:, 1] = 0.5 * height * (1.0 + np.tanh(stretch * eta) / np.tanh(stretch))
+        return q
+    return hex_box(nx, ny, nz, (0.0, 0.0, 0.0), (length, height, width), warp=warp, flat=flat,
+                   names=["inlet", "outlet", "lower", "upper", "front", "back"],
+                   kinds=["inlet", "outlet", "wall", "wall", "symmetry", "symmetry"])
 
 
 def cavity_2d(n: int) -> PolyMesh:
@@ -184,6 +203,58 @@ def warped_box(n: int, amplitude=0.08, seed=7) -> PolyMesh:
                    kinds=["wall"] * 6)
 
 
+
+
+def cylinder_ogrid(n_theta: int, n_r: int, r0: float = 0.5, radius: float = 15.0, growth: float = 1.05,
+                   dz: float = 0.1) -> PolyMesh:
+    """O-grid of hexahedra around a circular cylinder (diameter 2 r0), one cell thick.
+
+    Radial layers grow geometrically by `growth` from the cylinder to `radius`.
+    Cell (a, b) has radial index a and angular index b (angles wrap around), index
+    a + n_r b.  Patches: cylinder, inlet (outer faces with x < 0), outlet (outer
+    faces with x >= 0), front, back.
+    """
+    a = np.arange(n_r + 1)
+    h0 = (radius - r0) * (growth - 1.0) / (growth ** n_r - 1.0) if growth != 1.0 else (radius - r0) / n_r
+    r = r0 + (h0 * (growth ** a - 1.0) / (growth - 1.0) if growth != 1.0 else h0 * a)
+    th = 2.0 * np.pi * np.arange(n_theta) / n_theta
+    A, B, Cz = np.meshgrid(np.arange(n_r + 1), np.arange(n_theta), np.arange(2), indexing="ij")
+    A, B, Cz = A.ravel(order="F"), B.ravel(order="F"), Cz.ravel(order="F")
+    verts = np.stack([r[A] * np.cos(th[B]), r[A] * np.sin(th[B]), dz * Cz], axis=1)
+
+    def vid(i, j, k):
+        return i + (n_r + 1) * ((j % n_theta) + n_theta * k)
+
+    def cid(i, j):
+        return i + n_r * (j % n_theta)
+    # radial faces between (a-1, b) and (a, b)
+    I, J = np.meshgrid(np.arange(1, n_r), np.arange(n_theta), indexing="ij")
+    I, J = I.ravel(), J.ravel()
+    rings_a = np.stack([vid(I, J, 0), vid(I, J + 1, 0), vid(I, J + 1, 1), vid(I, J, 1)], axis=1)
+    own_a, nbr_a = cid(I - 1, J), cid(I, J)
+    # angular faces between (a, b-1) and (a, b), wrapping at b = 0
+    I2, J2 = np.meshgrid(np.arange(n_r), np.arange(n_theta), indexing="ij")
+    I2, J2 = I2.ravel(), J2.ravel()
+    rings_b = np.stack([vid(I2, J2, 0), vid(I2, J2, 1), vid(I2 + 1, J2, 1), vid(I2 + 1, J2, 0)], axis=1)
+    own_b, nbr_b = cid(I2, J2 - 1), cid(I2, J2)
+    # boundary faces
+    jj = np.arange(n_theta)
+    ring_cyl = np.stack([vid(0, jj, 0), vid(0, jj + 1, 0), vid(0, jj + 1, 1), vid(0, jj, 1)], axis=1)
+    ring_out = np.stack([vid(n_r, jj, 0), vid(n_r, jj + 1, 0), vid(n_r, jj + 1, 1), vid(n_r, jj, 1)], axis=1)
+    mid = 0.5 * (np.cos(th) + np.cos(th + 2 * np.pi / n_theta))
+    out_patch = np.where(mid < 0.0, 1, 2)
+    ii, jj2 = np.meshgrid(np.arange(n_r), np.arange(n_theta), indexing="ij")
+    ii, jj2 = ii.ravel(), jj2.ravel()
+    ring_front = np.stack([vid(ii, jj2, 0), vid(ii + 1, jj2, 0), vid(ii + 1, jj2 + 1, 0), vid(ii, jj2 + 1, 0)], axis=1)
+    ring_back = np.stack([vid(ii, jj2, 1), vid(ii + 1, jj2, 1), vid(ii + 1, jj2 + 1, 1), vid(ii, jj2 + 1, 1)], axis=1)
+    rings = np.concatenate([rings_a, rings_b, ring_cyl, ring_out, ring_front, ring_back]).astype(np.int64)
+    owner = np.concatenate([own_a, own_b, cid(0, jj), cid(n_r - 1, jj), cid(ii, jj2), cid(ii, jj2)]).astype(np.int32)
+    n_int = len(own_a) + len(own_b)
+    neighbour = np.concatenate([nbr_a, nbr_b, np.full(len(owner) - n_int, -1)]).astype(np.int32)
+    patch = np.concatenate([np.full(n_int, -1), np.zeros(n_theta), out_patch, np.full(len(ii), 3),
+                            np.full(len(ii), 4)]).astype(np.int32)
+    return PolyMesh(verts, list(rings), owner, neighbour, patch, ["cylinder", "inlet", "outlet", "front", "back"],
+                    ["wall", "inlet", "outlet", "symmetry", "symmetry"])
 
 
 def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, kinds=None) -> PolyMesh:

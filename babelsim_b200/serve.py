@@ -1,0 +1,160 @@
+"""Serving loop for steady SIMPLE requests (continuous batching at outer-iteration granularity).
+
+Each request carries a case description: a polyhedral mesh, the lid (or inlet) speed
+and the viscosity.  The server admits arrived requests in arrival order while the
+device-memory estimate of everything admitted stays within the HBM budget and a
+slot is free, keeps every admitted solve's fields, matrices and AMG hierarchy
+resident on the device, advances the active solves one outer iteration each in
+turn, and retires a solve when it converges (or reaches its iteration cap),
+freeing its memory for the next admission.  All work runs on one device stream:
+a request's computation is the same sequence of kernels whether it runs alone or
+interleaved with others, so its result is identical in both cases.
+
+The reference serves no requests: its unit of work is one `babelsim-solve` run per
+case (src/runtime/application.cpp:238-272), which is the per-request semantics here.
+"""
+from __future__ import annotations
+
+import heapq
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    id: int
+    arrival: float              # seconds after the stream starts
+    mesh: object                # meshgen.PolyMesh (six patches; lid on patch 3)
+    speed: float = 1.0          # lid speed
+    nu: float = 1e-2            # kinematic = dynamic viscosity (density 1)
+    max_iterations: int = 200
+    tolerance: float = 1e-5     # momentum / velocity / pressure-change tolerance of the outer loop
+
+
+@dataclass
+class Result:
+    id: int
+    cells: int
+    arrival: float
+    admitted: float
+    finished: float
+    iterations: int
+    converged: bool
+    U: np.ndarray | None = None
+    p: np.ndarray | None = None
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+def device_bytes(n_cells: int, n_faces: int) -> int:
+    """Device-memory estimate of one resident SIMPLE solve: geometry (152 B per face,
+    40 B per cell), fields and workspaces (~60 doubles per cell), two LDU systems on
+    the cell-to-face pattern, the AMG hierarchy with its SELL copies (~1.6x the
+    level-0 matrix) and Krylov workspaces."""
+    matrix = 8 * n_cells + 12 * 2 * n_faces
+    return int(152 * n_faces + 40 * n_cells + 480 * n_cells + 2 * matrix + 1.6 * (matrix + 8 * 2 * n_faces) +
+               16 * 8 * n_cells)
+
+
+@dataclass
+class _Active:
+    req: Request
+    mesh: object
+    sim: object
+    admitted: float
+    bytes: int
+    iterations: int = 0
+
+
+@dataclass
+class Server:
+    ctx: object
+    hbm_budget: int = 150 * 2**30
+    slots: int = 8
+    keep_fields: bool = False
+    solver_precision: int = 0
+    log: list = field(default_factory=list)
+
+    def _start(self, req: Request):
+        import babelsim_b200 as bsg
+        m = bsg.Mesh.from_polyhedral(self.ctx, req.mesh)
+        opts = bsg.options("linear", "greenGauss", "upwind", "orthogonal")
+        sim = bsg.Simple(m, 1.0, req.nu, 0.7, 0.3, 1, 1e-6, req.tolerance, req.tolerance, req.tolerance, opts, opts,
+                         bsg.solver_config("bcgs", "bjacobi", 1e-14, 1e-8, 1000),
+                         bsg.solver_config("cg", "hypre", 1e-14, 1e-8, 1000, precision=self.solver_precision))
+        for patch in range(6):
+            sim.set_boundary("U", patch, "fixedValue", (req.speed, 0.0, 0.0) if patch == 3 else (0.0, 0.0, 0.0))
+            sim.set_boundary("p", patch, "zeroGradient")
+        sim.set_fields(np.zeros((m.n_cells, 3)), np.zeros(m.n_cells))
+        return m, sim
+
+    def run(self, requests: list[Request], clock=time.perf_counter) -> list[Result]:
+        """Serve `requests` (arrival times relative to the call) and return one Result each."""
+        pending = sorted(requests, key=lambda r: (r.arrival, r.id))
+        queue: list[tuple[float, int, Request]] = []
+        active: list[_Active] = []
+        results: list[Result] = []
+        used = 0
+        t0 = clock()
+        i = 0
+        turn = 0
+        while i < len(pending) or queue or active:
+            now = clock() - t0
+            while i < len(pending) and pending[i].arrival <= now:
+                heapq.heappush(queue, (pending[i].arrival, pending[i].id, pending[i]))
+                i += 1
+            # admission in arrival order under the slot count and the memory budget
+            while queue and len(active) < self.slots:
+                req = queue[0][2]
+                need = device_bytes(req.mesh.n_cells, len(req.mesh.owner))
+                if need > self.hbm_budget:
+                    heapq.heappop(queue)
+                    results.append(Result(req.id, req.mesh.n_cells, req.arrival, now, now, 0, False))
+                    self.log.append(("rejected", req.id, need))
+                    continue
+                if used + need > self.hbm_budget:
+                    break
+                heapq.heappop(queue)
+                m, sim = self._start(req)
+                used += need
+                active.append(_Active(req, m, sim, clock() - t0, need))
+                self.log.append(("admitted", req.id, need))
+            if not active:
+                if i < len(pending):  # idle until the next arrival
+                    wait = pending[i].arrival - (clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                continue
+            # one outer iteration of every active solve, in admission order
+            done = []
+            for a in active:
+                rep = a.sim.iterate(1)
+                a.iterations = rep.iterations
+                if rep.converged or rep.status == 2 or a.iterations >= a.req.max_iterations:
+                    done.append((a, rep))
+            for a, rep in done:
+                U = p = None
+                if self.keep_fields:
+                    U, p, _ = a.sim.fields()
+                a.sim.close()
+                a.mesh.close()
+                used -= a.bytes
+                active.remove(a)
+                results.append(Result(a.req.id, a.req.mesh.n_cells, a.req.arrival, a.admitted, clock() - t0,
+                                      a.iterations, bool(rep.converged), U, p))
+                self.log.append(("retired", a.req.id, a.iterations))
+            turn += 1
+        return sorted(results, key=lambda r: r.id)
+
+
+def summary(results: list[Result], wall: float) -> dict:
+    lat = np.array([r.latency for r in results if r.finished > r.admitted or r.iterations > 0])
+    cells = sum(r.cells * r.iterations for r in results)
+    return {"solves": len(results), "solves_per_s": len(results) / wall,
+            "p50_latency_s": float(np.percentile(lat, 50)) if lat.size else None,
+            "p99_latency_s": float(np.percentile(lat, 99)) if lat.size else None,
+            "converged": int(sum(r.converged for r in results)), "cell_iters_per_s": cells / wall}

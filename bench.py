@@ -211,6 +211,210 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_serving(args):
+    """Serving workload: a seeded Poisson stream of steady SIMPLE cavity requests (hex and
+    jittered-Voronoi cubes, cells log-uniform, lid speed uniform 0.5-2, nu log-uniform 1e-3-1e-2),
+    admitted under an HBM budget and served with continuous batching (babelsim_b200.serve)."""
+    import babelsim_b200 as bsg
+    from babelsim_b200 import meshgen, serve
+    rng = np.random.default_rng(SEED)
+    pool = {("hex", n): meshgen.hex_box(n, n, n) for n in (16, 20, 26, 32, 40, 46)}
+    for n in (16, 24, 32):
+        pool[("voronoi", n)] = meshgen.voronoi_cube(n, 0.3, SEED + n)
+    keys = sorted(pool, key=lambda k: pool[k].n_cells)
+    sizes = np.array([pool[k].n_cells for k in keys], float)
+    reqs, t = [], 0.0
+    for i in range(args.requests):
+        target = np.exp(rng.uniform(np.log(4000), np.log(1e5)))
+        k = keys[int(np.argmin(np.abs(np.log(sizes) - np.log(target))))]
+        t += rng.exponential(1.0 / args.arrival_rate)
+        reqs.append(serve.Request(i, t, pool[k], speed=float(rng.uniform(0.5, 2.0)),
+                                  nu=float(np.exp(rng.uniform(np.log(1e-3), np.log(1e-2)))),
+                                  max_iterations=args.max_outer, tolerance=1e-4))
+    ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    srv = serve.Server(ctx, hbm_budget=150 * 2**30, slots=args.slots)
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    out = serve.summary(res, wall)
+    # each request solved alone on the same GPU (arrival at 0, nothing else running)
+    alone = []
+    for r in reqs:
+        solo = serve.Server(ctx, hbm_budget=150 * 2**30, slots=1)
+        rr = solo.run([serve.Request(r.id, 0.0, r.mesh, r.speed, r.nu, r.max_iterations, r.tolerance)])[0]
+        alone.append(rr.latency)
+    ratio = np.array([res[i].latency / alone[i] for i in range(len(reqs))])
+    line = {"metric": "served solves/s (steady SIMPLE cavity requests)", "value": out["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.requests} seeded requests, cells log-uniform 4k-100k (hex and "
+                                   f"jittered-Voronoi cubes), Poisson arrivals {args.arrival_rate}/s, "
+                                   f"{args.slots} slots, 150 GiB budget, outer tolerance 1e-4 or "
+                                   f"{args.max_outer} iterations", "slots": args.slots},
+            "p50_latency_s": out["p50_latency_s"], "p99_latency_s": out["p99_latency_s"],
+            "converged": out["converged"], "cell_iters_per_s": out["cell_iters_per_s"], "wall_s": wall,
+            "isolated_solve_s": {"p50": float(np.percentile(alone, 50)), "p99": float(np.percentile(alone, 99))},
+            "latency_over_isolated": {"p50": float(np.percentile(ratio, 50)), "p99": float(np.percentile(ratio, 99))},
+            "p99_latency_over_isolated_p99": out["p99_latency_s"] / float(np.percentile(alone, 99))}
+    print(json.dumps(line))
+    ctx.close()
+
+
+def _reference_run(case_writer, steps_label):
+    """Run the reference's own sources (oracle/_ref) on a case written by `case_writer(dir)`;
+    returns (seconds, run info)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "babelsim-oracle")
+    if not os.path.exists(exe):
+        return None, None
+    work = tempfile.mkdtemp(prefix=f"bsg_ref_{steps_label}_")
+    case_writer(work)
+    out = os.path.join(work, "out")
+    res = subprocess.run([exe, work, out], env=dict(os.environ, OMP_NUM_THREADS="1"), capture_output=True,
+                         text=True, timeout=900)
+    if not os.path.exists(os.path.join(out, "run.json")):
+        raise RuntimeError(f"reference run failed (exit {res.returncode}): {res.stderr[-300:]}")
+    info = json.load(open(os.path.join(out, "run.json")))
+    return float(info["solver_seconds"]), info
+
+
+def run_piso_cylinder(args):
+    """Transient PISO (BDF2, 2 correctors, 1 non-orthogonal corrector) past a cylinder D = 1 on a
+    hex O-grid (radial growth 1.05 to 15 D), nu 0.01, inlet u = 1; metric cell-steps/s.  The
+    default dt 0.001 keeps the Courant number near the cylinder below 1 on the 2000-cell
+    circumference (dt 0.005 gives about 3 there and the impulsive start diverges)."""
+    import babelsim_b200 as bsg
+    from babelsim_b200 import meshgen
+    n_theta, n_r = args.theta_cells, args.radial_cells
+    poly = meshgen.cylinder_ogrid(n_theta, n_r, 0.5, 15.0, 1.05)
+    ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    mesh = bsg.Mesh.from_polyhedral(ctx, poly)
+    N = mesh.n_cells
+    o = bsg.options("linear", "leastSquares", "linearUpwind", "corrected")
+    steps = args.steps
+    out = {}
+    for precision in (0, 2):
+        sim = bsg.Piso(mesh, 1.0, 0.01, 1.0, 1, 2, None, None, 1, 1e-7, 1e-7, 1e-6, 1e-7, "bdf2", 0.0, 1e9, args.dt,
+                       o, o, bsg.solver_config("bcgs", "bjacobi", 1e-12, 1e-8, 1000),
+                       bsg.solver_config("cg", "hypre", 1e-13, 1e-9, 1500, precision=precision))
+        bcsU = [("fixedValue", (0, 0, 0)), ("fixedValue", (1, 0, 0)), ("zeroGradient", 0), ("symmetry", 0),
+                ("symmetry", 0)]
+        bcsP = [("zeroGradient", 0), ("zeroGradient", 0), ("fixedValue", 0), ("symmetry", 0), ("symmetry", 0)]
+        for pi, (t, v) in enumerate(bcsU):
+            sim.set_boundary("U", pi, t, v)
+        for pi, (t, v) in enumerate(bcsP):
+            sim.set_boundary("p", pi, t, v)
+        U0 = np.zeros((N, 3))
+        U0[:, 0] = 1.0
+        sim.set_fields(U0, np.zeros(N))
+        sim.advance(max(args.warmup, 3))
+        ctx.synchronize()
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            ctx.record(0)
+            rep = sim.advance(steps)
+            ctx.record(1)
+            ms = ctx.elapsed_ms(0, 1)
+        out[precision] = (ms, rep, clocks.summary())
+        sim.close()
+    ms, rep, clk = out[0]
+    # the reference's own runPiso on a 10x smaller O-grid, 4 steps, 1 core
+    from make_golden import write_case  # noqa: E402
+    small = meshgen.cylinder_ogrid(max(n_theta // 4, 16), max(n_r // 2, 8), 0.5, 15.0, 1.05 ** 2)
+    bU = [("fixedValue", (0.0, 0.0, 0.0)), ("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0)),
+          ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    bP = [("zeroGradient", 0.0), ("zeroGradient", 0.0), ("fixedValue", 0.0), ("symmetry", 0.0), ("symmetry", 0.0)]
+    meth = {"momentum": dict(interpolation="linear", gradient="leastSquares", convection="linearUpwind",
+                             diffusion="corrected")}
+    meth["pressureCorrection"] = dict(meth["momentum"])
+    sol = {"maxIterations": 1, "nCorrectors": 2, "nonOrthogonalCorrections": 1, "velocityRelaxation": 1.0,
+           "continuityTolerance": 1e-7, "velocityTolerance": 1e-7, "momentumTolerance": 1e-6,
+           "pressureCorrectionTolerance": 1e-7, "equation.momentum.kspType": "bcgs",
+           "equation.momentum.pcType": "bjacobi", "equation.momentum.absoluteTolerance": 1e-12,
+           "equation.momentum.relativeTolerance": 1e-8, "equation.momentum.maxIterations": 1000,
+           "equation.pressureCorrection.kspType": "cg", "equation.pressureCorrection.pcType": "hypre",
+           "equation.pressureCorrection.absoluteTolerance": 1e-13,
+           "equation.pressureCorrection.relativeTolerance": 1e-9,
+           "equation.pressureCorrection.maxIterations": 1500}
+    cb = None
+    try:
+        secs, info = _reference_run(lambda d: write_case(d, small, bU, bP, meth, sol, {"density": 1.0,
+                                    "dynamicViscosity": 0.01}, solver="piso", time="bdf2",
+                                    control=(0.0, 4 * args.dt, args.dt)), "piso")
+        if secs:
+            cb = {"value": small.n_cells * 4 / secs, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+                  "sample": f"reference runPiso, {small.n_cells}-cell O-grid, 4 steps (whole run timed), "
+                            f"status {info['status']}"}
+    except Exception as exc:  # the baseline is reported, never required for the GPU number
+        cb = {"value": None, "error": str(exc)[:200]}
+    line = {"metric": "cell-steps/s (transient PISO, BDF2, flow past a cylinder)", "value": N * steps / (ms / 1e3),
+            "unit": "cell-steps/s", "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms / steps, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"PISO cylinder O-grid {n_theta}x{n_r} = {N} cells, radial growth 1.05 to 15 D, "
+                                   f"Re 100, dt {args.dt}, 2 correctors, 1 non-orthogonal corrector",
+                       "cells": N},
+            "mixed_precision": {"value": N * steps / (out[2][0] / 1e3), "unit": "cell-steps/s",
+                                "precision": "fp64 flexible PCG + fp32 AMG V-cycle"},
+            "cpu_baseline": cb, "clocks": clk,
+            "last_report": {"courant_max": rep.courant_max, "mass": rep.mass, "coupling": rep.coupling,
+                            "pressure_iterations": rep.pressure_iterations,
+                            "momentum_iterations": rep.momentum_iterations}}
+    print(json.dumps(line))
+    mesh.close()
+    ctx.close()
+
+
+def run_komega_channel(args):
+    """Steady SIMPLE with k-omega in a plane channel (2 pi x 2 x pi, tanh wall clustering),
+    inlet/outlet (the reference has no periodic patches), nu 1e-4; metric cell-iters/s."""
+    import babelsim_b200 as bsg
+    from babelsim_b200 import meshgen
+    nx, ny, nz = args.channel_cells
+    poly = meshgen.channel(nx, ny, nz)
+    ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    mesh = bsg.Mesh.from_polyhedral(ctx, poly)
+    N = mesh.n_cells
+    o = bsg.options("linear", "greenGauss", "linearUpwind", "orthogonal")
+    t = bsg.options("linear", "greenGauss", "upwind", "orthogonal")
+    sim = bsg.Simple(mesh, 1.0, 1e-4, 0.7, 0.3, 0, 1e-8, 1e-7, 1e-6, 1e-6, o, o,
+                     bsg.solver_config("bcgs", "bjacobi", 1e-14, 1e-8, 1000),
+                     bsg.solver_config("cg", "hypre", 1e-14, 1e-8, 1000))
+    sim.enable_komega(k_transport=t, omega_transport=t,
+                      k_solver=bsg.solver_config("bcgs", "bjacobi", 1e-18, 1e-8, 1000),
+                      omega_solver=bsg.solver_config("bcgs", "bjacobi", 1e-18, 1e-8, 1000))
+    U = [("fixedValue", (1.0, 0, 0)), ("zeroGradient", 0), ("fixedValue", (0, 0, 0)), ("fixedValue", (0, 0, 0)),
+         ("symmetry", 0), ("symmetry", 0)]
+    P = [("zeroGradient", 0), ("fixedValue", 0), ("zeroGradient", 0), ("zeroGradient", 0), ("symmetry", 0),
+         ("symmetry", 0)]
+    K = [("fixedValue", 3.75e-3), ("zeroGradient", 0), ("fixedValue", 1e-12), ("fixedValue", 1e-12),
+         ("symmetry", 0), ("symmetry", 0)]
+    W = [("fixedValue", 10.0), ("zeroGradient", 0), ("fixedValue", 1e4), ("fixedValue", 1e4), ("symmetry", 0),
+         ("symmetry", 0)]
+    for name, bcs in (("U", U), ("p", P), ("k", K), ("omega", W)):
+        for pi, (tp, v) in enumerate(bcs):
+            sim.set_boundary(name, pi, tp, v)
+    sim.set_turbulence_fields(np.full(N, 3.75e-3), np.full(N, 10.0))
+    U0 = np.zeros((N, 3))
+    U0[:, 0] = 1.0
+    sim.set_fields(U0, np.zeros(N))
+    sim.iterate(max(args.warmup, 3))
+    ctx.synchronize()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        ctx.record(0)
+        rep = sim.iterate(args.steps)
+        ctx.record(1)
+        ms = ctx.elapsed_ms(0, 1)
+    line = {"metric": "cell-iters/s (steady SIMPLE + k-omega, plane channel)", "value": N * args.steps / (ms / 1e3),
+            "unit": "cell-iters/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"k-omega channel {nx}x{ny}x{nz} = {N} cells, tanh wall clustering, "
+                                   "inlet/outlet, nu 1e-4", "cells": N},
+            "clocks": clocks.summary(),
+            "last_report": {"status": rep.status, "rU": rep.rU, "turbulence_change": rep.turbulence_change,
+                            "pressure_iterations": rep.pressure_iterations}}
+    print(json.dumps(line))
+    sim.close()
+    mesh.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,9 +424,25 @@ def main():
     ap.add_argument("--cells", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison run")
+    ap.add_argument("--workload", default="cavity", choices=["cavity", "serving", "piso-cylinder", "komega-channel"])
+    ap.add_argument("--theta-cells", type=int, default=2000)
+    ap.add_argument("--dt", type=float, default=0.001)
+    ap.add_argument("--radial-cells", type=int, default=100)
+    ap.add_argument("--channel-cells", type=int, nargs=3, default=[200, 160, 125])
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--arrival-rate", type=float, default=8.0)
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--max-outer", type=int, default=150)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serving":
+        return run_serving(args)
+    if args.workload == "piso-cylinder":
+        sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+        return run_piso_cylinder(args)
+    if args.workload == "komega-channel":
+        return run_komega_channel(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

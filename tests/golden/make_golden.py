@@ -290,6 +290,13 @@ def main_piso():
     make_piso("piso_warped5_euler", meshgen.warped_box(5), Uw, pw, methods("linearUpwind", "leastSquares", "corrected"),
               piso_solution(3, 2), {"density": 1.0, "dynamicViscosity": 0.01}, "euler", 0.0, 0.02,
               [0.02, 0.04, 0.06, 0.08])
+    # flow past a cylinder on a small O-grid: inlet, outlet (p = 0), BDF2, corrected diffusion
+    Uc = [("fixedValue", (0.0, 0.0, 0.0)), ("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0)),
+          ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    pc = [("zeroGradient", 0.0), ("zeroGradient", 0.0), ("fixedValue", 0.0), ("symmetry", 0.0), ("symmetry", 0.0)]
+    make_piso("piso_cylinder_ogrid", meshgen.cylinder_ogrid(48, 12, radius=6.0, growth=1.15), Uc, pc,
+              methods("linearUpwind", "leastSquares", "corrected"), piso_solution(2, 1),
+              {"density": 1.0, "dynamicViscosity": 0.01}, "bdf2", 0.0, 0.05, [0.05, 0.1, 0.15])
 
 
 def main():

@@ -16,7 +16,7 @@ from oracle import fvm, geometry, piso, rans, simple  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
-PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler"]
+PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler", "piso_cylinder_ogrid"]
 RANS_CASES = ["komega_channel", "komega_warped5"]
 GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
             "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",

@@ -1,0 +1,96 @@
+"""Serving-loop scheduling (admission under an HBM budget, slots, retirement, latency) on the host,
+with the device solve replaced by a stand-in that converges after a set number of outer iterations."""
+import numpy as np
+
+from babelsim_b200 import serve
+
+
+class FakeMesh:
+    def __init__(self, n_cells, n_faces):
+        self.n_cells = n_cells
+        self.owner = np.zeros(n_faces, dtype=np.int32)
+
+    def close(self):
+        pass
+
+
+class FakeReport:
+    def __init__(self, it, done):
+        self.iterations = it
+        self.converged = done
+        self.status = 0 if done else 1
+
+
+class FakeSim:
+    def __init__(self, needed, trace, rid):
+        self.needed, self.it, self.trace, self.rid = needed, 0, trace, rid
+
+    def iterate(self, k):
+        self.it += k
+        self.trace.append(self.rid)
+        return FakeReport(self.it, self.it >= self.needed)
+
+    def fields(self):
+        return None, None, None
+
+    def close(self):
+        pass
+
+
+class Clock:
+    """A clock that advances one unit per reading, so arrivals are reached deterministically."""
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        self.t += 1.0
+        return self.t
+
+
+def _server(budget, slots, needed, trace):
+    srv = serve.Server(ctx=None, hbm_budget=budget, slots=slots)
+    srv._start = lambda req: (FakeMesh(req.mesh.n_cells, 1), FakeSim(needed[req.id], trace, req.id))
+    return srv
+
+
+def test_admission_respects_slots_budget_and_order():
+    reqs = [serve.Request(i, arrival=0.0, mesh=FakeMesh(1000 * (i + 1), 3000 * (i + 1))) for i in range(5)]
+    need = {r.id: 3 for r in reqs}
+    one = serve.device_bytes(1000, 3000)
+    budget = serve.device_bytes(1000, 3000) + serve.device_bytes(2000, 6000)  # the first two fit together
+    trace = []
+    srv = _server(budget, slots=4, needed=need, trace=trace)
+    res = srv.run(reqs, clock=Clock())
+    assert [r.id for r in res] == list(range(5))
+    assert all(r.converged and r.iterations == 3 for r in res[:2])
+    admitted = [e[1] for e in srv.log if e[0] == "admitted"]
+    assert admitted[:2] == [0, 1]
+    # request 4 needs more than the whole budget: rejected, never admitted
+    assert ("rejected", 4, serve.device_bytes(5000, 15000)) in srv.log and 4 not in admitted
+    # at no time is more admitted than the budget
+    live, peak = 0, 0
+    for kind, rid, val in srv.log:
+        if kind == "admitted":
+            live += val
+        elif kind == "retired":
+            live -= serve.device_bytes(1000 * (rid + 1), 3000 * (rid + 1))
+        peak = max(peak, live)
+    assert peak <= budget and one > 0
+
+
+def test_round_robin_and_refill():
+    reqs = [serve.Request(i, arrival=0.0, mesh=FakeMesh(100, 300)) for i in range(3)]
+    trace = []
+    srv = _server(10**12, slots=2, needed={0: 2, 1: 4, 2: 1}, trace=trace)
+    res = srv.run(reqs, clock=Clock())
+    # 0 and 1 alternate; 2 takes 0's slot when 0 retires
+    assert trace[:4] == [0, 1, 0, 1]
+    assert trace[4] == 1 and 2 in trace[4:6]
+    assert [r.iterations for r in res] == [2, 4, 1]
+    assert all(r.latency > 0 for r in res)
+    s = serve.summary(res, wall=10.0)
+    assert s["solves"] == 3 and s["converged"] == 3 and s["p99_latency_s"] >= s["p50_latency_s"]
+
+
+def test_device_bytes_grows_with_size():
+    assert serve.device_bytes(10**6, 7 * 10**6) > 10 * serve.device_bytes(10**5, 7 * 10**5) * 0.99
