@@ -6,4 +6,4 @@ package loads it and offers the same vocabulary from Python.
 """
 from ._lib import BsgError, lib  # noqa: F401
 from .api import (Context, Equation, Field, Mesh, Piso, Simple, div_flux, flux, grad, interpolate,  # noqa: F401
-                  normal_gradient, options, solve_ldu, solver_config)
+                  normal_gradient, options, solve_ldu, solver_config, write_results)

@@ -447,3 +447,21 @@ class Piso:
         if self.h:
             lib().bsg_piso_destroy(self.h)
             self.h = None
+
+
+def write_results(time_directory: str, time_name: str, poly, fields: dict):
+    """Write cell fields in the reference's result format (bsg_write_results): one CSV per field
+    under <time_directory>/rank-0000 with metadata.bs and mesh.geometry.  `fields` maps a name
+    to an (n_cells,) or (n_cells, 3) or (n_cells, 9) array in the caller's cell numbering."""
+    off, ids = poly.flat()
+    names = list(fields)
+    arrays = [f64(np.asarray(fields[k], dtype=np.float64).reshape(poly.n_cells, -1)) for k in names]
+    comps = np.array([a.shape[1] for a in arrays], dtype=np.int32)
+    name_arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
+    val_arr = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    verts = f64(poly.vertices)
+    owner, nbr, patch = i32(poly.owner), i32(poly.neighbour), i32(poly.patch)
+    off, ids = i32(off), i32(ids)
+    check(lib().bsg_write_results(str(time_directory).encode(), time_name.encode(), len(verts), ptr(verts),
+                                  len(owner), ptr(off), ptr(ids), ptr(owner), ptr(nbr), ptr(patch),
+                                  len(poly.patch_names), len(names), name_arr, ptr(comps), val_arr))

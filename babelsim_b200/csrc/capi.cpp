@@ -5,6 +5,7 @@
 #include "fvm.h"
 #include "linalg.h"
 #include "piso.h"
+#include "results.h"
 #include "simple.h"
 
 #include <algorithm>
@@ -405,6 +406,24 @@ int bsg_mesh_validate_polyhedral(int32_t n_vertices, const double* vertices, int
                                                                     neighbour, patch, n_patches);
         if (n_cells_out) *n_cells_out = h.n_cells;
         if (orthogonal_out) *orthogonal_out = h.orthogonal ? 1 : 0;
+    });
+}
+
+int bsg_write_results(const char* time_directory, const char* time_name, int32_t n_vertices, const double* vertices,
+                      int32_t n_faces, const int32_t* offsets, const int32_t* ids, const int32_t* owner,
+                      const int32_t* neighbour, const int32_t* patch, int32_t n_patches, int32_t n_fields,
+                      const char* const* names, const int32_t* components, const double* const* values) {
+    return guard(nullptr, [&] {
+        require(time_directory && time_name && vertices && offsets && ids && owner && neighbour && patch && names &&
+                    components && values && n_fields > 0,
+                "null argument");
+        std::vector<bsg::ResultField> fields(n_fields);
+        for (int i = 0; i < n_fields; ++i) {
+            require(names[i] != nullptr, "null field name");
+            fields[i] = bsg::ResultField{names[i], components[i], values[i]};
+        }
+        bsg::writeResults(time_directory, time_name, n_vertices, vertices, n_faces, offsets, ids, owner, neighbour,
+                          patch, n_patches, fields);
     });
 }
 

@@ -182,6 +182,16 @@ int bsg_mesh_validate_polyhedral(int32_t n_vertices, const double* vertices, int
                                  const int32_t* face_point_offsets, const int32_t* face_point_ids,
                                  const int32_t* owner, const int32_t* neighbour, const int32_t* patch,
                                  int32_t n_patches, int32_t* n_cells_out, int32_t* orthogonal_out);
+/* Write cell fields in the reference's result format (src/parallel/parallel_writer.cpp:42-171):
+ * <time_directory>/rank-0000/<name>.csv, metadata.bs and mesh.geometry, one rank.  Host only:
+ * the polyhedral description gives the cell centres and the cell vertex lists; values are in
+ * the caller's cell numbering, `components[i]` doubles per cell (1, 3 or 9).  The reference's
+ * restart reader (field file `internal file <time_directory>`) and tools read the result. */
+int bsg_write_results(const char* time_directory, const char* time_name, int32_t n_vertices,
+                      const double* vertices, int32_t n_faces, const int32_t* face_point_offsets,
+                      const int32_t* face_point_ids, const int32_t* owner, const int32_t* neighbour,
+                      const int32_t* patch, int32_t n_patches, int32_t n_fields, const char* const* names,
+                      const int32_t* components, const double* const* values);
 /* n_cells, n_faces, n_interior_faces, n_patches, orthogonal flag. */
 int bsg_mesh_sizes(const bsg_mesh* mesh, int64_t out[5]);
 /* Copy one geometry array (a bsg_mesh_geometry member name, e.g.

@@ -43,7 +43,10 @@ def vec(v):
 
 
 def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics, solver="simple", time="steady",
-               control=(0.0, 0.0, 1.0), extra_fields=()):
+               control=(0.0, 0.0, 1.0), extra_fields=(), internal=None):
+    """A BabelSim case directory.  `internal` maps U/p to an `internal` specification line
+    (e.g. "file <results-dir>") instead of a zero uniform initial value."""
+    internal = internal or {}
     os.makedirs(os.path.join(path, "mesh"), exist_ok=True)
     os.makedirs(os.path.join(path, "fields", "initial"), exist_ok=True)
     os.makedirs(os.path.join(path, "numerics"), exist_ok=True)
@@ -66,10 +69,13 @@ def write_case(path, mesh, U_bcs, p_bcs, methods, solution, physics, solver="sim
     with open(os.path.join(path, "numerics", "solution.bs"), "w") as f:
         f.write("".join(f"{k} {v}\n" for k, v in solution.items()))
 
+    internal_spec = internal
+
     def field(name, kind, bcs, internal=0.0):
+        spec = internal_spec.get(name) if internal_spec else None
         lines = [f"field {name}", "{", f"    type {kind}", "    location cell",
-                 "    internal uniform " + ("(0 0 0)" if kind == "vector" else f"({internal!r})"), "    boundary",
-                 "    {"]
+                 "    internal " + (spec if spec else ("uniform (0 0 0)" if kind == "vector" else f"uniform ({internal!r})")),
+                 "    boundary", "    {"]
         for patch, (t, v) in zip(mesh.patch_names, bcs):
             if t in ("zeroGradient", "symmetry"):
                 lines.append(f"        {patch} {{ type {t} }}")
