@@ -29,7 +29,7 @@ EXPORTS = [
     "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_pcg_jacobi_static",
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
-    "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_set_turbulence_fields",
+    "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_enable_kepsilon", "bsg_simple_set_turbulence_fields",
     "bsg_simple_get_turbulence_fields", "bsg_simple_get_fields",
     "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
     "bsg_piso_get_fields", "bsg_piso_destroy",
@@ -110,6 +110,13 @@ class PisoReport(C.Structure):
                 ("correctors", C.c_int32), ("momentum_iterations", C.c_int32), ("pressure_iterations", C.c_int32)]
 
 
+class KEpsilonConfig(C.Structure):
+    _fields_ = [("c_mu", C.c_double), ("c1", C.c_double), ("c2", C.c_double), ("sigma_k", C.c_double),
+                ("sigma_epsilon", C.c_double), ("k_min", C.c_double), ("epsilon_min", C.c_double),
+                ("relaxation", C.c_double), ("tolerance", C.c_double), ("k_transport", Options),
+                ("epsilon_transport", Options), ("k_solver", SolverConfig), ("epsilon_solver", SolverConfig)]
+
+
 _lib = None
 
 
@@ -157,6 +164,7 @@ def lib():
             "bsg_simple_set_flux": [vp, vp],
             "bsg_simple_iterate": [vp, i32, C.POINTER(SimpleReport)],
             "bsg_simple_enable_komega": [vp, C.POINTER(KOmegaConfig)],
+            "bsg_simple_enable_kepsilon": [vp, C.POINTER(KEpsilonConfig)],
             "bsg_simple_set_turbulence_fields": [vp, vp, vp], "bsg_simple_get_turbulence_fields": [vp, vp, vp, vp], "bsg_simple_get_fields": [vp, vp, vp, vp],
             "bsg_simple_destroy": [vp],
             "bsg_piso_create": [vp, C.POINTER(PisoConfig), pp],

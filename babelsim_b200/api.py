@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (KOmegaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
+from ._lib import (KEpsilonConfig, KOmegaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
                    check, f64, i32, lib, ptr)
 
 BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
@@ -382,6 +382,16 @@ class Simple:
                            k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
                            omega_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
         check(lib().bsg_simple_enable_komega(self.h, C.byref(cfg)), self.mesh.ctx.h)
+
+    def enable_kepsilon(self, c_mu=0.09, c1=1.44, c2=1.92, sigma_k=1.0, sigma_epsilon=1.3, k_min=1e-12,
+                        epsilon_min=1e-12, relaxation=0.7, tolerance=1e-6, k_transport=None, epsilon_transport=None,
+                        k_solver=None, epsilon_solver=None):
+        """turbulenceModel kEpsilon (before set_fields); k and epsilon then take boundary conditions."""
+        cfg = KEpsilonConfig(c_mu, c1, c2, sigma_k, sigma_epsilon, k_min, epsilon_min, relaxation, tolerance,
+                             k_transport or options(), epsilon_transport or options(),
+                             k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
+                             epsilon_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
+        check(lib().bsg_simple_enable_kepsilon(self.h, C.byref(cfg)), self.mesh.ctx.h)
 
     def set_turbulence_fields(self, k, omega):
         check(lib().bsg_simple_set_turbulence_fields(self.h, ptr(f64(k)), ptr(f64(omega))), self.mesh.ctx.h)

@@ -846,8 +846,10 @@ int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int
         if (n == "U") s->solver->U().setBoundary(patch, type, value);
         else if (n == "p") s->solver->p().setBoundary(patch, type, value);
         else if (n == "k" && t) t->k().setBoundary(patch, type, value);
-        else if (n == "omega" && t) t->omega().setBoundary(patch, type, value);
-        else bsg::fail(bsg::kArgument, "SIMPLE boundary field must be U or p (k, omega with a k-omega model)");
+        else if (n == "omega" && t && t->config().kind == 0) t->omega().setBoundary(patch, type, value);
+        else if (n == "epsilon" && t && t->config().kind == 1) t->omega().setBoundary(patch, type, value);
+        else bsg::fail(bsg::kArgument,
+                       "SIMPLE boundary field must be U or p (k and omega or epsilon with a two-equation model)");
     });
 }
 
@@ -913,6 +915,28 @@ int bsg_simple_enable_komega(bsg_simple* s, const bsg_komega_config* c) {
         k.omega_options = options(&c->omega_transport);
         k.k_solver = solverConfig(&c->k_solver);
         k.omega_solver = solverConfig(&c->omega_solver);
+        s->solver->enableKOmega(k);
+    });
+}
+
+int bsg_simple_enable_kepsilon(bsg_simple* s, const bsg_kepsilon_config* c) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && c, "null argument");
+        bsg::KOmegaConfig k;
+        k.kind = 1;
+        k.c_mu = c->c_mu;
+        k.c1 = c->c1;
+        k.c2 = c->c2;
+        k.sigma_k = c->sigma_k;
+        k.sigma_omega = c->sigma_epsilon;
+        k.k_min = c->k_min;
+        k.omega_min = c->epsilon_min;
+        k.relaxation = c->relaxation;
+        k.tolerance = c->tolerance;
+        k.k_options = options(&c->k_transport);
+        k.omega_options = options(&c->epsilon_transport);
+        k.k_solver = solverConfig(&c->k_solver);
+        k.omega_solver = solverConfig(&c->epsilon_solver);
         s->solver->enableKOmega(k);
     });
 }

@@ -82,6 +82,55 @@ __global__ void kTransportCoefficients(int n, double rho, double mu, double beta
     wproduction[i] = ((gamma * p) * w[i]) / fmax(k[i], k_min);
 }
 
+// k-epsilon: mut = Cmu rho k k / max(epsilon, epsilonMin) on cells and boundary traces (k_epsilon.cpp:122-125)
+__global__ void kViscosityKE(int n, double crho, double mu, double eps_min, const double* __restrict__ k,
+                             const double* __restrict__ e, double* __restrict__ mut, double* __restrict__ mueff) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = ((crho * k[i]) * k[i]) / fmax(e[i], eps_min);
+    mut[i] = v;
+    mueff[i] = v + mu;
+}
+
+__global__ void kViscosityTraceKE(MeshView m, BcView bk, BcView be, const double* __restrict__ k,
+                                  const double* __restrict__ e, double crho, double mu, double eps_min,
+                                  double* __restrict__ mut_tr, double* __restrict__ mueff_tr) {
+    const int fb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fb >= m.n_boundary) return;
+    double kt[1], et[1];
+    boundaryTrace<1>(m, bk, k, fb, NAN, kt);
+    boundaryTrace<1>(m, be, e, fb, NAN, et);
+    const double v = ((crho * kt[0]) * kt[0]) / fmax(et[0], eps_min);
+    mut_tr[fb] = v;
+    mueff_tr[fb] = v + mu;
+}
+
+// Frozen k-epsilon coefficients (k_epsilon.cpp:70-77): production, diffusivities mu + mut/sigma,
+// k sink rho eps/k, epsilon sink C2 rho eps/k, epsilon source C1 P eps/k.
+__global__ void kTransportCoefficientsKE(int n, double rho, double mu, double c1, double c2, double inv_sk,
+                                         double inv_se, double k_min, const double* __restrict__ G,
+                                         const double* __restrict__ mut, const double* __restrict__ k,
+                                         const double* __restrict__ e, double* __restrict__ production,
+                                         double* __restrict__ kdiff, double* __restrict__ ediff,
+                                         double* __restrict__ ksink, double* __restrict__ esink,
+                                         double* __restrict__ eproduction) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double p = mut[i] * strainSquared(G + 9 * i);
+    production[i] = p;
+    kdiff[i] = inv_sk * mut[i] + mu;
+    ediff[i] = inv_se * mut[i] + mu;
+    const double eok = e[i] / fmax(k[i], k_min);
+    ksink[i] = rho * eok;
+    esink[i] = (c2 * rho) * eok;
+    eproduction[i] = (c1 * p) * eok;
+}
+
+__global__ void kBoundMin(int n, double lo, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = fmax(x[i], lo);
+}
+
 __global__ void kDiffusivityTrace(int nb, double mu, double sigma_k, double sigma_w, const double* __restrict__ mut_tr,
                                   double* __restrict__ kdiff_tr, double* __restrict__ wdiff_tr) {
     const int fb = blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,9 +257,10 @@ KOmegaModel::KOmegaModel(DeviceMesh& mesh, const KOmegaConfig& cfg)
     : m_(mesh), ctx_(*mesh.ctx), cfg_(cfg), k_(mesh, 0, 1), omega_(mesh, 0, 1), mut_(mesh, 0, 1), muEff_(mesh, 0, 1),
       kDiff_(mesh, 0, 1), wDiff_(mesh, 0, 1), krylov_(*mesh.ctx) {
     if (!(cfg.rho > 0) || !(cfg.mu > 0)) fail(kArgument, "density and dynamicViscosity must be positive");
+    if (cfg.kind != 0 && cfg.kind != 1) fail(kArgument, "unknown two-equation turbulence model");
     for (double v : {cfg.beta_star, cfg.beta, cfg.gamma, cfg.sigma_k, cfg.sigma_omega, cfg.k_min, cfg.omega_min,
-                     cfg.viscosity_ratio_max, cfg.tolerance})
-        if (!(v > 0) || !std::isfinite(v)) fail(kArgument, "k-omega constants and bounds must be positive and finite");
+                     cfg.viscosity_ratio_max, cfg.tolerance, cfg.c_mu, cfg.c1, cfg.c2})
+        if (!(v > 0) || !std::isfinite(v)) fail(kArgument, "turbulence model constants and bounds must be positive and finite");
     if (!(cfg.relaxation > 0 && cfg.relaxation <= 1)) fail(kArgument, "turbulenceRelaxation must be in (0,1]");
     if (cfg.momentum_options.interpolation != 0)
         fail(kArgument, "the device stress-remainder divergence reconstructs the tensor rows linearly");
@@ -230,12 +280,26 @@ KOmegaModel::~KOmegaModel() = default;
 
 void KOmegaModel::boundOmega() {
     const int N = m_.n_cells;
+    if (cfg_.kind == 1) {  // epsilon = max(epsilon, epsilonMin) (k_epsilon.cpp:118)
+        launch(ctx_, kBoundMin, N, N, cfg_.omega_min, omega_.v.data());
+        return;
+    }
     launch(ctx_, kBoundOmega, N, N, cfg_.omega_min, cfg_.rho, cfg_.viscosity_ratio_max * cfg_.mu,
            (const double*)k_.v.data(), omega_.v.data());
 }
 
 void KOmegaModel::updateViscosity() {
     const int N = m_.n_cells;
+    if (cfg_.kind == 1) {
+        const double crho = cfg_.c_mu * cfg_.rho;
+        launch(ctx_, kViscosityKE, N, N, crho, cfg_.mu, cfg_.omega_min, (const double*)k_.v.data(),
+               (const double*)omega_.v.data(), mut_.v.data(), muEff_.v.data());
+        if (m_.n_boundary)
+            launch(ctx_, kViscosityTraceKE, m_.n_boundary, view(m_), k_.bcView(), omega_.bcView(),
+                   (const double*)k_.v.data(), (const double*)omega_.v.data(), crho, cfg_.mu, cfg_.omega_min,
+                   mut_.trace.data(), muEff_.trace.data());
+        return;
+    }
     launch(ctx_, kViscosity, N, N, cfg_.rho, cfg_.mu, cfg_.omega_min, (const double*)k_.v.data(),
            (const double*)omega_.v.data(), mut_.v.data(), muEff_.v.data());
     if (m_.n_boundary)
@@ -277,12 +341,22 @@ TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
     U.setFluxContext(phi);
     updateViscosity();
     gradient(U, cfg_.momentum_options.gradient, G_);
-    launch(ctx_, kTransportCoefficients, N, N, cfg_.rho, cfg_.mu, cfg_.beta, cfg_.gamma, cfg_.sigma_k, cfg_.sigma_omega,
-           cfg_.k_min, (const double*)G_.data(), (const double*)mut_.v.data(), (const double*)k_.v.data(),
-           (const double*)omega_.v.data(), production_.data(), kDiff_.v.data(), wDiff_.v.data(),
-           wDestruction_.data(), wProduction_.data());
-    if (nb) launch(ctx_, kDiffusivityTrace, nb, nb, cfg_.mu, cfg_.sigma_k, cfg_.sigma_omega,
-                   (const double*)mut_.trace.data(), kDiff_.trace.data(), wDiff_.trace.data());
+    const bool ke = cfg_.kind == 1;
+    if (ke) {
+        launch(ctx_, kTransportCoefficientsKE, N, N, cfg_.rho, cfg_.mu, cfg_.c1, cfg_.c2, 1.0 / cfg_.sigma_k,
+               1.0 / cfg_.sigma_omega, cfg_.k_min, (const double*)G_.data(), (const double*)mut_.v.data(),
+               (const double*)k_.v.data(), (const double*)omega_.v.data(), production_.data(), kDiff_.v.data(),
+               wDiff_.v.data(), kSink_.data(), wDestruction_.data(), wProduction_.data());
+        if (nb) launch(ctx_, kDiffusivityTrace, nb, nb, cfg_.mu, 1.0 / cfg_.sigma_k, 1.0 / cfg_.sigma_omega,
+                       (const double*)mut_.trace.data(), kDiff_.trace.data(), wDiff_.trace.data());
+    } else {
+        launch(ctx_, kTransportCoefficients, N, N, cfg_.rho, cfg_.mu, cfg_.beta, cfg_.gamma, cfg_.sigma_k,
+               cfg_.sigma_omega, cfg_.k_min, (const double*)G_.data(), (const double*)mut_.v.data(),
+               (const double*)k_.v.data(), (const double*)omega_.v.data(), production_.data(), kDiff_.v.data(),
+               wDiff_.v.data(), wDestruction_.data(), wProduction_.data());
+        if (nb) launch(ctx_, kDiffusivityTrace, nb, nb, cfg_.mu, cfg_.sigma_k, cfg_.sigma_omega,
+                       (const double*)mut_.trace.data(), kDiff_.trace.data(), wDiff_.trace.data());
+    }
     double* h = ctx_.pinned;
     auto solveOne = [&](DeviceEquation& eq, DeviceField& x, DeviceField& diff, const double* sink, const double* src,
                         const double* previous, const SolverConfig& scfg, Reducer& red, double& r0) {
@@ -306,15 +380,24 @@ TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
         res.linear_converged = res.linear_converged && o.status == 0;
         res.healthy = res.healthy && o.status != 2 && std::isfinite(o.final_) && std::isfinite(r0);
     };
-    // omega first, then k with the new omega in its sink (k_omega.cpp:83-110)
     double rW = 0.0, rK = 0.0;
-    solveOne(*weq_, omega_, wDiff_, wDestruction_.data(), wProduction_.data(), prevW_.data(), cfg_.omega_solver, redW_,
-             rW);
-    if (!res.healthy) return res;
-    boundOmega();
-    launch(ctx_, kScaled, N, N, cfg_.beta_star * cfg_.rho, (const double*)omega_.v.data(), kSink_.data());
-    solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK);
-    if (!res.healthy) return res;
+    if (ke) {
+        // k first, then epsilon, one frozen closure state (k_epsilon.cpp:79-103)
+        solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK);
+        if (!res.healthy) return res;
+        solveOne(*weq_, omega_, wDiff_, wDestruction_.data(), wProduction_.data(), prevW_.data(), cfg_.omega_solver,
+                 redW_, rW);
+        if (!res.healthy) return res;
+    } else {
+        // omega first, then k with the new omega in its sink (k_omega.cpp:83-110)
+        solveOne(*weq_, omega_, wDiff_, wDestruction_.data(), wProduction_.data(), prevW_.data(), cfg_.omega_solver,
+                 redW_, rW);
+        if (!res.healthy) return res;
+        boundOmega();
+        launch(ctx_, kScaled, N, N, cfg_.beta_star * cfg_.rho, (const double*)omega_.v.data(), kSink_.data());
+        solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK);
+        if (!res.healthy) return res;
+    }
     // boundTransportFields(); updateViscosity() (k_omega.cpp:114-116)
     k_.setFluxContext(phi);
     omega_.setFluxContext(phi);

@@ -12,10 +12,15 @@
 
 namespace bsg {
 
+// Two-equation eddy-viscosity models: kind 0 Wilcox-1988m k-omega (k_omega.cpp),
+// kind 1 standard k-epsilon (k_epsilon.cpp).  The second transported field
+// (omega or epsilon) uses the omega_* members of the configuration.
 struct KOmegaConfig {
+    int kind = 0;
     double rho = 1.0, mu = 1e-3;
     double beta_star = 0.09, beta = 3.0 / 40.0, gamma = 5.0 / 9.0, sigma_k = 0.5, sigma_omega = 0.5;
     double k_min = 1e-12, omega_min = 1e-12, viscosity_ratio_max = 1e5;
+    double c_mu = 0.09, c1 = 1.44, c2 = 1.92;  // k-epsilon (sigma_k, sigma_omega = sigmaEpsilon, omega_min = epsilonMin)
     double relaxation = 0.7, tolerance = 1e-6;
     Options k_options, omega_options, momentum_options;
     SolverConfig k_solver, omega_solver;

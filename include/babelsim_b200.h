@@ -328,6 +328,19 @@ typedef struct {
     bsg_solver_config omega_solver;
 } bsg_komega_config;
 
+/* standard k-epsilon (src/physics/RANS/k_epsilon.cpp:25-128): physics keys kEpsilonCmu/C1/C2/
+ * SigmaK/SigmaEpsilon, kMin, epsilonMin; equation controls kTransport and epsilonTransport. */
+typedef struct {
+    double c_mu, c1, c2, sigma_k, sigma_epsilon;
+    double k_min, epsilon_min;
+    double relaxation;
+    double tolerance;
+    bsg_options k_transport;
+    bsg_options epsilon_transport;
+    bsg_solver_config k_solver;
+    bsg_solver_config epsilon_solver;
+} bsg_kepsilon_config;
+
 int bsg_simple_create(bsg_mesh* mesh, const bsg_simple_config* config, bsg_simple** out);
 /* Boundary constraint of "U" or "p" on one patch (the case's fields/initial). */
 int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int32_t type,
@@ -346,9 +359,12 @@ int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report*
  * before set_fields; then "k" and "omega" take boundary conditions through
  * bsg_simple_set_boundary and initial values through set_turbulence_fields. */
 int bsg_simple_enable_komega(bsg_simple* s, const bsg_komega_config* config);
-int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* omega);
-/* k, omega and the turbulent viscosity mut (n_cells each; NULL skips). */
-int bsg_simple_get_turbulence_fields(const bsg_simple* s, double* k, double* omega, double* mut);
+/* turbulenceModel kEpsilon: as above, with "k" and "epsilon". */
+int bsg_simple_enable_kepsilon(bsg_simple* s, const bsg_kepsilon_config* config);
+/* initial k and the second transported field (omega or epsilon) */
+int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* second);
+/* k, the second transported field and the turbulent viscosity mut (n_cells each; NULL skips). */
+int bsg_simple_get_turbulence_fields(const bsg_simple* s, double* k, double* second, double* mut);
 int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi);
 int bsg_simple_destroy(bsg_simple* s);
 

@@ -1,4 +1,5 @@
-"""Wilcox-1988m k-omega, restated from src/physics/RANS/k_omega.cpp and model.cpp.  TEST INFRASTRUCTURE ONLY.
+"""Wilcox-1988m k-omega and standard k-epsilon, restated from src/physics/RANS/k_omega.cpp,
+k_epsilon.cpp and model.cpp.  TEST INFRASTRUCTURE ONLY.
 
 Derived fields carry boundary traces exactly as the reference's calculated
 fields do (include/babelsim/field.h:262-320, math.h:184-258): every pointwise
@@ -194,3 +195,92 @@ class KOmega:
         self.update_viscosity()
         return dict(d=max(fvm.relative_change(self.omega.v, prev_w), fvm.relative_change(self.k.v, prev_k)),
                     r=max(r_w, r_k))
+
+
+@dataclass
+class KEpsilonConstants:
+    """Model constants and bounds (k_epsilon.cpp:31-39)."""
+    c_mu: float = 0.09
+    c1: float = 1.44
+    c2: float = 1.92
+    sigma_k: float = 1.0
+    sigma_epsilon: float = 1.3
+    k_min: float = 1e-12
+    epsilon_min: float = 1e-12
+    relaxation: float = 0.7
+    tolerance: float = 1e-6
+
+
+class KEpsilon(KOmega):
+    """KEpsilon (k_epsilon.cpp:25-128) on oracle fields: k first, then epsilon, one frozen closure state."""
+
+    def __init__(self, geo, k: fvm.Field, epsilon: fvm.Field, rho, mu, c: KEpsilonConstants, k_opts, eps_opts,
+                 momentum_opts, phi0):
+        self.geo, self.k, self.eps, self.rho, self.mu, self.c = geo, k, epsilon, rho, mu, c
+        self.k_opts, self.eps_opts, self.mom_opts = k_opts, eps_opts, momentum_opts
+        self.bf = np.nonzero(geo.neighbour < 0)[0]
+        nf = geo.n_faces
+        self.mut_v = np.zeros(geo.n_cells)
+        self.mut_tr = np.zeros(nf)
+        self.mueff_v = np.full(geo.n_cells, mu)
+        self.mueff_tr = np.full(nf, mu)
+        self.bound_transport_fields(phi0)
+        self.update_viscosity()
+
+    @property
+    def omega(self):  # the second transported field, for callers that read both
+        return self.eps
+
+    def bound_transport_fields(self, phi):
+        self.k.flux = np.array(phi, dtype=np.float64)
+        self.eps.flux = np.array(phi, dtype=np.float64)
+        self.k.v = np.maximum(self.k.v, self.c.k_min)
+        self.eps.v = np.maximum(self.eps.v, self.c.epsilon_min)
+
+    def update_viscosity(self):
+        """mut = Cmu rho k k / max(epsilon, epsilonMin); muEff = mu + mut (k_epsilon.cpp:122-125)."""
+        emin = self.c.epsilon_min
+        cr = self.c.c_mu * self.rho
+        self.mut_v = ((cr * self.k.v) * self.k.v) / np.maximum(self.eps.v, emin)
+        kt, et = self._trace(self.k), self._trace(self.eps)
+        self.mut_tr = np.zeros(self.geo.n_faces)
+        b = self.bf
+        self.mut_tr[b] = ((cr * kt[b]) * kt[b]) / np.maximum(et[b], emin)
+        self.mueff_v = self.mut_v + self.mu
+        self.mueff_tr = self.mut_tr + self.mu
+
+    def solve_transport(self, U: fvm.Field, phi):
+        """KEpsilon::solveTransport (k_epsilon.cpp:62-111), steady."""
+        geo, c, rho, mu = self.geo, self.c, self.rho, self.mu
+        prev_k, prev_e = self.k.v.copy(), self.eps.v.copy()
+        U.flux = np.array(phi, dtype=np.float64)
+        self.update_viscosity()
+        G = fvm.gradient(U, self.mom_opts["gradient"])
+        production = self.mut_v * strain_squared(G)
+        k_diff = fvm.Field(geo, (1.0 / c.sigma_k) * self.mut_v + mu, None, trace=(1.0 / c.sigma_k) * self.mut_tr + mu)
+        e_diff = fvm.Field(geo, (1.0 / c.sigma_epsilon) * self.mut_v + mu, None,
+                           trace=(1.0 / c.sigma_epsilon) * self.mut_tr + mu)
+        eok = self.eps.v / np.maximum(self.k.v, c.k_min)
+        k_destruction = rho * eok
+        e_destruction = (c.c2 * rho) * eok
+        e_production = (c.c1 * production) * eok
+        keq = fvm.Equation(self.k, self.k_opts, {})
+        fvm.eq_div(keq, phi, rho)
+        fvm.eq_laplacian(keq, k_diff, -1.0)
+        keq.ldu.diag = keq.ldu.diag + (1.0 * k_destruction) * geo.volume
+        fvm.eq_source(keq, production)
+        r_k = fvm.relative_residual(keq.ldu, self.k.v)
+        fvm.eq_relax(keq, prev_k, c.relaxation)
+        self.k.v = _solve(keq.ldu.matrix(), keq.ldu.source)
+        eeq = fvm.Equation(self.eps, self.eps_opts, {})
+        fvm.eq_div(eeq, phi, rho)
+        fvm.eq_laplacian(eeq, e_diff, -1.0)
+        eeq.ldu.diag = eeq.ldu.diag + (1.0 * e_destruction) * geo.volume
+        fvm.eq_source(eeq, e_production)
+        r_e = fvm.relative_residual(eeq.ldu, self.eps.v)
+        fvm.eq_relax(eeq, prev_e, c.relaxation)
+        self.eps.v = _solve(eeq.ldu.matrix(), eeq.ldu.source)
+        self.bound_transport_fields(phi)
+        self.update_viscosity()
+        return dict(d=max(fvm.relative_change(self.k.v, prev_k), fvm.relative_change(self.eps.v, prev_e)),
+                    r=max(r_k, r_e))

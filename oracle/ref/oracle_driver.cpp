@@ -96,7 +96,7 @@ int main(int argc, char** argv) {
         writeVector(f, "p", detail::fieldValues(problem.existingScalarField("p")));
         writeVector(f, "phi", detail::fieldValues(problem.existingFaceField("phi")));
         // turbulence fields, when the case has a model
-        for (const char* name : {"k", "omega", "mut", "muEffective"}) {
+        for (const char* name : {"k", "omega", "epsilon", "nuTilda", "mut", "muEffective"}) {
             try {
                 writeVector(f, name, detail::fieldValues(problem.existingScalarField(name)));
             } catch (const std::exception&) {

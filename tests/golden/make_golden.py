@@ -200,11 +200,12 @@ def make_piso(name, mesh, U_bcs, p_bcs, methods, solution, physics, time, start,
     print(name, "written", len(ends), "steps")
 
 
-def make_rans(name, mesh, U_bcs, p_bcs, k_field, w_field, methods, solution, physics, K):
-    """Steady SIMPLE with the reference's k-omega model: U, p, phi, k, omega after iterations 1..K."""
+def make_rans(name, mesh, U_bcs, p_bcs, k_field, w_field, methods, solution, physics, K, second="omega"):
+    """Steady SIMPLE with the reference's k-omega (or k-epsilon) model: U, p, phi, k and the second
+    transported field after iterations 1..K (stored under omega_* for both models)."""
     work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
     write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics,
-               extra_fields=[("k",) + tuple(k_field), ("omega",) + tuple(w_field)])
+               extra_fields=[("k",) + tuple(k_field), (second,) + tuple(w_field)])
     data = {}
     offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
     data["mesh_vertices"] = mesh.vertices
@@ -214,31 +215,31 @@ def make_rans(name, mesh, U_bcs, p_bcs, k_field, w_field, methods, solution, phy
     for k in range(1, K + 1):
         fields, geo, info, _ = run(work, k)
         data[f"U_{k}"] = fields["U"].reshape(-1, 3)
-        for key in ("p", "phi", "k", "omega", "mut", "muEffective"):
-            data[f"{key}_{k}"] = fields[key]
+        for key in ("p", "phi", "k", second, "mut", "muEffective"):
+            data[f"{'omega' if key == second else key}_{k}"] = fields[key]
     for key, arr in geo.items():
         data["geo_" + key] = arr
     meta = dict(patch_names=mesh.patch_names, patch_kinds=mesh.patch_kinds,
                 U_bcs=[(t, list(map(float, v))) for t, v in U_bcs], p_bcs=[(t, float(v)) for t, v in p_bcs],
                 k_internal=k_field[0], k_bcs=[(t, float(v)) for t, v in k_field[1]],
                 omega_internal=w_field[0], omega_bcs=[(t, float(v)) for t, v in w_field[1]],
-                methods=methods, solution=solution, physics=physics, K=K)
+                methods=methods, solution=solution, physics=physics, K=K, second=second)
     data["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
     shutil.rmtree(work)
     print(name, "written", K, "iterations")
 
 
-def rans_methods(conv="upwind", grad="greenGauss", diff="orthogonal", turb_conv="upwind"):
+def rans_methods(conv="upwind", grad="greenGauss", diff="orthogonal", turb_conv="upwind", second="omega"):
     o = dict(interpolation="linear", gradient=grad, convection=conv, diffusion=diff)
     t = dict(o, convection=turb_conv)
-    return {"momentum": o, "pressureCorrection": o, "kTransport": t, "omegaTransport": t}
+    return {"momentum": o, "pressureCorrection": o, "kTransport": t, f"{second}Transport": t}
 
 
-def rans_solution():
+def rans_solution(second="omega"):
     sol = config1_solution(1e-12)
     sol.update({"turbulenceRelaxation": 0.7, "turbulenceTolerance": 1e-6})
-    for eq in ("kTransport", "omegaTransport"):
+    for eq in ("kTransport", f"{second}Transport"):
         sol.update({f"equation.{eq}.kspType": "bcgs", f"equation.{eq}.pcType": "bjacobi",
                     f"equation.{eq}.absoluteTolerance": 1e-18, f"equation.{eq}.relativeTolerance": 1e-12,
                     f"equation.{eq}.maxIterations": 2000})
@@ -270,6 +271,14 @@ def main_rans():
     ww = [("fixedValue", 500.0)] * 6
     make_rans("komega_warped5", meshgen.warped_box(5), Uw, pw, (1e-3, kw), (5.0, ww),
               rans_methods("linearUpwind", "leastSquares", "corrected"), rans_solution(), komega, K=3)
+    # standard k-epsilon in the same channel
+    keps = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "kEpsilon", "kEpsilonCmu": 0.09,
+            "kEpsilonC1": 1.44, "kEpsilonC2": 1.92, "kEpsilonSigmaK": 1.0, "kEpsilonSigmaEpsilon": 1.3,
+            "kMin": 1e-12, "epsilonMin": 1e-12}
+    eb = [("fixedValue", 2.0e-4), ("zeroGradient", 0.0), ("fixedValue", 1e-10), ("fixedValue", 1e-10),
+          ("symmetry", 0.0), ("symmetry", 0.0)]
+    make_rans("kepsilon_channel", ch, U, p, (3.75e-3, kb), (2.0e-4, eb), rans_methods("linearUpwind", second="epsilon"),
+              rans_solution("epsilon"), keps, K=4, second="epsilon")
 
 
 def piso_solution(n_correctors=2, non_orth=1, p_rtol=1e-12):

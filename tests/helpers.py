@@ -128,3 +128,20 @@ def komega_factory(g: "Golden"):
         return rans.KOmega(geo, k, w, ph["density"], ph["dynamicViscosity"], komega_constants(g),
                            m["kTransport"], m["omegaTransport"], m["momentum"], phi0)
     return make
+
+
+def kepsilon_factory(g: "Golden"):
+    """Model factory for oracle.simple.run_simple(turbulence=...) from a k-epsilon fixture."""
+    ph, sol, m = g.meta["physics"], g.meta["solution"], g.meta["methods"]
+    c = rans.KEpsilonConstants(ph["kEpsilonCmu"], ph["kEpsilonC1"], ph["kEpsilonC2"], ph["kEpsilonSigmaK"],
+                               ph["kEpsilonSigmaEpsilon"], ph["kMin"], ph["epsilonMin"], sol["turbulenceRelaxation"],
+                               sol["turbulenceTolerance"])
+    kb = [(fvm.BC_NAMES[t], v) for t, v in g.meta["k_bcs"]]
+    eb = [(fvm.BC_NAMES[t], v) for t, v in g.meta["omega_bcs"]]
+
+    def make(geo, phi0):
+        k = fvm.Field(geo, np.full(geo.n_cells, g.meta["k_internal"]), kb)
+        e = fvm.Field(geo, np.full(geo.n_cells, g.meta["omega_internal"]), eb)
+        return rans.KEpsilon(geo, k, e, ph["density"], ph["dynamicViscosity"], c, m["kTransport"],
+                             m["epsilonTransport"], m["momentum"], phi0)
+    return make

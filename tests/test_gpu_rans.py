@@ -1,6 +1,7 @@
-"""k-omega SIMPLE on the GPU vs the reference's own runSimple + KOmega, through the C ABI.
+"""k-omega and k-epsilon SIMPLE on the GPU vs the reference's own runSimple + KOmega /
+KEpsilon, through the C ABI.
 
-Tolerance: 1e-8 relative L2 on U, p, phi, k, omega and mut after every outer
+Tolerance: 1e-8 relative L2 on U, p, phi, k, omega (epsilon) and mut after every outer
 iteration (every linear solve at rtol 1e-12 on both sides; the transported
 turbulence equations are non-symmetric and run BiCGStab with Jacobi here,
 against the reference's Krylov backend at the same tolerance).
@@ -35,11 +36,21 @@ def _komega_simple(bsg, g, m, pc="hypre"):
                      bsg.options(**s.momentum), bsg.options(**s.pressure),
                      _solver(bsg, sol, "momentum", "bcgs", "bjacobi", 2000),
                      _solver(bsg, sol, "pressureCorrection", "cg", pc))
-    c = komega_constants(g)
-    sim.enable_komega(c.beta_star, c.beta, c.gamma, c.sigma_k, c.sigma_omega, c.k_min, c.omega_min,
-                      c.viscosity_ratio_max, c.relaxation, c.tolerance, bsg.options(**meth["kTransport"]),
-                      bsg.options(**meth["omegaTransport"]), _solver(bsg, sol, "kTransport", "bcgs", "bjacobi", 2000),
-                      _solver(bsg, sol, "omegaTransport", "bcgs", "bjacobi", 2000))
+    second = g.meta.get("second", "omega")
+    if second == "epsilon":
+        sim.enable_kepsilon(ph["kEpsilonCmu"], ph["kEpsilonC1"], ph["kEpsilonC2"], ph["kEpsilonSigmaK"],
+                            ph["kEpsilonSigmaEpsilon"], ph["kMin"], ph["epsilonMin"], sol["turbulenceRelaxation"],
+                            sol["turbulenceTolerance"], bsg.options(**meth["kTransport"]),
+                            bsg.options(**meth["epsilonTransport"]),
+                            _solver(bsg, sol, "kTransport", "bcgs", "bjacobi", 2000),
+                            _solver(bsg, sol, "epsilonTransport", "bcgs", "bjacobi", 2000))
+    else:
+        c = komega_constants(g)
+        sim.enable_komega(c.beta_star, c.beta, c.gamma, c.sigma_k, c.sigma_omega, c.k_min, c.omega_min,
+                          c.viscosity_ratio_max, c.relaxation, c.tolerance, bsg.options(**meth["kTransport"]),
+                          bsg.options(**meth["omegaTransport"]),
+                          _solver(bsg, sol, "kTransport", "bcgs", "bjacobi", 2000),
+                          _solver(bsg, sol, "omegaTransport", "bcgs", "bjacobi", 2000))
     for p, (t, v) in enumerate(g.meta["U_bcs"]):
         sim.set_boundary("U", p, t, v)
     for p, (t, v) in enumerate(g.meta["p_bcs"]):
@@ -47,14 +58,14 @@ def _komega_simple(bsg, g, m, pc="hypre"):
     for p, (t, v) in enumerate(g.meta["k_bcs"]):
         sim.set_boundary("k", p, t, v)
     for p, (t, v) in enumerate(g.meta["omega_bcs"]):
-        sim.set_boundary("omega", p, t, v)
+        sim.set_boundary(second, p, t, v)
     n = m.n_cells
     sim.set_turbulence_fields(np.full(n, g.meta["k_internal"]), np.full(n, g.meta["omega_internal"]))
     sim.set_fields(np.zeros((n, 3)), np.zeros(n))
     return sim
 
 
-@pytest.mark.parametrize("name", RANS_CASES)
+@pytest.mark.parametrize("name", RANS_CASES + ["kepsilon_channel"])
 def test_komega_simple_every_iteration_matches_reference(ctx, name):
     import babelsim_b200 as bsg
     g = Golden(name)

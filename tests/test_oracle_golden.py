@@ -9,8 +9,8 @@ solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
 import numpy as np
 import pytest
 
-from helpers import (CASES, PISO_CASES, RANS_CASES, Golden, komega_factory, piso_settings, ref_system_groups, rel,
-                     rel_l2)
+from helpers import (CASES, PISO_CASES, RANS_CASES, Golden, kepsilon_factory, komega_factory, piso_settings,
+                     ref_system_groups, rel, rel_l2)
 from oracle import fvm, simple
 
 
@@ -139,7 +139,7 @@ def test_bdf2_weights_variable_step():
     assert abs(a0 * y(t0) - a1 * y(t0 - h0) - a2 * y(t0 - h0 - h1) - 2 * t0) < 1e-12
 
 
-@pytest.mark.parametrize("name", RANS_CASES)
+@pytest.mark.parametrize("name", RANS_CASES + ["kepsilon_channel"])
 def test_komega_simple_iterations_match_reference(name):
     """SIMPLE with the Wilcox-1988m k-omega model: the restatement (calculated boundary traces of
     mut/muEff/diffusivities, stress remainder divergence, omega-then-k transport with bounding)
@@ -149,7 +149,8 @@ def test_komega_simple_iterations_match_reference(name):
     s = g.settings()
     s.mu = g.meta["physics"]["dynamicViscosity"]
     for k in range(1, g.K + 1):
-        st = simple.run_simple(geo, g.U_bcs(), g.p_bcs(), s, iterations=k, turbulence=komega_factory(g))
+        model = kepsilon_factory(g) if name.startswith("kepsilon") else komega_factory(g)
+        st = simple.run_simple(geo, g.U_bcs(), g.p_bcs(), s, iterations=k, turbulence=model)
         for key, mine in (("U", st.U), ("p", st.p), ("phi", st.phi), ("k", st.k), ("omega", st.omega),
                           ("mut", st.mut)):
             assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k)
