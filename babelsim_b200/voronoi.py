@@ -8,8 +8,8 @@ tessellation is the dual of the Delaunay tetrahedralisation (scipy/qhull):
 Voronoi vertices are tetrahedron circumcentres and the face between sites i
 and j is the ring of circumcentres of the tetrahedra around edge (i,j), ordered
 by angle about the ring's mean point in the bisector plane.  Coincident
-circumcentres (cospherical site groups, which the mirror planes create) are
-merged at 1e-9/n.  Everything after the triangulation is vectorised numpy.
+circumcentres (cospherical site groups, which the mirror planes create) closer
+than 1e-9/n are merged.  Everything after the triangulation is vectorised numpy.
 """
 from __future__ import annotations
 
@@ -38,13 +38,26 @@ def _circumcentres(p):
     return c, np.abs(det)
 
 
-def _merge_ids(c, tol):
-    """Ids that agree for points equal after quantisation at `tol` (64-bit hash of the cell)."""
-    q = np.round(c / tol).astype(np.int64).view(np.uint64)
-    h = (q[:, 0] * np.uint64(0x9E3779B97F4A7C15)) ^ (q[:, 1] * np.uint64(0xC2B2AE3D27D4EB4F)) ^ \
-        (q[:, 2] * np.uint64(0x165667B19E3779F9))
-    _, inv = np.unique(h, return_inverse=True)
-    return inv.ravel()
+def _merge_ids(c, good, tol):
+    """Vertex ids of the circumcentres: those of `good` tetrahedra closer than `tol` (transitively)
+    share an id, every other tetrahedron gets an id of its own.
+
+    Pairs come from a KD-tree and ids are connected components, so two centres
+    a rounding error apart always merge (a quantisation grid would split the
+    pairs that straddle a grid boundary and leave a non-manifold cell surface).
+    """
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    from scipy.spatial import cKDTree
+    idx = np.nonzero(good)[0]
+    pairs = cKDTree(c[idx]).query_pairs(tol, output_type="ndarray")
+    n = len(idx)
+    graph = coo_matrix((np.ones(len(pairs), np.int8), (pairs[:, 0], pairs[:, 1])), shape=(n, n))
+    n_comp, label = connected_components(graph, directed=False)
+    out = np.empty(len(c), np.int64)
+    out[idx] = label
+    out[~good] = n_comp + np.arange(len(c) - n)
+    return out
 
 
 def _face_areas(ids, sizes, verts):
@@ -151,7 +164,7 @@ def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, 
     tets = Delaunay(pts).simplices.astype(np.int64)
     cc, det = _circumcentres(pts[tets])
     good = det > 1e-12 * h ** 3
-    vid_of_tet = _merge_ids(cc, 1e-9 * h)
+    vid_of_tet = _merge_ids(cc, good, 1e-9 * h)
     pairs = np.array([(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)])
     ea = tets[:, pairs[:, 0]].ravel()
     eb = tets[:, pairs[:, 1]].ravel()

@@ -31,6 +31,23 @@ def test_voronoi_cube_is_a_closed_tessellation(n):
     assert validate_polyhedral(pm) == (n ** 3, False)
 
 
+def test_voronoi_vertex_merge_has_no_grid_boundaries():
+    """Circumcentres a rounding error apart merge even where they straddle a multiple of the
+    tolerance (the 216000-cell cube had such a pair), and chains merge transitively."""
+    from babelsim_b200.voronoi import _merge_ids
+    tol = 1e-9
+    c = np.array([[0.5 * tol * (1 - 1e-6), 0, 0], [0.5 * tol * (1 + 1e-6), 0, 0], [1.0, 0, 0],
+                  [1.0 + 0.9 * tol, 0, 0], [1.0 + 1.8 * tol, 0, 0], [0.5 * tol, 0, 0]])
+    good = np.array([True, True, True, True, True, False])
+    ids = _merge_ids(c, good, tol)
+    assert ids[0] == ids[1] and ids[2] == ids[3] == ids[4] and ids[0] != ids[2]
+    assert ids[5] not in ids[:5]
+
+
+def test_voronoi_cube_216000_cells_is_valid():
+    assert validate_polyhedral(meshgen.voronoi_cube(60)) == (216000, False)
+
+
 def test_voronoi_cube_is_seeded():
     a, b = meshgen.voronoi_cube(5, seed=1), meshgen.voronoi_cube(5, seed=1)
     c = meshgen.voronoi_cube(5, seed=2)
