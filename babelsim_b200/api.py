@@ -115,17 +115,18 @@ class Mesh:
         self.orthogonal = bool(orth)
 
     @classmethod
-    def from_polyhedral(cls, ctx: Context, poly):
-        """Geometry computed by the library from a polyhedral description (see meshgen.PolyMesh)."""
+    def from_polyhedral(cls, ctx: Context, poly, host_geometry: bool = False):
+        """Geometry computed by the library from a polyhedral description (see meshgen.PolyMesh),
+        on the device (default) or on the host (`host_geometry`); both give identical bits."""
         off, ids = poly.flat() if hasattr(poly, "flat") else (
             np.concatenate([[0], np.cumsum([len(f) for f in poly.faces])]), np.concatenate(poly.faces))
         offsets, ids = i32(off), i32(ids)
         verts = f64(poly.vertices)
         owner, nbr, patch = i32(poly.owner), i32(poly.neighbour), i32(poly.patch)
         h = C.c_void_p()
-        check(lib().bsg_mesh_create_polyhedral(ctx.h, len(verts), ptr(verts), len(owner), ptr(offsets), ptr(ids),
-                                               ptr(owner), ptr(nbr), ptr(patch), len(poly.patch_names),
-                                               C.byref(h)), ctx.h)
+        create = lib().bsg_mesh_create_polyhedral_host if host_geometry else lib().bsg_mesh_create_polyhedral
+        check(create(ctx.h, len(verts), ptr(verts), len(owner), ptr(offsets), ptr(ids), ptr(owner), ptr(nbr),
+                     ptr(patch), len(poly.patch_names), C.byref(h)), ctx.h)
         m = cls(ctx, h, len(poly.patch_names))
         m.patch_names = list(poly.patch_names)
         return m

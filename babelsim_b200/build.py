@@ -20,8 +20,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbabelsim_b200.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["mesh.cpp", "fvm.cu", "krylov.cu", "amg.cu", "pcg_persistent.cu", "pcg_sell.cu", "simple.cu", "piso.cu", "rans.cu", "results.cpp", "capi.cpp"]
+SOURCES = ["mesh.cpp", "geometry.cu", "fvm.cu", "krylov.cu", "amg.cu", "pcg_persistent.cu", "pcg_sell.cu", "simple.cu", "piso.cu", "rans.cu", "results.cpp", "capi.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# The device geometry reproduces the host geometry bit for bit: no FMA contraction there.
+EXTRA = {"geometry.cu": ["-fmad=false"]}
 
 
 def nvcc():
@@ -44,7 +46,7 @@ def compile_one(src):
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
     lang = ["-x", "cu"] if src.endswith(".cu") else []
-    cmd = [nvcc()] + flags() + lang + ["-c", path, "-o", obj]
+    cmd = [nvcc()] + flags() + EXTRA.get(src, []) + lang + ["-c", path, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{res.stdout}\n{res.stderr}")

@@ -170,7 +170,6 @@ struct DeviceMesh {
     DeviceArray<double> face_stage;      // staging for face fields crossing the ABI
     // host copies kept for setup work (AMG aggregation, exports)
     std::vector<int> h_own, h_nbr, h_cf_ptr, h_cf_col, h_cf_face, h_bown, h_cb_ptr;
-    std::vector<double> h_dcoef;
     // device arrays
     DeviceArray<double> V, rV, xc;
     DeviceArray<int> own, nbr;
@@ -183,7 +182,8 @@ struct DeviceMesh {
     DeviceArray<int> slot_own, slot_nbr;
     // scratch for the first Green-Gauss pass (3*9*n_cells doubles at most)
     DeviceArray<double> ws_grad_pass1;
-    // external geometry copy for bsg_mesh_export (host)
+    // external geometry copy for bsg_mesh_export (host; filled on first export when the
+    // geometry was computed on the device)
     std::vector<double> ext_Sf, ext_xf, ext_area, ext_n, ext_w, ext_dcoef, ext_k, ext_skew, ext_xc, ext_V;
     std::vector<int> ext_owner, ext_nbr, ext_patch;
 };
@@ -202,6 +202,20 @@ HostGeometry computePolyhedralGeometry(int n_vertices, const double* vertices, i
                                        const int* owner, const int* neighbour, const int* patch,
                                        int n_patches);
 std::unique_ptr<DeviceMesh> buildDeviceMesh(Context& ctx, const HostGeometry& g);
+// The integer checks of Mesh::polyhedral's input; returns the cell count.
+int validatePolyhedralTopology(int n_vertices, int n_faces, const int* offsets, const int* ids, const int* owner,
+                               const int* neighbour, const int* patch, int n_patches);
+// Internal face order, cell->face lists and matrix slots (host counting passes, then uploaded).
+void buildTopology(DeviceMesh& m, Context& ctx, int n_cells, int n_faces, int n_patches, const int* owner,
+                   const int* neighbour, const int* patch);
+// Mesh::polyhedral with the geometry computed on the device, bit-identical to
+// computePolyhedralGeometry (geometry.cu).
+std::unique_ptr<DeviceMesh> buildDeviceMeshPolyhedral(Context& ctx, int n_vertices, const double* vertices,
+                                                      int n_faces, const int* offsets, const int* ids,
+                                                      const int* owner, const int* neighbour, const int* patch,
+                                                      int n_patches);
+// Fills the caller-numbered host geometry (ext_*) from the device arrays if it is absent.
+void ensureExternalGeometry(DeviceMesh& m);
 
 // Launch helpers.
 inline unsigned gridFor(long long n, int block) {

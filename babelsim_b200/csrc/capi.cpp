@@ -378,6 +378,24 @@ int bsg_mesh_create_polyhedral(bsg_context* ctx, int32_t n_vertices, const doubl
                                const int32_t* neighbour, const int32_t* patch, int32_t n_patches, bsg_mesh** out) {
     return guard(ctx, [&] {
         require(ctx && vertices && offsets && ids && owner && neighbour && patch && out, "null argument");
+        auto* m = new bsg_mesh{ctx, nullptr};
+        try {
+            m->mesh = bsg::buildDeviceMeshPolyhedral(*ctx->ctx, n_vertices, vertices, n_faces, offsets, ids, owner,
+                                                     neighbour, patch, n_patches);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int bsg_mesh_create_polyhedral_host(bsg_context* ctx, int32_t n_vertices, const double* vertices, int32_t n_faces,
+                                    const int32_t* offsets, const int32_t* ids, const int32_t* owner,
+                                    const int32_t* neighbour, const int32_t* patch, int32_t n_patches,
+                                    bsg_mesh** out) {
+    return guard(ctx, [&] {
+        require(ctx && vertices && offsets && ids && owner && neighbour && patch && out, "null argument");
         const bsg::HostGeometry h = bsg::computePolyhedralGeometry(n_vertices, vertices, n_faces, offsets, ids, owner,
                                                                     neighbour, patch, n_patches);
         auto* m = new bsg_mesh{ctx, nullptr};
@@ -437,7 +455,8 @@ int bsg_mesh_sizes(const bsg_mesh* mesh, int64_t out[5]) {
 int bsg_mesh_export(const bsg_mesh* mesh, const char* name, void* host_out) {
     return guard(ctxOf(mesh), [&] {
         require(mesh && name && host_out, "null argument");
-        const bsg::DeviceMesh& m = *mesh->mesh;
+        bsg::DeviceMesh& m = *mesh->mesh;
+        bsg::ensureExternalGeometry(m);
         const std::string n(name);
         auto put = [&](const auto& v) { std::memcpy(host_out, v.data(), v.size() * sizeof(v[0])); };
         if (n == "face_owner") put(m.ext_owner);

@@ -107,11 +107,10 @@ V3 vtx(const double* verts, int i) { return {verts[3 * i], verts[3 * i + 1], ver
 
 }  // namespace
 
-HostGeometry computePolyhedralGeometry(int n_vertices, const double* verts, int n_faces,
-                                       const int* offsets, const int* ids, const int* owner,
-                                       const int* neighbour, const int* patch, int n_patches) {
+int validatePolyhedralTopology(int n_vertices, int n_faces, const int* offsets, const int* ids, const int* owner,
+                               const int* neighbour, const int* patch, int n_patches) {
     if (n_vertices <= 0 || n_faces <= 0 || n_patches <= 0) fail(kArgument, "polyhedral mesh arrays are empty");
-    HostGeometry g;
+    if (offsets[0] != 0) fail(kArgument, "polyhedral face offsets must start at 0");
     int n_cells = 0;
     for (int f = 0; f < n_faces; ++f) {
         if (owner[f] < 0 || neighbour[f] < -1 || neighbour[f] == owner[f])
@@ -122,9 +121,19 @@ HostGeometry computePolyhedralGeometry(int n_vertices, const double* verts, int 
             fail(kArgument, "internal polyhedral face cannot belong to a boundary patch");
         if (neighbour[f] < 0 && (patch[f] < 0 || patch[f] >= n_patches))
             fail(kArgument, "boundary polyhedral face " + std::to_string(f) + " has invalid patch");
+        if (offsets[f + 1] < offsets[f]) fail(kArgument, "polyhedral face offsets decrease");
         for (int k = offsets[f]; k < offsets[f + 1]; ++k)
             if (ids[k] < 0 || ids[k] >= n_vertices) fail(kArgument, "face references an invalid vertex");
     }
+    return n_cells;
+}
+
+HostGeometry computePolyhedralGeometry(int n_vertices, const double* verts, int n_faces,
+                                       const int* offsets, const int* ids, const int* owner,
+                                       const int* neighbour, const int* patch, int n_patches) {
+    HostGeometry g;
+    const int n_cells = validatePolyhedralTopology(n_vertices, n_faces, offsets, ids, owner, neighbour, patch,
+                                                   n_patches);
     g.n_cells = n_cells;
     g.n_faces = n_faces;
     g.n_patches = n_patches;
@@ -302,93 +311,57 @@ HostGeometry computePolyhedralGeometry(int n_vertices, const double* verts, int 
     return g;
 }
 
-std::unique_ptr<DeviceMesh> buildDeviceMesh(Context& ctx, const HostGeometry& g) {
-    if (g.n_cells <= 0 || g.n_faces <= 0) fail(kArgument, "mesh has no cells or faces");
-    auto m = std::make_unique<DeviceMesh>();
+void buildTopology(DeviceMesh& mesh, Context& ctx, int N, int F, int n_patches, const int* owner, const int* nbr,
+                   const int* patch) {
+    if (N <= 0 || F <= 0) fail(kArgument, "mesh has no cells or faces");
+    DeviceMesh* m = &mesh;
     m->ctx = &ctx;
-    const int N = g.n_cells, F = g.n_faces;
     m->n_cells = N;
     m->n_faces = F;
-    m->n_patches = g.n_patches;
-    m->orthogonal = g.orthogonal;
+    m->n_patches = n_patches;
+    // interior and boundary faces, each stably ordered by owner (a counting sort)
+    std::vector<int> count_i(N + 1, 0), count_b(N + 1, 0);
     for (int f = 0; f < F; ++f) {
-        if (g.owner[f] < 0 || g.owner[f] >= N || g.nbr[f] >= N || g.nbr[f] < -1)
+        if (owner[f] < 0 || owner[f] >= N || nbr[f] >= N || nbr[f] < -1)
             fail(kArgument, "face owner/neighbour out of range");
-        if (g.nbr[f] < 0 && (g.patch[f] < 0 || g.patch[f] >= g.n_patches))
+        if (nbr[f] < 0 && (patch[f] < 0 || patch[f] >= n_patches))
             fail(kArgument, "boundary face has an invalid patch");
-        if (g.nbr[f] >= 0) m->interior_ext.push_back(f);
-        else m->boundary_ext.push_back(f);
+        ++(nbr[f] >= 0 ? count_i : count_b)[owner[f] + 1];
     }
-    auto byOwner = [&](int a, int b) { return g.owner[a] < g.owner[b]; };
-    std::stable_sort(m->interior_ext.begin(), m->interior_ext.end(), byOwner);
-    std::stable_sort(m->boundary_ext.begin(), m->boundary_ext.end(), byOwner);
-    const int Fi = static_cast<int>(m->interior_ext.size()), Fb = static_cast<int>(m->boundary_ext.size());
+    for (int c = 0; c < N; ++c) { count_i[c + 1] += count_i[c]; count_b[c + 1] += count_b[c]; }
+    const int Fi = count_i[N], Fb = count_b[N];
+    m->interior_ext.assign(Fi, 0);
+    m->boundary_ext.assign(Fb, 0);
+    for (int f = 0; f < F; ++f) {
+        if (nbr[f] >= 0) m->interior_ext[count_i[owner[f]]++] = f;
+        else m->boundary_ext[count_b[owner[f]]++] = f;
+    }
     m->n_interior = Fi;
     m->n_boundary = Fb;
     m->face_kind.assign(F, 0);
     m->face_slot.assign(F, 0);
     for (int i = 0; i < Fi; ++i) { m->face_kind[m->interior_ext[i]] = 0; m->face_slot[m->interior_ext[i]] = i; }
     for (int i = 0; i < Fb; ++i) { m->face_kind[m->boundary_ext[i]] = 1; m->face_slot[m->boundary_ext[i]] = i; }
+    cudaStream_t s = ctx.stream;
     {
         // caller face -> internal face position (interior first), for device-side reordering
         std::vector<int> perm(F);
         for (int f = 0; f < F; ++f) perm[f] = m->face_kind[f] == 0 ? m->face_slot[f] : Fi + m->face_slot[f];
-        m->face_perm.upload(perm, ctx.stream);
+        m->face_perm.upload(perm, s);
     }
-
-    auto gather1 = [](const std::vector<double>& a, const std::vector<int>& idx) {
-        std::vector<double> o(idx.size());
-        for (std::size_t i = 0; i < idx.size(); ++i) o[i] = a[idx[i]];
-        return o;
-    };
-    auto gather3 = [](const std::vector<double>& a, const std::vector<int>& idx) {
-        std::vector<double> o(3 * idx.size());
-        for (std::size_t i = 0; i < idx.size(); ++i)
-            for (int c = 0; c < 3; ++c) o[3 * i + c] = a[3 * idx[i] + c];
-        return o;
-    };
-    cudaStream_t s = ctx.stream;
-    // interior faces
     m->h_own.resize(Fi);
     m->h_nbr.resize(Fi);
-    for (int i = 0; i < Fi; ++i) { m->h_own[i] = g.owner[m->interior_ext[i]]; m->h_nbr[i] = g.nbr[m->interior_ext[i]]; }
-    m->h_dcoef = gather1(g.dcoef, m->interior_ext);
+    for (int i = 0; i < Fi; ++i) { m->h_own[i] = owner[m->interior_ext[i]]; m->h_nbr[i] = nbr[m->interior_ext[i]]; }
     m->own.upload(m->h_own, s);
     m->nbr.upload(m->h_nbr, s);
-    m->w.upload(gather1(g.weight, m->interior_ext), s);
-    m->dcoef.upload(m->h_dcoef, s);
-    m->area.upload(gather1(g.area, m->interior_ext), s);
-    m->Sf.upload(gather3(g.Sf, m->interior_ext), s);
-    m->xf.upload(gather3(g.xf, m->interior_ext), s);
-    m->kvec.upload(gather3(g.kvec, m->interior_ext), s);
-    m->skew.upload(gather3(g.skew, m->interior_ext), s);
-    // boundary faces
     m->h_bown.resize(Fb);
     std::vector<int> bpatch(Fb);
-    std::vector<double> bdist(Fb);
     for (int i = 0; i < Fb; ++i) {
-        const int f = m->boundary_ext[i], o = g.owner[f];
-        m->h_bown[i] = o;
-        bpatch[i] = g.patch[f];
-        double d = 0.0;
-        for (int c = 0; c < 3; ++c) d += (g.xf[3 * f + c] - g.xc[3 * o + c]) * g.normal[3 * f + c];
-        bdist[i] = d;
+        m->h_bown[i] = owner[m->boundary_ext[i]];
+        bpatch[i] = patch[m->boundary_ext[i]];
     }
     m->bown.upload(m->h_bown, s);
     m->bpatch.upload(bpatch, s);
-    m->bdcoef.upload(gather1(g.dcoef, m->boundary_ext), s);
-    m->barea.upload(gather1(g.area, m->boundary_ext), s);
-    m->bdist.upload(bdist, s);
-    m->bSf.upload(gather3(g.Sf, m->boundary_ext), s);
-    m->bxf.upload(gather3(g.xf, m->boundary_ext), s);
-    m->bn.upload(gather3(g.normal, m->boundary_ext), s);
-    m->bk.upload(gather3(g.kvec, m->boundary_ext), s);
-    // cells
-    std::vector<double> rV(N);
-    for (int c = 0; c < N; ++c) rV[c] = 1.0 / g.V[c];
-    m->V.upload(g.V, s);
-    m->rV.upload(rV, s);
-    m->xc.upload(g.xc, s);
     // cell -> interior face CSR, faces of a row in increasing internal face order
     m->h_cf_ptr.assign(N + 1, 0);
     for (int i = 0; i < Fi; ++i) { ++m->h_cf_ptr[m->h_own[i] + 1]; ++m->h_cf_ptr[m->h_nbr[i] + 1]; }
@@ -416,8 +389,60 @@ std::unique_ptr<DeviceMesh> buildDeviceMesh(Context& ctx, const HostGeometry& g)
     for (int i = 0; i < Fb; ++i) ++m->h_cb_ptr[m->h_bown[i] + 1];
     for (int c = 0; c < N; ++c) m->h_cb_ptr[c + 1] += m->h_cb_ptr[c];
     m->cb_ptr.upload(m->h_cb_ptr, s);
+    m->ext_owner.assign(owner, owner + F);
+    m->ext_nbr.assign(nbr, nbr + F);
+    m->ext_patch.assign(patch, patch + F);
+}
+
+std::unique_ptr<DeviceMesh> buildDeviceMesh(Context& ctx, const HostGeometry& g) {
+    if (g.n_cells <= 0 || g.n_faces <= 0) fail(kArgument, "mesh has no cells or faces");
+    auto m = std::make_unique<DeviceMesh>();
+    const int N = g.n_cells;
+    buildTopology(*m, ctx, N, g.n_faces, g.n_patches, g.owner.data(), g.nbr.data(), g.patch.data());
+    m->orthogonal = g.orthogonal;
+    auto gather1 = [](const std::vector<double>& a, const std::vector<int>& idx) {
+        std::vector<double> o(idx.size());
+        for (std::size_t i = 0; i < idx.size(); ++i) o[i] = a[idx[i]];
+        return o;
+    };
+    auto gather3 = [](const std::vector<double>& a, const std::vector<int>& idx) {
+        std::vector<double> o(3 * idx.size());
+        for (std::size_t i = 0; i < idx.size(); ++i)
+            for (int c = 0; c < 3; ++c) o[3 * i + c] = a[3 * idx[i] + c];
+        return o;
+    };
+    cudaStream_t s = ctx.stream;
+    const int Fb = m->n_boundary;
+    // interior faces
+    m->w.upload(gather1(g.weight, m->interior_ext), s);
+    m->dcoef.upload(gather1(g.dcoef, m->interior_ext), s);
+    m->area.upload(gather1(g.area, m->interior_ext), s);
+    m->Sf.upload(gather3(g.Sf, m->interior_ext), s);
+    m->xf.upload(gather3(g.xf, m->interior_ext), s);
+    m->kvec.upload(gather3(g.kvec, m->interior_ext), s);
+    m->skew.upload(gather3(g.skew, m->interior_ext), s);
+    // boundary faces
+    std::vector<double> bdist(Fb);
+    for (int i = 0; i < Fb; ++i) {
+        const int f = m->boundary_ext[i], o = g.owner[f];
+        double d = 0.0;
+        for (int c = 0; c < 3; ++c) d += (g.xf[3 * f + c] - g.xc[3 * o + c]) * g.normal[3 * f + c];
+        bdist[i] = d;
+    }
+    m->bdcoef.upload(gather1(g.dcoef, m->boundary_ext), s);
+    m->barea.upload(gather1(g.area, m->boundary_ext), s);
+    m->bdist.upload(bdist, s);
+    m->bSf.upload(gather3(g.Sf, m->boundary_ext), s);
+    m->bxf.upload(gather3(g.xf, m->boundary_ext), s);
+    m->bn.upload(gather3(g.normal, m->boundary_ext), s);
+    m->bk.upload(gather3(g.kvec, m->boundary_ext), s);
+    // cells
+    std::vector<double> rV(N);
+    for (int c = 0; c < N; ++c) rV[c] = 1.0 / g.V[c];
+    m->V.upload(g.V, s);
+    m->rV.upload(rV, s);
+    m->xc.upload(g.xc, s);
     // caller-numbered geometry for exports
-    m->ext_owner = g.owner; m->ext_nbr = g.nbr; m->ext_patch = g.patch;
     m->ext_Sf = g.Sf; m->ext_xf = g.xf; m->ext_area = g.area; m->ext_n = g.normal; m->ext_w = g.weight;
     m->ext_dcoef = g.dcoef; m->ext_k = g.kvec; m->ext_skew = g.skew; m->ext_xc = g.xc; m->ext_V = g.V;
     ctx.sync();

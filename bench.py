@@ -460,7 +460,15 @@ def main():
     poly = mesh_for(n_side)
     t_mesh = time.time() - t0
     ctx = bsg.Context(local)
+    # Mesh ingest (Mesh::polyhedral): geometry on the device, and at N=1 the host geometry beside it.
+    t0 = time.perf_counter()
     mesh = bsg.Mesh.from_polyhedral(ctx, poly)
+    ingest = {"device_geometry_s": round(time.perf_counter() - t0, 3)}
+    if world == 1:
+        t0 = time.perf_counter()
+        host_mesh = bsg.Mesh.from_polyhedral(ctx, poly, host_geometry=True)
+        ingest["host_geometry_s"] = round(time.perf_counter() - t0, 3)
+        host_mesh.close()
     N, F, Fi = mesh.n_cells, mesh.n_faces, mesh.n_interior
     s = case_settings()
     sim = build_simple(bsg, mesh, s)
@@ -582,7 +590,7 @@ def main():
                            "l2": "working set >> 126 MB L2, no flush", "parallelism": f"replicas x{world}",
                            "mesh_seconds": round(t_mesh, 1)},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "mixed_precision": mixed,
-                "gpu_launches": launches,
+                "gpu_launches": launches, "mesh_ingest": ingest,
                 "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
                 "pressure_iterations_per_solve": round(prof["pcg_amg_persistent"][3] / prof["pcg_amg_persistent"][0], 1)
                 if "pcg_amg_persistent" in prof else None,

@@ -166,13 +166,21 @@ int bsg_context_event_elapsed(bsg_context* ctx, int32_t start_slot, int32_t stop
  * for a reference Mesh: pass its MeshStorage arrays).
  * bsg_mesh_create_polyhedral computes the geometry itself from a polyhedral
  * description (Mesh::polyhedral, src/core/mesh.cpp:321-564; the
- * BABELSIM_MESH 3 face list, src/io/mesh_reader.cpp:44-111). */
+ * BABELSIM_MESH 3 face list, src/io/mesh_reader.cpp:44-111) on the device,
+ * bit-identical to the host computation; bsg_mesh_create_polyhedral_host
+ * computes the same geometry on the host and uploads it.  Both reject the
+ * meshes Mesh::polyhedral rejects, with the same message. */
 int bsg_mesh_create(bsg_context* ctx, const bsg_mesh_geometry* geometry, bsg_mesh** out);
 int bsg_mesh_create_polyhedral(bsg_context* ctx, int32_t n_vertices, const double* vertices,
                                int32_t n_faces, const int32_t* face_point_offsets,
                                const int32_t* face_point_ids, const int32_t* owner,
                                const int32_t* neighbour, const int32_t* patch, int32_t n_patches,
                                bsg_mesh** out);
+int bsg_mesh_create_polyhedral_host(bsg_context* ctx, int32_t n_vertices, const double* vertices,
+                                    int32_t n_faces, const int32_t* face_point_offsets,
+                                    const int32_t* face_point_ids, const int32_t* owner,
+                                    const int32_t* neighbour, const int32_t* patch, int32_t n_patches,
+                                    bsg_mesh** out);
 int bsg_mesh_destroy(bsg_mesh* mesh);
 /* Host-only check of a polyhedral description: computes the geometry exactly as
  * bsg_mesh_create_polyhedral does (no device needed) and reports the first
