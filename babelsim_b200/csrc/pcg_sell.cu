@@ -11,7 +11,10 @@ namespace cg = cooperative_groups;
 namespace bsg {
 namespace {
 
-constexpr int SB = 256;  // threads per block
+#ifndef BSG_SELL_SB
+#define BSG_SELL_SB 256
+#endif
+constexpr int SB = BSG_SELL_SB;  // threads per block
 // Minimum resident blocks per SM the register budget must allow: 3 (80 registers)
 // measured faster than 4 (64) on the 1M-cell pressure solves, 2 (128) slower.
 #ifndef BSG_SELL_MIN_BLOCKS
@@ -117,6 +120,23 @@ __device__ __forceinline__ double emitRow(const VCycleView<TV>& V, const VLevel<
 
 // z = M r with M the V-cycle; returns this thread's share of r.z.  Level 0's b
 // and w were written by the phase that produced r.
+// Lanes per row on a level: the largest power of two (at most 32) that still
+// gives every (slice, lane-group) unit its own warp; 1 on the fine levels.
+__device__ __forceinline__ int splitOf(int nslices, int nwarps) {
+    int K = 1;
+    while (K < 32 && static_cast<long long>(nslices) * K * 2 <= nwarps) K *= 2;
+    return K;
+}
+
+// Unit u of a split sweep: slice s, the row r within it and this lane's part q.
+struct SplitUnit {
+    int s, r, q;
+};
+__device__ __forceinline__ SplitUnit splitUnit(int u, int K, int lane) {
+    const int rows = 32 / K;
+    return {u / K, (u % K) * rows + lane / K, lane % K};
+}
+
 template <class TK, class TV>
 __device__ double vcycle(cg::grid_group& g, const VCycleView<TV>& V, const TK* r, TK* z, const PhaseLog& log) {
     const Lanes c = lanes();
@@ -138,10 +158,20 @@ __device__ double vcycle(cg::grid_group& g, const VCycleView<TV>& V, const TK* r
             mark(log, 10 + l);
         }
         const TV* xs = V.nu >= 2 ? f.x : f.w;
-        for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
-            const int i = 32 * s + c.lane;
-            const TV ax = sellRow(f.A, s, c.lane, [&](int j) { return xs[j]; });
-            if (i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
+        const int K = splitOf(f.A.nslices, c.nwarps);
+        if (K == 1) {
+            for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+                const int i = 32 * s + c.lane;
+                const TV ax = sellRow(f.A, s, c.lane, [&](int j) { return xs[j]; });
+                if (i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
+            }
+        } else {
+            for (int u = c.gwarp; u < f.A.nslices * K; u += c.nwarps) {
+                const SplitUnit su = splitUnit(u, K, c.lane);
+                const int i = 32 * su.s + su.r;
+                const TV ax = sellRowSplit(f.A, su.s, su.r, su.q, K, [&](int j) { return xs[j]; });
+                if (su.q == 0 && i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
+            }
         }
         g.sync();
         mark(log, 30 + l);
@@ -190,14 +220,33 @@ __device__ double vcycle(cg::grid_group& g, const VCycleView<TV>& V, const TK* r
         const VLevel<TV> fin = l > 0 ? V.lv[l - 1] : f;
         const bool single = V.nu < 2;
         const TV* y = f.x;
-        for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
-            const int i = 32 * s + c.lane;
-            const TV ay = sellRow(f.A, s, c.lane, [&](int j) { return y[j]; });
-            if (i < f.A.n) {
-                const TV yi = y[i];
-                const TV v = yi + f.rd[i] * (f.b[i] - (f.A.diag[i] * yi + ay));
-                if (single) rz += emitRow<TK, TV>(V, fin, l, i, v, r, z);
-                else f.t[i] = v;
+        const int K = single && l > 0 ? splitOf(f.A.nslices, c.nwarps) : 1;
+        if (K == 1) {
+            for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+                const int i = 32 * s + c.lane;
+                const TV ay = sellRow(f.A, s, c.lane, [&](int j) { return y[j]; });
+                if (i < f.A.n) {
+                    const TV yi = y[i];
+                    const TV v = yi + f.rd[i] * (f.b[i] - (f.A.diag[i] * yi + ay));
+                    if (single) rz += emitRow<TK, TV>(V, fin, l, i, v, r, z);
+                    else f.t[i] = v;
+                }
+            }
+        } else {
+            // coarse level, one smoothing step: the K lanes of a row share its push into the finer level
+            const TV* from = fin.w;
+            for (int u = c.gwarp; u < f.A.nslices * K; u += c.nwarps) {
+                const SplitUnit su = splitUnit(u, K, c.lane);
+                const int i = 32 * su.s + su.r;
+                const TV ay = sellRowSplit(f.A, su.s, su.r, su.q, K, [&](int j) { return y[j]; });
+                if (i < f.A.n) {
+                    const TV yi = y[i];
+                    const TV add = V.gamma * (yi + f.rd[i] * (f.b[i] - (f.A.diag[i] * yi + ay)));
+                    for (int m = fin.agg_ptr[i] + su.q; m < fin.agg_ptr[i + 1]; m += K) {
+                        const int ii = fin.agg_rows[m];
+                        fin.x[ii] = from[ii] + add;
+                    }
+                }
             }
         }
         if (!single) {

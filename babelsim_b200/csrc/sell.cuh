@@ -99,6 +99,33 @@ __device__ __forceinline__ T sellRow(const SellMat<T>& A, int s, int lane, Y y) 
     return a0 + a1;
 }
 
+// The same row sum split over K consecutive lanes (K a power of two, 2..32): lane q
+// of the group takes entries q, q + K, ... of row r of slice s, and the group's
+// partial sums are combined in a fixed butterfly order, so every lane of the
+// group returns the same, deterministic total.  For levels whose slices leave
+// warps idle: the dependent index -> gather chain of a wide row gets K times
+// shorter.  Every lane of the warp must call it (the butterfly uses the full mask).
+template <class T, class Y>
+__device__ __forceinline__ T sellRowSplit(const SellMat<T>& A, int s, int r, int q, int K, Y y) {
+    const int beg = A.sptr[s];
+    const int w = (A.sptr[s + 1] - beg) >> 5;
+    const int* __restrict__ c = A.col + beg + r;
+    const T* __restrict__ v = A.val + beg + r;
+    T a0 = T(0), a1 = T(0);
+    int k = q;
+    for (; k + K < w; k += 2 * K) {
+        const int c0 = __ldg(c + 32 * k), c1 = __ldg(c + 32 * (k + K));
+        const T v0 = __ldg(v + 32 * k), v1 = __ldg(v + 32 * (k + K));
+        const T y0 = y(c0), y1 = y(c1);
+        a0 += v0 * y0;
+        a1 += v1 * y1;
+    }
+    if (k < w) a0 += __ldg(v + 32 * k) * y(__ldg(c + 32 * k));
+    T a = a0 + a1;
+    for (int o = K >> 1; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    return a;
+}
+
 // Values of a CSR matrix (FP64) scattered into SELL positions, converted to T;
 // diag and omega/diag converted alongside.  Padding entries are never written.
 template <class T>
