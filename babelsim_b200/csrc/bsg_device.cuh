@@ -16,6 +16,7 @@ struct MeshView {
     const int *bown, *bpatch;
     const double *bdcoef, *barea, *bdist, *bSf, *bxf, *bn, *bk;
     const int *cf_ptr, *cf_face, *cf_col, *cb_ptr;
+    const int *slot_own, *slot_nbr;  // the owner-row and neighbour-row matrix slots of each interior face
 };
 
 inline MeshView view(const DeviceMesh& m) {
@@ -24,7 +25,7 @@ inline MeshView view(const DeviceMesh& m) {
                     m.xf.data(), m.kvec.data(), m.skew.data(), m.bown.data(), m.bpatch.data(),
                     m.bdcoef.data(), m.barea.data(), m.bdist.data(), m.bSf.data(), m.bxf.data(),
                     m.bn.data(), m.bk.data(), m.cf_ptr.data(), m.cf_face.data(), m.cf_col.data(),
-                    m.cb_ptr.data()};
+                    m.cb_ptr.data(), m.slot_own.data(), m.slot_nbr.data()};
 }
 
 // Boundary constraints of one cell field.  A calculated field has `trace`

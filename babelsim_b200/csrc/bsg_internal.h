@@ -182,6 +182,8 @@ struct DeviceMesh {
     DeviceArray<int> slot_own, slot_nbr;
     // scratch for the first Green-Gauss pass (3*9*n_cells doubles at most)
     DeviceArray<double> ws_grad_pass1;
+    // per-slot records of the face pass of diffusion assembly ((1 + C) * 2 n_interior doubles)
+    DeviceArray<double> ws_slots;
     // external geometry copy for bsg_mesh_export (host; filled on first export when the
     // geometry was computed on the device)
     std::vector<double> ext_Sf, ext_xf, ext_area, ext_n, ext_w, ext_dcoef, ext_k, ext_skew, ext_xc, ext_V;

@@ -363,37 +363,67 @@ __global__ void kAddConvection(MeshView m, BcView b, const double* __restrict__ 
 // addScalarDiffusion / addVectorDiffusion (operators.cpp:1287-1438) as a row
 // gather, every contribution multiplied by `mult` (accumulate(..., -factor),
 // procedural_equation.cpp:62-70).  kf == nullptr means the constant kc.
+// Interior faces of a diffusion term, once per face: the coefficient gamma*dcoef
+// off both matrix slots, and per slot the record {coefficient, +-gamma*(corrected -
+// orthogonal normal gradient)} (sign + on the owner's slot) that the cell pass sums
+// (addScalarDiffusion / addVectorDiffusion, operators.cpp:1287-1438, with
+// integratedNormalGradient 857-954 and limitNonOrthogonalCorrection 499-513).
+template <int C>
+__global__ void kDiffusionFaces(MeshView m, const double* __restrict__ x, const double* __restrict__ g,
+                                const double* __restrict__ kf, double kc, int method, double mult,
+                                double* __restrict__ val, double* __restrict__ slots) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.n_interior) return;
+    const int so = m.slot_own[f], sn = m.slot_nbr[f];
+    double* ro = slots + static_cast<long long>(1 + C) * so;
+    double* rn = slots + static_cast<long long>(1 + C) * sn;
+    const double gam = kf ? kf[f] : kc;
+    if (gam == 0.0) {
+#pragma unroll
+        for (int c = 0; c <= C; ++c) { ro[c] = 0.0; rn[c] = 0.0; }
+        return;
+    }
+    const double coef = gam * m.dcoef[f];
+    val[so] -= mult * coef;
+    val[sn] -= mult * coef;
+    ro[0] = coef;
+    rn[0] = coef;
+    if (method == 0) return;
+    const int o = m.own[f], n = m.nbr[f];
+    const double w = m.w[f];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const double orth = m.dcoef[f] * (x[C * n + c] - x[C * o + c]);
+        const double* go = g + 3 * (C * o + c);
+        const double* gn = g + 3 * (C * n + c);
+        const double corr = m.kvec[3 * f] * (w * go[0] + (1.0 - w) * gn[0]) +
+                            m.kvec[3 * f + 1] * (w * go[1] + (1.0 - w) * gn[1]) +
+                            m.kvec[3 * f + 2] * (w * go[2] + (1.0 - w) * gn[2]);
+        const double ing = orth + limitCorrection(orth, corr, method);
+        const double v = gam * (ing - orth);
+        ro[1 + c] = v;
+        rn[1 + c] = -v;
+    }
+}
+
+// Cell pass of a diffusion term: the slot records of the cell's interior faces
+// (in slot order) and its boundary faces, into diag and the explicit source.
 template <int C>
 __global__ void kAddDiffusion(MeshView m, BcView b, const double* __restrict__ x, const double* __restrict__ g,
                               const double* __restrict__ kf, double kc, int method, double mult,
-                              double* __restrict__ diag, double* __restrict__ val, double* __restrict__ src) {
+                              const double* __restrict__ slots, double* __restrict__ diag,
+                              double* __restrict__ src) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.n_cells) return;
     double d = 0.0, s[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) s[c] = 0.0;
     for (int k = m.cf_ptr[i]; k < m.cf_ptr[i + 1]; ++k) {
-        const int f = m.cf_face[k];
-        const double gam = kf ? kf[f] : kc;
-        if (gam == 0.0) continue;
-        const int o = m.own[f], n = m.nbr[f];
-        const double coef = gam * m.dcoef[f];
-        d += coef;
-        val[k] -= mult * coef;
+        const double* r = slots + static_cast<long long>(1 + C) * k;
+        d += r[0];
         if (method != 0) {
-            const double w = m.w[f];
-            const double sgn = o == i ? 1.0 : -1.0;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const double orth = m.dcoef[f] * (x[C * n + c] - x[C * o + c]);
-                const double* go = g + 3 * (C * o + c);
-                const double* gn = g + 3 * (C * n + c);
-                const double corr = m.kvec[3 * f] * (w * go[0] + (1.0 - w) * gn[0]) +
-                                    m.kvec[3 * f + 1] * (w * go[1] + (1.0 - w) * gn[1]) +
-                                    m.kvec[3 * f + 2] * (w * go[2] + (1.0 - w) * gn[2]);
-                const double ing = orth + limitCorrection(orth, corr, method);
-                s[c] += sgn * (gam * (ing - orth));
-            }
+            for (int c = 0; c < C; ++c) s[c] += r[1 + c];
         }
     }
     for (int fb = m.cb_ptr[i]; fb < m.cb_ptr[i + 1]; ++fb) {
@@ -536,6 +566,11 @@ __global__ void kReaction(int n, const double* __restrict__ V, const double* __r
 }
 
 // flag[0] = 1 when any value is not positive and finite (flag[1]: any non-finite).
+__global__ void kFill(int n, double v, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = v;
+}
+
 __global__ void kCheckValues(int n, const double* __restrict__ a, int* __restrict__ flag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -978,18 +1013,26 @@ void addLaplacian(DeviceEquation& eq, DeviceField* coef, double k, double factor
         }
     } else {
         if (k < 0.0) fail(kArgument, "diffusivity must be non-negative and finite");
-        std::vector<double> h(m.n_faces, k);
-        snap->kf.upload(h, ctx.stream);
+        snap->kf.resize(m.n_faces);
+        launch(ctx, kFill, m.n_faces, m.n_faces, k, snap->kf.data());
     }
     const double* g = o.diffusion != 0 ? eq.unknownGradient(o.gradient) : nullptr;
     const BcView b = x.bcView();
     const double mult = -factor;
-    if (x.comps == 1)
-        launch(ctx, kAddDiffusion<1>, m.n_cells, view(m), b, (const double*)x.v.data(), g,
-               (const double*)snap->kf.data(), 0.0, o.diffusion, mult, eq.diag.data(), eq.val.data(), eq.src.data());
-    else
-        launch(ctx, kAddDiffusion<3>, m.n_cells, view(m), b, (const double*)x.v.data(), g,
-               (const double*)snap->kf.data(), 0.0, o.diffusion, mult, eq.diag.data(), eq.val.data(), eq.src.data());
+    const std::size_t slot_doubles = static_cast<std::size_t>(1 + x.comps) * 2 * m.n_interior;
+    if (m.ws_slots.size() < slot_doubles) m.ws_slots.resize(slot_doubles);
+    const double* kfd = snap->kf.data();
+    if (x.comps == 1) {
+        launch(ctx, kDiffusionFaces<1>, m.n_interior, view(m), (const double*)x.v.data(), g, kfd, 0.0, o.diffusion,
+               mult, eq.val.data(), m.ws_slots.data());
+        launch(ctx, kAddDiffusion<1>, m.n_cells, view(m), b, (const double*)x.v.data(), g, kfd, 0.0, o.diffusion,
+               mult, (const double*)m.ws_slots.data(), eq.diag.data(), eq.src.data());
+    } else {
+        launch(ctx, kDiffusionFaces<3>, m.n_interior, view(m), (const double*)x.v.data(), g, kfd, 0.0, o.diffusion,
+               mult, eq.val.data(), m.ws_slots.data());
+        launch(ctx, kAddDiffusion<3>, m.n_cells, view(m), b, (const double*)x.v.data(), g, kfd, 0.0, o.diffusion,
+               mult, (const double*)m.ws_slots.data(), eq.diag.data(), eq.src.data());
+    }
     if (x.comps == 1) {
         snap->correction.resize(m.n_faces);
         if (o.diffusion != 0)
