@@ -4,6 +4,8 @@
 #include "bsg_device.cuh"
 #include "pcg_sell.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -176,6 +178,69 @@ __global__ void kDenseInverse(int n, const int* __restrict__ ptr, const int* __r
     }
 }
 
+// The same in-place Gauss-Jordan inverse on a cluster of kDenseCluster CTAs that
+// keeps the matrix in distributed shared memory: CTA q owns rows [q*rows, (q+1)*rows).
+// Step k: every CTA holds pivot row k in its own buffer pk[k & 1] (pushed there by
+// the row's owner during step k - 1), saves its rows' column k, updates its rows
+// exactly as kDenseInverse does, and the owner of row k + 1 pushes that row's new
+// values into every CTA's other buffer; one cluster barrier ends the step.  The
+// barrier orders the pushes of step k before their reads in step k + 1, and the
+// reads of a buffer in step k - 1 before its overwrite in step k.
+constexpr int kDenseCluster = 8;
+
+__global__ void __cluster_dims__(kDenseCluster, 1, 1)
+    kDenseInverseCluster(int n, int rows, const int* __restrict__ ptr, const int* __restrict__ col,
+                         const double* __restrict__ diag, const double* __restrict__ val, double* __restrict__ M) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ double sh[];
+    double* Ml = sh;                                   // rows x n, this CTA's rows
+    double* pk = sh + static_cast<long long>(rows) * n;  // two pivot-row buffers of n
+    double* pc = pk + 2 * n;                           // column k of this CTA's rows
+    const int q = static_cast<int>(cluster.block_rank());
+    const int r0 = q * rows, r1 = min(n, r0 + rows), nr = max(0, r1 - r0);
+    for (int e = threadIdx.x; e < nr * n; e += blockDim.x) Ml[e] = 0.0;
+    __syncthreads();
+    for (int li = threadIdx.x; li < nr; li += blockDim.x) {
+        const int i = r0 + li;
+        Ml[static_cast<long long>(li) * n + i] = diag[i];
+        for (int k = ptr[i]; k < ptr[i + 1]; ++k) Ml[static_cast<long long>(li) * n + col[k]] += val[k];
+    }
+    __syncthreads();
+    // row 0 into every CTA's buffer 0
+    if (q == 0)
+        for (int e = threadIdx.x; e < kDenseCluster * n; e += blockDim.x) {
+            double* dst = cluster.map_shared_rank(pk, e / n);
+            dst[e % n] = Ml[e % n];
+        }
+    cluster.sync();
+    for (int k = 0; k < n; ++k) {
+        const double* prow = pk + (k & 1) * n;
+        const double p = 1.0 / prow[k];
+        for (int li = threadIdx.x; li < nr; li += blockDim.x) pc[li] = Ml[static_cast<long long>(li) * n + k];
+        __syncthreads();
+        for (int e = threadIdx.x; e < nr * n; e += blockDim.x) {
+            const int li = e / n, j = e - li * n, i = r0 + li;
+            double v;
+            if (i == k) v = j == k ? p : prow[j] * p;
+            else if (j == k) v = -pc[li] * p;
+            else v = Ml[e] - pc[li] * prow[j] * p;
+            Ml[e] = v;
+        }
+        __syncthreads();
+        const int next = k + 1;
+        if (next < n && next >= r0 && next < r1) {
+            const double* src = Ml + static_cast<long long>(next - r0) * n;
+            for (int e = threadIdx.x; e < kDenseCluster * n; e += blockDim.x) {
+                double* dst = cluster.map_shared_rank(pk + (next & 1) * n, e / n);
+                dst[e % n] = src[e % n];
+            }
+        }
+        cluster.sync();
+    }
+    for (int e = threadIdx.x; e < nr * n; e += blockDim.x) M[static_cast<long long>(r0) * n + e] = Ml[e];
+}
+
 __global__ void kDenseSolve(int n, const double* __restrict__ Minv, const double* __restrict__ b, double* __restrict__ x) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = 0.0;
@@ -250,6 +315,23 @@ __global__ void kCopy(int n, const double* __restrict__ a, double* __restrict__ 
     if (i < n) b[i] = a[i];
 }
 
+}  // namespace
+
+namespace {
+// Dynamic shared memory of one CTA of the cluster inverse (the rest of the SM's
+// 228 KB stays for the driver's reserve).
+constexpr std::size_t kDenseClusterSmem = 200 * 1024;
+
+bool clusterReady() {
+    static int ok = -1;
+    if (ok < 0) {
+        ok = cudaFuncSetAttribute(kDenseInverseCluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kDenseClusterSmem)) == cudaSuccess;
+        if (ok && std::getenv("BSG_DENSE_SINGLE_BLOCK")) ok = 0;
+        cudaGetLastError();
+    }
+    return ok == 1;
+}
 }  // namespace
 
 AmgPreconditioner::AmgPreconditioner(DeviceMesh& mesh, const SolverConfig& cfg)
@@ -435,6 +517,12 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
         ctx_.launched();
     }
     Level* last = levels_.back();
+    const int crow = (last->n + kDenseCluster - 1) / kDenseCluster;
+    const std::size_t csmem = sizeof(double) * (static_cast<std::size_t>(crow) * last->n + 2 * last->n + crow);
+    if (csmem <= kDenseClusterSmem && clusterReady()) {
+        kDenseInverseCluster<<<kDenseCluster, 512, csmem, ctx_.stream>>>(last->n, crow, last->dptr, last->dcol,
+                                                                         last->ddiag, last->dval, last->dense.data());
+    } else
     kDenseInverse<<<1, 1024, 2 * sizeof(double) * last->n, ctx_.stream>>>(last->n, last->dptr, last->dcol, last->ddiag,
                                                                          last->dval, last->dense.data());
     ctx_.launched();
