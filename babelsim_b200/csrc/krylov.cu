@@ -8,6 +8,7 @@
 // iterations issued after convergence return immediately.
 #include "amg.h"
 #include "pcg_sell.cuh"
+#include "sell.cuh"
 #include "bsg_device.cuh"
 #include "linalg.h"
 
@@ -347,6 +348,92 @@ __global__ void kBiSpmvT(Dcsr<double> A, const double* __restrict__ sh, double* 
     }
     writePartial<2 * C>(acc2, partial);
 }
+// The two BiCGStab products on the SELL-32 copy of the matrix (one warp per slice
+// of 32 rows, one lane per row, column indices and values read as contiguous
+// warp-wide transactions, four entries in flight per lane): kBiSpmvV's and
+// kBiSpmvT's results and partial sums.
+template <int C>
+__device__ __forceinline__ void sellRowC(const SellMat<double>& S, int sl, int lane, const double* __restrict__ x,
+                                         double acc[C]) {
+    const int beg = S.sptr[sl], w = (S.sptr[sl + 1] - beg) >> 5;
+    const int* __restrict__ cp = S.col + beg + lane;
+    const double* __restrict__ vp = S.val + beg + lane;
+    double a[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) a[c] = 0.0;
+    int k = 0;
+    for (; k + 4 <= w; k += 4) {
+        int cc[4];
+        double vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            cc[u] = __ldg(cp + 32 * (k + u));
+            vv[u] = __ldg(vp + 32 * (k + u));
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int c = 0; c < C; ++c) a[c] += vv[u] * x[C * cc[u] + c];
+    }
+    for (; k < w; ++k) {
+        const int j = __ldg(cp + 32 * k);
+        const double v = __ldg(vp + 32 * k);
+#pragma unroll
+        for (int c = 0; c < C; ++c) a[c] += v * x[C * j + c];
+    }
+    const int i = 32 * sl + lane;
+    const double d = i < S.n ? S.diag[i] : 0.0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = (i < S.n ? d * x[C * i + c] : 0.0) + a[c];
+}
+
+template <int C>
+__global__ void kBiSpmvVSell(SellMat<double> S, const double* __restrict__ ph, double* __restrict__ v,
+                             const double* __restrict__ r0, double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double acc2[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc2[c] = 0.0;
+    const int lane = threadIdx.x & 31, nw = gridDim.x * (kBlock / 32);
+    for (int sl = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); sl < S.nslices; sl += nw) {
+        double acc[C];
+        sellRowC<C>(S, sl, lane, ph, acc);
+        const int i = 32 * sl + lane;
+        if (i < S.n) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                v[C * i + c] = acc[c];
+                acc2[c] += r0[C * i + c] * acc[c];
+            }
+        }
+    }
+    writePartial<C>(acc2, partial);
+}
+
+template <int C>
+__global__ void kBiSpmvTSell(SellMat<double> S, const double* __restrict__ sh, double* __restrict__ t,
+                             const double* __restrict__ sv, double* __restrict__ partial, const Scalars* s) {
+    if (allDone(s)) return;
+    double acc2[2 * C];
+#pragma unroll
+    for (int c = 0; c < 2 * C; ++c) acc2[c] = 0.0;
+    const int lane = threadIdx.x & 31, nw = gridDim.x * (kBlock / 32);
+    for (int sl = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5); sl < S.nslices; sl += nw) {
+        double acc[C];
+        sellRowC<C>(S, sl, lane, sh, acc);
+        const int i = 32 * sl + lane;
+        if (i < S.n) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                t[C * i + c] = acc[c];
+                acc2[2 * c] += acc[c] * acc[c];
+                acc2[2 * c + 1] += acc[c] * sv[C * i + c];
+            }
+        }
+    }
+    writePartial<2 * C>(acc2, partial);
+}
+
 template <int C>
 __global__ void kBiOmega(int blocks, const double* __restrict__ partial, Scalars* s) {
     if (allDone(s)) return;
@@ -478,7 +565,46 @@ struct KrylovSolver::Impl {
     DeviceArray<Scalars> sc;
     DeviceArray<PcgState> pst;
     DeviceArray<float> r32, s32, z32, p32a, p32b, q32, d32;  // FP32 inner solve of the refined path
+    // SELL-32 copy of the matrix the BiCGStab products read: the pattern of the
+    // last CSR pattern seen (a solver's systems all live on one mesh's cell->face
+    // pattern, so it is built once), the values re-scattered for every solve.
+    struct SellCopy {
+        const int* ptr = nullptr;
+        const int* col = nullptr;
+        int n = 0;
+        long long nnz = -1;
+        int nslices = 0;
+        DeviceArray<int> sptr, scol;
+        DeviceArray<double> sval;
+    } sell;
     explicit Impl(Context& c) : ctx(c) { sc.resize(1); }
+    SellMat<double> sellOf(const Dcsr<double>& A) {
+        if (sell.ptr != A.ptr || sell.col != A.col || sell.n != A.n || sell.nnz != A.nnz_off) {
+            std::vector<int> hp(A.n + 1), hc(std::max<long long>(A.nnz_off, 1));
+            BSG_CUDA(cudaMemcpyAsync(hp.data(), A.ptr, sizeof(int) * (A.n + 1), cudaMemcpyDeviceToHost, ctx.stream));
+            if (A.nnz_off > 0)
+                BSG_CUDA(cudaMemcpyAsync(hc.data(), A.col, sizeof(int) * A.nnz_off, cudaMemcpyDeviceToHost,
+                                         ctx.stream));
+            ctx.sync();
+            SellPattern pat;
+            pat.build(A.n, hp.data(), hc.data());
+            if (pat.col.empty()) pat.col.push_back(0);
+            sell.sptr.upload(pat.sptr, ctx.stream);
+            sell.scol.upload(pat.col, ctx.stream);
+            sell.sval.resize(pat.col.size());
+            sell.sval.zero(ctx.stream);   // padding entries stay zero
+            sell.nslices = pat.nslices;
+            sell.ptr = A.ptr;
+            sell.col = A.col;
+            sell.n = A.n;
+            sell.nnz = A.nnz_off;
+        }
+        kCsrToSell<double><<<gridFor(A.n, kBlock), kBlock, 0, ctx.stream>>>(
+            A.n, A.ptr, A.val, A.diag, sell.sptr.data(), 1.0, sell.sval.data(), nullptr, nullptr);
+        BSG_CUDA(cudaGetLastError());
+        ++ctx.launches;
+        return SellMat<double>{A.n, sell.nslices, sell.sptr.data(), sell.scol.data(), sell.sval.data(), A.diag};
+    }
     int grid(int n) const {
         const long long g = (static_cast<long long>(n) + kBlock - 1) / kBlock;
         return static_cast<int>(std::max<long long>(1, std::min<long long>(g, 4LL * ctx.sm_count)));
@@ -811,6 +937,7 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
     const int n = A.n;
     m.ensure(C * static_cast<std::size_t>(n));
     const int g = m.grid(n);
+    const SellMat<double> S = m.sellOf(A);
     if (!cfg.warm_start) BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * C * n, ctx.stream));
     double* result = m.partial.data() + 8 * 4096 - 8;
     // r = b - A x with per-component squared norms; also ||b|| per component.
@@ -863,8 +990,8 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
                                                               m.ph.data(), m.sc.data());
                 {
                     BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
-                    kBiSpmvV<C><<<g, kBlock, 0, ctx.stream>>>(A, m.ph.data(), m.v.data(), m.r0.data(),
-                                                              m.partial.data(), m.sc.data());
+                    kBiSpmvVSell<C><<<g, kBlock, 0, ctx.stream>>>(S, m.ph.data(), m.v.data(), m.r0.data(),
+                                                                  m.partial.data(), m.sc.data());
                 }
                 kBiAlpha<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 kBiS<C><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.v.data(), m.sh.data(), m.partial.data(),
@@ -872,8 +999,8 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
                 kBiCheckS<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 {
                     BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
-                    kBiSpmvT<C><<<g, kBlock, 0, ctx.stream>>>(A, m.sh.data(), m.t.data(), m.r.data(),
-                                                              m.partial.data(), m.sc.data());
+                    kBiSpmvTSell<C><<<g, kBlock, 0, ctx.stream>>>(S, m.sh.data(), m.t.data(), m.r.data(),
+                                                                  m.partial.data(), m.sc.data());
                 }
                 kBiOmega<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 kBiUpdate<C><<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.ph.data(), m.sh.data(), m.t.data(),
