@@ -135,11 +135,12 @@ def algorithmic_bytes(name, N, nnz_off, amg_rows):
 
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte,
-# measured by one capture of the kernel on this workload (profiles/ summaries).
-# kPcgSell, first pressure solve of the 1M-cell Voronoi cavity (33 CG iterations):
-# 35.69 GB of DRAM traffic for 37.34 GB of algorithmic bytes
-# (profiles/kPcgSell_simple_1M_voronoi.md).
-DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.956}
+# measured by one capture of the kernel (profiles/ summaries).  kPcgSell, first
+# pressure solve of the 512000-cell Voronoi cavity of the same generator and
+# settings (32 CG iterations): 16.05 GB of DRAM traffic for 18.50 GB of algorithmic
+# bytes (profiles/kPcgSell_simple_512k_voronoi.md).  Both grow with cells and CG
+# iterations in proportion, so the ratio scales the 1M-cell launches.
+DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.868}
 
 
 def load_peaks():
