@@ -143,6 +143,10 @@ class KOmega:
     def effective_viscosity(self):
         return fvm.Field(self.geo, self.mueff_v.copy(), None, trace=self.mueff_tr.copy())
 
+    def transported(self):
+        """The model's transported fields by state name (the second one is stored as omega)."""
+        return {"k": self.k, "omega": self.omega}
+
     def stress_remainder_divergence(self, U: fvm.Field):
         """math::div(muEff (grad(U)^T - 2/3 tr(grad U) I)) (model.cpp:65-69, operators.cpp:1568-1591)."""
         G = fvm.gradient(U, self.mom_opts["gradient"])
@@ -284,3 +288,119 @@ class KEpsilon(KOmega):
         self.update_viscosity()
         return dict(d=max(fvm.relative_change(self.k.v, prev_k), fvm.relative_change(self.eps.v, prev_e)),
                     r=max(r_k, r_e))
+
+
+@dataclass
+class SpalartAllmarasConstants:
+    """Model constants and bounds (spalart_allmaras.cpp:31-45); cw1 defaults to cb1/kappa^2 + (1 + cb2)/sigma."""
+    cb1: float = 0.1355
+    cb2: float = 0.622
+    sigma: float = 2.0 / 3.0
+    kappa: float = 0.41
+    cw2: float = 0.3
+    cw3: float = 2.0
+    cv1: float = 7.1
+    ct3: float = 1.2
+    ct4: float = 0.5
+    cw1: float | None = None
+    nu_tilda_min: float = 1e-14
+    wall_distance_min: float = 1e-12
+    relaxation: float = 0.7
+    tolerance: float = 1e-6
+
+    def __post_init__(self):
+        if self.cw1 is None:
+            self.cw1 = self.cb1 / (self.kappa * self.kappa) + (1.0 + self.cb2) / self.sigma
+
+
+def vorticity_magnitude(G):
+    """sqrt(2 sum_ij (0.5 (G_ij - G_ji))^2) per cell, summed row by row (spalart_allmaras.cpp:10-19)."""
+    s = np.zeros(G.shape[0])
+    for i in range(3):
+        for j in range(3):
+            rot = 0.5 * (G[:, i, j] - G[:, j, i])
+            s = s + rot * rot
+    return np.sqrt(2.0 * s)
+
+
+class SpalartAllmaras(KOmega):
+    """SpalartAllmaras (spalart_allmaras.cpp:23-154) on oracle fields: positive-variable SA with ft2 and
+    without the trip term; the wall distance is a given cell field."""
+
+    def __init__(self, geo, nu_tilda: fvm.Field, wall_distance, rho, mu, c: SpalartAllmarasConstants, nt_opts,
+                 momentum_opts, phi0):
+        self.geo, self.nt, self.rho, self.mu, self.c = geo, nu_tilda, rho, mu, c
+        self.wall_distance = np.asarray(wall_distance, dtype=np.float64)
+        self.nt_opts, self.mom_opts = nt_opts, momentum_opts
+        self.bf = np.nonzero(geo.neighbour < 0)[0]
+        nf = geo.n_faces
+        self.mut_v = np.zeros(geo.n_cells)
+        self.mut_tr = np.zeros(nf)
+        self.mueff_v = np.full(geo.n_cells, mu)
+        self.mueff_tr = np.full(nf, mu)
+        self.bound_transport_fields(phi0)
+        self.update_viscosity()
+
+    def transported(self):
+        return {"nuTilda": self.nt}
+
+    def _fv1(self, chi):
+        chi3 = (chi * chi) * chi
+        cv = self.c.cv1
+        return chi3 / (chi3 + (cv * cv) * cv)
+
+    def bound_transport_fields(self, phi):
+        self.nt.flux = np.array(phi, dtype=np.float64)
+        self.nt.v = np.maximum(self.nt.v, self.c.nu_tilda_min)
+
+    def update_viscosity(self):
+        """mut = rho nuTilda fv1(nuTilda / nu); muEff = mu + mut, with calculated traces (:137-140)."""
+        nu = self.mu / self.rho
+        self.mut_v = (self.rho * self.nt.v) * self._fv1(self.nt.v / nu)
+        tr = self._trace(self.nt)
+        b = self.bf
+        self.mut_tr = np.zeros(self.geo.n_faces)
+        self.mut_tr[b] = (self.rho * tr[b]) * self._fv1(tr[b] / nu)
+        self.mueff_v = self.mut_v + self.mu
+        self.mueff_tr = self.mut_tr + self.mu
+
+    def solve_transport(self, U: fvm.Field, phi):
+        """SpalartAllmaras::solveTransport (:65-122), steady (the time term is absent)."""
+        geo, c, rho, mu = self.geo, self.c, self.rho, self.mu
+        prev = self.nt.v.copy()
+        U.flux = np.array(phi, dtype=np.float64)
+        nt = self.nt.v
+        nu = mu / rho
+        chi = nt / nu
+        fv1 = self._fv1(chi)
+        fv2 = 1.0 - chi / (1.0 + chi * fv1)
+        ft2 = c.ct3 * np.exp(((-c.ct4) * chi) * chi)
+        distance = np.maximum(self.wall_distance, c.wall_distance_min)
+        inv_d2 = 1.0 / (distance * distance)
+        k2 = c.kappa * c.kappa
+        rotation = vorticity_magnitude(fvm.gradient(U, self.mom_opts["gradient"]))
+        mod_rot = np.maximum(rotation + ((nt * fv2) * inv_d2) / k2, 1e-30)
+        r = np.clip((nt * inv_d2) / (k2 * mod_rot), 0.0, 10.0)
+        g = r + c.cw2 * (r ** 6.0 - r)
+        cw3_6 = c.cw3 ** 6.0
+        fw = g * ((1.0 + cw3_6) / (g ** 6.0 + cw3_6)) ** (1.0 / 6.0)
+        production = (c.cb1 * (1.0 - ft2)) * mod_rot
+        destruction = ((c.cw1 * fw - (c.cb1 / k2) * ft2) * nt) * inv_d2
+        net = production - destruction
+        implicit = rho * np.maximum(-net, 0.0)
+        gnt = fvm.gradient(self.nt, self.nt_opts["gradient"])
+        grad_source = ((rho * c.cb2) / c.sigma) * np.einsum("ij,ij->i", gnt, gnt)
+        explicit = (rho * np.maximum(net, 0.0)) * nt + grad_source
+        tr = self._trace(self.nt)
+        diff = fvm.Field(geo, (mu + rho * nt) / c.sigma, None, trace=(mu + rho * tr) / c.sigma)
+        eq = fvm.Equation(self.nt, self.nt_opts, {})
+        fvm.eq_div(eq, phi, rho)
+        fvm.eq_laplacian(eq, diff, -1.0)
+        eq.ldu.diag = eq.ldu.diag + (1.0 * implicit) * geo.volume
+        fvm.eq_source(eq, explicit)
+        res = fvm.relative_residual(eq.ldu, self.nt.v)
+        fvm.eq_relax(eq, prev, c.relaxation)
+        self.nt.v = _solve(eq.ldu.matrix(), eq.ldu.source)
+        self.bound_transport_fields(phi)
+        self.update_viscosity()
+        return dict(d=fvm.relative_change(self.nt.v, prev), r=res)

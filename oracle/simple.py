@@ -138,7 +138,9 @@ def run_simple(geo, U_bcs, p_bcs, settings: SimpleSettings, U0=None, p0=None, it
         state.history.append(dict(rU=rU, dU=dU, dP=dP, mass=mass["relative"]))
         state.U, state.p, state.phi, state.iterations = U.v, p.v, phi, it + 1
         if model:
-            state.k, state.omega, state.mut = model.k.v, model.omega.v, model.mut_v
+            state.mut = model.mut_v
+            for name, f in model.transported().items():
+                setattr(state, name, f.v)
         if conv:
             state.converged = True
             break

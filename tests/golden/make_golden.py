@@ -281,6 +281,85 @@ def main_rans():
               rans_solution("epsilon"), keps, K=4, second="epsilon")
 
 
+def make_sa(name, mesh, U_bcs, p_bcs, nt_field, wall_distance, methods, solution, physics, K):
+    """Steady SIMPLE with the reference's Spalart-Allmaras model: U, p, phi, nuTilda, mut after iterations
+    1..K.  The wall distance is a given cell field (the reference reads it, it does not compute it),
+    written as a file-backed internal value."""
+    work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
+    write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics,
+               extra_fields=[("nuTilda",) + tuple(nt_field),
+                             ("wallDistance", 0.0, [("zeroGradient", 0.0)] * len(mesh.patch_names))],
+               internal={"wallDistance": "file wallDistance.data"})
+    with open(os.path.join(work, "fields", "initial", "wallDistance.data"), "w") as f:
+        f.write("".join(f"{i} {d!r}\n" for i, d in enumerate(map(float, wall_distance))))
+    data = {}
+    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    data["mesh_vertices"] = mesh.vertices
+    data["mesh_offsets"] = offsets
+    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
+    data["wall_distance"] = np.asarray(wall_distance, dtype=np.float64)
+    for k in range(1, K + 1):
+        fields, geo, info, _ = run(work, k)
+        data[f"U_{k}"] = fields["U"].reshape(-1, 3)
+        for key in ("p", "phi", "nuTilda", "mut", "muEffective"):
+            data[f"{key}_{k}"] = fields[key]
+    for key, arr in geo.items():
+        data["geo_" + key] = arr
+    meta = dict(patch_names=mesh.patch_names, patch_kinds=mesh.patch_kinds,
+                U_bcs=[(t, list(map(float, v))) for t, v in U_bcs], p_bcs=[(t, float(v)) for t, v in p_bcs],
+                nuTilda_internal=nt_field[0], nuTilda_bcs=[(t, float(v)) for t, v in nt_field[1]],
+                methods=methods, solution=solution, physics=physics, K=K)
+    data["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
+    shutil.rmtree(work)
+    print(name, "written", K, "iterations")
+
+
+def _cell_centres(mesh):
+    from oracle import geometry
+    return geometry.compute_geometry(geometry.PolyMesh(mesh.vertices, mesh.rings(), mesh.owner, mesh.neighbour,
+                                                       mesh.patch, mesh.patch_names, mesh.patch_kinds)).xc
+
+
+def main_sa():
+    sa = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "SA", "saNuTildaMin": 1e-14,
+          "saWallDistanceMin": 1e-12, "saCb1": 0.1355, "saCb2": 0.622, "saSigma": 2.0 / 3.0, "saKappa": 0.41,
+          "saCw2": 0.3, "saCw3": 2.0, "saCv1": 7.1, "saCt3": 1.2, "saCt4": 0.5}
+
+    def methods_sa(conv="upwind", grad="greenGauss", diff="orthogonal"):
+        o = dict(interpolation="linear", gradient=grad, convection=conv, diffusion=diff)
+        return {"momentum": o, "pressureCorrection": o, "nuTildaTransport": dict(o, convection="upwind")}
+
+    def solution_sa():
+        sol = config1_solution(1e-12)
+        sol.update({"turbulenceRelaxation": 0.7, "turbulenceTolerance": 1e-6,
+                    "equation.nuTildaTransport.kspType": "bcgs", "equation.nuTildaTransport.pcType": "bjacobi",
+                    "equation.nuTildaTransport.absoluteTolerance": 1e-18,
+                    "equation.nuTildaTransport.relativeTolerance": 1e-12,
+                    "equation.nuTildaTransport.maxIterations": 2000})
+        return sol
+    ch = meshgen.hex_box(16, 8, 1, hi=(4.0, 1.0, 0.25),
+                         names=["inlet", "outlet", "lower", "upper", "front", "back"],
+                         kinds=["inlet", "outlet", "wall", "wall", "symmetry", "symmetry"])
+    U = [("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0)), ("fixedValue", (0.0, 0.0, 0.0)),
+         ("fixedValue", (0.0, 0.0, 0.0)), ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    p = [("zeroGradient", 0.0), ("fixedValue", 0.0), ("zeroGradient", 0.0), ("zeroGradient", 0.0),
+         ("symmetry", 0.0), ("symmetry", 0.0)]
+    ntb = [("fixedValue", 3e-3), ("zeroGradient", 0.0), ("fixedValue", 0.0), ("fixedValue", 0.0),
+           ("symmetry", 0.0), ("symmetry", 0.0)]
+    y = _cell_centres(ch)[:, 1]
+    make_sa("sa_channel", ch, U, p, (3e-3, ntb), np.minimum(y, 1.0 - y), methods_sa("linearUpwind"),
+            solution_sa(), sa, K=4)
+    wb = meshgen.warped_box(5)
+    Uw = [("fixedValue", (0.0, 0.0, 0.0))] * 3 + [("fixedValue", (1.0, 0.0, 0.0))] + [("fixedValue", (0.0, 0.0, 0.0))] * 2
+    pw = [("zeroGradient", 0.0)] * 6
+    xc = _cell_centres(wb)
+    d = np.minimum(np.minimum(xc, 1.0 - xc).min(axis=1), 1.0)
+    make_sa("sa_warped5", wb, Uw, pw, (2e-3, [("fixedValue", 0.0)] * 6), d,
+            methods_sa("linearUpwind", "leastSquares", "corrected"), solution_sa(), sa, K=3)
+
+
 def piso_solution(n_correctors=2, non_orth=1, p_rtol=1e-12):
     return {"maxIterations": 1, "nCorrectors": n_correctors, "nonOrthogonalCorrections": non_orth,
             "velocityRelaxation": 1.0, "continuityTolerance": 1e-7, "velocityTolerance": 1e-7,
@@ -337,7 +416,10 @@ if __name__ == "__main__":
         main_piso()
     elif len(sys.argv) > 1 and sys.argv[1] == "rans":
         main_rans()
+    elif len(sys.argv) > 1 and sys.argv[1] == "sa":
+        main_sa()
     else:
         main()
         main_piso()
         main_rans()
+        main_sa()

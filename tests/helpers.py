@@ -18,6 +18,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
 PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler", "piso_cylinder_ogrid"]
 RANS_CASES = ["komega_channel", "komega_warped5"]
+SA_CASES = ["sa_channel", "sa_warped5"]
 GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
             "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",
             "face_skewness", "cell_centres", "cell_volumes", "orthogonal_geometry"]
@@ -144,4 +145,24 @@ def kepsilon_factory(g: "Golden"):
         e = fvm.Field(geo, np.full(geo.n_cells, g.meta["omega_internal"]), eb)
         return rans.KEpsilon(geo, k, e, ph["density"], ph["dynamicViscosity"], c, m["kTransport"],
                              m["epsilonTransport"], m["momentum"], phi0)
+    return make
+
+
+def sa_constants(g: "Golden") -> rans.SpalartAllmarasConstants:
+    ph, sol = g.meta["physics"], g.meta["solution"]
+    return rans.SpalartAllmarasConstants(ph["saCb1"], ph["saCb2"], ph["saSigma"], ph["saKappa"], ph["saCw2"],
+                                         ph["saCw3"], ph["saCv1"], ph["saCt3"], ph["saCt4"], None,
+                                         ph["saNuTildaMin"], ph["saWallDistanceMin"], sol["turbulenceRelaxation"],
+                                         sol["turbulenceTolerance"])
+
+
+def sa_factory(g: "Golden"):
+    """Model factory for oracle.simple.run_simple(turbulence=...) from a Spalart-Allmaras fixture."""
+    ph, m = g.meta["physics"], g.meta["methods"]
+    nb = [(fvm.BC_NAMES[t], v) for t, v in g.meta["nuTilda_bcs"]]
+
+    def make(geo, phi0):
+        nt = fvm.Field(geo, np.full(geo.n_cells, g.meta["nuTilda_internal"]), nb)
+        return rans.SpalartAllmaras(geo, nt, g["wall_distance"], ph["density"], ph["dynamicViscosity"],
+                                    sa_constants(g), m["nuTildaTransport"], m["momentum"], phi0)
     return make

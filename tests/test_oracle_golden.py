@@ -9,8 +9,8 @@ solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
 import numpy as np
 import pytest
 
-from helpers import (CASES, PISO_CASES, RANS_CASES, Golden, kepsilon_factory, komega_factory, piso_settings,
-                     ref_system_groups, rel, rel_l2)
+from helpers import (CASES, PISO_CASES, RANS_CASES, SA_CASES, Golden, kepsilon_factory, komega_factory,
+                     piso_settings, ref_system_groups, rel, rel_l2, sa_factory)
 from oracle import fvm, simple
 
 
@@ -154,6 +154,31 @@ def test_komega_simple_iterations_match_reference(name):
         for key, mine in (("U", st.U), ("p", st.p), ("phi", st.phi), ("k", st.k), ("omega", st.omega),
                           ("mut", st.mut)):
             assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k)
+
+
+@pytest.mark.parametrize("name", SA_CASES)
+def test_spalart_allmaras_simple_iterations_match_reference(name):
+    """SIMPLE with the Spalart-Allmaras model (given wall distance): the restatement of the closure
+    functions, the implicit/explicit split of the net reaction, the cb2 gradient source and the calculated
+    traces of mut/muEff/diffusivity reproduces the reference's U, p, phi, nuTilda, mut every iteration."""
+    g = Golden(name)
+    geo = g.oracle_geometry()
+    s = g.settings()
+    s.mu = g.meta["physics"]["dynamicViscosity"]
+    for k in range(1, g.K + 1):
+        st = simple.run_simple(geo, g.U_bcs(), g.p_bcs(), s, iterations=k, turbulence=sa_factory(g))
+        for key, mine in (("U", st.U), ("p", st.p), ("phi", st.phi), ("nuTilda", st.nuTilda), ("mut", st.mut)):
+            assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
+
+
+def test_vorticity_magnitude_known_answers():
+    """sqrt(2 W:W) is the vorticity magnitude: 2w for a solid rotation at angular rate w, zero for pure strain."""
+    from oracle import rans
+    w = 1.7
+    rot = np.array([[[0.0, -w, 0.0], [w, 0.0, 0.0], [0.0, 0.0, 0.0]]])
+    strain = np.array([[[1.0, 2.0, 0.0], [2.0, -1.0, 0.0], [0.0, 0.0, 0.0]]])
+    assert abs(rans.vorticity_magnitude(rot)[0] - 2.0 * w) < 1e-15
+    assert rans.vorticity_magnitude(strain)[0] == 0.0
 
 
 def test_strain_squared_known_answers():
