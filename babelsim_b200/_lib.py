@@ -30,7 +30,8 @@ EXPORTS = [
     "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_pcg_jacobi_static",
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
-    "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_enable_kepsilon", "bsg_simple_set_turbulence_fields",
+    "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_enable_kepsilon",
+    "bsg_simple_enable_spalart_allmaras", "bsg_simple_set_wall_distance", "bsg_simple_set_turbulence_fields",
     "bsg_simple_get_turbulence_fields", "bsg_simple_get_fields",
     "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
     "bsg_piso_get_fields", "bsg_piso_destroy",
@@ -118,6 +119,12 @@ class KEpsilonConfig(C.Structure):
                 ("epsilon_transport", Options), ("k_solver", SolverConfig), ("epsilon_solver", SolverConfig)]
 
 
+class SaConfig(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("cb1", "cb2", "sigma", "kappa", "cw1", "cw2", "cw3", "cv1", "ct3", "ct4",
+                                          "nu_tilda_min", "wall_distance_min", "relaxation", "tolerance")] + \
+        [("nu_tilda_transport", Options), ("nu_tilda_solver", SolverConfig)]
+
+
 _lib = None
 
 
@@ -167,6 +174,8 @@ def lib():
             "bsg_simple_iterate": [vp, i32, C.POINTER(SimpleReport)],
             "bsg_simple_enable_komega": [vp, C.POINTER(KOmegaConfig)],
             "bsg_simple_enable_kepsilon": [vp, C.POINTER(KEpsilonConfig)],
+            "bsg_simple_enable_spalart_allmaras": [vp, C.POINTER(SaConfig)],
+            "bsg_simple_set_wall_distance": [vp, vp],
             "bsg_simple_set_turbulence_fields": [vp, vp, vp], "bsg_simple_get_turbulence_fields": [vp, vp, vp, vp], "bsg_simple_get_fields": [vp, vp, vp, vp],
             "bsg_simple_destroy": [vp],
             "bsg_piso_create": [vp, C.POINTER(PisoConfig), pp],

@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (KEpsilonConfig, KOmegaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
+from ._lib import (KEpsilonConfig, KOmegaConfig, SaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
                    check, f64, i32, lib, ptr)
 
 BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
@@ -394,13 +394,33 @@ class Simple:
                              epsilon_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
         check(lib().bsg_simple_enable_kepsilon(self.h, C.byref(cfg)), self.mesh.ctx.h)
 
-    def set_turbulence_fields(self, k, omega):
-        check(lib().bsg_simple_set_turbulence_fields(self.h, ptr(f64(k)), ptr(f64(omega))), self.mesh.ctx.h)
+    def enable_spalart_allmaras(self, cb1=0.1355, cb2=0.622, sigma=2.0 / 3.0, kappa=0.41, cw1=0.0, cw2=0.3, cw3=2.0,
+                                cv1=7.1, ct3=1.2, ct4=0.5, nu_tilda_min=1e-14, wall_distance_min=1e-12,
+                                relaxation=0.7, tolerance=1e-6, nu_tilda_transport=None, nu_tilda_solver=None):
+        """turbulenceModel SA (before set_fields); "nuTilda" then takes boundary conditions and the wall
+        distance comes from set_wall_distance.  cw1 <= 0 takes cb1/kappa^2 + (1 + cb2)/sigma."""
+        cfg = SaConfig(cb1, cb2, sigma, kappa, cw1, cw2, cw3, cv1, ct3, ct4, nu_tilda_min, wall_distance_min,
+                       relaxation, tolerance, nu_tilda_transport or options(),
+                       nu_tilda_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
+        check(lib().bsg_simple_enable_spalart_allmaras(self.h, C.byref(cfg)), self.mesh.ctx.h)
+        self._one_equation = True
+
+    def set_wall_distance(self, d):
+        """The wall distance of every cell (an input of the Spalart-Allmaras model, as in the reference)."""
+        check(lib().bsg_simple_set_wall_distance(self.h, ptr(f64(d))), self.mesh.ctx.h)
+
+    def set_turbulence_fields(self, k, second):
+        """Initial k and omega / epsilon; k is None for Spalart-Allmaras, whose field is nuTilda."""
+        kp = None if k is None else ptr(f64(k))
+        check(lib().bsg_simple_set_turbulence_fields(self.h, kp, ptr(f64(second))), self.mesh.ctx.h)
 
     def turbulence_fields(self):
+        """(k, second transported field, mut); k is None for Spalart-Allmaras."""
         n = self.mesh.n_cells
-        k, w, mut = np.zeros(n), np.zeros(n), np.zeros(n)
-        check(lib().bsg_simple_get_turbulence_fields(self.h, ptr(k), ptr(w), ptr(mut)), self.mesh.ctx.h)
+        one = getattr(self, "_one_equation", False)
+        k, w, mut = (None if one else np.zeros(n)), np.zeros(n), np.zeros(n)
+        check(lib().bsg_simple_get_turbulence_fields(self.h, None if one else ptr(k), ptr(w), ptr(mut)),
+              self.mesh.ctx.h)
         return k, w, mut
 
     def fields(self):

@@ -864,11 +864,13 @@ int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int
         bsg::KOmegaModel* t = s->solver->turbulence();
         if (n == "U") s->solver->U().setBoundary(patch, type, value);
         else if (n == "p") s->solver->p().setBoundary(patch, type, value);
-        else if (n == "k" && t) t->k().setBoundary(patch, type, value);
+        else if (n == "k" && t && t->config().kind != 2) t->k().setBoundary(patch, type, value);
+        else if (n == "nuTilda" && t && t->config().kind == 2) t->omega().setBoundary(patch, type, value);
         else if (n == "omega" && t && t->config().kind == 0) t->omega().setBoundary(patch, type, value);
         else if (n == "epsilon" && t && t->config().kind == 1) t->omega().setBoundary(patch, type, value);
         else bsg::fail(bsg::kArgument,
-                       "SIMPLE boundary field must be U or p (k and omega or epsilon with a two-equation model)");
+                       "SIMPLE boundary field must be U or p (k and omega or epsilon with a two-equation model, "
+                       "nuTilda with Spalart-Allmaras)");
     });
 }
 
@@ -960,12 +962,48 @@ int bsg_simple_enable_kepsilon(bsg_simple* s, const bsg_kepsilon_config* c) {
     });
 }
 
-int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* omega) {
+int bsg_simple_enable_spalart_allmaras(bsg_simple* s, const bsg_sa_config* c) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
-        require(s && k && omega, "null argument");
+        require(s && c, "null argument");
+        bsg::KOmegaConfig k;
+        k.kind = 2;
+        k.sa_cb1 = c->cb1;
+        k.sa_cb2 = c->cb2;
+        k.sa_sigma = c->sigma;
+        k.sa_kappa = c->kappa;
+        k.sa_cw1 = c->cw1;
+        k.sa_cw2 = c->cw2;
+        k.sa_cw3 = c->cw3;
+        k.sa_cv1 = c->cv1;
+        k.sa_ct3 = c->ct3;
+        k.sa_ct4 = c->ct4;
+        k.omega_min = c->nu_tilda_min;
+        k.wall_distance_min = c->wall_distance_min;
+        k.relaxation = c->relaxation;
+        k.tolerance = c->tolerance;
+        k.omega_options = options(&c->nu_tilda_transport);
+        k.omega_solver = solverConfig(&c->nu_tilda_solver);
+        s->solver->enableKOmega(k);
+    });
+}
+
+int bsg_simple_set_wall_distance(bsg_simple* s, const double* wall_distance) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && wall_distance, "null argument");
         bsg::KOmegaModel* t = s->solver->turbulence();
         if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
-        t->k().uploadExternal(k);
+        t->setWallDistance(wall_distance);
+    });
+}
+
+int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* omega) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && omega, "null argument");
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        if (t->config().kind == 2) require(k == nullptr, "the Spalart-Allmaras model has no k");
+        else require(k != nullptr, "null argument");
+        if (k) t->k().uploadExternal(k);
         t->omega().uploadExternal(omega);
     });
 }
@@ -975,6 +1013,7 @@ int bsg_simple_get_turbulence_fields(const bsg_simple* s, double* k, double* ome
         require(s != nullptr, "null argument");
         bsg::KOmegaModel* t = s->solver->turbulence();
         if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        if (k && t->config().kind == 2) bsg::fail(bsg::kArgument, "the Spalart-Allmaras model has no k");
         if (k) t->k().downloadExternal(k);
         if (omega) t->omega().downloadExternal(omega);
         if (mut) t->turbulentViscosity().downloadExternal(mut);

@@ -1,4 +1,4 @@
-// Wilcox-1988m k-omega transport on the device (see rans.h).
+// Eddy-viscosity model transport on the device: k-omega, k-epsilon, Spalart-Allmaras (see rans.h).
 #include "bsg_device.cuh"
 #include "rans.h"
 
@@ -139,6 +139,85 @@ __global__ void kDiffusivityTrace(int nb, double mu, double sigma_k, double sigm
     wdiff_tr[fb] = sigma_w * mut_tr[fb] + mu;
 }
 
+// ---- Spalart-Allmaras (spalart_allmaras.cpp)
+struct SaConstants {
+    double rho, mu, nu, cb1, cb2, sigma, kappa2, cw1, cw2, cw3_6, cv1, ct3, ct4, dmin;
+};
+
+// fv1 = chi^3 / (chi^3 + cv1^3) (spalart_allmaras.cpp:125-130)
+__device__ __forceinline__ double saFv1(double chi, double cv1) {
+    const double c3 = (chi * chi) * chi;
+    return c3 / (c3 + (cv1 * cv1) * cv1);
+}
+
+// mut = rho nuTilda fv1(nuTilda / nu), muEff = mu + mut on cells (:137-140)
+__global__ void kViscositySA(int n, SaConstants c, const double* __restrict__ nt, double* __restrict__ mut,
+                             double* __restrict__ mueff) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = (c.rho * nt[i]) * saFv1(nt[i] / c.nu, c.cv1);
+    mut[i] = v;
+    mueff[i] = v + c.mu;
+}
+
+// the same on the boundary trace of nuTilda (mut_tr, mueff_tr), and/or the transport diffusivity
+// (mu + rho nuTilda) / sigma there (diff_tr); a null output is skipped
+__global__ void kTraceSA(MeshView m, BcView bn, const double* __restrict__ nt, SaConstants c,
+                         double* __restrict__ mut_tr, double* __restrict__ mueff_tr, double* __restrict__ diff_tr) {
+    const int fb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fb >= m.n_boundary) return;
+    double t[1];
+    boundaryTrace<1>(m, bn, nt, fb, NAN, t);
+    if (mut_tr) {
+        const double v = (c.rho * t[0]) * saFv1(t[0] / c.nu, c.cv1);
+        mut_tr[fb] = v;
+        mueff_tr[fb] = v + c.mu;
+    }
+    if (diff_tr) diff_tr[fb] = (c.mu + c.rho * t[0]) / c.sigma;
+}
+
+// Closure functions at the current iterate and the frozen coefficients of the nuTilda equation
+// (:69-103): implicit destruction rho max(-a, 0), explicit source rho max(a, 0) nuTilda + rho cb2 /
+// sigma |grad nuTilda|^2 with a = production - destruction rate, diffusivity (mu + rho nuTilda) / sigma.
+// G row c = gradient of velocity component c; gn = gradient of nuTilda.
+__global__ void kCoefficientsSA(int n, SaConstants c, const double* __restrict__ G, const double* __restrict__ gn,
+                                const double* __restrict__ ntv, const double* __restrict__ dist,
+                                double* __restrict__ implicit, double* __restrict__ explicit_src,
+                                double* __restrict__ diff) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double nt = ntv[i];
+    const double chi = nt / c.nu;
+    const double fv1 = saFv1(chi, c.cv1);
+    const double fv2 = 1.0 - chi / (1.0 + chi * fv1);
+    const double ft2 = c.ct3 * exp(((-c.ct4) * chi) * chi);
+    const double d = fmax(dist[i], c.dmin);
+    const double inv_d2 = 1.0 / (d * d);
+    const double* g = G + 9 * i;
+    double sum = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const double rot = 0.5 * (g[3 * a + b] - g[3 * b + a]);
+            sum += rot * rot;
+        }
+    const double rotation = sqrt(2.0 * sum);
+    const double mod_rot = fmax(rotation + ((nt * fv2) * inv_d2) / c.kappa2, 1e-30);
+    double r = (nt * inv_d2) / (c.kappa2 * mod_rot);
+    r = r < 0.0 ? 0.0 : (10.0 < r ? 10.0 : r);
+    const double gg = r + c.cw2 * (pow(r, 6.0) - r);
+    const double fw = gg * pow((1.0 + c.cw3_6) / (pow(gg, 6.0) + c.cw3_6), 1.0 / 6.0);
+    const double production = (c.cb1 * (1.0 - ft2)) * mod_rot;
+    const double destruction = ((c.cw1 * fw - (c.cb1 / c.kappa2) * ft2) * nt) * inv_d2;
+    const double net = production - destruction;
+    implicit[i] = c.rho * fmax(-net, 0.0);
+    const double* q = gn + 3 * i;
+    const double grad_source = ((c.rho * c.cb2) / c.sigma) * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+    explicit_src[i] = (c.rho * fmax(net, 0.0)) * nt + grad_source;
+    diff[i] = (c.mu + c.rho * nt) / c.sigma;
+}
+
 __global__ void kScaled(int n, double a, const double* __restrict__ x, double* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = a * x[i];
@@ -251,13 +330,36 @@ void makeCalculated(DeviceField& f, int n_boundary) {
     f.trace.resize(static_cast<std::size_t>(n_boundary) * f.comps);
 }
 
+SaConstants saConstants(const KOmegaConfig& k) {
+    SaConstants c;
+    c.rho = k.rho;
+    c.mu = k.mu;
+    c.nu = k.mu / k.rho;
+    c.cb1 = k.sa_cb1;
+    c.cb2 = k.sa_cb2;
+    c.sigma = k.sa_sigma;
+    c.kappa2 = k.sa_kappa * k.sa_kappa;
+    c.cw1 = k.sa_cw1 > 0.0 ? k.sa_cw1 : k.sa_cb1 / (k.sa_kappa * k.sa_kappa) + (1.0 + k.sa_cb2) / k.sa_sigma;
+    c.cw2 = k.sa_cw2;
+    c.cw3_6 = std::pow(k.sa_cw3, 6.0);
+    c.cv1 = k.sa_cv1;
+    c.ct3 = k.sa_ct3;
+    c.ct4 = k.sa_ct4;
+    c.dmin = k.wall_distance_min;
+    return c;
+}
+
 }  // namespace
 
 KOmegaModel::KOmegaModel(DeviceMesh& mesh, const KOmegaConfig& cfg)
     : m_(mesh), ctx_(*mesh.ctx), cfg_(cfg), k_(mesh, 0, 1), omega_(mesh, 0, 1), mut_(mesh, 0, 1), muEff_(mesh, 0, 1),
       kDiff_(mesh, 0, 1), wDiff_(mesh, 0, 1), krylov_(*mesh.ctx) {
     if (!(cfg.rho > 0) || !(cfg.mu > 0)) fail(kArgument, "density and dynamicViscosity must be positive");
-    if (cfg.kind != 0 && cfg.kind != 1) fail(kArgument, "unknown two-equation turbulence model");
+    if (cfg.kind < 0 || cfg.kind > 2) fail(kArgument, "unknown turbulence model");
+    if (cfg.kind == 2)
+        for (double v : {cfg.sa_cb1, cfg.sa_cb2, cfg.sa_sigma, cfg.sa_kappa, cfg.sa_cw2, cfg.sa_cw3, cfg.sa_cv1,
+                         cfg.sa_ct3, cfg.sa_ct4, cfg.wall_distance_min})
+            if (!(v > 0) || !std::isfinite(v)) fail(kArgument, "Spalart-Allmaras constants and bounds must be positive and finite");
     for (double v : {cfg.beta_star, cfg.beta, cfg.gamma, cfg.sigma_k, cfg.sigma_omega, cfg.k_min, cfg.omega_min,
                      cfg.viscosity_ratio_max, cfg.tolerance, cfg.c_mu, cfg.c1, cfg.c2})
         if (!(v > 0) || !std::isfinite(v)) fail(kArgument, "turbulence model constants and bounds must be positive and finite");
@@ -274,13 +376,25 @@ KOmegaModel::KOmegaModel(DeviceMesh& mesh, const KOmegaConfig& cfg)
     for (DeviceArray<double>* a : {&production_, &wDestruction_, &wProduction_, &kSink_, &prevK_, &prevW_}) a->resize(N);
     keq_ = std::make_unique<DeviceEquation>(k_, cfg.k_options);
     weq_ = std::make_unique<DeviceEquation>(omega_, cfg.omega_options);
+    if (cfg.kind == 2) {
+        wallDist_.resize(N);
+        gradNt_.resize(3 * N);
+    }
+}
+
+void KOmegaModel::setWallDistance(const double* host) {
+    if (cfg_.kind != 2) fail(kState, "a wall distance belongs to the Spalart-Allmaras model");
+    for (int i = 0; i < m_.n_cells; ++i)
+        if (!std::isfinite(host[i])) fail(kNumeric, "wall distance must be finite");
+    wallDist_.upload(host, m_.n_cells, ctx_.stream);
+    wall_set_ = true;
 }
 
 KOmegaModel::~KOmegaModel() = default;
 
 void KOmegaModel::boundOmega() {
     const int N = m_.n_cells;
-    if (cfg_.kind == 1) {  // epsilon = max(epsilon, epsilonMin) (k_epsilon.cpp:118)
+    if (cfg_.kind >= 1) {  // epsilon = max(epsilon, epsilonMin) (k_epsilon.cpp:118), nuTilda likewise (:132-135)
         launch(ctx_, kBoundMin, N, N, cfg_.omega_min, omega_.v.data());
         return;
     }
@@ -290,6 +404,14 @@ void KOmegaModel::boundOmega() {
 
 void KOmegaModel::updateViscosity() {
     const int N = m_.n_cells;
+    if (cfg_.kind == 2) {
+        const SaConstants c = saConstants(cfg_);
+        launch(ctx_, kViscositySA, N, N, c, (const double*)omega_.v.data(), mut_.v.data(), muEff_.v.data());
+        if (m_.n_boundary)
+            launch(ctx_, kTraceSA, m_.n_boundary, view(m_), omega_.bcView(), (const double*)omega_.v.data(), c,
+                   mut_.trace.data(), muEff_.trace.data(), (double*)nullptr);
+        return;
+    }
     if (cfg_.kind == 1) {
         const double crho = cfg_.c_mu * cfg_.rho;
         launch(ctx_, kViscosityKE, N, N, crho, cfg_.mu, cfg_.omega_min, (const double*)k_.v.data(),
@@ -309,6 +431,14 @@ void KOmegaModel::updateViscosity() {
 }
 
 void KOmegaModel::start(const DeviceField& phi) {
+    if (cfg_.kind == 2) {
+        // boundTransportField(); updateViscosity() (spalart_allmaras.cpp:50-56)
+        if (!wall_set_) fail(kState, "the Spalart-Allmaras model needs the wall distance before the fields are set");
+        omega_.setFluxContext(phi);
+        boundOmega();
+        updateViscosity();
+        return;
+    }
     // boundTransportFields() then updateViscosity() (k_omega.cpp:51-56, 130-136)
     k_.setFluxContext(phi);
     omega_.setFluxContext(phi);
@@ -333,6 +463,7 @@ void KOmegaModel::stressRemainderDivergence(DeviceField& U, double* out) {
 }
 
 TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
+    if (cfg_.kind == 2) return solveSpalartAllmaras(U, phi);
     BSG_PROFILE(ctx_, "komega_transport");
     const int N = m_.n_cells, nb = m_.n_boundary;
     TransportResult res;
@@ -414,6 +545,59 @@ TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
     res.change = std::max(dW, dK);
     res.residual = std::max(rW, rK);
     res.healthy = res.healthy && std::isfinite(res.change);
+    return res;
+}
+
+// SpalartAllmaras::solveTransport, steady (spalart_allmaras.cpp:65-122): closure functions at the
+// current iterate, one nuTilda equation (convection, diffusion, implicit destruction, explicit
+// source), relaxation, solve, bounding, viscosity update.
+TransportResult KOmegaModel::solveSpalartAllmaras(DeviceField& U, DeviceField& phi) {
+    BSG_PROFILE(ctx_, "sa_transport");
+    const int N = m_.n_cells, nb = m_.n_boundary;
+    TransportResult res;
+    copyAsync(ctx_, prevW_.data(), omega_.v.data(), N);
+    U.setFluxContext(phi);
+    const SaConstants c = saConstants(cfg_);
+    gradient(U, cfg_.momentum_options.gradient, G_);
+    gradient(omega_, cfg_.omega_options.gradient, gradNt_);
+    launch(ctx_, kCoefficientsSA, N, N, c, (const double*)G_.data(), (const double*)gradNt_.data(),
+           (const double*)omega_.v.data(), (const double*)wallDist_.data(), wDestruction_.data(),
+           wProduction_.data(), wDiff_.v.data());
+    if (nb)
+        launch(ctx_, kTraceSA, nb, view(m_), omega_.bcView(), (const double*)omega_.v.data(), c, (double*)nullptr,
+               (double*)nullptr, wDiff_.trace.data());
+    DeviceEquation& eq = *weq_;
+    eq.reset();
+    addConvection(eq, phi, cfg_.rho, eq.options);
+    addLaplacian(eq, &wDiff_, 0.0, -1.0, eq.options);
+    addReaction(eq, wDestruction_.data(), 0.0, 1.0);
+    addSource(eq, wProduction_.data(), 1.0);
+    relativeResidualNorms(eq, omega_.v.data(), redW_);
+    double* h = ctx_.pinned;
+    BSG_CUDA(cudaMemcpyAsync(h, redW_.result.data(), 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    ctx_.sync();
+    const double r0 = std::sqrt(h[0]) / std::max(std::sqrt(h[1]) + std::sqrt(h[2]), 1e-30);
+    relax(eq, prevW_.data(), cfg_.relaxation);
+    Dcsr<double> A{N, m_.cf_ptr.data(), m_.cf_col.data(), eq.diag.data(), eq.val.data(), 2LL * m_.n_interior};
+    JacobiPreconditioner jac;
+    jac.diag = eq.diag.data();
+    jac.n = N;
+    const SolverConfig& scfg = cfg_.omega_solver;
+    const SolveOutcome o = scfg.solver == 0 ? krylov_.solveScalar(A, scfg, &jac, eq.src.data(), omega_.v.data())
+                                            : krylov_.solveBicgstab(A, scfg, eq.src.data(), omega_.v.data());
+    res.iterations = o.iterations;
+    res.linear_converged = o.status == 0;
+    res.residual = r0;
+    res.healthy = o.status != 2 && std::isfinite(o.final_) && std::isfinite(r0);
+    if (!res.healthy) return res;
+    omega_.setFluxContext(phi);
+    boundOmega();
+    updateViscosity();
+    relativeChangeNorms(ctx_, omega_.v.data(), prevW_.data(), N, redDW_);
+    BSG_CUDA(cudaMemcpyAsync(h, redDW_.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    ctx_.sync();
+    res.change = std::sqrt(h[0]) / std::max(std::sqrt(h[1]), 1e-30);
+    res.healthy = std::isfinite(res.change);
     return res;
 }
 

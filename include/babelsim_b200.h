@@ -349,6 +349,18 @@ typedef struct {
     bsg_solver_config epsilon_solver;
 } bsg_kepsilon_config;
 
+/* Spalart-Allmaras (src/physics/RANS/spalart_allmaras.cpp:23-154): physics keys saCb1, saCb2,
+ * saSigma, saKappa, saCw1 (<= 0: cb1/kappa^2 + (1 + cb2)/sigma), saCw2, saCw3, saCv1, saCt3, saCt4,
+ * saNuTildaMin, saWallDistanceMin; equation control nuTildaTransport. */
+typedef struct {
+    double cb1, cb2, sigma, kappa, cw1, cw2, cw3, cv1, ct3, ct4;
+    double nu_tilda_min, wall_distance_min;
+    double relaxation;
+    double tolerance;
+    bsg_options nu_tilda_transport;
+    bsg_solver_config nu_tilda_solver;
+} bsg_sa_config;
+
 int bsg_simple_create(bsg_mesh* mesh, const bsg_simple_config* config, bsg_simple** out);
 /* Boundary constraint of "U" or "p" on one patch (the case's fields/initial). */
 int bsg_simple_set_boundary(bsg_simple* s, const char* field, int32_t patch, int32_t type,
@@ -369,9 +381,15 @@ int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report*
 int bsg_simple_enable_komega(bsg_simple* s, const bsg_komega_config* config);
 /* turbulenceModel kEpsilon: as above, with "k" and "epsilon". */
 int bsg_simple_enable_kepsilon(bsg_simple* s, const bsg_kepsilon_config* config);
-/* initial k and the second transported field (omega or epsilon) */
+/* turbulenceModel SA: "nuTilda" takes boundary conditions, set_turbulence_fields takes k = NULL and
+ * the initial nuTilda, and the wall distance (n_cells, the reference's wallDistance input field, which
+ * it reads and does not compute) must be given before set_fields. */
+int bsg_simple_enable_spalart_allmaras(bsg_simple* s, const bsg_sa_config* config);
+int bsg_simple_set_wall_distance(bsg_simple* s, const double* wall_distance);
+/* initial k and the second transported field (omega, epsilon, or nuTilda with k = NULL) */
 int bsg_simple_set_turbulence_fields(bsg_simple* s, const double* k, const double* second);
-/* k, the second transported field and the turbulent viscosity mut (n_cells each; NULL skips). */
+/* k, the second transported field and the turbulent viscosity mut (n_cells each; NULL skips;
+ * k must be NULL for the one-equation model). */
 int bsg_simple_get_turbulence_fields(const bsg_simple* s, double* k, double* second, double* mut);
 int bsg_simple_get_fields(const bsg_simple* s, double* U, double* p, double* phi);
 int bsg_simple_destroy(bsg_simple* s);

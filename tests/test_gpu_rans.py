@@ -1,5 +1,5 @@
-"""k-omega and k-epsilon SIMPLE on the GPU vs the reference's own runSimple + KOmega /
-KEpsilon, through the C ABI.
+"""k-omega, k-epsilon and Spalart-Allmaras SIMPLE on the GPU vs the reference's own runSimple +
+KOmega / KEpsilon / SpalartAllmaras, through the C ABI.
 
 Tolerance: 1e-8 relative L2 on U, p, phi, k, omega (epsilon) and mut after every outer
 iteration (every linear solve at rtol 1e-12 on both sides; the transported
@@ -9,7 +9,7 @@ against the reference's Krylov backend at the same tolerance).
 import numpy as np
 import pytest
 
-from helpers import RANS_CASES, Golden, komega_constants, rel_l2
+from helpers import RANS_CASES, SA_CASES, Golden, komega_constants, rel_l2
 from oracle import fvm
 
 pytestmark = pytest.mark.gpu
@@ -78,6 +78,48 @@ def test_komega_simple_every_iteration_matches_reference(ctx, name):
         kk, w, mut = sim.turbulence_fields()
         for key, mine in (("U", U), ("p", p), ("phi", phi), ("k", kk), ("omega", w), ("mut", mut)):
             assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-8, (key, k)
+        assert np.isfinite(r.turbulence_change) and r.turbulence_residual > 0
+    sim.close()
+    m.close()
+
+
+@pytest.mark.parametrize("name", SA_CASES)
+def test_spalart_allmaras_simple_every_iteration_matches_reference(ctx, name):
+    """One-equation model with a given wall distance: U, p, phi, nuTilda and mut after every outer
+    iteration within 1e-8 of the reference (linear solves at rtol 1e-12 on both sides)."""
+    import babelsim_b200 as bsg
+    g = Golden(name)
+    m = bsg.Mesh.from_polyhedral(ctx, g.poly)
+    s = g.settings()
+    ph, sol, meth = g.meta["physics"], g.meta["solution"], g.meta["methods"]
+    sim = bsg.Simple(m, ph["density"], ph["dynamicViscosity"], s.alpha_u, s.alpha_p, s.non_orthogonal_corrections,
+                     s.mass_tolerance, s.velocity_tolerance, s.momentum_tolerance, s.pressure_tolerance,
+                     bsg.options(**s.momentum), bsg.options(**s.pressure),
+                     _solver(bsg, sol, "momentum", "bcgs", "bjacobi", 2000),
+                     _solver(bsg, sol, "pressureCorrection", "cg", "hypre"))
+    sim.enable_spalart_allmaras(ph["saCb1"], ph["saCb2"], ph["saSigma"], ph["saKappa"], 0.0, ph["saCw2"],
+                                ph["saCw3"], ph["saCv1"], ph["saCt3"], ph["saCt4"], ph["saNuTildaMin"],
+                                ph["saWallDistanceMin"], sol["turbulenceRelaxation"], sol["turbulenceTolerance"],
+                                bsg.options(**meth["nuTildaTransport"]),
+                                _solver(bsg, sol, "nuTildaTransport", "bcgs", "bjacobi", 2000))
+    for p, (t, v) in enumerate(g.meta["U_bcs"]):
+        sim.set_boundary("U", p, t, v)
+    for p, (t, v) in enumerate(g.meta["p_bcs"]):
+        sim.set_boundary("p", p, t, v)
+    for p, (t, v) in enumerate(g.meta["nuTilda_bcs"]):
+        sim.set_boundary("nuTilda", p, t, v)
+    n = m.n_cells
+    sim.set_wall_distance(g["wall_distance"])
+    sim.set_turbulence_fields(None, np.full(n, g.meta["nuTilda_internal"]))
+    sim.set_fields(np.zeros((n, 3)), np.zeros(n))
+    for k in range(1, g.K + 1):
+        r = sim.iterate(1)
+        assert r.status != 2 and r.iterations == k
+        U, p, phi = sim.fields()
+        kk, nt, mut = sim.turbulence_fields()
+        assert kk is None
+        for key, mine in (("U", U), ("p", p), ("phi", phi), ("nuTilda", nt), ("mut", mut)):
+            assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-8, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
         assert np.isfinite(r.turbulence_change) and r.turbulence_residual > 0
     sim.close()
     m.close()
