@@ -36,6 +36,9 @@ class PisoSettings:
     start_time: float = 0.0
     end_time: float = 1.0
     delta_t: float = 1e-3
+    turbulence_coupling: str = "iterated"
+    turbulence_max_iterations: int = 1000
+    turbulence_correctors: int | None = None
     momentum: dict = field(default_factory=lambda: dict(
         interpolation="linear", gradient="greenGauss", convection="upwind", diffusion="orthogonal"))
     pressure: dict = field(default_factory=lambda: dict(
@@ -139,8 +142,10 @@ class PisoState:
     history: list = field(default_factory=list)
 
 
-def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None) -> PisoState:
-    """runPiso (piso/main.cpp:60-301) for `steps` time steps (all, to end_time, when None)."""
+def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None, turbulence=None) -> PisoState:
+    """runPiso (piso/main.cpp:60-301) for `steps` time steps (all, to end_time, when None).
+    ``turbulence(geo, phi)`` builds an eddy-viscosity model (oracle.rans), created like rans::load
+    before phi = flux(U), i.e. with a zero face flux."""
     nc = geo.n_cells
     U = fvm.Field(geo, np.zeros((nc, 3)) if U0 is None else U0, U_bcs)
     p = fvm.Field(geo, np.zeros(nc) if p0 is None else p0, p_bcs)
@@ -149,6 +154,12 @@ def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None) -
     max_correctors = s.correctors if s.max_correctors is None else s.max_correctors
     V = geo.volume
     mu_field = fvm.Field(geo, np.full(nc, s.mu), [(fvm.ZERO_GRADIENT, 0.0)] * len(U_bcs))
+    model = turbulence(geo, np.zeros(geo.n_faces)) if turbulence is not None else None
+    segregated = s.turbulence_coupling == "segregated"
+    if model is not None:
+        model.set_transient(s.time)
+    t_corrections = s.turbulence_correctors or (
+        s.turbulence_max_iterations if model is not None and s.max_iterations == 1 and not segregated else 1)
     phi = fvm.flux(U, p_opts["interpolation"], p_opts["gradient"])
     U_old = History(U.copy())
     phi_old = History(phi.copy())
@@ -162,6 +173,8 @@ def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None) -
         step += 1
         U_old.save(U.copy(), dt)
         phi_old.save(phi.copy(), dt)
+        if model is not None:
+            model.save_old(dt)
         temporal = s.rho * temporal_flux_correction(U_old, phi_old, s.time, p_opts)
         converged = False
         for _ in range(s.max_iterations):
@@ -169,9 +182,11 @@ def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None) -
             mom = fvm.Equation(U, m_opts, {})
             eq_ddt(mom, s.rho, U_old, s.time)
             fvm.eq_div(mom, phi, s.rho)
-            fvm.eq_laplacian(mom, mu_field, -1.0)
+            fvm.eq_laplacian(mom, model.effective_viscosity() if model is not None else mu_field, -1.0)
             grad_p = fvm.gradient(p, p_opts["gradient"])
             fvm.eq_source(mom, -grad_p)
+            if model is not None:
+                fvm.eq_source(mom, model.stress_remainder_divergence(U))
             rU = fvm.relative_residual(mom.ldu, U.v)
             fvm.eq_relax(mom, U_prev, s.alpha_u)
             aP = mom.ldu.diag.copy()
@@ -211,18 +226,34 @@ def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None) -
                 used = corrector + 1
                 if used >= s.correctors and coupling <= s.coupling_tolerance:
                     break
+            t_ok, t_corr, dT, rT = True, 0, 0.0, 0.0
+            if model is not None:
+                # turbulence correctors at this time level (piso/main.cpp:239-254)
+                for _ in range(t_corrections):
+                    r = model.solve_transport(U, phi)
+                    dT, rT = r["d"], r["r"]
+                    t_corr += 1
+                    t_ok = dT <= model.c.tolerance and rT <= model.c.tolerance
+                    if t_ok:
+                        break
             dU = fvm.relative_change(U.v, U_prev)
             mass = fvm.flux_balance(geo, phi)["relative"]
             accepted = mass <= s.mass_tolerance and coupling <= s.coupling_tolerance
-            settled = rU <= s.momentum_tolerance and dU <= s.velocity_tolerance and dP <= s.pressure_tolerance
-            converged = accepted and (s.max_iterations == 1 or settled)
-            state.history.append(dict(step=step, rU=rU, dU=dU, dP=dP, mass=mass, coupling=coupling, correctors=used))
+            settled = (rU <= s.momentum_tolerance and dU <= s.velocity_tolerance and dP <= s.pressure_tolerance
+                       and t_ok)
+            converged = accepted and ((segregated or t_ok) if s.max_iterations == 1 else settled)
+            state.history.append(dict(step=step, rU=rU, dU=dU, dP=dP, mass=mass, coupling=coupling, correctors=used,
+                                      dTurb=dT, rTurb=rT, turbulence_corrections=t_corr))
             if not accepted:
                 state.status = "notConverged"
                 break
             if converged:
                 break
         state.U, state.p, state.phi, state.time, state.steps = U.v, p.v, phi, t, step
+        if model is not None:
+            state.mut = model.mut_v
+            for name, f in model.transported().items():
+                setattr(state, name, f.v)
         if not converged:
             state.status = "notConverged"
             return state

@@ -147,6 +147,25 @@ class KOmega:
         """The model's transported fields by state name (the second one is stored as omega)."""
         return {"k": self.k, "omega": self.omega}
 
+    # Transient use (runPiso): time::history of each transported field, saved once per
+    # physical step (saveOld), and equ::ddt(equation, rho, history) ahead of convection.
+    time_method = None
+    hist = None
+
+    def set_transient(self, method):
+        from .piso import History
+        self.time_method = method
+        self.hist = {name: History(f.copy()) for name, f in self.transported().items()}
+
+    def save_old(self, dt):
+        for name, f in self.transported().items():
+            self.hist[name].save(f.copy(), dt)
+
+    def _ddt(self, eq, name):
+        if self.hist is not None:
+            from .piso import eq_ddt
+            eq_ddt(eq, self.rho, self.hist[name], self.time_method)
+
     def stress_remainder_divergence(self, U: fvm.Field):
         """math::div(muEff (grad(U)^T - 2/3 tr(grad U) I)) (model.cpp:65-69, operators.cpp:1568-1591)."""
         G = fvm.gradient(U, self.mom_opts["gradient"])
@@ -178,6 +197,7 @@ class KOmega:
         w_production = ((c.gamma * production) * self.omega.v) / np.maximum(self.k.v, c.k_min)
         # omega first
         weq = fvm.Equation(self.omega, self.omega_opts, {})
+        self._ddt(weq, "omega")
         fvm.eq_div(weq, phi, rho)
         fvm.eq_laplacian(weq, w_diff, -1.0)
         weq.ldu.diag = weq.ldu.diag + (1.0 * w_destruction) * geo.volume
@@ -188,6 +208,7 @@ class KOmega:
         self.bound_omega()
         # then k, with the new omega in its sink
         keq = fvm.Equation(self.k, self.k_opts, {})
+        self._ddt(keq, "k")
         fvm.eq_div(keq, phi, rho)
         fvm.eq_laplacian(keq, k_diff, -1.0)
         keq.ldu.diag = keq.ldu.diag + (1.0 * ((c.beta_star * rho) * self.omega.v)) * geo.volume
@@ -269,6 +290,7 @@ class KEpsilon(KOmega):
         e_destruction = (c.c2 * rho) * eok
         e_production = (c.c1 * production) * eok
         keq = fvm.Equation(self.k, self.k_opts, {})
+        self._ddt(keq, "k")
         fvm.eq_div(keq, phi, rho)
         fvm.eq_laplacian(keq, k_diff, -1.0)
         keq.ldu.diag = keq.ldu.diag + (1.0 * k_destruction) * geo.volume
@@ -277,6 +299,7 @@ class KEpsilon(KOmega):
         fvm.eq_relax(keq, prev_k, c.relaxation)
         self.k.v = _solve(keq.ldu.matrix(), keq.ldu.source)
         eeq = fvm.Equation(self.eps, self.eps_opts, {})
+        self._ddt(eeq, "omega")
         fvm.eq_div(eeq, phi, rho)
         fvm.eq_laplacian(eeq, e_diff, -1.0)
         eeq.ldu.diag = eeq.ldu.diag + (1.0 * e_destruction) * geo.volume
@@ -394,6 +417,7 @@ class SpalartAllmaras(KOmega):
         tr = self._trace(self.nt)
         diff = fvm.Field(geo, (mu + rho * nt) / c.sigma, None, trace=(mu + rho * tr) / c.sigma)
         eq = fvm.Equation(self.nt, self.nt_opts, {})
+        self._ddt(eq, "nuTilda")
         fvm.eq_div(eq, phi, rho)
         fvm.eq_laplacian(eq, diff, -1.0)
         eq.ldu.diag = eq.ldu.diag + (1.0 * implicit) * geo.volume

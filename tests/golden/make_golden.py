@@ -171,10 +171,13 @@ def methods(conv="upwind", grad="greenGauss", diff="orthogonal"):
     return {"momentum": o, "pressureCorrection": o}
 
 
-def make_piso(name, mesh, U_bcs, p_bcs, methods, solution, physics, time, start, dt, ends):
-    """Transient fixture: the reference's runPiso to each end time in `ends` (one run per step)."""
+def make_piso(name, mesh, U_bcs, p_bcs, methods, solution, physics, time, start, dt, ends, extra_fields=(),
+              internal=None, files=None, turbulence_keys=(), extra_meta=None, arrays=None):
+    """Transient fixture: the reference's runPiso to each end time in `ends` (one run per step).  With a
+    turbulence model: `extra_fields` / `internal` / `files` give its input fields and `turbulence_keys`
+    the fields stored after each step."""
     work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
-    data = {}
+    data = dict(arrays or {})
     offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
     data["mesh_vertices"] = mesh.vertices
     data["mesh_offsets"] = offsets
@@ -182,18 +185,24 @@ def make_piso(name, mesh, U_bcs, p_bcs, methods, solution, physics, time, start,
     data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
     for k, end in enumerate(ends, start=1):
         write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics, solver="piso", time=time,
-                   control=(start, end, dt))
+                   control=(start, end, dt), extra_fields=extra_fields, internal=internal)
+        for fname, text in (files or {}).items():
+            with open(os.path.join(work, "fields", "initial", fname), "w") as f:
+                f.write(text)
         fields, geo, info, _ = run(work, solution.get("maxIterations", 1))
         if info["status"] != 0:
             raise RuntimeError(f"{name}: reference PISO did not complete step {k}: {info}")
         data[f"U_{k}"] = fields["U"].reshape(-1, 3)
         data[f"p_{k}"] = fields["p"]
         data[f"phi_{k}"] = fields["phi"]
+        for key in turbulence_keys:
+            data[f"{key}_{k}"] = fields[key]
     for key, arr in geo.items():
         data["geo_" + key] = arr
     meta = dict(patch_names=mesh.patch_names, patch_kinds=mesh.patch_kinds, U_bcs=[(t, list(map(float, v)))
                 for t, v in U_bcs], p_bcs=[(t, float(v)) for t, v in p_bcs], methods=methods,
                 solution=solution, physics=physics, K=len(ends), time=time, start=start, dt=dt, ends=list(ends))
+    meta.update(extra_meta or {})
     data["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **data)
     shutil.rmtree(work)
@@ -393,6 +402,54 @@ def main_piso():
               {"density": 1.0, "dynamicViscosity": 0.01}, "bdf2", 0.0, 0.05, [0.05, 0.1, 0.15])
 
 
+def main_piso_rans():
+    """runPiso with a turbulence model (rans::load inside piso/main.cpp:98-121, transport after the
+    correctors at every time level, 239-254): k-omega on the channel with BDF2, Spalart-Allmaras with Euler."""
+    ch = meshgen.hex_box(16, 8, 1, hi=(4.0, 1.0, 0.25),
+                         names=["inlet", "outlet", "lower", "upper", "front", "back"],
+                         kinds=["inlet", "outlet", "wall", "wall", "symmetry", "symmetry"])
+    U = [("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0)), ("fixedValue", (0.0, 0.0, 0.0)),
+         ("fixedValue", (0.0, 0.0, 0.0)), ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    p = [("zeroGradient", 0.0), ("fixedValue", 0.0), ("zeroGradient", 0.0), ("zeroGradient", 0.0),
+         ("symmetry", 0.0), ("symmetry", 0.0)]
+    turb_sol = {"turbulenceRelaxation": 0.7, "turbulenceTolerance": 1e-6, "turbulenceMaxIterations": 400}
+
+    def eq_controls(eq):
+        return {f"equation.{eq}.kspType": "bcgs", f"equation.{eq}.pcType": "bjacobi",
+                f"equation.{eq}.absoluteTolerance": 1e-18, f"equation.{eq}.relativeTolerance": 1e-12,
+                f"equation.{eq}.maxIterations": 2000}
+    # k-omega, BDF2
+    komega = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "kOmega", "kOmegaBetaStar": 0.09,
+              "kOmegaBeta": 0.075, "kOmegaGamma": 5.0 / 9.0, "kOmegaSigmaK": 0.5, "kOmegaSigmaOmega": 0.5,
+              "kMin": 1e-12, "omegaMin": 1e-10, "maxTurbulentViscosityRatio": 1e5}
+    kb = [("fixedValue", 3.75e-3), ("zeroGradient", 0.0), ("fixedValue", 1e-12), ("fixedValue", 1e-12),
+          ("symmetry", 0.0), ("symmetry", 0.0)]
+    wb = [("fixedValue", 2.0), ("zeroGradient", 0.0), ("fixedValue", 800.0), ("fixedValue", 800.0),
+          ("symmetry", 0.0), ("symmetry", 0.0)]
+    sol = dict(piso_solution(2, 1), **turb_sol, **eq_controls("kTransport"), **eq_controls("omegaTransport"))
+    m = rans_methods("linearUpwind")
+    make_piso("piso_komega_channel", ch, U, p, m, sol, komega, "bdf2", 0.0, 0.05, [0.05, 0.1, 0.15, 0.2],
+              extra_fields=[("k", 3.75e-3, kb), ("omega", 2.0, wb)], turbulence_keys=("k", "omega", "mut"),
+              extra_meta=dict(k_internal=3.75e-3, k_bcs=kb, omega_internal=2.0, omega_bcs=wb, second="omega"))
+    # Spalart-Allmaras, Euler
+    sa = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "SA", "saNuTildaMin": 1e-14,
+          "saWallDistanceMin": 1e-12, "saCb1": 0.1355, "saCb2": 0.622, "saSigma": 2.0 / 3.0, "saKappa": 0.41,
+          "saCw2": 0.3, "saCw3": 2.0, "saCv1": 7.1, "saCt3": 1.2, "saCt4": 0.5}
+    ntb = [("fixedValue", 3e-3), ("zeroGradient", 0.0), ("fixedValue", 0.0), ("fixedValue", 0.0),
+           ("symmetry", 0.0), ("symmetry", 0.0)]
+    y = _cell_centres(ch)[:, 1]
+    d = np.minimum(y, 1.0 - y)
+    o = dict(interpolation="linear", gradient="greenGauss", convection="linearUpwind", diffusion="orthogonal")
+    msa = {"momentum": o, "pressureCorrection": o, "nuTildaTransport": dict(o, convection="upwind")}
+    sol = dict(piso_solution(2, 1), **turb_sol, **eq_controls("nuTildaTransport"))
+    make_piso("piso_sa_channel", ch, U, p, msa, sol, sa, "euler", 0.0, 0.05, [0.05, 0.1, 0.15],
+              extra_fields=[("nuTilda", 3e-3, ntb), ("wallDistance", 0.0, [("zeroGradient", 0.0)] * 6)],
+              internal={"wallDistance": "file wallDistance.data"},
+              files={"wallDistance.data": "".join(f"{i} {v!r}\n" for i, v in enumerate(map(float, d)))},
+              turbulence_keys=("nuTilda", "mut"), arrays={"wall_distance": d},
+              extra_meta=dict(nuTilda_internal=3e-3, nuTilda_bcs=ntb))
+
+
 def main():
     if not os.path.exists(ORACLE):
         sys.exit(f"{ORACLE} missing: run `make -C oracle/ref` first")
@@ -418,8 +475,11 @@ if __name__ == "__main__":
         main_rans()
     elif len(sys.argv) > 1 and sys.argv[1] == "sa":
         main_sa()
+    elif len(sys.argv) > 1 and sys.argv[1] == "piso_rans":
+        main_piso_rans()
     else:
         main()
         main_piso()
         main_rans()
         main_sa()
+        main_piso_rans()

@@ -9,9 +9,9 @@ solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
 import numpy as np
 import pytest
 
-from helpers import (CASES, PISO_CASES, RANS_CASES, SA_CASES, Golden, kepsilon_factory, komega_factory,
+from helpers import (CASES, PISO_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, Golden, kepsilon_factory, komega_factory,
                      piso_settings, ref_system_groups, rel, rel_l2, sa_factory)
-from oracle import fvm, simple
+from oracle import fvm, piso, simple
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -168,6 +168,22 @@ def test_spalart_allmaras_simple_iterations_match_reference(name):
     for k in range(1, g.K + 1):
         st = simple.run_simple(geo, g.U_bcs(), g.p_bcs(), s, iterations=k, turbulence=sa_factory(g))
         for key, mine in (("U", st.U), ("p", st.p), ("phi", st.phi), ("nuTilda", st.nuTilda), ("mut", st.mut)):
+            assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
+
+
+@pytest.mark.parametrize("name", PISO_RANS_CASES)
+def test_piso_with_turbulence_matches_reference(name):
+    """runPiso with an eddy-viscosity model: transient model histories saved once per step, ddt ahead
+    of convection in the transport equations, transport corrected at each time level until
+    turbulenceTolerance; U, p, phi and the model fields after every step."""
+    g = Golden(name)
+    geo = g.oracle_geometry()
+    model = sa_factory(g) if "_sa_" in name else komega_factory(g)
+    keys = ("nuTilda", "mut") if "_sa_" in name else ("k", "omega", "mut")
+    for k in range(1, g.K + 1):
+        st = piso.run_piso(geo, g.U_bcs(), g.p_bcs(), piso_settings(g, g.meta["ends"][k - 1]), turbulence=model)
+        assert st.status == "completed"
+        for key, mine in [("U", st.U), ("p", st.p), ("phi", st.phi)] + [(key, getattr(st, key)) for key in keys]:
             assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
 
 
