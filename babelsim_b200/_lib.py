@@ -34,7 +34,9 @@ EXPORTS = [
     "bsg_simple_enable_spalart_allmaras", "bsg_simple_set_wall_distance", "bsg_simple_set_turbulence_fields",
     "bsg_simple_get_turbulence_fields", "bsg_simple_get_fields",
     "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
-    "bsg_piso_get_fields", "bsg_piso_destroy",
+    "bsg_piso_get_fields", "bsg_piso_destroy", "bsg_piso_enable_komega", "bsg_piso_enable_kepsilon",
+    "bsg_piso_enable_spalart_allmaras", "bsg_piso_set_wall_distance", "bsg_piso_set_turbulence_fields",
+    "bsg_piso_get_turbulence_fields",
 ]
 
 
@@ -109,7 +111,13 @@ class PisoReport(C.Structure):
     _fields_ = [("steps", C.c_int32), ("time", C.c_double), ("status", C.c_int32), ("accepted", C.c_int32),
                 ("mass", C.c_double), ("dU", C.c_double), ("rU", C.c_double), ("dP", C.c_double),
                 ("coupling", C.c_double), ("courant_max", C.c_double), ("courant_mean", C.c_double),
-                ("correctors", C.c_int32), ("momentum_iterations", C.c_int32), ("pressure_iterations", C.c_int32)]
+                ("correctors", C.c_int32), ("momentum_iterations", C.c_int32), ("pressure_iterations", C.c_int32),
+                ("turbulence_change", C.c_double), ("turbulence_residual", C.c_double),
+                ("turbulence_corrections", C.c_int32)]
+
+
+class PisoTurbulenceControls(C.Structure):
+    _fields_ = [("coupling", C.c_int32), ("max_iterations", C.c_int32), ("correctors", C.c_int32)]
 
 
 class KEpsilonConfig(C.Structure):
@@ -182,6 +190,11 @@ def lib():
             "bsg_piso_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_piso_set_fields": [vp, vp, vp],
             "bsg_piso_advance": [vp, i32, C.POINTER(PisoReport)], "bsg_piso_get_fields": [vp, vp, vp, vp],
             "bsg_piso_destroy": [vp],
+            "bsg_piso_enable_komega": [vp, C.POINTER(KOmegaConfig), C.POINTER(PisoTurbulenceControls)],
+            "bsg_piso_enable_kepsilon": [vp, C.POINTER(KEpsilonConfig), C.POINTER(PisoTurbulenceControls)],
+            "bsg_piso_enable_spalart_allmaras": [vp, C.POINTER(SaConfig), C.POINTER(PisoTurbulenceControls)],
+            "bsg_piso_set_wall_distance": [vp, vp], "bsg_piso_set_turbulence_fields": [vp, vp, vp],
+            "bsg_piso_get_turbulence_fields": [vp, vp, vp, vp],
         }
         for name in EXPORTS:
             fn = getattr(L, name)

@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (KEpsilonConfig, KOmegaConfig, SaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
+from ._lib import (KEpsilonConfig, KOmegaConfig, PisoTurbulenceControls, SaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
                    check, f64, i32, lib, ptr)
 
 BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
@@ -334,8 +334,71 @@ def solve_ldu(mesh: Mesh, cfg: SolverConfig, diag, upper, lower, source, x0=None
     return x, list(res)
 
 
-class Simple:
+class _TurbulenceModels:
+    """rans::load for a flow solver (src/physics/RANS/model.cpp:24-53): k-omega, k-epsilon or
+    Spalart-Allmaras, its boundary conditions, initial fields and outputs.  Subclasses name their C
+    entry-point prefix."""
+    _prefix = ""
+
+    def _fn(self, name):
+        return getattr(lib(), self._prefix + name)
+
+    def _enable(self, model, cfg):
+        check(self._fn("enable_" + model)(self.h, C.byref(cfg)), self.mesh.ctx.h)
+
+    def enable_komega(self, beta_star=0.09, beta=0.075, gamma=5.0 / 9.0, sigma_k=0.5, sigma_omega=0.5, k_min=1e-12,
+                      omega_min=1e-12, max_viscosity_ratio=1e5, relaxation=0.7, tolerance=1e-6, k_transport=None,
+                      omega_transport=None, k_solver=None, omega_solver=None):
+        """turbulenceModel kOmega (before set_fields); k and omega then take boundary conditions."""
+        cfg = KOmegaConfig(beta_star, beta, gamma, sigma_k, sigma_omega, k_min, omega_min, max_viscosity_ratio,
+                           relaxation, tolerance, k_transport or options(), omega_transport or options(),
+                           k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
+                           omega_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
+        self._enable("komega", cfg)
+
+    def enable_kepsilon(self, c_mu=0.09, c1=1.44, c2=1.92, sigma_k=1.0, sigma_epsilon=1.3, k_min=1e-12,
+                        epsilon_min=1e-12, relaxation=0.7, tolerance=1e-6, k_transport=None, epsilon_transport=None,
+                        k_solver=None, epsilon_solver=None):
+        """turbulenceModel kEpsilon (before set_fields); k and epsilon then take boundary conditions."""
+        cfg = KEpsilonConfig(c_mu, c1, c2, sigma_k, sigma_epsilon, k_min, epsilon_min, relaxation, tolerance,
+                             k_transport or options(), epsilon_transport or options(),
+                             k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
+                             epsilon_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
+        self._enable("kepsilon", cfg)
+
+    def enable_spalart_allmaras(self, cb1=0.1355, cb2=0.622, sigma=2.0 / 3.0, kappa=0.41, cw1=0.0, cw2=0.3, cw3=2.0,
+                                cv1=7.1, ct3=1.2, ct4=0.5, nu_tilda_min=1e-14, wall_distance_min=1e-12,
+                                relaxation=0.7, tolerance=1e-6, nu_tilda_transport=None, nu_tilda_solver=None):
+        """turbulenceModel SA (before set_fields); "nuTilda" then takes boundary conditions and the wall
+        distance comes from set_wall_distance.  cw1 <= 0 takes cb1/kappa^2 + (1 + cb2)/sigma."""
+        cfg = SaConfig(cb1, cb2, sigma, kappa, cw1, cw2, cw3, cv1, ct3, ct4, nu_tilda_min, wall_distance_min,
+                       relaxation, tolerance, nu_tilda_transport or options(),
+                       nu_tilda_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
+        self._enable("spalart_allmaras", cfg)
+        self._one_equation = True
+
+    def set_wall_distance(self, d):
+        """The wall distance of every cell (an input of the Spalart-Allmaras model, as in the reference)."""
+        check(self._fn("set_wall_distance")(self.h, ptr(f64(d))), self.mesh.ctx.h)
+
+    def set_turbulence_fields(self, k, second):
+        """Initial k and omega / epsilon; k is None for Spalart-Allmaras, whose field is nuTilda."""
+        kp = None if k is None else ptr(f64(k))
+        check(self._fn("set_turbulence_fields")(self.h, kp, ptr(f64(second))), self.mesh.ctx.h)
+
+    def turbulence_fields(self):
+        """(k, second transported field, mut); k is None for Spalart-Allmaras."""
+        n = self.mesh.n_cells
+        one = getattr(self, "_one_equation", False)
+        k, w, mut = (None if one else np.zeros(n)), np.zeros(n), np.zeros(n)
+        check(self._fn("get_turbulence_fields")(self.h, None if one else ptr(k), ptr(w), ptr(mut)),
+              self.mesh.ctx.h)
+        return k, w, mut
+
+
+class Simple(_TurbulenceModels):
     """Steady SIMPLE on the device (bsg_simple), simple/main.cpp:11-131."""
+    _prefix = "bsg_simple_"
 
     def __init__(self, mesh: Mesh, rho=1.0, mu=0.01, alpha_u=0.7, alpha_p=0.3, non_orthogonal_corrections=1,
                  continuity_tolerance=1e-8, velocity_tolerance=1e-7, momentum_tolerance=1e-6,
@@ -374,55 +437,6 @@ class Simple:
         check(lib().bsg_simple_iterate(self.h, max_iterations, C.byref(r)), self.mesh.ctx.h)
         return r
 
-    def enable_komega(self, beta_star=0.09, beta=0.075, gamma=5.0 / 9.0, sigma_k=0.5, sigma_omega=0.5, k_min=1e-12,
-                      omega_min=1e-12, max_viscosity_ratio=1e5, relaxation=0.7, tolerance=1e-6, k_transport=None,
-                      omega_transport=None, k_solver=None, omega_solver=None):
-        """turbulenceModel kOmega (before set_fields); k and omega then take boundary conditions."""
-        cfg = KOmegaConfig(beta_star, beta, gamma, sigma_k, sigma_omega, k_min, omega_min, max_viscosity_ratio,
-                           relaxation, tolerance, k_transport or options(), omega_transport or options(),
-                           k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
-                           omega_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
-        check(lib().bsg_simple_enable_komega(self.h, C.byref(cfg)), self.mesh.ctx.h)
-
-    def enable_kepsilon(self, c_mu=0.09, c1=1.44, c2=1.92, sigma_k=1.0, sigma_epsilon=1.3, k_min=1e-12,
-                        epsilon_min=1e-12, relaxation=0.7, tolerance=1e-6, k_transport=None, epsilon_transport=None,
-                        k_solver=None, epsilon_solver=None):
-        """turbulenceModel kEpsilon (before set_fields); k and epsilon then take boundary conditions."""
-        cfg = KEpsilonConfig(c_mu, c1, c2, sigma_k, sigma_epsilon, k_min, epsilon_min, relaxation, tolerance,
-                             k_transport or options(), epsilon_transport or options(),
-                             k_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000),
-                             epsilon_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
-        check(lib().bsg_simple_enable_kepsilon(self.h, C.byref(cfg)), self.mesh.ctx.h)
-
-    def enable_spalart_allmaras(self, cb1=0.1355, cb2=0.622, sigma=2.0 / 3.0, kappa=0.41, cw1=0.0, cw2=0.3, cw3=2.0,
-                                cv1=7.1, ct3=1.2, ct4=0.5, nu_tilda_min=1e-14, wall_distance_min=1e-12,
-                                relaxation=0.7, tolerance=1e-6, nu_tilda_transport=None, nu_tilda_solver=None):
-        """turbulenceModel SA (before set_fields); "nuTilda" then takes boundary conditions and the wall
-        distance comes from set_wall_distance.  cw1 <= 0 takes cb1/kappa^2 + (1 + cb2)/sigma."""
-        cfg = SaConfig(cb1, cb2, sigma, kappa, cw1, cw2, cw3, cv1, ct3, ct4, nu_tilda_min, wall_distance_min,
-                       relaxation, tolerance, nu_tilda_transport or options(),
-                       nu_tilda_solver or solver_config("bcgs", "bjacobi", 1e-18, 1e-10, 1000))
-        check(lib().bsg_simple_enable_spalart_allmaras(self.h, C.byref(cfg)), self.mesh.ctx.h)
-        self._one_equation = True
-
-    def set_wall_distance(self, d):
-        """The wall distance of every cell (an input of the Spalart-Allmaras model, as in the reference)."""
-        check(lib().bsg_simple_set_wall_distance(self.h, ptr(f64(d))), self.mesh.ctx.h)
-
-    def set_turbulence_fields(self, k, second):
-        """Initial k and omega / epsilon; k is None for Spalart-Allmaras, whose field is nuTilda."""
-        kp = None if k is None else ptr(f64(k))
-        check(lib().bsg_simple_set_turbulence_fields(self.h, kp, ptr(f64(second))), self.mesh.ctx.h)
-
-    def turbulence_fields(self):
-        """(k, second transported field, mut); k is None for Spalart-Allmaras."""
-        n = self.mesh.n_cells
-        one = getattr(self, "_one_equation", False)
-        k, w, mut = (None if one else np.zeros(n)), np.zeros(n), np.zeros(n)
-        check(lib().bsg_simple_get_turbulence_fields(self.h, None if one else ptr(k), ptr(w), ptr(mut)),
-              self.mesh.ctx.h)
-        return k, w, mut
-
     def fields(self):
         m = self.mesh
         U, p, phi = np.zeros((m.n_cells, 3)), np.zeros(m.n_cells), np.zeros(m.n_faces)
@@ -435,8 +449,20 @@ class Simple:
             self.h = None
 
 
-class Piso:
-    """Transient PISO on the device (bsg_piso), piso/main.cpp:60-301."""
+class Piso(_TurbulenceModels):
+    """Transient PISO on the device (bsg_piso), piso/main.cpp:60-301.  A turbulence model is enabled
+    with enable_komega / enable_kepsilon / enable_spalart_allmaras after set_turbulence_controls
+    (runPiso's turbulenceCoupling, turbulenceMaxIterations, turbulenceCorrectors)."""
+    _prefix = "bsg_piso_"
+    _controls = None
+
+    def set_turbulence_controls(self, coupling="iterated", max_iterations=1000, correctors=0):
+        self._controls = PisoTurbulenceControls({"iterated": 0, "segregated": 1}[coupling], max_iterations,
+                                                correctors)
+
+    def _enable(self, model, cfg):
+        ctl = self._controls or PisoTurbulenceControls(0, 1000, 0)
+        check(self._fn("enable_" + model)(self.h, C.byref(cfg), C.byref(ctl)), self.mesh.ctx.h)
 
     def __init__(self, mesh: Mesh, rho=1.0, mu=0.01, alpha_u=1.0, max_iterations=1, correctors=2,
                  max_correctors=None, coupling_tolerance=None, non_orthogonal_corrections=1,

@@ -918,72 +918,86 @@ int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report*
     });
 }
 
+namespace {
+bsg::KOmegaConfig komegaConfigOf(const bsg_komega_config* c) {
+    bsg::KOmegaConfig k;
+    k.beta_star = c->beta_star;
+    k.beta = c->beta;
+    k.gamma = c->gamma;
+    k.sigma_k = c->sigma_k;
+    k.sigma_omega = c->sigma_omega;
+    k.k_min = c->k_min;
+    k.omega_min = c->omega_min;
+    k.viscosity_ratio_max = c->max_viscosity_ratio;
+    k.relaxation = c->relaxation;
+    k.tolerance = c->tolerance;
+    k.k_options = options(&c->k_transport);
+    k.omega_options = options(&c->omega_transport);
+    k.k_solver = solverConfig(&c->k_solver);
+    k.omega_solver = solverConfig(&c->omega_solver);
+    return k;
+}
+
+bsg::KOmegaConfig kepsilonConfigOf(const bsg_kepsilon_config* c) {
+    bsg::KOmegaConfig k;
+    k.kind = 1;
+    k.c_mu = c->c_mu;
+    k.c1 = c->c1;
+    k.c2 = c->c2;
+    k.sigma_k = c->sigma_k;
+    k.sigma_omega = c->sigma_epsilon;
+    k.k_min = c->k_min;
+    k.omega_min = c->epsilon_min;
+    k.relaxation = c->relaxation;
+    k.tolerance = c->tolerance;
+    k.k_options = options(&c->k_transport);
+    k.omega_options = options(&c->epsilon_transport);
+    k.k_solver = solverConfig(&c->k_solver);
+    k.omega_solver = solverConfig(&c->epsilon_solver);
+    return k;
+}
+
+bsg::KOmegaConfig saConfigOf(const bsg_sa_config* c) {
+    bsg::KOmegaConfig k;
+    k.kind = 2;
+    k.sa_cb1 = c->cb1;
+    k.sa_cb2 = c->cb2;
+    k.sa_sigma = c->sigma;
+    k.sa_kappa = c->kappa;
+    k.sa_cw1 = c->cw1;
+    k.sa_cw2 = c->cw2;
+    k.sa_cw3 = c->cw3;
+    k.sa_cv1 = c->cv1;
+    k.sa_ct3 = c->ct3;
+    k.sa_ct4 = c->ct4;
+    k.omega_min = c->nu_tilda_min;
+    k.wall_distance_min = c->wall_distance_min;
+    k.relaxation = c->relaxation;
+    k.tolerance = c->tolerance;
+    k.omega_options = options(&c->nu_tilda_transport);
+    k.omega_solver = solverConfig(&c->nu_tilda_solver);
+    return k;
+}
+}  // namespace
+
 int bsg_simple_enable_komega(bsg_simple* s, const bsg_komega_config* c) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && c, "null argument");
-        bsg::KOmegaConfig k;
-        k.beta_star = c->beta_star;
-        k.beta = c->beta;
-        k.gamma = c->gamma;
-        k.sigma_k = c->sigma_k;
-        k.sigma_omega = c->sigma_omega;
-        k.k_min = c->k_min;
-        k.omega_min = c->omega_min;
-        k.viscosity_ratio_max = c->max_viscosity_ratio;
-        k.relaxation = c->relaxation;
-        k.tolerance = c->tolerance;
-        k.k_options = options(&c->k_transport);
-        k.omega_options = options(&c->omega_transport);
-        k.k_solver = solverConfig(&c->k_solver);
-        k.omega_solver = solverConfig(&c->omega_solver);
-        s->solver->enableKOmega(k);
+        s->solver->enableKOmega(komegaConfigOf(c));
     });
 }
 
 int bsg_simple_enable_kepsilon(bsg_simple* s, const bsg_kepsilon_config* c) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && c, "null argument");
-        bsg::KOmegaConfig k;
-        k.kind = 1;
-        k.c_mu = c->c_mu;
-        k.c1 = c->c1;
-        k.c2 = c->c2;
-        k.sigma_k = c->sigma_k;
-        k.sigma_omega = c->sigma_epsilon;
-        k.k_min = c->k_min;
-        k.omega_min = c->epsilon_min;
-        k.relaxation = c->relaxation;
-        k.tolerance = c->tolerance;
-        k.k_options = options(&c->k_transport);
-        k.omega_options = options(&c->epsilon_transport);
-        k.k_solver = solverConfig(&c->k_solver);
-        k.omega_solver = solverConfig(&c->epsilon_solver);
-        s->solver->enableKOmega(k);
+        s->solver->enableKOmega(kepsilonConfigOf(c));
     });
 }
 
 int bsg_simple_enable_spalart_allmaras(bsg_simple* s, const bsg_sa_config* c) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && c, "null argument");
-        bsg::KOmegaConfig k;
-        k.kind = 2;
-        k.sa_cb1 = c->cb1;
-        k.sa_cb2 = c->cb2;
-        k.sa_sigma = c->sigma;
-        k.sa_kappa = c->kappa;
-        k.sa_cw1 = c->cw1;
-        k.sa_cw2 = c->cw2;
-        k.sa_cw3 = c->cw3;
-        k.sa_cv1 = c->cv1;
-        k.sa_ct3 = c->ct3;
-        k.sa_ct4 = c->ct4;
-        k.omega_min = c->nu_tilda_min;
-        k.wall_distance_min = c->wall_distance_min;
-        k.relaxation = c->relaxation;
-        k.tolerance = c->tolerance;
-        k.omega_options = options(&c->nu_tilda_transport);
-        k.omega_solver = solverConfig(&c->nu_tilda_solver);
-        s->solver->enableKOmega(k);
+        s->solver->enableKOmega(saConfigOf(c));
     });
 }
 
@@ -1073,9 +1087,80 @@ int bsg_piso_set_boundary(bsg_piso* s, const char* field, int32_t patch, int32_t
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && field, "null argument");
         const std::string n(field);
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        const int kind = t ? t->config().kind : -1;
         if (n == "U") s->solver->U().setBoundary(patch, type, value);
         else if (n == "p") s->solver->p().setBoundary(patch, type, value);
-        else bsg::fail(bsg::kArgument, "PISO boundary field must be U or p");
+        else if (n == "k" && t && kind != 2) t->k().setBoundary(patch, type, value);
+        else if ((n == "omega" && kind == 0) || (n == "epsilon" && kind == 1) || (n == "nuTilda" && kind == 2))
+            t->omega().setBoundary(patch, type, value);
+        else bsg::fail(bsg::kArgument, "PISO boundary field must be U or p, or a field of the turbulence model");
+    });
+}
+
+namespace {
+void enablePisoTurbulence(bsg_piso* s, bsg::KOmegaConfig k, const bsg_piso_turbulence_controls* tc) {
+    bsg::PisoTurbulenceControls c;
+    if (tc) {
+        c.segregated = tc->coupling != 0;
+        c.max_iterations = tc->max_iterations > 0 ? tc->max_iterations : 1000;
+        c.correctors = tc->correctors;
+    }
+    s->solver->enableTurbulence(k, c);
+}
+}  // namespace
+
+int bsg_piso_enable_komega(bsg_piso* s, const bsg_komega_config* c, const bsg_piso_turbulence_controls* tc) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && c, "null argument");
+        enablePisoTurbulence(s, komegaConfigOf(c), tc);
+    });
+}
+
+int bsg_piso_enable_kepsilon(bsg_piso* s, const bsg_kepsilon_config* c, const bsg_piso_turbulence_controls* tc) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && c, "null argument");
+        enablePisoTurbulence(s, kepsilonConfigOf(c), tc);
+    });
+}
+
+int bsg_piso_enable_spalart_allmaras(bsg_piso* s, const bsg_sa_config* c, const bsg_piso_turbulence_controls* tc) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && c, "null argument");
+        enablePisoTurbulence(s, saConfigOf(c), tc);
+    });
+}
+
+int bsg_piso_set_wall_distance(bsg_piso* s, const double* wall_distance) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && wall_distance, "null argument");
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        t->setWallDistance(wall_distance);
+    });
+}
+
+int bsg_piso_set_turbulence_fields(bsg_piso* s, const double* k, const double* second) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && second, "null argument");
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        if (t->config().kind == 2) require(k == nullptr, "the Spalart-Allmaras model has no k");
+        else require(k != nullptr, "null argument");
+        if (k) t->k().uploadExternal(k);
+        t->omega().uploadExternal(second);
+    });
+}
+
+int bsg_piso_get_turbulence_fields(const bsg_piso* s, double* k, double* second, double* mut) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s != nullptr, "null argument");
+        bsg::KOmegaModel* t = s->solver->turbulence();
+        if (!t) bsg::fail(bsg::kState, "no turbulence model is enabled");
+        if (k && t->config().kind == 2) bsg::fail(bsg::kArgument, "the Spalart-Allmaras model has no k");
+        if (k) t->k().downloadExternal(k);
+        if (second) t->omega().downloadExternal(second);
+        if (mut) t->turbulentViscosity().downloadExternal(mut);
     });
 }
 
@@ -1107,6 +1192,9 @@ int bsg_piso_advance(bsg_piso* s, int32_t steps, bsg_piso_report* report) {
             report->correctors = r.correctors;
             report->momentum_iterations = r.momentum_iterations;
             report->pressure_iterations = r.pressure_iterations;
+            report->turbulence_change = r.turbulence_change;
+            report->turbulence_residual = r.turbulence_residual;
+            report->turbulence_corrections = r.turbulence_corrections;
         }
     });
 }

@@ -178,7 +178,33 @@ PisoSolver::PisoSolver(DeviceMesh& mesh, const PisoConfig& cfg)
 
 PisoSolver::~PisoSolver() = default;
 
+void PisoSolver::enableTurbulence(const KOmegaConfig& cfg, const PisoTurbulenceControls& controls) {
+    if (started_) fail(kState, "the turbulence model must be chosen before the fields are set");
+    if (controls.segregated && cfg_.max_iterations != 1)
+        fail(kArgument, "segregated turbulence requires one PISO momentum pass");
+    if (controls.segregated && cfg.relaxation != 1.0)
+        fail(kArgument, "single-pass transient turbulence requires turbulenceRelaxation 1");
+    if (controls.max_iterations < 1) fail(kArgument, "turbulenceMaxIterations must be at least 1");
+    if (controls.segregated && controls.correctors > 1)
+        fail(kArgument, "segregated turbulence requires one transport correction");
+    if (controls.correctors > controls.max_iterations)
+        fail(kArgument, "turbulenceCorrectors must not exceed turbulenceMaxIterations");
+    KOmegaConfig c = cfg;
+    c.rho = cfg_.rho;
+    c.mu = cfg_.mu;
+    c.momentum_options = cfg_.momentum;
+    turb_ = std::make_unique<KOmegaModel>(m_, c);
+    turb_->setTransient(cfg_.time_method);
+    tctl_ = controls;
+    divStress_.resize(3 * static_cast<std::size_t>(m_.n_cells));
+}
+
 void PisoSolver::start() {
+    if (turb_) {
+        // rans::load runs while phi is still the zero face field it was created as (piso/main.cpp:62, 98)
+        phi_.v.zero(ctx_.stream);
+        turb_->start(phi_);
+    }
     faceFlux(U_, cfg_.pressure.interpolation, cfg_.pressure.gradient, phi_);  // piso/main.cpp:122
     // time::history(U), time::history(phi): both levels start as copies (history.h:8)
     for (DeviceField* h : {&Uprev_lvl_, &Uolder_lvl_}) {
@@ -239,6 +265,7 @@ bool PisoSolver::step() {
     time_ = next;
     ++step_;
     saveHistory(dt);
+    if (turb_) turb_->saveOld(dt);
     // rho * temporalFluxCorrection(U_old, phi_old) (piso/main.cpp:164-165)
     {
         BSG_PROFILE(ctx_, "piso_temporal_flux");
@@ -276,9 +303,14 @@ bool PisoSolver::step() {
             mom.reset();
             addTimeTerm(mom, nullptr, cfg_.rho, Uprev_lvl_.v.data(), Uolder_lvl_.v.data(), tw);
             addConvection(mom, phi_, cfg_.rho, cfg_.momentum);
-            addLaplacian(mom, &muEff_, 0.0, -1.0, cfg_.momentum);
+            addLaplacian(mom, turb_ ? &turb_->effectiveViscosity() : &muEff_, 0.0, -1.0, cfg_.momentum);
             gradient(p_, cfg_.pressure.gradient, gradP_);
             addSource(mom, gradP_.data(), -1.0);
+            if (turb_) {
+                // explicit remainder of the eddy-viscosity stress (piso/main.cpp:178-180)
+                turb_->stressRemainderDivergence(U_, divStress_.data());
+                addSource(mom, divStress_.data(), 1.0);
+            }
         }
         relativeResidualNorms(mom, U_.v.data(), redR_);
         relax(mom, Uiter_.data(), cfg_.alpha_u);
@@ -368,6 +400,27 @@ bool PisoSolver::step() {
         }
         report_.pressure_iterations = p_iters;
         report_.correctors = used;
+        // turbulence correctors at this time level (piso/main.cpp:239-254)
+        bool turb_converged = true, turb_linear = true;
+        report_.turbulence_corrections = 0;
+        if (turb_) {
+            const int corrections = tctl_.correctors > 0 ? tctl_.correctors
+                                    : (cfg_.max_iterations == 1 && !tctl_.segregated ? tctl_.max_iterations : 1);
+            for (int c = 0; c < corrections; ++c) {
+                const TransportResult tr = turb_->solveTransport(U_, phi_);
+                ++report_.turbulence_corrections;
+                report_.turbulence_change = tr.change;
+                report_.turbulence_residual = tr.residual;
+                if (!(tr.healthy && std::isfinite(tr.change) && std::isfinite(tr.residual))) {
+                    report_.status = 2;
+                    return false;
+                }
+                turb_linear = tr.linear_converged;
+                turb_converged = turb_linear && tr.change <= turb_->config().tolerance &&
+                                 tr.residual <= turb_->config().tolerance;
+                if (!turb_linear || turb_converged) break;
+            }
+        }
         // diagnostics (piso/main.cpp:266-281)
         relativeChangeNorms(ctx_, U_.v.data(), Uiter_.data(), 3LL * N, redU_);
         fluxBalance(m_, phi_.v.data(), redM_);
@@ -399,11 +452,11 @@ bool PisoSolver::step() {
             report_.status = 2;
             return false;
         }
-        const bool linear_ok = mom_ok && p_ok;
+        const bool linear_ok = mom_ok && p_ok && turb_linear;
         const bool accepted = linear_ok && mass <= cfg_.mass_tolerance && coupling <= cfg_.coupling_tolerance;
         const bool settled = rU <= cfg_.momentum_tolerance && dU <= cfg_.velocity_tolerance &&
-                             dP <= cfg_.pressure_tolerance;
-        converged = accepted && (cfg_.max_iterations == 1 || settled);
+                             dP <= cfg_.pressure_tolerance && turb_converged;
+        converged = accepted && (cfg_.max_iterations == 1 ? (tctl_.segregated || turb_converged) : settled);
         report_.accepted = accepted;
         if (!accepted) { report_.status = 1; return false; }
         if (converged) break;

@@ -3,6 +3,7 @@
 
 #include "fvm.h"
 #include "linalg.h"
+#include "rans.h"
 
 #include <memory>
 
@@ -21,6 +22,14 @@ struct PisoConfig {
     SolverConfig momentum_solver, pressure_solver;
 };
 
+// runPiso's turbulence controls (piso/main.cpp:99-120).
+struct PisoTurbulenceControls {
+    bool segregated = false;        // turbulenceCoupling segregated (else iterated)
+    int max_iterations = 1000;      // turbulenceMaxIterations
+    int correctors = 0;             // turbulenceCorrectors; <= 0: max_iterations with one PISO pass and
+                                    // iterated coupling, else 1
+};
+
 struct PisoReport {
     int steps = 0;
     double time = 0.0;
@@ -28,6 +37,8 @@ struct PisoReport {
     bool accepted = true;
     double mass = 0, dU = 0, rU = 0, dP = 0, coupling = 0, courant_max = 0, courant_mean = 0;
     int correctors = 0, momentum_iterations = 0, pressure_iterations = 0;
+    double turbulence_change = 0, turbulence_residual = 0;
+    int turbulence_corrections = 0;
 };
 
 class PisoSolver {
@@ -37,6 +48,9 @@ public:
     DeviceField& U() { return U_; }
     DeviceField& p() { return p_; }
     DeviceField& phi() { return phi_; }
+    // rans::load (piso/main.cpp:98-121): an eddy-viscosity model; call before start().
+    void enableTurbulence(const KOmegaConfig& cfg, const PisoTurbulenceControls& controls);
+    KOmegaModel* turbulence() { return turb_.get(); }
     // Initial state: phi = flux(U) with the pressure options (piso/main.cpp:122).
     void start();
     // Advance up to `steps` time steps (fewer at the end time or on a rejected step).
@@ -64,6 +78,9 @@ private:
     DeviceArray<int> flags_;
     PisoReport report_;
     bool started_ = false;
+    std::unique_ptr<KOmegaModel> turb_;
+    PisoTurbulenceControls tctl_;
+    DeviceArray<double> divStress_;
 };
 
 }  // namespace bsg

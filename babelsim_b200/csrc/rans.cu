@@ -382,6 +382,38 @@ KOmegaModel::KOmegaModel(DeviceMesh& mesh, const KOmegaConfig& cfg)
     }
 }
 
+void KOmegaModel::setTransient(int method) {
+    if (method != 1 && method != 2) fail(kArgument, "transient turbulence needs the Euler or BDF2 time scheme");
+    time_method_ = method;
+    const std::size_t N = m_.n_cells;
+    for (DeviceArray<double>* a : {&wPrevLvl_, &wOlderLvl_}) { a->resize(N); a->zero(ctx_.stream); }
+    if (cfg_.kind != 2)
+        for (DeviceArray<double>* a : {&kPrevLvl_, &kOlderLvl_}) { a->resize(N); a->zero(ctx_.stream); }
+    tdt_ = tprev_dt_ = 0.0;
+    tlevels_ = 0;
+}
+
+void KOmegaModel::saveOld(double dt) {
+    // History::save for each transported field (k_omega.cpp:58-62, k_epsilon.cpp:57-60, spalart_allmaras.cpp:61-63)
+    const int N = m_.n_cells;
+    copyAsync(ctx_, wOlderLvl_.data(), wPrevLvl_.data(), N);
+    copyAsync(ctx_, wPrevLvl_.data(), omega_.v.data(), N);
+    if (cfg_.kind != 2) {
+        copyAsync(ctx_, kOlderLvl_.data(), kPrevLvl_.data(), N);
+        copyAsync(ctx_, kPrevLvl_.data(), k_.v.data(), N);
+    }
+    tprev_dt_ = tdt_;
+    tdt_ = dt;
+    ++tlevels_;
+}
+
+void KOmegaModel::timeTerm(DeviceEquation& eq, const DeviceArray<double>& previous, const DeviceArray<double>& older) {
+    if (!time_method_) return;
+    // BDF2 starts as Euler until two levels exist (procedural_equation.cpp:225-231)
+    const int method = (time_method_ == 2 && tlevels_ < 2) ? 1 : time_method_;
+    addTimeTerm(eq, nullptr, cfg_.rho, previous.data(), older.data(), timeWeights(method, tdt_, tprev_dt_, true));
+}
+
 void KOmegaModel::setWallDistance(const double* host) {
     if (cfg_.kind != 2) fail(kState, "a wall distance belongs to the Spalart-Allmaras model");
     for (int i = 0; i < m_.n_cells; ++i)
@@ -490,8 +522,10 @@ TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
     }
     double* h = ctx_.pinned;
     auto solveOne = [&](DeviceEquation& eq, DeviceField& x, DeviceField& diff, const double* sink, const double* src,
-                        const double* previous, const SolverConfig& scfg, Reducer& red, double& r0) {
+                        const double* previous, const SolverConfig& scfg, Reducer& red, double& r0,
+                        const DeviceArray<double>& hprev, const DeviceArray<double>& holder) {
         eq.reset();
+        timeTerm(eq, hprev, holder);
         addConvection(eq, phi, cfg_.rho, eq.options);
         addLaplacian(eq, &diff, 0.0, -1.0, eq.options);
         addReaction(eq, sink, 0.0, 1.0);
@@ -514,19 +548,21 @@ TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
     double rW = 0.0, rK = 0.0;
     if (ke) {
         // k first, then epsilon, one frozen closure state (k_epsilon.cpp:79-103)
-        solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK);
+        solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK,
+                 kPrevLvl_, kOlderLvl_);
         if (!res.healthy) return res;
         solveOne(*weq_, omega_, wDiff_, wDestruction_.data(), wProduction_.data(), prevW_.data(), cfg_.omega_solver,
-                 redW_, rW);
+                 redW_, rW, wPrevLvl_, wOlderLvl_);
         if (!res.healthy) return res;
     } else {
         // omega first, then k with the new omega in its sink (k_omega.cpp:83-110)
         solveOne(*weq_, omega_, wDiff_, wDestruction_.data(), wProduction_.data(), prevW_.data(), cfg_.omega_solver,
-                 redW_, rW);
+                 redW_, rW, wPrevLvl_, wOlderLvl_);
         if (!res.healthy) return res;
         boundOmega();
         launch(ctx_, kScaled, N, N, cfg_.beta_star * cfg_.rho, (const double*)omega_.v.data(), kSink_.data());
-        solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK);
+        solveOne(*keq_, k_, kDiff_, kSink_.data(), production_.data(), prevK_.data(), cfg_.k_solver, redK_, rK,
+                 kPrevLvl_, kOlderLvl_);
         if (!res.healthy) return res;
     }
     // boundTransportFields(); updateViscosity() (k_omega.cpp:114-116)
@@ -568,6 +604,7 @@ TransportResult KOmegaModel::solveSpalartAllmaras(DeviceField& U, DeviceField& p
                (double*)nullptr, wDiff_.trace.data());
     DeviceEquation& eq = *weq_;
     eq.reset();
+    timeTerm(eq, wPrevLvl_, wOlderLvl_);
     addConvection(eq, phi, cfg_.rho, eq.options);
     addLaplacian(eq, &wDiff_, 0.0, -1.0, eq.options);
     addReaction(eq, wDestruction_.data(), 0.0, 1.0);

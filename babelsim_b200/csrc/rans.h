@@ -46,6 +46,10 @@ public:
     DeviceField& omega() { return omega_; }
     // Spalart-Allmaras: the given wall distance of every cell (the reference reads it as an input field).
     void setWallDistance(const double* host);
+    // Transient use (runPiso): `method` 1 Euler, 2 BDF2; saveOld stores every transported field's
+    // history once per physical step, and the transport equations then take equ::ddt(rho, history).
+    void setTransient(int method);
+    void saveOld(double dt);
     DeviceField& effectiveViscosity() { return muEff_; }
     DeviceField& turbulentViscosity() { return mut_; }
     const KOmegaConfig& config() const { return cfg_; }
@@ -70,6 +74,12 @@ private:
     DeviceArray<double> G_, Gtr_, T_, Ttr_, production_, wDestruction_, wProduction_, kSink_, prevK_, prevW_;
     DeviceArray<double> wallDist_, gradNt_;
     bool wall_set_ = false;
+    int time_method_ = 0;
+    DeviceArray<double> kPrevLvl_, kOlderLvl_, wPrevLvl_, wOlderLvl_;
+    double tdt_ = 0.0, tprev_dt_ = 0.0;
+    int tlevels_ = 0;
+    // equ::ddt(eq, rho, history) when transient (a no-op when steady)
+    void timeTerm(DeviceEquation& eq, const DeviceArray<double>& previous, const DeviceArray<double>& older);
     TransportResult solveSpalartAllmaras(DeviceField& U, DeviceField& phi);
     Reducer redW_, redK_, redDW_, redDK_;
 };

@@ -432,7 +432,18 @@ typedef struct {
     int32_t correctors;
     int32_t momentum_iterations;
     int32_t pressure_iterations;
+    double turbulence_change;           /* dTurb, rTurb of the last turbulence correction */
+    double turbulence_residual;
+    int32_t turbulence_corrections;     /* turbulence transport solves in the last pass */
 } bsg_piso_report;
+
+/* runPiso's turbulence controls (src/physics/piso/main.cpp:99-120). */
+typedef struct {
+    int32_t coupling;                   /* turbulenceCoupling: 0 iterated, 1 segregated */
+    int32_t max_iterations;             /* turbulenceMaxIterations (<= 0: 1000) */
+    int32_t correctors;                 /* turbulenceCorrectors (<= 0: the reference's default, max_iterations
+                                           with one PISO pass and iterated coupling, else 1) */
+} bsg_piso_turbulence_controls;
 
 int bsg_piso_create(bsg_mesh* mesh, const bsg_piso_config* config, bsg_piso** out);
 int bsg_piso_set_boundary(bsg_piso* s, const char* field, int32_t patch, int32_t type, const double* value);
@@ -441,6 +452,19 @@ int bsg_piso_set_fields(bsg_piso* s, const double* U, const double* p);
 /* Advance up to `steps` time steps (fewer at end_time or when a step is rejected). */
 int bsg_piso_advance(bsg_piso* s, int32_t steps, bsg_piso_report* report);
 int bsg_piso_get_fields(const bsg_piso* s, double* U, double* p, double* phi);
+/* rans::load in runPiso (piso/main.cpp:98-121): the model of turbulenceModel kOmega, kEpsilon or SA,
+ * after create and before set_fields; its fields take boundary conditions through
+ * bsg_piso_set_boundary ("k", "omega" / "epsilon" / "nuTilda") and initial values through
+ * bsg_piso_set_turbulence_fields (k = NULL for SA); SA needs bsg_piso_set_wall_distance.  Each time
+ * step saves the model's histories, the transport equations take the configured time term, and the
+ * transport is corrected after the pressure correctors until turbulenceTolerance. */
+int bsg_piso_enable_komega(bsg_piso* s, const bsg_komega_config* config, const bsg_piso_turbulence_controls* c);
+int bsg_piso_enable_kepsilon(bsg_piso* s, const bsg_kepsilon_config* config, const bsg_piso_turbulence_controls* c);
+int bsg_piso_enable_spalart_allmaras(bsg_piso* s, const bsg_sa_config* config,
+                                     const bsg_piso_turbulence_controls* c);
+int bsg_piso_set_wall_distance(bsg_piso* s, const double* wall_distance);
+int bsg_piso_set_turbulence_fields(bsg_piso* s, const double* k, const double* second);
+int bsg_piso_get_turbulence_fields(const bsg_piso* s, double* k, double* second, double* mut);
 int bsg_piso_destroy(bsg_piso* s);
 
 #ifdef __cplusplus

@@ -7,7 +7,7 @@ against the reference's Krylov solves at the same tolerance).
 import numpy as np
 import pytest
 
-from helpers import PISO_CASES, Golden, piso_settings, rel_l2
+from helpers import PISO_CASES, PISO_RANS_CASES, Golden, komega_constants, piso_settings, rel_l2
 from oracle import fvm, piso
 
 pytestmark = pytest.mark.gpu
@@ -152,3 +152,56 @@ def test_ddt_reaction_apply_residual(ctx, method, vector):
     if method == "bdf2":
         with pytest.raises(bsg.BsgError):
             eq.ddt(2.0, bsg.Field(m, "cell", comps, prev), dt, "bdf2")  # no older level
+
+
+@pytest.mark.parametrize("name", PISO_RANS_CASES)
+def test_piso_with_turbulence_every_step_matches_reference(ctx, name):
+    """runPiso with k-omega (BDF2) or Spalart-Allmaras (Euler): the model's histories saved each step,
+    its transport (with the time term) corrected after the pressure correctors until
+    turbulenceTolerance; U, p, phi and the model's fields after every step within 1e-8."""
+    import babelsim_b200 as bsg
+    g = Golden(name)
+    m = bsg.Mesh.from_polyhedral(ctx, g.poly)
+    sim = _piso(ctx, g, m)
+    ph, sol, meth = g.meta["physics"], g.meta["solution"], g.meta["methods"]
+    sim.set_turbulence_controls("iterated", sol["turbulenceMaxIterations"], 0)
+
+    def solver(eq):
+        return bsg.solver_config("bcgs", "bjacobi", sol[f"equation.{eq}.absoluteTolerance"],
+                                 sol[f"equation.{eq}.relativeTolerance"], 2000)
+    n = m.n_cells
+    sa = "_sa_" in name
+    if sa:
+        sim.enable_spalart_allmaras(ph["saCb1"], ph["saCb2"], ph["saSigma"], ph["saKappa"], 0.0, ph["saCw2"],
+                                    ph["saCw3"], ph["saCv1"], ph["saCt3"], ph["saCt4"], ph["saNuTildaMin"],
+                                    ph["saWallDistanceMin"], sol["turbulenceRelaxation"], sol["turbulenceTolerance"],
+                                    bsg.options(**meth["nuTildaTransport"]), solver("nuTildaTransport"))
+        for p, (t, v) in enumerate(g.meta["nuTilda_bcs"]):
+            sim.set_boundary("nuTilda", p, t, v)
+        sim.set_wall_distance(g["wall_distance"])
+        sim.set_turbulence_fields(None, np.full(n, g.meta["nuTilda_internal"]))
+        keys = ("nuTilda", "mut")
+    else:
+        c = komega_constants(g)
+        sim.enable_komega(c.beta_star, c.beta, c.gamma, c.sigma_k, c.sigma_omega, c.k_min, c.omega_min,
+                          c.viscosity_ratio_max, c.relaxation, c.tolerance, bsg.options(**meth["kTransport"]),
+                          bsg.options(**meth["omegaTransport"]), solver("kTransport"), solver("omegaTransport"))
+        for p, (t, v) in enumerate(g.meta["k_bcs"]):
+            sim.set_boundary("k", p, t, v)
+        for p, (t, v) in enumerate(g.meta["omega_bcs"]):
+            sim.set_boundary("omega", p, t, v)
+        sim.set_turbulence_fields(np.full(n, g.meta["k_internal"]), np.full(n, g.meta["omega_internal"]))
+        keys = ("k", "omega", "mut")
+    sim.set_fields(np.zeros((n, 3)), np.zeros(n))
+    for k in range(1, g.K + 1):
+        r = sim.advance(1)
+        assert r.steps == k and r.accepted and r.turbulence_corrections >= 1
+        U, p, phi = sim.fields()
+        kk, second, mut = sim.turbulence_fields()
+        mine = dict(U=U, p=p, phi=phi, mut=mut, **({"nuTilda": second} if sa else {"k": kk, "omega": second}))
+        for key in ("U", "p", "phi") + keys:
+            assert rel_l2(mine[key], g[f"{key}_{k}"]) <= 1e-8, (key, k, rel_l2(mine[key], g[f"{key}_{k}"]))
+        assert r.turbulence_change <= sol["turbulenceTolerance"] and r.turbulence_residual <= sol["turbulenceTolerance"]
+    assert r.status == 0
+    sim.close()
+    m.close()
