@@ -36,7 +36,7 @@ EXPORTS = [
     "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
     "bsg_piso_get_fields", "bsg_piso_destroy", "bsg_piso_enable_komega", "bsg_piso_enable_kepsilon",
     "bsg_piso_enable_spalart_allmaras", "bsg_piso_set_wall_distance", "bsg_piso_set_turbulence_fields",
-    "bsg_piso_get_turbulence_fields",
+    "bsg_piso_get_turbulence_fields", "bsg_piso_initialize_potential_flow",
 ]
 
 
@@ -194,7 +194,7 @@ def lib():
             "bsg_piso_enable_kepsilon": [vp, C.POINTER(KEpsilonConfig), C.POINTER(PisoTurbulenceControls)],
             "bsg_piso_enable_spalart_allmaras": [vp, C.POINTER(SaConfig), C.POINTER(PisoTurbulenceControls)],
             "bsg_piso_set_wall_distance": [vp, vp], "bsg_piso_set_turbulence_fields": [vp, vp, vp],
-            "bsg_piso_get_turbulence_fields": [vp, vp, vp, vp],
+            "bsg_piso_get_turbulence_fields": [vp, vp, vp, vp], "bsg_piso_initialize_potential_flow": [vp, i32],
         }
         for name in EXPORTS:
             fn = getattr(L, name)

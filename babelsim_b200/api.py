@@ -486,6 +486,10 @@ class Piso(_TurbulenceModels):
                 np.pad(np.asarray(value, np.float64), (0, 3 - len(value))))
         check(lib().bsg_piso_set_boundary(self.h, field.encode(), patch, BC[kind], ptr(v)), self.mesh.ctx.h)
 
+    def initialize_potential_flow(self, initial_non_orthogonal_corrections=-1):
+        """initializePotentialFlow 1: a potential-flow start before the first step (before set_fields)."""
+        check(lib().bsg_piso_initialize_potential_flow(self.h, initial_non_orthogonal_corrections), self.mesh.ctx.h)
+
     def set_fields(self, U, p):
         check(lib().bsg_piso_set_fields(self.h, ptr(f64(U)), ptr(f64(p))), self.mesh.ctx.h)
 

@@ -1164,6 +1164,13 @@ int bsg_piso_get_turbulence_fields(const bsg_piso* s, double* k, double* second,
     });
 }
 
+int bsg_piso_initialize_potential_flow(bsg_piso* s, int32_t initial_non_orthogonal_corrections) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s != nullptr, "null argument");
+        s->solver->initializePotentialFlow(initial_non_orthogonal_corrections);
+    });
+}
+
 int bsg_piso_set_fields(bsg_piso* s, const double* U, const double* p) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && U && p, "null argument");

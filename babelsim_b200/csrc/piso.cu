@@ -12,6 +12,11 @@
 
 namespace bsg {
 namespace {
+__global__ void kSubtract(long long n, const double* __restrict__ a, double* __restrict__ out) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i < n) out[i] -= a[i];
+}
+
 constexpr int kBlock = 256;
 
 // temporalFluxCorrection (piso/main.cpp:19-55), times rho, interior faces only:
@@ -199,6 +204,45 @@ void PisoSolver::enableTurbulence(const KOmegaConfig& cfg, const PisoTurbulenceC
     divStress_.resize(3 * static_cast<std::size_t>(m_.n_cells));
 }
 
+void PisoSolver::initializePotentialFlow(int initial_non_orthogonal_corrections) {
+    if (started_) fail(kState, "the potential-flow start must be chosen before the fields are set");
+    if (initial_non_orthogonal_corrections > 20) fail(kArgument, "initialNonOrthogonalCorrections must be at most 20");
+    potential_start_ = true;
+    initial_non_orth_ = initial_non_orthogonal_corrections;
+}
+
+void PisoSolver::potentialFlowStart() {
+    // piso/main.cpp:123-146: pPrime = homogeneousLike(p); solves of laplacian(1) pPrime = div(phi);
+    // U -= grad(pPrime); phi += faceFlux(potential equation, pPrime)
+    const int N = m_.n_cells;
+    DeviceField pP(m_, 0, 1);
+    for (int patch = 0; patch < m_.n_patches; ++patch) {
+        const int t = p_.bcs[patch].type;
+        const double zero[3] = {0, 0, 0};
+        pP.setBoundary(patch, t == 0 ? 0 : (t == 4 ? 4 : 2), zero);
+    }
+    divFlux(phi_, divPhiH_);
+    const int corr = initial_non_orth_ >= 0 ? initial_non_orth_ : cfg_.non_orthogonal_corrections;
+    const int solves = cfg_.pressure.diffusion == 0 ? 1 : corr + 1;
+    DeviceEquation eq(pP, cfg_.pressure);
+    for (int k = 0; k < solves; ++k) {
+        eq.reset();
+        addLaplacian(eq, nullptr, 1.0, -1.0, cfg_.pressure);
+        addSource(eq, divPhiH_.data(), -1.0);
+        referenceIfUnanchored(eq, 0.0, flags_.data());
+        Dcsr<double> P{N, m_.cf_ptr.data(), m_.cf_col.data(), eq.diag.data(), eq.val.data(), 2LL * m_.n_interior};
+        if (auto* jac = dynamic_cast<JacobiPreconditioner*>(ppc_.get())) { jac->diag = eq.diag.data(); jac->n = N; }
+        if (auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get())) amg->update(P, k == 0);
+        const SolveOutcome o = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), eq.src.data(), pP.v.data());
+        if (o.status != 0) fail(kNumeric, "the initial potential-flow solve did not converge");
+    }
+    gradient(pP, cfg_.pressure.gradient, gradP_);
+    launch(ctx_, kSubtract, 3LL * N, 3LL * N, (const double*)gradP_.data(), U_.v.data());
+    faceFluxEquation(eq, pP.v.data(), pflux_);
+    addArrays(ctx_, phi_.v.data(), phi_.v.data(), pflux_.data(), m_.n_faces);
+    U_.setFluxContext(phi_);
+}
+
 void PisoSolver::start() {
     if (turb_) {
         // rans::load runs while phi is still the zero face field it was created as (piso/main.cpp:62, 98)
@@ -206,6 +250,10 @@ void PisoSolver::start() {
         turb_->start(phi_);
     }
     faceFlux(U_, cfg_.pressure.interpolation, cfg_.pressure.gradient, phi_);  // piso/main.cpp:122
+    const int pcType = cfg_.pressure_solver.preconditioner;
+    if (pcType == 2 || pcType == 3) ppc_ = std::make_unique<AmgPreconditioner>(m_, cfg_.pressure_solver);
+    else ppc_ = std::make_unique<JacobiPreconditioner>();
+    if (potential_start_) potentialFlowStart();
     // time::history(U), time::history(phi): both levels start as copies (history.h:8)
     for (DeviceField* h : {&Uprev_lvl_, &Uolder_lvl_}) {
         copyAsync(ctx_, h->v.data(), U_.v.data(), 3LL * m_.n_cells);
@@ -219,9 +267,6 @@ void PisoSolver::start() {
     dt_ = prev_dt_ = 0.0;
     time_ = cfg_.start_time;
     step_ = 0;
-    const int pcType = cfg_.pressure_solver.preconditioner;
-    if (pcType == 2 || pcType == 3) ppc_ = std::make_unique<AmgPreconditioner>(m_, cfg_.pressure_solver);
-    else ppc_ = std::make_unique<JacobiPreconditioner>();
     report_ = PisoReport{};
     report_.time = time_;
     started_ = true;

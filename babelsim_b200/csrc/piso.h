@@ -51,6 +51,10 @@ public:
     // rans::load (piso/main.cpp:98-121): an eddy-viscosity model; call before start().
     void enableTurbulence(const KOmegaConfig& cfg, const PisoTurbulenceControls& controls);
     KOmegaModel* turbulence() { return turb_.get(); }
+    // initializePotentialFlow (piso/main.cpp:123-146): before the first step, potential solves on the
+    // initial flux imbalance correct U and phi; `initial_non_orthogonal_corrections` < 0 takes
+    // nonOrthogonalCorrections.  Call before start().
+    void initializePotentialFlow(int initial_non_orthogonal_corrections);
     // Initial state: phi = flux(U) with the pressure options (piso/main.cpp:122).
     void start();
     // Advance up to `steps` time steps (fewer at the end time or on a rejected step).
@@ -79,6 +83,9 @@ private:
     PisoReport report_;
     bool started_ = false;
     std::unique_ptr<KOmegaModel> turb_;
+    bool potential_start_ = false;
+    int initial_non_orth_ = -1;
+    void potentialFlowStart();
     PisoTurbulenceControls tctl_;
     DeviceArray<double> divStress_;
 };

@@ -447,6 +447,11 @@ typedef struct {
 
 int bsg_piso_create(bsg_mesh* mesh, const bsg_piso_config* config, bsg_piso** out);
 int bsg_piso_set_boundary(bsg_piso* s, const char* field, int32_t patch, int32_t type, const double* value);
+/* solution key initializePotentialFlow 1 (src/physics/piso/main.cpp:123-146): call before set_fields;
+ * the start then solves laplacian(1) pPrime = div(phi) (homogeneous pressure constraints,
+ * initialNonOrthogonalCorrections + 1 solves with corrected diffusion; < 0 takes
+ * nonOrthogonalCorrections) and corrects U -= grad(pPrime), phi += its face flux. */
+int bsg_piso_initialize_potential_flow(bsg_piso* s, int32_t initial_non_orthogonal_corrections);
 /* Initial U (3*n_cells) and p (n_cells); phi becomes flux(U) with the pressure options. */
 int bsg_piso_set_fields(bsg_piso* s, const double* U, const double* p);
 /* Advance up to `steps` time steps (fewer at end_time or when a step is rejected). */

@@ -36,6 +36,8 @@ class PisoSettings:
     start_time: float = 0.0
     end_time: float = 1.0
     delta_t: float = 1e-3
+    initialize_potential_flow: bool = False
+    initial_non_orthogonal_corrections: int | None = None
     turbulence_coupling: str = "iterated"
     turbulence_max_iterations: int = 1000
     turbulence_correctors: int | None = None
@@ -161,6 +163,23 @@ def run_piso(geo, U_bcs, p_bcs, s: PisoSettings, U0=None, p0=None, steps=None, t
     t_corrections = s.turbulence_correctors or (
         s.turbulence_max_iterations if model is not None and s.max_iterations == 1 and not segregated else 1)
     phi = fvm.flux(U, p_opts["interpolation"], p_opts["gradient"])
+    if s.initialize_potential_flow:
+        # a conservative initial flux from a potential solve (piso/main.cpp:123-146)
+        init_corr = s.non_orthogonal_corrections if s.initial_non_orthogonal_corrections is None \
+            else s.initial_non_orthogonal_corrections
+        n_solves = 1 if p_opts["diffusion"] == "orthogonal" else init_corr + 1
+        pP = fvm.Field(geo, np.zeros(nc), fvm.homogeneous_bcs(p_bcs))
+        imbalance = fvm.divergence_flux(geo, phi)
+        peq = None
+        for _ in range(n_solves):
+            peq = fvm.Equation(pP, p_opts, {})
+            fvm.eq_laplacian(peq, 1.0, -1.0)
+            fvm.eq_source(peq, -imbalance)
+            fvm.eq_reference_if_unanchored(peq, 0.0)
+            pP.v = _solve(peq.ldu.matrix(), peq.ldu.source)
+        U.v = U.v - fvm.gradient(pP, p_opts["gradient"])
+        phi = phi + fvm.eq_face_flux(peq, pP.v)
+        U.flux = phi.copy()
     U_old = History(U.copy())
     phi_old = History(phi.copy())
     state = PisoState(U.v, p.v, phi, s.start_time)

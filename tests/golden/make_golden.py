@@ -402,6 +402,28 @@ def main_piso():
               {"density": 1.0, "dynamicViscosity": 0.01}, "bdf2", 0.0, 0.05, [0.05, 0.1, 0.15])
 
 
+def main_piso_potential():
+    """runPiso with initializePotentialFlow 1 (piso/main.cpp:123-146) on the inlet/outlet channel from
+    rest: the first step starts from the potential-flow velocity and flux.  Corrected diffusion on the
+    warped box exercises the non-orthogonal potential solves."""
+    ch = meshgen.hex_box(16, 8, 1, hi=(4.0, 1.0, 0.25),
+                         names=["inlet", "outlet", "lower", "upper", "front", "back"],
+                         kinds=["inlet", "outlet", "wall", "wall", "symmetry", "symmetry"])
+    U = [("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0)), ("fixedValue", (0.0, 0.0, 0.0)),
+         ("fixedValue", (0.0, 0.0, 0.0)), ("symmetry", (0, 0, 0)), ("symmetry", (0, 0, 0))]
+    p = [("zeroGradient", 0.0), ("fixedValue", 0.0), ("zeroGradient", 0.0), ("zeroGradient", 0.0),
+         ("symmetry", 0.0), ("symmetry", 0.0)]
+    sol = dict(piso_solution(2, 1), initializePotentialFlow=1)
+    make_piso("piso_potential_channel", ch, U, p, methods("linearUpwind"), sol,
+              {"density": 1.0, "dynamicViscosity": 0.01}, "euler", 0.0, 0.05, [0.05, 0.1])
+    wb = meshgen.warped_box(5, amplitude=0.08)
+    Uw = [("fixedValue", (1.0, 0.0, 0.0)), ("zeroGradient", (0, 0, 0))] + [("fixedValue", (0.0, 0.0, 0.0))] * 4
+    pw = [("zeroGradient", 0.0), ("fixedValue", 0.0)] + [("zeroGradient", 0.0)] * 4
+    sol = dict(piso_solution(2, 2), initializePotentialFlow=1, initialNonOrthogonalCorrections=3)
+    make_piso("piso_potential_warped5", wb, Uw, pw, methods("linearUpwind", "leastSquares", "corrected"), sol,
+              {"density": 1.0, "dynamicViscosity": 0.01}, "bdf2", 0.0, 0.02, [0.02, 0.04])
+
+
 def main_piso_rans():
     """runPiso with a turbulence model (rans::load inside piso/main.cpp:98-121, transport after the
     correctors at every time level, 239-254): k-omega on the channel with BDF2, Spalart-Allmaras with Euler."""
@@ -477,9 +499,12 @@ if __name__ == "__main__":
         main_sa()
     elif len(sys.argv) > 1 and sys.argv[1] == "piso_rans":
         main_piso_rans()
+    elif len(sys.argv) > 1 and sys.argv[1] == "piso_potential":
+        main_piso_potential()
     else:
         main()
         main_piso()
         main_rans()
         main_sa()
         main_piso_rans()
+        main_piso_potential()

@@ -20,6 +20,7 @@ PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler", "piso_cylinder_ogrid"]
 RANS_CASES = ["komega_channel", "komega_warped5"]
 SA_CASES = ["sa_channel", "sa_warped5"]
 PISO_RANS_CASES = ["piso_komega_channel", "piso_sa_channel"]
+PISO_POTENTIAL_CASES = ["piso_potential_channel", "piso_potential_warped5"]
 GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
             "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",
             "face_skewness", "cell_centres", "cell_volumes", "orthogonal_geometry"]
@@ -109,7 +110,9 @@ def piso_settings(g: "Golden", end_time=None) -> piso.PisoSettings:
                              start_time=g.meta["start"], delta_t=g.meta["dt"],
                              end_time=g.meta["ends"][-1] if end_time is None else end_time,
                              momentum=m["momentum"], pressure=m["pressureCorrection"],
-                             turbulence_max_iterations=sol.get("turbulenceMaxIterations", 1000))
+                             turbulence_max_iterations=sol.get("turbulenceMaxIterations", 1000),
+                             initialize_potential_flow=bool(sol.get("initializePotentialFlow", 0)),
+                             initial_non_orthogonal_corrections=sol.get("initialNonOrthogonalCorrections"))
 
 
 def komega_constants(g: "Golden") -> rans.KOmegaConstants:

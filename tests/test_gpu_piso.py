@@ -7,7 +7,7 @@ against the reference's Krylov solves at the same tolerance).
 import numpy as np
 import pytest
 
-from helpers import PISO_CASES, PISO_RANS_CASES, Golden, komega_constants, piso_settings, rel_l2
+from helpers import PISO_CASES, PISO_POTENTIAL_CASES, PISO_RANS_CASES, Golden, komega_constants, piso_settings, rel_l2
 from oracle import fvm, piso
 
 pytestmark = pytest.mark.gpu
@@ -203,5 +203,26 @@ def test_piso_with_turbulence_every_step_matches_reference(ctx, name):
             assert rel_l2(mine[key], g[f"{key}_{k}"]) <= 1e-8, (key, k, rel_l2(mine[key], g[f"{key}_{k}"]))
         assert r.turbulence_change <= sol["turbulenceTolerance"] and r.turbulence_residual <= sol["turbulenceTolerance"]
     assert r.status == 0
+    sim.close()
+    m.close()
+
+
+@pytest.mark.parametrize("pc", ["hypre", "jacobi"])
+@pytest.mark.parametrize("name", PISO_POTENTIAL_CASES)
+def test_piso_potential_flow_start_matches_reference(ctx, name, pc):
+    """initializePotentialFlow: the potential solves before the first step, then every step within 1e-8."""
+    import babelsim_b200 as bsg
+    g = Golden(name)
+    m = bsg.Mesh.from_polyhedral(ctx, g.poly)
+    sim = _piso(ctx, g, m, pc)
+    sim.initialize_potential_flow(g.meta["solution"].get("initialNonOrthogonalCorrections", -1))
+    n = m.n_cells
+    sim.set_fields(np.zeros((n, 3)), np.zeros(n))
+    for k in range(1, g.K + 1):
+        r = sim.advance(1)
+        assert r.steps == k and r.accepted
+        U, p, phi = sim.fields()
+        for key, mine in (("U", U), ("p", p), ("phi", phi)):
+            assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-8, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
     sim.close()
     m.close()

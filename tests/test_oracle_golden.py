@@ -9,7 +9,7 @@ solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
 import numpy as np
 import pytest
 
-from helpers import (CASES, PISO_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, Golden, kepsilon_factory, komega_factory,
+from helpers import (CASES, PISO_CASES, PISO_POTENTIAL_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, Golden, kepsilon_factory, komega_factory,
                      piso_settings, ref_system_groups, rel, rel_l2, sa_factory)
 from oracle import fvm, piso, simple
 
@@ -184,6 +184,19 @@ def test_piso_with_turbulence_matches_reference(name):
         st = piso.run_piso(geo, g.U_bcs(), g.p_bcs(), piso_settings(g, g.meta["ends"][k - 1]), turbulence=model)
         assert st.status == "completed"
         for key, mine in [("U", st.U), ("p", st.p), ("phi", st.phi)] + [(key, getattr(st, key)) for key in keys]:
+            assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
+
+
+@pytest.mark.parametrize("name", PISO_POTENTIAL_CASES)
+def test_piso_potential_flow_start_matches_reference(name):
+    """initializePotentialFlow: potential solves on the initial flux imbalance (homogeneous pressure
+    constraints, unit diffusivity), U -= grad(pPrime), phi += faceFlux; then the normal time steps."""
+    g = Golden(name)
+    geo = g.oracle_geometry()
+    for k in range(1, g.K + 1):
+        st = piso.run_piso(geo, g.U_bcs(), g.p_bcs(), piso_settings(g, g.meta["ends"][k - 1]))
+        assert st.status == "completed"
+        for key, mine in (("U", st.U), ("p", st.p), ("phi", st.phi)):
             assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
 
 
