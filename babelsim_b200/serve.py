@@ -54,10 +54,29 @@ def device_bytes(n_cells: int, n_faces: int) -> int:
     """Device-memory estimate of one resident SIMPLE solve: geometry (152 B per face,
     40 B per cell), fields and workspaces (~60 doubles per cell), two LDU systems on
     the cell-to-face pattern, the AMG hierarchy with its SELL copies (~1.6x the
-    level-0 matrix) and Krylov workspaces."""
+    level-0 matrix), the SELL copy of the momentum matrix (~1.3x its off-diagonal
+    entries, 12 B each), the per-slot records of the diffusion face pass (64 B per
+    face) and Krylov workspaces."""
     matrix = 8 * n_cells + 12 * 2 * n_faces
     return int(152 * n_faces + 40 * n_cells + 480 * n_cells + 2 * matrix + 1.6 * (matrix + 8 * 2 * n_faces) +
-               16 * 8 * n_cells)
+               1.3 * 12 * 2 * n_faces + 64 * n_faces + 16 * 8 * n_cells)
+
+
+def shard(requests: list[Request], world: int, rank: int) -> list[Request]:
+    """This rank's requests when a stream is served by `world` GPUs, each with its own admission
+    loop and no data exchanged between them: in arrival order, every request goes to the rank with
+    the least predicted work so far (cells x iteration cap; ties to the lower rank).  Every rank
+    computes the same assignment from the same stream, so the shards partition it."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    load = [0.0] * world
+    mine = []
+    for r in sorted(requests, key=lambda q: (q.arrival, q.id)):
+        k = min(range(world), key=lambda i: (load[i], i))
+        load[k] += float(r.mesh.n_cells) * r.max_iterations
+        if k == rank:
+            mine.append(r)
+    return mine
 
 
 @dataclass

@@ -94,3 +94,59 @@ def test_round_robin_and_refill():
 
 def test_device_bytes_grows_with_size():
     assert serve.device_bytes(10**6, 7 * 10**6) > 10 * serve.device_bytes(10**5, 7 * 10**5) * 0.99
+
+
+class _SizedMesh:
+    def __init__(self, n):
+        self.n_cells = n
+
+
+def _stream(n=40, seed=3):
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(0.1, n))
+    return [serve.Request(i, float(t[i]), _SizedMesh(int(rng.integers(4000, 100000))), max_iterations=100)
+            for i in range(n)]
+
+
+def test_shards_partition_the_stream_and_balance_work():
+    reqs = _stream()
+    for world in (1, 2, 3, 4):
+        shards = [serve.shard(reqs, world, r) for r in range(world)]
+        ids = sorted(q.id for s in shards for q in s)
+        assert ids == list(range(len(reqs)))
+        loads = [sum(q.mesh.n_cells * q.max_iterations for q in s) for s in shards]
+        biggest = max(q.mesh.n_cells * q.max_iterations for q in reqs)
+        assert max(loads) - min(loads) <= biggest
+        for s in shards:
+            assert [q.arrival for q in s] == sorted(q.arrival for q in s)
+
+
+def _shard_worker(rank, world, port, out):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    mine = [q.id for q in serve.shard(_stream(), world, rank)]
+    gathered = [None] * world
+    dist.all_gather_object(gathered, mine)
+    if rank == 0:
+        out.put(gathered)
+    dist.destroy_process_group()
+
+
+def test_two_ranks_agree_on_the_partition_over_gloo():
+    """Two processes (gloo, the multi-GPU launch shape without GPUs) each compute their shard of the
+    same seeded stream; the gathered shards are disjoint and cover it."""
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    gathered = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sorted(gathered[0] + gathered[1]) == list(range(40)) and not set(gathered[0]) & set(gathered[1])
