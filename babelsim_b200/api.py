@@ -30,7 +30,7 @@ def options(interpolation="linear", gradient="greenGauss", convection="upwind", 
 
 
 def solver_config(ksp="cg", pc="jacobi", atol=1e-14, rtol=1e-10, max_iterations=1000, warm_start=False,
-                  amg_max_levels=12, amg_coarse_size=48, amg_smoothing_steps=1, precision=0) -> SolverConfig:
+                  amg_max_levels=12, amg_coarse_size=400, amg_smoothing_steps=1, precision=0) -> SolverConfig:
     return SolverConfig(KSP[ksp], PC[pc], atol, rtol, max_iterations, int(warm_start), 8, 2.0, amg_max_levels,
                         amg_coarse_size, amg_smoothing_steps, precision)
 

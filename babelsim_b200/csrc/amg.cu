@@ -187,6 +187,9 @@ __global__ void kDenseInverse(int n, const int* __restrict__ ptr, const int* __r
 // barrier orders the pushes of step k before their reads in step k + 1, and the
 // reads of a buffer in step k - 1 before its overwrite in step k.
 constexpr int kDenseCluster = 8;
+// Largest coarsest level whose rows, pivot buffers and column copy fit 8 CTAs of 200 KB:
+// ceil(n/8) n + 2n + ceil(n/8) doubles per CTA.
+constexpr int kAmgCoarsestRows = 440;
 
 __global__ void __cluster_dims__(kDenseCluster, 1, 1)
     kDenseInverseCluster(int n, int rows, const int* __restrict__ ptr, const int* __restrict__ col,
@@ -214,19 +217,30 @@ __global__ void __cluster_dims__(kDenseCluster, 1, 1)
             dst[e % n] = Ml[e % n];
         }
     cluster.sync();
+    // each thread owns one column slot of `rpp` rows per pass (one division, outside the step loop)
+    const int bd = static_cast<int>(blockDim.x);
+    const int rpp = n >= bd ? 1 : bd / n;
+    const int tj = n >= bd ? static_cast<int>(threadIdx.x) : static_cast<int>(threadIdx.x) % n;
+    const int tr = n >= bd ? 0 : static_cast<int>(threadIdx.x) / n;
+    const int jstep = n >= bd ? bd : n;
     for (int k = 0; k < n; ++k) {
         const double* prow = pk + (k & 1) * n;
         const double p = 1.0 / prow[k];
         for (int li = threadIdx.x; li < nr; li += blockDim.x) pc[li] = Ml[static_cast<long long>(li) * n + k];
         __syncthreads();
-        for (int e = threadIdx.x; e < nr * n; e += blockDim.x) {
-            const int li = e / n, j = e - li * n, i = r0 + li;
-            double v;
-            if (i == k) v = j == k ? p : prow[j] * p;
-            else if (j == k) v = -pc[li] * p;
-            else v = Ml[e] - pc[li] * prow[j] * p;
-            Ml[e] = v;
-        }
+        if (tr < rpp)
+            for (int li = tr; li < nr; li += rpp) {
+                const int i = r0 + li;
+                double* row = Ml + static_cast<long long>(li) * n;
+                const double c = pc[li];
+                for (int j = tj; j < n; j += jstep) {
+                    double v;
+                    if (i == k) v = j == k ? p : prow[j] * p;
+                    else if (j == k) v = -c * p;
+                    else v = row[j] - c * prow[j] * p;
+                    row[j] = v;
+                }
+            }
         __syncthreads();
         const int next = k + 1;
         if (next < n && next >= r0 && next < r1) {
@@ -366,7 +380,10 @@ void AmgPreconditioner::buildStructure(const Dcsr<double>& A) {
     BSG_CUDA(cudaMemcpyAsync(cur.diag.data(), A.diag, sizeof(double) * A.n, cudaMemcpyDeviceToHost, ctx_.stream));
     BSG_CUDA(cudaMemcpyAsync(cur.val.data(), A.val, sizeof(double) * A.nnz_off, cudaMemcpyDeviceToHost, ctx_.stream));
     ctx_.sync();
-    const int coarse_target = std::max(std::min(cfg_.amg_coarse_size, 256), 16);
+    // Coarsening stops at the configured size, at most kAmgCoarsestRows: a coarsest level that
+    // size still fits the cluster inverse's distributed shared memory, and every level removed
+    // saves the V-cycle its phases, whose cost is latency, not size, on small levels.
+    const int coarse_target = std::max(std::min(cfg_.amg_coarse_size, kAmgCoarsestRows), 16);
     const int max_levels = std::max(2, cfg_.amg_max_levels);
     auto* l0 = new Level();
     l0->n = A.n;
@@ -520,7 +537,7 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
     const int crow = (last->n + kDenseCluster - 1) / kDenseCluster;
     const std::size_t csmem = sizeof(double) * (static_cast<std::size_t>(crow) * last->n + 2 * last->n + crow);
     if (csmem <= kDenseClusterSmem && clusterReady()) {
-        kDenseInverseCluster<<<kDenseCluster, 512, csmem, ctx_.stream>>>(last->n, crow, last->dptr, last->dcol,
+        kDenseInverseCluster<<<kDenseCluster, 1024, csmem, ctx_.stream>>>(last->n, crow, last->dptr, last->dcol,
                                                                          last->ddiag, last->dval, last->dense.data());
     } else
     kDenseInverse<<<1, 1024, 2 * sizeof(double) * last->n, ctx_.stream>>>(last->n, last->dptr, last->dcol, last->ddiag,

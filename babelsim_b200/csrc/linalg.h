@@ -29,7 +29,7 @@ struct SolverConfig {
     bool warm_start = false;
     int rebuild_interval = 8;
     double reuse_growth = 2.0;
-    int amg_max_levels = 12, amg_coarse_size = 48, amg_smoothing_steps = 2;
+    int amg_max_levels = 12, amg_coarse_size = 400, amg_smoothing_steps = 2;
     int precision = 0;         // 0 FP64, 1 FP32 inner iterations with FP64 refinement
 };
 
