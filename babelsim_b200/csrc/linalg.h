@@ -2,6 +2,8 @@
 // CSR), Krylov solvers with device-resident scalars, preconditioners.
 #pragma once
 
+#include <algorithm>
+
 #include "bsg_internal.h"
 
 #include <memory>
@@ -41,6 +43,45 @@ struct SolveOutcome {
 };
 
 class AmgPreconditioner;
+
+// When a preconditioner built for an earlier matrix version is reused (lagged), as
+// PetscLinearSystem does (src/backend/petsc_linear_system.cpp:257-324, 446-470): a
+// rebuild is due when rebuild_interval matrix versions or right-hand-side solves
+// have passed since the last setup, or when a lagged solve needed more than
+// reuse_growth times the iterations the fresh preconditioner needed; a lagged solve
+// that fails is retried once with a fresh preconditioner.
+struct PcReusePolicy {
+    long long matrix_updates = 0, pc_matrix_update = -1, pc_setups = 0, rhs_solves = 0;
+    int fresh = 0;
+    bool force_rebuild = true;
+    // Before a solve: true when the preconditioner must be rebuilt for this matrix.
+    bool needRebuild(bool matrix_changed, const SolverConfig& cfg) {
+        if (matrix_changed) ++matrix_updates;
+        if (!matrix_changed && !force_rebuild) return false;
+        const bool reuse = pc_setups != 0 && !force_rebuild &&
+                           matrix_updates - pc_matrix_update < cfg.rebuild_interval &&
+                           rhs_solves < cfg.rebuild_interval;
+        force_rebuild = false;
+        if (!reuse) rebuilt();
+        return !reuse;
+    }
+    void rebuilt() {
+        ++pc_setups;
+        pc_matrix_update = matrix_updates;
+        rhs_solves = 0;
+        fresh = 0;
+    }
+    bool lagged() const { return pc_matrix_update != matrix_updates; }
+    // After a solve with `attempt_iterations` iterations of the final attempt.
+    void afterSolve(int status, int attempt_iterations, int total_iterations, const SolverConfig& cfg) {
+        if (status == 0) {
+            if (!lagged()) fresh = std::max(fresh, attempt_iterations);
+            else if (attempt_iterations > cfg.reuse_growth * static_cast<double>(std::max(fresh, 1)))
+                force_rebuild = true;
+        }
+        if (total_iterations > 0) ++rhs_solves;
+    }
+};
 
 // Preconditioner application z = M^-1 r for a single right-hand side.
 struct Preconditioner {

@@ -233,6 +233,7 @@ void PisoSolver::potentialFlowStart() {
         Dcsr<double> P{N, m_.cf_ptr.data(), m_.cf_col.data(), eq.diag.data(), eq.val.data(), 2LL * m_.n_interior};
         if (auto* jac = dynamic_cast<JacobiPreconditioner*>(ppc_.get())) { jac->diag = eq.diag.data(); jac->n = N; }
         if (auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get())) amg->update(P, k == 0);
+        if (k == 0) preuse_.force_rebuild = true;   // the first time step's matrix needs its own hierarchy
         const SolveOutcome o = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), eq.src.data(), pP.v.data());
         if (o.status != 0) fail(kNumeric, "the initial potential-flow solve did not converge");
     }
@@ -406,12 +407,29 @@ bool PisoSolver::step() {
                 Dcsr<double> P{N, m_.cf_ptr.data(), m_.cf_col.data(), peq.diag.data(), peq.val.data(),
                                2LL * m_.n_interior};
                 if (auto* jac = dynamic_cast<JacobiPreconditioner*>(ppc_.get())) { jac->diag = peq.diag.data(); jac->n = N; }
-                if (auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get())) {
+                auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get());
+                bool lagged = false;
+                if (amg) {
                     BSG_PROFILE(ctx_, "amg_numeric_setup");
-                    amg->update(P, first_matrix);  // one matrix per time step: rAUf is frozen
+                    // one matrix per time step (rAUf is frozen), lagged across steps like the reference
+                    amg->update(P, preuse_.needRebuild(first_matrix, cfg_.pressure_solver));
+                    lagged = preuse_.lagged();
                 }
                 first_matrix = false;
-                const SolveOutcome po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), p_.v.data());
+                SolveOutcome po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), p_.v.data());
+                int attempt = po.iterations;
+                if (amg && lagged && po.status != 0) {
+                    {
+                        BSG_PROFILE(ctx_, "amg_numeric_setup");
+                        amg->update(P, true);
+                    }
+                    preuse_.rebuilt();
+                    const int first = po.iterations;
+                    po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), p_.v.data());
+                    attempt = po.iterations;
+                    po.iterations += first;
+                }
+                if (amg) preuse_.afterSolve(po.status, attempt, po.iterations, cfg_.pressure_solver);
                 if (po.status == 2 || !std::isfinite(po.final_)) { report_.status = 2; return false; }
                 p_ok = p_ok && po.status == 0;
                 p_iters += po.iterations;

@@ -83,6 +83,7 @@ private:
     PisoReport report_;
     bool started_ = false;
     std::unique_ptr<KOmegaModel> turb_;
+    PcReusePolicy preuse_;      // lag of the pressure AMG across matrix versions
     bool potential_start_ = false;
     int initial_non_orth_ = -1;
     void potentialFlowStart();

@@ -186,11 +186,28 @@ void SimpleSolver::outerIteration() {
         }
         Dcsr<double> P{N, m_.cf_ptr.data(), m_.cf_col.data(), peq.diag.data(), peq.val.data(), 2LL * m_.n_interior};
         if (auto* jac = dynamic_cast<JacobiPreconditioner*>(ppc_.get())) { jac->diag = peq.diag.data(); jac->n = N; }
-        if (auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get())) {
+        auto* amg = dynamic_cast<AmgPreconditioner*>(ppc_.get());
+        bool lagged = false;
+        if (amg) {
             BSG_PROFILE(ctx_, "amg_numeric_setup");
-            amg->update(P, corr == 0);
+            amg->update(P, preuse_.needRebuild(corr == 0, cfg_.pressure_solver));
+            lagged = preuse_.lagged();
         }
-        const SolveOutcome po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), pP_.v.data());
+        SolveOutcome po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), pP_.v.data());
+        int attempt = po.iterations;
+        if (amg && lagged && po.status != 0) {
+            // a failed lagged solve is retried once with a fresh preconditioner
+            {
+                BSG_PROFILE(ctx_, "amg_numeric_setup");
+                amg->update(P, true);
+            }
+            preuse_.rebuilt();
+            const int first = po.iterations;
+            po = krylov_.solveScalar(P, cfg_.pressure_solver, ppc_.get(), peq.src.data(), pP_.v.data());
+            attempt = po.iterations;
+            po.iterations += first;
+        }
+        if (amg) preuse_.afterSolve(po.status, attempt, po.iterations, cfg_.pressure_solver);
         if (po.status == 2 || !std::isfinite(po.final_)) { report_.status = 2; return; }
         p_ok = p_ok && po.status == 0;
         p_iters += po.iterations;

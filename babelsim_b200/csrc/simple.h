@@ -55,6 +55,7 @@ private:
     DeviceField U_, p_, phi_, pP_, muEff_, rAU_, phiH_;
     std::unique_ptr<DeviceEquation> mom_, peq_;
     std::unique_ptr<KOmegaModel> turb_;
+    PcReusePolicy preuse_;      // lag of the pressure AMG across matrix versions
     DeviceArray<double> divStress_;
     KrylovSolver krylov_;
     std::unique_ptr<Preconditioner> ppc_;
