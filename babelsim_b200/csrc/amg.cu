@@ -507,7 +507,12 @@ void AmgPreconditioner::update(const Dcsr<double>& A, bool numeric) {
     Level* l0 = levels_[0];
     l0->dptr = A.ptr; l0->dcol = A.col; l0->ddiag = A.diag; l0->dval = A.val;
     if (!numeric) {
-        // hierarchy kept; the level-0 Krylov matrix always follows the matrix being solved
+        // coarse levels kept; the level-0 matrix and its Jacobi weights always follow the matrix being
+        // solved, so a lagged V-cycle smooths the new matrix with its own diagonal (a fresh fine
+        // smoother over a lagged coarse correction stays a symmetric positive definite cycle; old
+        // weights on a new matrix can stop smoothing when the diagonal moves between versions)
+        kRdiag<<<gridFor(l0->n, kBlock), kBlock, 0, ctx_.stream>>>(l0->n, omega_, l0->ddiag, l0->rdiag.data());
+        ctx_.launched();
         kCsrToSell<double><<<gridFor(l0->n, kBlock), kBlock, 0, ctx_.stream>>>(
             l0->n, l0->dptr, l0->dval, l0->ddiag, l0->s_ptr.data(), omega_, l0->s_val.data(), nullptr, nullptr);
         ctx_.launched();
