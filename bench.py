@@ -137,10 +137,10 @@ def algorithmic_bytes(name, N, nnz_off, amg_rows):
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte,
 # measured by one capture of the kernel (profiles/ summaries).  kPcgSell, first
 # pressure solve of the 512000-cell Voronoi cavity of the same generator and
-# settings (32 CG iterations): 16.05 GB of DRAM traffic for 18.50 GB of algorithmic
+# settings (30 CG iterations): 15.03 GB of DRAM traffic for 17.35 GB of algorithmic
 # bytes (profiles/kPcgSell_simple_512k_voronoi.md).  Both grow with cells and CG
 # iterations in proportion, so the ratio scales the 1M-cell launches.
-DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.868}
+DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.866}
 
 
 def load_peaks():
