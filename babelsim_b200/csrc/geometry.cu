@@ -7,9 +7,11 @@
 //   kCellReference  per cell: mean of its faces' points (mesh.cpp:361-377)
 //   kFaceGeometry   per face: fan or ear-clipping triangles, area vector,
 //                   outward orientation, centre, area, unit normal
-//   kCellGeometry   per cell: closed, consistently oriented surface
-//                   (Mesh::validate, mesh.cpp:709-756), volume and centroid
-//                   from tetrahedra about the reference point (mesh.cpp:486-519)
+//   kCellGeometry   per cell: vector areas close (Mesh::validate, mesh.cpp:709-730),
+//                   volume and centroid from tetrahedra about the reference point
+//                   (mesh.cpp:486-519)
+//   kCellEdges      one warp per cell: every edge of the outward rings appears
+//                   exactly twice, once in each direction (mesh.cpp:731-756)
 //   kFaceCoefficients per face: orthogonal coefficient, non-orthogonal vector,
 //                   interpolation weight, skewness (mesh.cpp:521-564)
 // Every expression is evaluated in the host code's order and this unit is
@@ -294,27 +296,7 @@ __global__ void kCellGeometry(int N, const double* __restrict__ verts, const int
         flag(err, c);
         return;
     }
-    // every edge of the outward rings appears exactly twice, once in each direction (mesh.cpp:731-756)
-    for (int k = k0; k < k1; ++k) {
-        const int e = cface[k], f = e >= 0 ? e : -e - 1;
-        const Ring r{ids + off[f], off[f + 1] - off[f], (fflags[f] & kFlipped) != 0};
-        for (int i = 0; i < r.n; ++i) {
-            int from, to;
-            edgeOf(r, i, e < 0, from, to);
-            int same = 0, opposite = 0;
-            for (int kk = k0; kk < k1; ++kk) {
-                const int e2 = cface[kk], f2 = e2 >= 0 ? e2 : -e2 - 1;
-                const Ring r2{ids + off[f2], off[f2 + 1] - off[f2], (fflags[f2] & kFlipped) != 0};
-                for (int j = 0; j < r2.n; ++j) {
-                    int a, b;
-                    edgeOf(r2, j, e2 < 0, a, b);
-                    same += (a == from && b == to);
-                    opposite += (a == to && b == from);
-                }
-            }
-            if (same != 1 || opposite != 1) { flag(err, c); return; }
-        }
-    }
+    // the edge check of Mesh::validate runs in kCellEdges
     // volume and centroid from tetrahedra about the reference point (mesh.cpp:486-519)
     const D3 rp = ld3(ref, c);
     double vol = 0.0;
@@ -339,6 +321,83 @@ __global__ void kCellGeometry(int N, const double* __restrict__ verts, const int
     if (!(vol > 0.0) || !isfinite(vol)) { flag(err, c); return; }
     V[c] = vol;
     st3(xc, c, D3{mom.x / vol, mom.y / vol, mom.z / vol});
+}
+
+// Every edge of a cell's outward rings appears exactly twice, once in each direction
+// (mesh.cpp:731-756), scanning the rings in global memory (cells with many edges).
+__device__ bool edgesClosed(const int* __restrict__ off, const int* __restrict__ ids, const int* __restrict__ cface,
+                            const unsigned char* __restrict__ fflags, int k0, int k1) {
+    for (int k = k0; k < k1; ++k) {
+        const int e = cface[k], f = e >= 0 ? e : -e - 1;
+        const Ring r{ids + off[f], off[f + 1] - off[f], (fflags[f] & kFlipped) != 0};
+        for (int i = 0; i < r.n; ++i) {
+            int from, to;
+            edgeOf(r, i, e < 0, from, to);
+            int same = 0, opposite = 0;
+            for (int kk = k0; kk < k1; ++kk) {
+                const int e2 = cface[kk], f2 = e2 >= 0 ? e2 : -e2 - 1;
+                const Ring r2{ids + off[f2], off[f2 + 1] - off[f2], (fflags[f2] & kFlipped) != 0};
+                for (int j = 0; j < r2.n; ++j) {
+                    int a, b;
+                    edgeOf(r2, j, e2 < 0, a, b);
+                    same += (a == from && b == to);
+                    opposite += (a == to && b == from);
+                }
+            }
+            if (same != 1 || opposite != 1) return false;
+        }
+    }
+    return true;
+}
+
+// The same check with one warp per cell: the cell's directed edges (at most kEdgeCap) are staged in
+// shared memory and each lane compares its share of them against all; larger cells take edgesClosed.
+constexpr int kEdgeWarps = 8, kEdgeCap = 256;
+
+__global__ void __launch_bounds__(32 * kEdgeWarps) kCellEdges(int N, const int* __restrict__ off,
+                                                               const int* __restrict__ ids,
+                                                               const int* __restrict__ cptr,
+                                                               const int* __restrict__ cface,
+                                                               const unsigned char* __restrict__ fflags, int* err) {
+    __shared__ int2 edges[kEdgeWarps][kEdgeCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kEdgeWarps + warp;
+    if (c >= N) return;                       // whole warp
+    const int k0 = cptr[c], k1 = cptr[c + 1];
+    int total = 0;
+    for (int k = k0; k < k1; ++k) {
+        const int e = cface[k], f = e >= 0 ? e : -e - 1;
+        total += off[f + 1] - off[f];
+    }
+    if (total > kEdgeCap) {
+        if (lane == 0 && !edgesClosed(off, ids, cface, fflags, k0, k1)) flag(err, c);
+        return;
+    }
+    int2* mine = edges[warp];
+    int base = 0;
+    for (int k = k0; k < k1; ++k) {
+        const int e = cface[k], f = e >= 0 ? e : -e - 1;
+        const Ring r{ids + off[f], off[f + 1] - off[f], (fflags[f] & kFlipped) != 0};
+        for (int i = lane; i < r.n; i += 32) {
+            int from, to;
+            edgeOf(r, i, e < 0, from, to);
+            mine[base + i] = make_int2(from, to);
+        }
+        base += r.n;
+    }
+    __syncwarp();
+    bool ok = true;
+    for (int q = lane; q < total; q += 32) {
+        const int2 x = mine[q];
+        int same = 0, opposite = 0;
+        for (int t = 0; t < total; ++t) {
+            const int2 y = mine[t];
+            same += (y.x == x.x && y.y == x.y);
+            opposite += (y.x == x.y && y.y == x.x);
+        }
+        ok = ok && same == 1 && opposite == 1;
+    }
+    if (!ok) flag(err, c);
 }
 
 __global__ void kFaceCoefficients(int F, const int* __restrict__ owner, const int* __restrict__ neighbour,
@@ -524,6 +583,12 @@ std::unique_ptr<DeviceMesh> buildDeviceMeshPolyhedral(Context& ctx, int n_vertic
                                                   d_cface.data(), fflags.data(), scratch_off.data(), scratch.data(),
                                                   Sf.data(), area.data(), ref.data(), m->V.data(), m->xc.data(),
                                                   err.data());
+        ctx.launched();
+    }
+    {
+        BSG_PROFILE(ctx, "kCellEdges");
+        kCellEdges<<<gridFor(N, kEdgeWarps), 32 * kEdgeWarps, 0, s>>>(N, d_off.data(), d_ids.data(), d_cptr.data(),
+                                                                      d_cface.data(), fflags.data(), err.data());
         ctx.launched();
     }
     if (readFlag(ctx, err) != INT_MAX) rejected();
