@@ -453,6 +453,17 @@ def main_piso_rans():
     make_piso("piso_komega_channel", ch, U, p, m, sol, komega, "bdf2", 0.0, 0.05, [0.05, 0.1, 0.15, 0.2],
               extra_fields=[("k", 3.75e-3, kb), ("omega", 2.0, wb)], turbulence_keys=("k", "omega", "mut"),
               extra_meta=dict(k_internal=3.75e-3, k_bcs=kb, omega_internal=2.0, omega_bcs=wb, second="omega"))
+    # standard k-epsilon, BDF2
+    keps = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "kEpsilon", "kEpsilonCmu": 0.09,
+            "kEpsilonC1": 1.44, "kEpsilonC2": 1.92, "kEpsilonSigmaK": 1.0, "kEpsilonSigmaEpsilon": 1.3,
+            "kMin": 1e-12, "epsilonMin": 1e-12}
+    eb = [("fixedValue", 2.0e-4), ("zeroGradient", 0.0), ("fixedValue", 1e-10), ("fixedValue", 1e-10),
+          ("symmetry", 0.0), ("symmetry", 0.0)]
+    sol = dict(piso_solution(2, 1), **turb_sol, **eq_controls("kTransport"), **eq_controls("epsilonTransport"))
+    make_piso("piso_kepsilon_channel", ch, U, p, rans_methods("linearUpwind", second="epsilon"), sol, keps, "bdf2",
+              0.0, 0.05, [0.05, 0.1, 0.15], extra_fields=[("k", 3.75e-3, kb), ("epsilon", 2.0e-4, eb)],
+              turbulence_keys=("k", "epsilon", "mut"),
+              extra_meta=dict(k_internal=3.75e-3, k_bcs=kb, omega_internal=2.0e-4, omega_bcs=eb, second="epsilon"))
     # Spalart-Allmaras, Euler
     sa = {"density": 1.0, "dynamicViscosity": 0.001, "turbulenceModel": "SA", "saNuTildaMin": 1e-14,
           "saWallDistanceMin": 1e-12, "saCb1": 0.1355, "saCb2": 0.622, "saSigma": 2.0 / 3.0, "saKappa": 0.41,

@@ -19,7 +19,7 @@ CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
 PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler", "piso_cylinder_ogrid"]
 RANS_CASES = ["komega_channel", "komega_warped5"]
 SA_CASES = ["sa_channel", "sa_warped5"]
-PISO_RANS_CASES = ["piso_komega_channel", "piso_sa_channel"]
+PISO_RANS_CASES = ["piso_komega_channel", "piso_kepsilon_channel", "piso_sa_channel"]
 PISO_POTENTIAL_CASES = ["piso_potential_channel", "piso_potential_warped5"]
 GEO_KEYS = ["face_owner", "face_neighbour", "face_patch", "face_centres", "face_area_vectors", "face_areas",
             "face_normals", "face_owner_weights", "face_orthogonal_coefficients", "face_non_orthogonal",

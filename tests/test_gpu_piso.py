@@ -156,7 +156,7 @@ def test_ddt_reaction_apply_residual(ctx, method, vector):
 
 @pytest.mark.parametrize("name", PISO_RANS_CASES)
 def test_piso_with_turbulence_every_step_matches_reference(ctx, name):
-    """runPiso with k-omega (BDF2) or Spalart-Allmaras (Euler): the model's histories saved each step,
+    """runPiso with k-omega or k-epsilon (BDF2) or Spalart-Allmaras (Euler): the model's histories saved each step,
     its transport (with the time term) corrected after the pressure correctors until
     turbulenceTolerance; U, p, phi and the model's fields after every step within 1e-8."""
     import babelsim_b200 as bsg
@@ -182,23 +182,31 @@ def test_piso_with_turbulence_every_step_matches_reference(ctx, name):
         sim.set_turbulence_fields(None, np.full(n, g.meta["nuTilda_internal"]))
         keys = ("nuTilda", "mut")
     else:
-        c = komega_constants(g)
-        sim.enable_komega(c.beta_star, c.beta, c.gamma, c.sigma_k, c.sigma_omega, c.k_min, c.omega_min,
-                          c.viscosity_ratio_max, c.relaxation, c.tolerance, bsg.options(**meth["kTransport"]),
-                          bsg.options(**meth["omegaTransport"]), solver("kTransport"), solver("omegaTransport"))
+        second = g.meta.get("second", "omega")
+        if second == "epsilon":
+            sim.enable_kepsilon(ph["kEpsilonCmu"], ph["kEpsilonC1"], ph["kEpsilonC2"], ph["kEpsilonSigmaK"],
+                                ph["kEpsilonSigmaEpsilon"], ph["kMin"], ph["epsilonMin"], sol["turbulenceRelaxation"],
+                                sol["turbulenceTolerance"], bsg.options(**meth["kTransport"]),
+                                bsg.options(**meth["epsilonTransport"]), solver("kTransport"),
+                                solver("epsilonTransport"))
+        else:
+            c = komega_constants(g)
+            sim.enable_komega(c.beta_star, c.beta, c.gamma, c.sigma_k, c.sigma_omega, c.k_min, c.omega_min,
+                              c.viscosity_ratio_max, c.relaxation, c.tolerance, bsg.options(**meth["kTransport"]),
+                              bsg.options(**meth["omegaTransport"]), solver("kTransport"), solver("omegaTransport"))
         for p, (t, v) in enumerate(g.meta["k_bcs"]):
             sim.set_boundary("k", p, t, v)
         for p, (t, v) in enumerate(g.meta["omega_bcs"]):
-            sim.set_boundary("omega", p, t, v)
+            sim.set_boundary(second, p, t, v)
         sim.set_turbulence_fields(np.full(n, g.meta["k_internal"]), np.full(n, g.meta["omega_internal"]))
-        keys = ("k", "omega", "mut")
+        keys = ("k", second, "mut")
     sim.set_fields(np.zeros((n, 3)), np.zeros(n))
     for k in range(1, g.K + 1):
         r = sim.advance(1)
         assert r.steps == k and r.accepted and r.turbulence_corrections >= 1
         U, p, phi = sim.fields()
         kk, second, mut = sim.turbulence_fields()
-        mine = dict(U=U, p=p, phi=phi, mut=mut, **({"nuTilda": second} if sa else {"k": kk, "omega": second}))
+        mine = dict(U=U, p=p, phi=phi, mut=mut, **({"nuTilda": second} if sa else {"k": kk, keys[1]: second}))
         for key in ("U", "p", "phi") + keys:
             assert rel_l2(mine[key], g[f"{key}_{k}"]) <= 1e-8, (key, k, rel_l2(mine[key], g[f"{key}_{k}"]))
         assert r.turbulence_change <= sol["turbulenceTolerance"] and r.turbulence_residual <= sol["turbulenceTolerance"]

@@ -9,8 +9,8 @@ solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
 import numpy as np
 import pytest
 
-from helpers import (CASES, PISO_CASES, PISO_POTENTIAL_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, Golden, kepsilon_factory, komega_factory,
-                     piso_settings, ref_system_groups, rel, rel_l2, sa_factory)
+from helpers import (CASES, PISO_CASES, PISO_POTENTIAL_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, Golden,
+                     kepsilon_factory, komega_factory, piso_settings, ref_system_groups, rel, rel_l2, sa_factory)
 from oracle import fvm, piso, simple
 
 
@@ -178,12 +178,16 @@ def test_piso_with_turbulence_matches_reference(name):
     turbulenceTolerance; U, p, phi and the model fields after every step."""
     g = Golden(name)
     geo = g.oracle_geometry()
-    model = sa_factory(g) if "_sa_" in name else komega_factory(g)
-    keys = ("nuTilda", "mut") if "_sa_" in name else ("k", "omega", "mut")
+    if "_sa_" in name:
+        model, keys = sa_factory(g), {"nuTilda": "nuTilda", "mut": "mut"}
+    elif "kepsilon" in name:
+        model, keys = kepsilon_factory(g), {"k": "k", "epsilon": "omega", "mut": "mut"}
+    else:
+        model, keys = komega_factory(g), {"k": "k", "omega": "omega", "mut": "mut"}
     for k in range(1, g.K + 1):
         st = piso.run_piso(geo, g.U_bcs(), g.p_bcs(), piso_settings(g, g.meta["ends"][k - 1]), turbulence=model)
         assert st.status == "completed"
-        for key, mine in [("U", st.U), ("p", st.p), ("phi", st.phi)] + [(key, getattr(st, key)) for key in keys]:
+        for key, mine in [("U", st.U), ("p", st.p), ("phi", st.phi)] + [(f, getattr(st, a)) for f, a in keys.items()]:
             assert rel_l2(mine, g[f"{key}_{k}"]) <= 1e-9, (key, k, rel_l2(mine, g[f"{key}_{k}"]))
 
 
