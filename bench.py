@@ -43,6 +43,17 @@ def case_settings():
                 rtol=1e-10, atol=1e-14)
 
 
+def simple_config(n_side: int, world: int) -> dict:
+    """The cavity workload's `config`, shared by both arms so their lines name the same case."""
+    s = case_settings()
+    return {"workload": f"steady SIMPLE, {n_side ** 3}-cell jittered-Voronoi cube cavity (n={n_side}^3)",
+            "cells": n_side ** 3, "nu": s["mu"], "lid": 1.0, "convection": s["convection"],
+            "gradient": s["gradient"], "diffusion": s["diffusion"],
+            "non_orthogonal_corrections": s["non_orthogonal_corrections"], "solver_rtol": s["rtol"],
+            "momentum": "bcgs+jacobi", "pressure": "cg+amg", "precision": "fp64",
+            "l2": "working set >> 126 MB L2, no flush", "parallelism": f"replicas x{world}"}
+
+
 def mesh_for(n: int):
     """Generate (or reuse from /tmp) the jittered-Voronoi cube of n^3 cells."""
     from babelsim_b200 import meshgen
@@ -151,8 +162,9 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(seconds_budget=25.0):
-    """The reference's own sources (oracle/_ref) on a bounded sample of the workload, 1 core."""
+def cpu_baseline(seconds_budget=25.0, iterations=6, n=32):
+    """The reference's own sources (oracle/_ref) on a bounded sample of the workload, 1 core:
+    `iterations` outer iterations of the n^3-cell Voronoi cube, the first one excluded."""
     exe = os.path.join(ROOT, "oracle", "_ref", "babelsim-oracle")
     if not os.path.exists(exe):
         return None
@@ -160,7 +172,6 @@ def cpu_baseline(seconds_budget=25.0):
     from make_golden import write_case  # noqa: E402  (case writer shared with the fixture generator)
     from babelsim_b200 import meshgen
     s = case_settings()
-    n = 24
     pm = meshgen.voronoi_cube(n, 0.3, SEED)
     work = tempfile.mkdtemp(prefix="bsg_cpu_baseline_")
     U = [("fixedValue", (1.0, 0.0, 0.0) if p == 3 else (0.0, 0.0, 0.0)) for p in range(6)]
@@ -168,7 +179,6 @@ def cpu_baseline(seconds_budget=25.0):
     methods = {"momentum": dict(interpolation="linear", gradient=s["gradient"], convection=s["convection"],
                                 diffusion=s["diffusion"])}
     methods["pressureCorrection"] = dict(methods["momentum"])
-    iterations = 6
     sol = {"maxIterations": iterations, "velocityRelaxation": s["alpha_u"], "pressureRelaxation": s["alpha_p"],
            "nonOrthogonalCorrections": s["non_orthogonal_corrections"], "continuityTolerance": 1e-8,
            "velocityTolerance": 1e-7, "momentumTolerance": 1e-6, "pressureCorrectionTolerance": 1e-6,
@@ -199,14 +209,14 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cb = cpu_baseline()
+    cb = cpu_baseline(iterations=max(6, args.steps + 1))
     if cb is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/babelsim-oracle was not built here"}))
         return
     line = {"metric": METRIC, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "steady SIMPLE, jittered-Voronoi cube cavity (bounded CPU sample)"},
+            "config": simple_config(max(2, round(args.cells ** (1.0 / 3.0))), args.gpus),
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -611,13 +621,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": world, "steps": steps_done,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms / steps_done, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"steady SIMPLE, {N}-cell jittered-Voronoi cube cavity (n={n_side}^3)",
-                           "cells": N, "faces": F, "interior_faces": Fi, "nu": s["mu"], "lid": 1.0,
-                           "convection": s["convection"], "gradient": s["gradient"], "diffusion": s["diffusion"],
-                           "non_orthogonal_corrections": 2, "solver_rtol": s["rtol"],
-                           "momentum": "bcgs+jacobi", "pressure": "cg+amg", "precision": "fp64",
-                           "l2": "working set >> 126 MB L2, no flush", "parallelism": f"replicas x{world}",
-                           "mesh_seconds": round(t_mesh, 1)},
+                "config": simple_config(n_side, world),
+                "mesh": {"cells": N, "faces": F, "interior_faces": Fi, "generation_seconds": round(t_mesh, 1)},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "mixed_precision": mixed,
                 "gpu_launches": launches, "mesh_ingest": ingest,
                 "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
