@@ -57,6 +57,39 @@ __device__ __forceinline__ void finishSums(int blocks, const double* partial, do
     }
 }
 
+// A block's partial sums, then the grid's totals in the same launch: the last block to
+// arrive (counted on `ticket`, a device counter that starts at zero) sums every block's
+// partials with one warp in finishSums' order, so the totals do not depend on which block
+// arrives last, and calls `finish` on its thread 0, which also re-arms the counter.  It
+// replaces the one-warp launch that followed each reduction of the BiCGStab step.
+template <int NV, class F>
+__device__ __forceinline__ void reduceThenFinish(double v[NV], double* partial, unsigned* ticket, F finish) {
+    __shared__ int last;
+    blockSum<NV, kBlock>(v);
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < NV; ++j) partial[NV * blockIdx.x + j] = v[j];
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    const int lane = threadIdx.x;
+    double tot[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = 0.0;
+        for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) x += __ldcg(partial + NV * b + j);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        tot[j] = x;
+    }
+    if (lane == 0) {
+        finish(tot);
+        *ticket = 0u;
+    }
+}
+
 // y = A x (C components) fused with partial sums of dot(d, y) per component.
 template <int C>
 __device__ __forceinline__ void rowProduct(const Dcsr<double>& A, int i, const double* __restrict__ x, double acc[C]) {
@@ -220,7 +253,7 @@ __device__ __forceinline__ bool compActive(const Scalars* s, int c) { return s->
 
 template <int C>
 __global__ void kBiStart(int n, const double* __restrict__ r, double* __restrict__ r0, double* __restrict__ p,
-                         double* __restrict__ v, double* __restrict__ partial) {
+                         double* __restrict__ v, double* __restrict__ partial, Scalars* s, unsigned* ticket) {
     double acc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) acc[c] = 0.0;
@@ -234,7 +267,18 @@ __global__ void kBiStart(int n, const double* __restrict__ r, double* __restrict
             acc[c] += ri * ri;
         }
     }
-    writePartial<C>(acc, partial);
+    reduceThenFinish<C>(acc, partial, ticket, [&](const double* rr) {
+        int all = 1;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            s->rho[c] = rr[c];  // r0.r0
+            s->alpha[c] = 1.0; s->omega[c] = 1.0; s->beta[c] = 0.0;
+            s->rr[c] = rr[c];
+            if (s->done[c] == 0 && !(rr[c] > 0.0)) s->done[c] = 1;
+            if (s->done[c] == 0) all = 0;
+        }
+        s->all_done = all;
+    });
 }
 // rho_new = r0.r (given as partial of previous step), beta, p = r + beta (p - omega v), ph = p/d
 template <int C>
@@ -257,43 +301,10 @@ __global__ void kBiDirection(int n, const double* __restrict__ d, const double* 
         }
     }
 }
-// v = A ph, partial r0.v
-template <int C>
-__global__ void kBiSpmvV(Dcsr<double> A, const double* __restrict__ ph, double* __restrict__ v,
-                         const double* __restrict__ r0, double* __restrict__ partial, const Scalars* s) {
-    if (allDone(s)) return;
-    double acc2[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) acc2[c] = 0.0;
-    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
-        double acc[C];
-        rowProduct<C>(A, i, ph, acc);
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            v[C * i + c] = acc[c];
-            acc2[c] += r0[C * i + c] * acc[c];
-        }
-    }
-    writePartial<C>(acc2, partial);
-}
-template <int C>
-__global__ void kBiAlpha(int blocks, const double* __restrict__ partial, Scalars* s) {
-    if (allDone(s)) return;
-    double v[C];
-    finishSums<C>(blocks, partial, v);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            if (!compActive<C>(s, c)) continue;
-            if (!(fabs(v[c]) > 0.0) || !isfinite(v[c])) { s->done[c] = 2; continue; }
-            s->alpha[c] = s->rho[c] / v[c];
-        }
-    }
-}
 // s = r - alpha v (stored in r), sh = s/d, partial s.s
 template <int C>
 __global__ void kBiS(int n, const double* __restrict__ d, double* __restrict__ r, const double* __restrict__ v,
-                     double* __restrict__ sh, double* __restrict__ partial, const Scalars* s) {
+                     double* __restrict__ sh, double* __restrict__ partial, Scalars* s, unsigned* ticket) {
     if (allDone(s)) return;
     double al[C], acc[C];
     bool act[C];
@@ -310,48 +321,21 @@ __global__ void kBiS(int n, const double* __restrict__ d, double* __restrict__ r
             acc[c] += si * si;
         }
     }
-    writePartial<C>(acc, partial);
-}
-// early exit: if ||s|| <= target, x += alpha ph and the component is done
-template <int C>
-__global__ void kBiCheckS(int blocks, const double* __restrict__ partial, Scalars* s) {
-    if (allDone(s)) return;
-    double v[C];
-    finishSums<C>(blocks, partial, v);
-    if (threadIdx.x == 0) {
+    // early exit: if ||s|| <= target, x += alpha ph and the component is done
+    reduceThenFinish<C>(acc, partial, ticket, [&](const double* ss) {
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             if (!compActive<C>(s, c)) continue;
-            s->rr[c] = v[c];
-            if (!isfinite(v[c])) s->done[c] = 2;
-            else if (v[c] <= s->target2[c]) s->done[c] = 3;  // half step accepted
+            s->rr[c] = ss[c];
+            if (!isfinite(ss[c])) s->done[c] = 2;
+            else if (ss[c] <= s->target2[c]) s->done[c] = 3;  // half step accepted
         }
-    }
-}
-// t = A sh, partials t.t, t.s (s lives in r)
-template <int C>
-__global__ void kBiSpmvT(Dcsr<double> A, const double* __restrict__ sh, double* __restrict__ t,
-                         const double* __restrict__ sv, double* __restrict__ partial, const Scalars* s) {
-    if (allDone(s)) return;
-    double acc2[2 * C];
-#pragma unroll
-    for (int c = 0; c < 2 * C; ++c) acc2[c] = 0.0;
-    for (int i = blockIdx.x * kBlock + threadIdx.x; i < A.n; i += gridDim.x * kBlock) {
-        double acc[C];
-        rowProduct<C>(A, i, sh, acc);
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            t[C * i + c] = acc[c];
-            acc2[2 * c] += acc[c] * acc[c];
-            acc2[2 * c + 1] += acc[c] * sv[C * i + c];
-        }
-    }
-    writePartial<2 * C>(acc2, partial);
+    });
 }
 // The two BiCGStab products on the SELL-32 copy of the matrix (one warp per slice
 // of 32 rows, one lane per row, column indices and values read as contiguous
-// warp-wide transactions, four entries in flight per lane): kBiSpmvV's and
-// kBiSpmvT's results and partial sums.
+// warp-wide transactions, four entries in flight per lane), each with its dot
+// products and the scalar update that follows them.
 template <int C>
 __device__ __forceinline__ void sellRowC(const SellMat<double>& S, int sl, int lane, const double* __restrict__ x,
                                          double acc[C]) {
@@ -387,9 +371,11 @@ __device__ __forceinline__ void sellRowC(const SellMat<double>& S, int sl, int l
     for (int c = 0; c < C; ++c) acc[c] = (i < S.n ? d * x[C * i + c] : 0.0) + a[c];
 }
 
+// v = A ph, r0.v, alpha = rho / r0.v
 template <int C>
 __global__ void kBiSpmvVSell(SellMat<double> S, const double* __restrict__ ph, double* __restrict__ v,
-                             const double* __restrict__ r0, double* __restrict__ partial, const Scalars* s) {
+                             const double* __restrict__ r0, double* __restrict__ partial, Scalars* s,
+                             unsigned* ticket) {
     if (allDone(s)) return;
     double acc2[C];
 #pragma unroll
@@ -407,12 +393,21 @@ __global__ void kBiSpmvVSell(SellMat<double> S, const double* __restrict__ ph, d
             }
         }
     }
-    writePartial<C>(acc2, partial);
+    reduceThenFinish<C>(acc2, partial, ticket, [&](const double* r0v) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (!compActive<C>(s, c)) continue;
+            if (!(fabs(r0v[c]) > 0.0) || !isfinite(r0v[c])) { s->done[c] = 2; continue; }
+            s->alpha[c] = s->rho[c] / r0v[c];
+        }
+    });
 }
 
+// t = A sh, t.t and t.s (s lives in r), omega = t.s / t.t
 template <int C>
 __global__ void kBiSpmvTSell(SellMat<double> S, const double* __restrict__ sh, double* __restrict__ t,
-                             const double* __restrict__ sv, double* __restrict__ partial, const Scalars* s) {
+                             const double* __restrict__ sv, double* __restrict__ partial, Scalars* s,
+                             unsigned* ticket) {
     if (allDone(s)) return;
     double acc2[2 * C];
 #pragma unroll
@@ -431,28 +426,22 @@ __global__ void kBiSpmvTSell(SellMat<double> S, const double* __restrict__ sh, d
             }
         }
     }
-    writePartial<2 * C>(acc2, partial);
-}
-
-template <int C>
-__global__ void kBiOmega(int blocks, const double* __restrict__ partial, Scalars* s) {
-    if (allDone(s)) return;
-    double v[2 * C];
-    finishSums<2 * C>(blocks, partial, v);
-    if (threadIdx.x == 0) {
+    reduceThenFinish<2 * C>(acc2, partial, ticket, [&](const double* ts) {
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             if (!compActive<C>(s, c)) continue;
-            s->omega[c] = v[2 * c] > 0.0 ? v[2 * c + 1] / v[2 * c] : 0.0;
+            s->omega[c] = ts[2 * c] > 0.0 ? ts[2 * c + 1] / ts[2 * c] : 0.0;
         }
-    }
+    });
 }
-// x += alpha ph + omega sh; r = s - omega t; partials r.r and r0.r.  Components
-// that accepted the half step (done == 3) take x += alpha ph only.
+
+// x += alpha ph + omega sh; r = s - omega t; r.r and r0.r, then the convergence
+// check and beta, rho for the next step.  Components that accepted the half step
+// (done == 3) take x += alpha ph only.
 template <int C>
 __global__ void kBiUpdate(int n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ ph,
                           const double* __restrict__ sh, const double* __restrict__ t, const double* __restrict__ r0,
-                          double* __restrict__ partial, const Scalars* s) {
+                          double* __restrict__ partial, Scalars* s, unsigned* ticket) {
     if (allDone(s)) return;
     double al[C], om[C], acc[2 * C];
     int mode[C];
@@ -474,14 +463,7 @@ __global__ void kBiUpdate(int n, double* __restrict__ x, double* __restrict__ r,
             acc[2 * c + 1] += r0[C * i + c] * ri;
         }
     }
-    writePartial<2 * C>(acc, partial);
-}
-template <int C>
-__global__ void kBiCheck(int blocks, const double* __restrict__ partial, Scalars* s) {
-    if (allDone(s)) return;
-    double v[2 * C];
-    finishSums<2 * C>(blocks, partial, v);
-    if (threadIdx.x == 0) {
+    reduceThenFinish<2 * C>(acc, partial, ticket, [&](const double* v) {
         int all = 1;
 #pragma unroll
         for (int c = 0; c < C; ++c) {
@@ -499,26 +481,8 @@ __global__ void kBiCheck(int blocks, const double* __restrict__ partial, Scalars
 #pragma unroll
         for (int c = 0; c < C; ++c) if (compActive<C>(s, c)) all = 0;
         s->all_done = all;
-    }
+    });
 }
-template <int C>
-__global__ void kBiInit(int blocks, const double* __restrict__ partial, Scalars* s) {
-    double v[C];
-    finishSums<C>(blocks, partial, v);
-    if (threadIdx.x == 0) {
-        int all = 1;
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            s->rho[c] = v[c];            // r0.r0
-            s->alpha[c] = 1.0; s->omega[c] = 1.0; s->beta[c] = 0.0;
-            s->rr[c] = v[c];
-            if (s->done[c] == 0 && !(v[c] > 0.0)) s->done[c] = 1;
-            if (s->done[c] == 0) all = 0;
-        }
-        s->all_done = all;
-    }
-}
-
 // r = b - A x for C interleaved components, partials of |r_c|^2 and |b_c|^2.
 template <int C>
 __global__ void kResidualC(Dcsr<double> A, const double* __restrict__ b, const double* __restrict__ x,
@@ -563,6 +527,7 @@ struct KrylovSolver::Impl {
     Context& ctx;
     DeviceArray<double> r, z, p, q, r0, v, ph, sh, t, partial, tmp;
     DeviceArray<Scalars> sc;
+    DeviceArray<unsigned> ticket;  // arrivals of the current reduction (reduceThenFinish), zero between launches
     DeviceArray<PcgState> pst;
     DeviceArray<float> r32, s32, z32, p32a, p32b, q32, d32;  // FP32 inner solve of the refined path
     // SELL-32 copy of the matrix the BiCGStab products read: the pattern of the
@@ -577,7 +542,11 @@ struct KrylovSolver::Impl {
         DeviceArray<int> sptr, scol;
         DeviceArray<double> sval;
     } sell;
-    explicit Impl(Context& c) : ctx(c) { sc.resize(1); }
+    explicit Impl(Context& c) : ctx(c) {
+        sc.resize(1);
+        ticket.resize(1);
+        ticket.zero(c.stream);
+    }
     SellMat<double> sellOf(const Dcsr<double>& A) {
         if (sell.ptr != A.ptr || sell.col != A.col || sell.n != A.n || sell.nnz != A.nnz_off) {
             std::vector<int> hp(A.n + 1), hc(std::max<long long>(A.nnz_off, 1));
@@ -980,9 +949,10 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
         }
         s.max_iters = cfg.max_iterations;
         BSG_CUDA(cudaMemcpyAsync(m.sc.data(), &s, sizeof(s), cudaMemcpyHostToDevice, ctx.stream));
-        kBiStart<C><<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.r0.data(), m.p.data(), m.v.data(), m.partial.data());
-        kBiInit<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
-        ctx.launches += 2;
+        BSG_CUDA(cudaMemsetAsync(m.ticket.data(), 0, sizeof(unsigned), ctx.stream));
+        kBiStart<C><<<g, kBlock, 0, ctx.stream>>>(n, m.r.data(), m.r0.data(), m.p.data(), m.v.data(), m.partial.data(),
+                                                  m.sc.data(), m.ticket.data());
+        ctx.launches += 1;
         Scalars h{};
         for (;;) {
             for (int it = 0; it < check_interval; ++it) {
@@ -991,22 +961,18 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
                 {
                     BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
                     kBiSpmvVSell<C><<<g, kBlock, 0, ctx.stream>>>(S, m.ph.data(), m.v.data(), m.r0.data(),
-                                                                  m.partial.data(), m.sc.data());
+                                                                  m.partial.data(), m.sc.data(), m.ticket.data());
                 }
-                kBiAlpha<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 kBiS<C><<<g, kBlock, 0, ctx.stream>>>(n, A.diag, m.r.data(), m.v.data(), m.sh.data(), m.partial.data(),
-                                                      m.sc.data());
-                kBiCheckS<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
+                                                      m.sc.data(), m.ticket.data());
                 {
                     BSG_PROFILE(ctx, "bicgstab3_spmv_dot");
                     kBiSpmvTSell<C><<<g, kBlock, 0, ctx.stream>>>(S, m.sh.data(), m.t.data(), m.r.data(),
-                                                                  m.partial.data(), m.sc.data());
+                                                                  m.partial.data(), m.sc.data(), m.ticket.data());
                 }
-                kBiOmega<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
                 kBiUpdate<C><<<g, kBlock, 0, ctx.stream>>>(n, x, m.r.data(), m.ph.data(), m.sh.data(), m.t.data(),
-                                                           m.r0.data(), m.partial.data(), m.sc.data());
-                kBiCheck<C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), m.sc.data());
-                ctx.launches += 9;
+                                                           m.r0.data(), m.partial.data(), m.sc.data(), m.ticket.data());
+                ctx.launches += 5;
             }
             BSG_CUDA(cudaGetLastError());
             BSG_CUDA(cudaMemcpyAsync(ctx.pinned, m.sc.data(), sizeof(Scalars), cudaMemcpyDeviceToHost, ctx.stream));
