@@ -206,6 +206,8 @@ void PisoSolver::enableTurbulence(const KOmegaConfig& cfg, const PisoTurbulenceC
 
 void PisoSolver::initializePotentialFlow(int initial_non_orthogonal_corrections) {
     if (started_) fail(kState, "the potential-flow start must be chosen before the fields are set");
+    // negative: the key is absent and nonOrthogonalCorrections applies; otherwise the reference's
+    // range, settings.integer(..., 0, 20) (piso/main.cpp:89-90)
     if (initial_non_orthogonal_corrections > 20) fail(kArgument, "initialNonOrthogonalCorrections must be at most 20");
     potential_start_ = true;
     initial_non_orth_ = initial_non_orthogonal_corrections;
