@@ -7,7 +7,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 namespace cg = cooperative_groups;
@@ -378,15 +377,18 @@ int persistentGrid(Context& ctx) {
 // matrix, right-hand side and solution in its own device memory.
 //
 // Host code must not hand the symbol itself to a kernel: in host code it is a
-// host-side stand-in, not a device address.  The device address is looked up
-// once per device, with that device current, by cudaGetSymbolAddress; the first
-// call on a device does that set-up, so make the first call before any stream
-// capture.  Nothing in the scratch has to start at zero: the solver state is
-// written from the host before every launch, and each launch writes every
-// vector entry and reduction partial before it reads it (x is zeroed by the
-// kernel for the zero initial guess).  Every call shares the same scratch and
-// it keeps the last call's contents, so calls that overlap on the GPU race:
-// issue them one at a time.
+// host-side stand-in, not a device address.  Every call looks the device
+// address up with cudaGetSymbolAddress, with the caller's device current, so a
+// context re-created after cudaDeviceReset never sees a stale address.  A call
+// runs on the legacy default stream with synchronous copies, so it must not be
+// made while any stream of the device is being captured, and data the caller
+// wrote on other streams must be complete (synchronised) before the call.
+// Nothing in the scratch has to start at zero: the solver state is written from
+// the host before every launch, and each launch writes every vector entry and
+// reduction partial before it reads it (x is zeroed by the kernel for the zero
+// initial guess).  Every call shares the same scratch and it keeps the last
+// call's contents, so calls that overlap on the GPU race: issue them one at a
+// time.
 constexpr int kStaticMaxRows = 131072;
 constexpr int kStaticMaxBlocks = 4096;
 static __device__ __align__(256) double g_static_scratch[5 * kStaticMaxRows + 2 * NVMAX * kStaticMaxBlocks];
@@ -397,23 +399,16 @@ struct StaticScratch {
     double* base = nullptr;
     PcgState* state = nullptr;
 };
-StaticScratch g_static_by_device[64];
-std::mutex g_static_mutex;
 
+// Device addresses of the static scratch on the current device.
 StaticScratch staticScratch() {
-    int dev = 0;
-    checkCuda(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev < 0 || dev >= 64) fail(kArgument, "device index out of range for the static scratch table");
-    std::lock_guard<std::mutex> lock(g_static_mutex);
-    StaticScratch& s = g_static_by_device[dev];
-    if (!s.base) {
-        void* p = nullptr;
-        checkCuda(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(scratch)");
-        void* q = nullptr;
-        checkCuda(cudaGetSymbolAddress(&q, g_static_state), "cudaGetSymbolAddress(state)");
-        s.base = static_cast<double*>(p);
-        s.state = static_cast<PcgState*>(q);
-    }
+    StaticScratch s;
+    void* p = nullptr;
+    checkCuda(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(scratch)");
+    void* q = nullptr;
+    checkCuda(cudaGetSymbolAddress(&q, g_static_state), "cudaGetSymbolAddress(state)");
+    s.base = static_cast<double*>(p);
+    s.state = static_cast<PcgState*>(q);
     return s;
 }
 }  // namespace

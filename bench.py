@@ -154,11 +154,10 @@ def algorithmic_bytes(name, N, nnz_off, amg_rows):
 
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte,
-# measured by one capture of the kernel (profiles/ summaries).  kPcgSell, first
-# pressure solve of the 512000-cell Voronoi cavity of the same generator and
-# settings (30 CG iterations): 15.03 GB of DRAM traffic for 17.35 GB of algorithmic
-# bytes (profiles/kPcgSell_simple_512k_voronoi.md).  Both grow with cells and CG
-# iterations in proportion, so the ratio scales the 1M-cell launches.
+# measured by one ncu capture of the kernel: kPcgSell, first pressure solve of the
+# 512000-cell Voronoi cavity of the same generator and settings (30 CG iterations),
+# 15.03 GB of DRAM traffic for 17.35 GB of algorithmic bytes.  Both grow with cells
+# and CG iterations in proportion, so the ratio scales the 1M-cell launches.
 DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.866}
 
 
@@ -170,7 +169,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(seconds_budget=25.0, iterations=6, n=32):
+# Side of the Voronoi cube the CPU runs: a bounded sample of the 1M-cell workload
+# (same generator, seed, physics and solver controls, 48^3 = 110592 cells) that the
+# reference's sources finish in about half a minute on one core.
+CPU_SAMPLE_SIDE = 48
+
+
+def cpu_baseline(seconds_budget=25.0, iterations=4, n=CPU_SAMPLE_SIDE):
     """The reference's own sources (oracle/_ref) on a bounded sample of the workload, 1 core:
     `iterations` outer iterations of the n^3-cell Voronoi cube, the first one excluded."""
     exe = os.path.join(ROOT, "oracle", "_ref", "babelsim-oracle")
@@ -207,24 +212,52 @@ def cpu_baseline(seconds_budget=25.0, iterations=6, n=32):
     intervals = max(int(info["reported_iteration_intervals"]), 1)
     secs = float(info["iteration_compute_seconds"]) or float(info["solver_seconds"])
     value = pm.n_cells * intervals / secs
-    return {"value": value, "unit": "cell-iters/s", "cores": 1, "kind": "reference",
-            "sample": f"reference finite-volume sources + CPU Krylov backend, {pm.n_cells}-cell Voronoi cube "
-                      f"(same generator and settings), {iterations} outer iterations, first excluded, "
-                      f"exit {res.returncode}"}
+    return {"value": value, "unit": "cell-iters/s", "cores": 1, "kind": "reference", "cells": pm.n_cells,
+            "sample": f"reference finite-volume sources (runSimple, operators, procedural equations) with a CPU "
+                      f"stand-in for the PETSc/Hypre backend (CG + aggregation AMG and BiCGStab + ILU(0), "
+                      f"preconditioners lagged per equation as PetscLinearSystem lags them), {pm.n_cells}-cell "
+                      f"Voronoi cube (same generator and settings as the device workload), {iterations} outer "
+                      f"iterations, first excluded, exit {res.returncode}",
+            "linear_solve_seconds": info.get("linear_solve_seconds"), "krylov_iterations": info.get("krylov_iterations"),
+            "preconditioner_setups": info.get("preconditioner_setups")}
+
+
+def device_on_sample(bsg, ctx, s, warmup, steps=5):
+    """The device path on the CPU baseline's own sample (the same mesh and settings), so the
+    two throughputs can be compared case for case as well as per cell."""
+    mesh = bsg.Mesh.from_polyhedral(ctx, mesh_for(CPU_SAMPLE_SIDE))
+    sim = build_simple(bsg, mesh, s)
+    sim.iterate(max(warmup, 3))
+    ctx.synchronize()
+    ctx.record(6)
+    sim.iterate(steps)
+    ctx.record(7)
+    ms = ctx.elapsed_ms(6, 7)
+    out = {"cells": mesh.n_cells, "value": mesh.n_cells * steps / (ms / 1e3), "unit": "cell-iters/s",
+           "ms_per_step": ms / steps, "steps": steps}
+    sim.close()
+    mesh.close()
+    return out
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cb = cpu_baseline(iterations=max(6, args.steps + 1))
+    # the bounded sample: --steps timed outer iterations (at most 5, so the run stays within a
+    # few minutes) after one excluded first iteration
+    timed = max(1, min(args.steps, 5))
+    cb = cpu_baseline(iterations=timed + 1)
     if cb is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/babelsim-oracle was not built here"}))
         return
-    line = {"metric": METRIC, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": simple_config(max(2, round(args.cells ** (1.0 / 3.0))), args.gpus),
+    config = simple_config(CPU_SAMPLE_SIDE, args.gpus)
+    config["parallelism"] = "1 process, 1 core (the reference is MPI-parallel; no MPI on this host)"
+    config["sample_of"] = (f"the {max(2, round(args.cells ** (1.0 / 3.0))) ** 3}-cell device workload: same "
+                           f"generator, seed, physics and solver controls, fewer cells; cell-iters/s is per cell")
+    line = {"metric": METRIC, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus, "steps": timed,
+            "warmup": 1, "ms_per_step": cb["cells"] / cb["value"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -620,18 +653,21 @@ def main():
                     "U": float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)),
                     "p": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}}
     cb = None
+    same_sample = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cb = cpu_baseline()
         except Exception as exc:  # the baseline is reported, never required for the GPU number
             cb = {"value": None, "error": str(exc)[:200]}
+        same_sample = device_on_sample(bsg, ctx, s, args.warmup)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": world, "steps": steps_done,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms / steps_done, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": simple_config(n_side, world),
                 "mesh": {"cells": N, "faces": F, "interior_faces": Fi, "generation_seconds": round(t_mesh, 1)},
-                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e, "mixed_precision": mixed,
+                "roofline": roofline, "cpu_baseline": cb, "device_on_cpu_sample": same_sample, "e2e": e2e,
+                "mixed_precision": mixed,
                 "gpu_launches": launches, "mesh_ingest": ingest,
                 "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
                 "pressure_iterations_per_solve": round(prof["pcg_amg_persistent"][3] / prof["pcg_amg_persistent"][0], 1)

@@ -284,8 +284,10 @@ int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t compo
  * systems are rejected with BSG_ERR_ARGUMENT.  x (device, n) receives the
  * solution from a zero initial guess; the acceptance contract is the same as
  * bsg_solve_ldu.  Runs on the default stream of the current device and returns
- * when the result is in `result`.  The first call on a device looks up the
- * scratch's device address (make it before any stream capture).  All calls
+ * when the result is in `result`.  Every call looks up the scratch's device
+ * address and uses synchronous copies on the legacy default stream, so no call
+ * may be made while a stream of the device is being captured, and data written
+ * on other streams must be complete before the call.  All calls
  * share the scratch: calls that overlap on the GPU race, so issue one at a time. */
 int bsg_pcg_jacobi_static(int32_t n, const int32_t* row_ptr, const int32_t* cols, const double* diag,
                           const double* vals, const double* b, double* x, double absolute_tolerance,

@@ -108,6 +108,11 @@ int main(int argc, char** argv) {
         json << "{\"status\": " << status << ", \"solver_seconds\": " << seconds
              << ", \"iteration_compute_seconds\": " << perf.iteration_compute_seconds
              << ", \"reported_iteration_intervals\": " << perf.reported_iteration_intervals
+             << ", \"linear_solves\": " << perf.linear_solves << ", \"krylov_iterations\": " << perf.krylov_iterations
+             << ", \"preconditioner_setups\": " << perf.preconditioner_setups
+             << ", \"preconditioner_reuses\": " << perf.preconditioner_reuses
+             << ", \"linear_solve_seconds\": " << perf.linear_solve_seconds
+             << ", \"preconditioner_seconds\": " << perf.preconditioner_seconds
              << ", \"cells\": " << mesh.cellCount() << ", \"faces\": " << mesh.faceCount() << "}\n";
     } catch (const std::exception& error) {
         std::fprintf(stderr, "oracle driver: %s\n", error.what());

@@ -116,10 +116,10 @@ def make(name, mesh, U_bcs, p_bcs, methods, solution, physics, K, converge_itera
     work = tempfile.mkdtemp(prefix=f"bsg_case_{name}_")
     write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics)
     data = {}
-    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    offsets, ids = mesh.flat()
     data["mesh_vertices"] = mesh.vertices
-    data["mesh_offsets"] = offsets
-    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_offsets"] = np.asarray(offsets, dtype=np.int32)
+    data["mesh_ids"] = np.asarray(ids, dtype=np.int32)
     data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
     for k in range(1, K + 1):
         fields, geo, info, systems = run(work, k, dump=(k == K))
@@ -216,10 +216,10 @@ def make_rans(name, mesh, U_bcs, p_bcs, k_field, w_field, methods, solution, phy
     write_case(work, mesh, U_bcs, p_bcs, methods, solution, physics,
                extra_fields=[("k",) + tuple(k_field), (second,) + tuple(w_field)])
     data = {}
-    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    offsets, ids = mesh.flat()
     data["mesh_vertices"] = mesh.vertices
-    data["mesh_offsets"] = offsets
-    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_offsets"] = np.asarray(offsets, dtype=np.int32)
+    data["mesh_ids"] = np.asarray(ids, dtype=np.int32)
     data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
     for k in range(1, K + 1):
         fields, geo, info, _ = run(work, k)
@@ -302,10 +302,10 @@ def make_sa(name, mesh, U_bcs, p_bcs, nt_field, wall_distance, methods, solution
     with open(os.path.join(work, "fields", "initial", "wallDistance.data"), "w") as f:
         f.write("".join(f"{i} {d!r}\n" for i, d in enumerate(map(float, wall_distance))))
     data = {}
-    offsets = np.concatenate([[0], np.cumsum([len(f) for f in mesh.faces])]).astype(np.int32)
+    offsets, ids = mesh.flat()
     data["mesh_vertices"] = mesh.vertices
-    data["mesh_offsets"] = offsets
-    data["mesh_ids"] = np.concatenate(mesh.faces).astype(np.int32)
+    data["mesh_offsets"] = np.asarray(offsets, dtype=np.int32)
+    data["mesh_ids"] = np.asarray(ids, dtype=np.int32)
     data["mesh_owner"], data["mesh_neighbour"], data["mesh_patch"] = mesh.owner, mesh.neighbour, mesh.patch
     data["wall_distance"] = np.asarray(wall_distance, dtype=np.float64)
     for k in range(1, K + 1):
@@ -491,7 +491,9 @@ def main():
     make("cavity12_upwind", meshgen.cavity_2d(12), U, p, methods(), config1_solution(1e-12),
          {"density": 1.0, "dynamicViscosity": 0.01}, K=3, converge_iterations=2000)
     # the reference's own 64x64x1 cavity mesh with config-1 settings, converged
-    ref_mesh = os.environ.get("BABELSIM_REFERENCE", "/root/reference") + "/cases/cavity/mesh/cavity.mesh"
+    # the reference checkout: $BABELSIM_REFERENCE, by default `reference` beside this repository
+    ref_root = os.environ.get("BABELSIM_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
+    ref_mesh = os.path.join(ref_root, "cases", "cavity", "mesh", "cavity.mesh")
     make("cavity64_config1", meshgen.read_mesh(ref_mesh), U, p, methods(), config1_solution(1e-12),
          {"density": 1.0, "dynamicViscosity": 0.01}, K=1, converge_iterations=5000)
     # non-orthogonal 3D: warped 5^3 box, LS gradient, corrected diffusion, linearUpwind, 2 correctors
@@ -501,8 +503,33 @@ def main():
          config1_solution(1e-12), {"density": 1.0, "dynamicViscosity": 0.01}, K=3, converge_iterations=3000)
 
 
+def config2_solution(rtol=1e-10):
+    """The 1M-cell polyhedral cavity's solver controls: relaxation 0.7 / 0.3, 2 non-orthogonal
+    correctors, momentum BiCGStab + block Jacobi and pressure CG + AMG, both to rtol 1e-10."""
+    sol = config1_solution(rtol)
+    sol["equation.momentum.relativeTolerance"] = rtol
+    sol["equation.momentum.absoluteTolerance"] = 1e-15
+    return sol
+
+
+def main_voronoi():
+    """Jittered-lattice Voronoi cubes (jitter 0.3h, seed 20261007: the generator and seed of the
+    1M-cell bench workload) with its settings: lid u = 1 on plus_y, nu = 1e-3, linearUpwind
+    convection, least-squares gradients, corrected diffusion, 2 non-orthogonal correctors."""
+    lid = [("fixedValue", (0.0, 0.0, 0.0))] * 3 + [("fixedValue", (1.0, 0.0, 0.0))] + \
+          [("fixedValue", (0.0, 0.0, 0.0))] * 2
+    walls_p = [("zeroGradient", 0.0)] * 6
+    m = methods("linearUpwind", "leastSquares", "corrected")
+    make("voronoi8_config2", meshgen.voronoi_cube(8, 0.3, 20261007), lid, walls_p, m, config2_solution(),
+         {"density": 1.0, "dynamicViscosity": 1e-3}, K=3, converge_iterations=4000)
+    make("voronoi12_config2", meshgen.voronoi_cube(12, 0.3, 20261007), lid, walls_p, m, config2_solution(),
+         {"density": 1.0, "dynamicViscosity": 1e-3}, K=2)
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "piso":
+    if len(sys.argv) > 1 and sys.argv[1] == "voronoi":
+        main_voronoi()
+    elif len(sys.argv) > 1 and sys.argv[1] == "piso":
         main_piso()
     elif len(sys.argv) > 1 and sys.argv[1] == "rans":
         main_rans()
@@ -519,3 +546,4 @@ if __name__ == "__main__":
         main_sa()
         main_piso_rans()
         main_piso_potential()
+        main_voronoi()

@@ -15,7 +15,9 @@ from babelsim_b200 import meshgen  # noqa: E402
 from oracle import fvm, geometry, piso, rans, simple  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected"]
+CASES = ["cavity12_upwind", "cavity64_config1", "warped5_corrected", "voronoi8_config2", "voronoi12_config2"]
+# jittered-Voronoi polyhedral cubes with the 1M-cell bench workload's settings
+VORONOI_CASES = ["voronoi8_config2", "voronoi12_config2"]
 PISO_CASES = ["piso_cavity12_bdf2", "piso_warped5_euler", "piso_cylinder_ogrid"]
 RANS_CASES = ["komega_channel", "komega_warped5"]
 SA_CASES = ["sa_channel", "sa_warped5"]
@@ -171,3 +173,23 @@ def sa_factory(g: "Golden"):
         return rans.SpalartAllmaras(geo, nt, g["wall_distance"], ph["density"], ph["dynamicViscosity"],
                                     sa_constants(g), m["nuTildaTransport"], m["momentum"], phi0)
     return make
+
+
+def fields_at_reference_count(make_sim, n, target):
+    """Run SIMPLE to convergence, then report the fields after exactly `target` outer
+    iterations (the reference's count): continuing past an earlier convergence, or
+    re-running when this run needed more.  Returns (report of the full run, U, p)."""
+    sim = make_sim()
+    sim.set_fields(np.zeros((n, 3)), np.zeros(n))
+    r = sim.iterate(6000)
+    if r.iterations > target:
+        sim.close()
+        sim = make_sim()
+        sim.set_fields(np.zeros((n, 3)), np.zeros(n))
+        sim.iterate(target)
+    done = min(r.iterations, target)
+    while done < target:
+        done = sim.iterate(1).iterations
+    U, p, _ = sim.fields()
+    sim.close()
+    return r, U, p

@@ -1,5 +1,6 @@
-"""bench.py's JSON contract on the CPU: the reference arm names the device arm's case, and the
-clock summary covers only the samples taken while the timed region ran."""
+"""bench.py's JSON contract on the CPU: the reference arm names the case it actually ran (the
+bounded CPU sample of the device workload), and the clock summary covers only the samples taken
+while the timed region ran."""
 import argparse
 import json
 import os
@@ -11,8 +12,10 @@ sys.path.insert(0, ROOT)
 import bench  # noqa: E402
 
 
-def test_reference_arm_prints_the_device_arms_config(monkeypatch, capsys):
-    fake = {"value": 1.0e4, "unit": "cell-iters/s", "cores": 1, "kind": "reference", "sample": "test"}
+def test_reference_arm_names_the_sample_it_ran(monkeypatch, capsys):
+    cells = bench.CPU_SAMPLE_SIDE ** 3
+    fake = {"value": 1.0e4, "unit": "cell-iters/s", "cores": 1, "kind": "reference", "sample": "test",
+            "cells": cells}
     seen = {}
 
     def fake_baseline(**kw):
@@ -25,10 +28,14 @@ def test_reference_arm_prints_the_device_arms_config(monkeypatch, capsys):
     bench.run_reference(args)
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert line["impl"] == "reference"
-    assert line["config"] == bench.simple_config(100, 1)
+    # the config describes the sample that ran, not the device arm's 1M-cell case
+    assert line["config"]["cells"] == cells == line["cpu_baseline"]["cells"]
+    assert str(cells) in line["config"]["workload"]
+    assert "1000000" in line["config"]["sample_of"]
     assert line["metric"] == bench.METRIC and line["unit"] == "cell-iters/s" and line["higher_is_better"] is True
     assert line["e2e"] == {"value": 1.0e4, "unit": "cell-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
-    assert seen["iterations"] == 11  # K timed outer iterations plus the excluded first one
+    assert seen["iterations"] == 6  # min(K, 5) timed outer iterations plus the excluded first one
+    assert line["steps"] == 5 and abs(line["ms_per_step"] - cells / 1.0e4 * 1e3) < 1e-9
 
 
 def test_reference_arm_other_ranks_print_nothing(monkeypatch, capsys):

@@ -3,12 +3,16 @@
 Tolerances (relative): geometry 1e-12; explicit operators and assembled LDU
 coefficients 1e-12 (FP64, different summation order only); linear solves at
 rtol 1e-12 vs a direct solve 1e-8; one SIMPLE iteration from the reference's
-own state 1e-9; converged SIMPLE fields 1e-7 (outer tolerance 1e-6).
+own state 1e-9; converged SIMPLE fields 1e-8 after the reference's own number of
+outer iterations (outer tolerance 1e-6; solver tolerance 1e-10 on the Voronoi
+cubes, 1e-12 elsewhere).  The jittered-Voronoi cubes (10-16 faces per cell,
+least-squares gradients, corrected diffusion, linearUpwind, 2 non-orthogonal
+correctors) are the 1M-cell bench workload's mesh class and settings.
 """
 import numpy as np
 import pytest
 
-from helpers import CASES, Golden, ref_system_groups, rel, rel_l2
+from helpers import CASES, VORONOI_CASES, Golden, fields_at_reference_count, ref_system_groups, rel, rel_l2
 from oracle import fvm, simple
 
 pytestmark = pytest.mark.gpu
@@ -132,7 +136,7 @@ def test_assembly(ctx, conv, diff):
             assert rel(deq.face_flux(bsg.Field(m, "cell", 1, sol)).download(), fvm.eq_face_flux(eq, sol)) < 1e-12
 
 
-@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"])
+@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"] + VORONOI_CASES)
 def test_simple_iteration_systems(ctx, name):
     """Momentum and pressure systems of iteration k assembled on the GPU from the reference's state k-1."""
     import babelsim_b200 as bsg
@@ -180,7 +184,9 @@ def test_simple_iteration_systems(ctx, name):
         ref = groups[k - 1]["pressure"][0]
         for key in ("diag", "upper", "lower"):
             assert rel(got[key], ref[key]) < 1e-12, (k, key)
-        assert rel(got["source"], ref["source"]) < 1e-10, k
+        # div(phiH) of this iteration's momentum solution: as close as that solve's tolerance
+        mom_rtol = g.meta["solution"]["equation.momentum.relativeTolerance"]
+        assert rel(got["source"], ref["source"]) < max(1e-10, 100 * mom_rtol), k
 
 
 @pytest.mark.parametrize("pc", ["jacobi", "hypre"])
@@ -239,7 +245,7 @@ def _simple(ctx, g, m, pc="jacobi"):
     return sim
 
 
-@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"])
+@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"] + VORONOI_CASES)
 def test_simple_one_iteration_from_reference_state(ctx, name):
     g = Golden(name)
     m = device_mesh(ctx, g)
@@ -258,16 +264,14 @@ def test_simple_one_iteration_from_reference_state(ctx, name):
 
 
 @pytest.mark.parametrize("name,pc", [("cavity12_upwind", "jacobi"), ("warped5_corrected", "hypre"),
-                                     ("cavity64_config1", "hypre")])
+                                     ("cavity64_config1", "hypre"), ("voronoi8_config2", "hypre"),
+                                     ("voronoi8_config2", "jacobi")])
 def test_simple_converged(ctx, name, pc):
     g = Golden(name)
     m = device_mesh(ctx, g)
-    sim = _simple(ctx, g, m, pc)
-    n = m.n_cells
-    sim.set_fields(np.zeros((n, 3)), np.zeros(n))
-    r = sim.iterate(6000)
+    target = int(g["conv_info"][1])
+    r, U, p = fields_at_reference_count(lambda: _simple(ctx, g, m, pc), m.n_cells, target)
     assert r.converged
-    assert abs(r.iterations - int(g["conv_info"][1])) <= 2
-    U, p, phi = sim.fields()
-    assert rel_l2(U, g["U_conv"]) < 1e-7
-    assert rel_l2(p, g["p_conv"]) < 1e-7
+    assert abs(r.iterations - target) <= 2
+    assert rel_l2(U, g["U_conv"]) < 1e-8
+    assert rel_l2(p, g["p_conv"]) < 1e-8

@@ -4,12 +4,13 @@ The fixtures come from tests/golden/make_golden.py, which runs the reference's
 unmodified finite-volume sources and SIMPLE loop (compiled serially by
 oracle/ref).  Tolerances: assembled coefficients 1e-12 relative; fields after
 one iteration from the reference's own state 1e-9 (the reference's Krylov
-solves stop at rtol 1e-12); converged fields 1e-7 (outer tolerance 1e-6).
+solves stop at rtol 1e-12, 1e-10 on the Voronoi cubes); converged fields 1e-8
+after the reference's own number of outer iterations (outer tolerance 1e-6).
 """
 import numpy as np
 import pytest
 
-from helpers import (CASES, PISO_CASES, PISO_POTENTIAL_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, Golden,
+from helpers import (CASES, PISO_CASES, PISO_POTENTIAL_CASES, PISO_RANS_CASES, RANS_CASES, SA_CASES, VORONOI_CASES, Golden,
                      kepsilon_factory, komega_factory, piso_settings, ref_system_groups, rel, rel_l2, sa_factory)
 from oracle import fvm, piso, simple
 
@@ -37,7 +38,7 @@ def _state(g, k):
     return g[f"U_{k}"], g[f"p_{k}"], g[f"phi_{k}"]
 
 
-@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"])
+@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"] + VORONOI_CASES)
 def test_one_iteration_systems_and_fields(name):
     g = Golden(name)
     geo = g.oracle_geometry()
@@ -54,8 +55,11 @@ def test_one_iteration_systems_and_fields(name):
         mom = cap["momentum_relaxed"]
         for key in ("diag", "upper", "lower", "source"):
             assert rel(getattr(mom, key), ref["momentum"][key].reshape(getattr(mom, key).shape)) < 1e-12, (k, key)
+        # the first pressure source is div(phiH) of this iteration's momentum solution: it agrees
+        # to the momentum solve's tolerance (1e-12 when that solve ran to rtol 1e-12)
+        mom_rtol = g.meta["solution"]["equation.momentum.relativeTolerance"]
         for j, (mine, theirs) in enumerate(zip(cap["pressure"], ref["pressure"])):
-            tol = 1e-12 if j == 0 else 1e-8
+            tol = max(1e-12, 100 * mom_rtol) if j == 0 else 1e-8
             for key in ("diag", "upper", "lower"):
                 assert rel(getattr(mine, key), theirs[key]) < 1e-12, (k, j, key)
             assert rel(mine.source, theirs["source"]) < tol, (k, j, "source")
@@ -64,14 +68,14 @@ def test_one_iteration_systems_and_fields(name):
         assert rel_l2(st.phi, g[f"phi_{k}"]) < 1e-9
 
 
-@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected"])
+@pytest.mark.parametrize("name", ["cavity12_upwind", "warped5_corrected", "voronoi8_config2"])
 def test_converged_fields(name):
     g = Golden(name)
     st = simple.run_simple(g.oracle_geometry(), g.U_bcs(), g.p_bcs(), g.settings(), iterations=5000)
     assert st.converged
-    assert abs(st.iterations - int(g["conv_info"][1])) <= 2
-    assert rel_l2(st.U, g["U_conv"]) < 1e-7
-    assert rel_l2(st.p, g["p_conv"]) < 1e-7
+    assert st.iterations == int(g["conv_info"][1])
+    assert rel_l2(st.U, g["U_conv"]) < 1e-8
+    assert rel_l2(st.p, g["p_conv"]) < 1e-8
 
 
 def test_operators_known_answers():
