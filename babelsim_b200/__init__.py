@@ -5,5 +5,5 @@ a C++17 host runtime behind the C ABI in include/babelsim_b200.h).  This
 package loads it and offers the same vocabulary from Python.
 """
 from ._lib import BsgError, lib  # noqa: F401
-from .api import (Context, Equation, Field, Mesh, Piso, Simple, div_flux, flux, grad, interpolate,  # noqa: F401
-                  normal_gradient, options, solve_ldu, solver_config, write_results)
+from .api import (Context, Equation, Field, LinearSystem, Mesh, Piso, Simple, div_flux, flux, grad,  # noqa: F401
+                  interpolate, normal_gradient, options, solve_ldu, solver_config, write_results)

@@ -28,6 +28,7 @@ EXPORTS = [
     "bsg_equation_create", "bsg_equation_destroy", "bsg_equ_reset", "bsg_equ_div", "bsg_equ_laplacian",
     "bsg_equ_source", "bsg_equ_ddt", "bsg_equ_reaction", "bsg_equ_apply", "bsg_equ_residual", "bsg_equ_relax", "bsg_equ_scale", "bsg_equ_reference_if_unanchored", "bsg_equ_face_flux",
     "bsg_equ_relative_residual", "bsg_equ_solve", "bsg_equ_download", "bsg_solve_ldu", "bsg_pcg_jacobi_static",
+    "bsg_system_create", "bsg_system_destroy", "bsg_system_solve", "bsg_system_counters_read",
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
     "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_enable_kepsilon",
@@ -54,6 +55,17 @@ class SolverConfig(C.Structure):
                 ("preconditioner_rebuild_interval", C.c_int32),
                 ("preconditioner_reuse_iteration_growth", C.c_double), ("amg_max_levels", C.c_int32),
                 ("amg_coarse_size", C.c_int32), ("amg_smoothing_steps", C.c_int32), ("precision", C.c_int32)]
+
+
+class SystemCounters(C.Structure):
+    """bsg_system_counters (EquationPerformanceCounters of one persistent system)."""
+    _fields_ = [("linear_solves", C.c_uint64), ("krylov_iterations", C.c_uint64),
+                ("matrix_value_updates", C.c_uint64), ("rhs_only_solves", C.c_uint64),
+                ("preconditioner_setups", C.c_uint64), ("preconditioner_reuses", C.c_uint64),
+                ("preconditioner_retries", C.c_uint64), ("true_residual_checks", C.c_uint64),
+                ("matrix_update_seconds", C.c_double), ("preconditioner_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("last_status", C.c_int32), ("last_initial_residual", C.c_double),
+                ("last_final_residual", C.c_double), ("last_relative_residual", C.c_double)]
 
 
 class SolveResult(C.Structure):
@@ -176,6 +188,9 @@ def lib():
             "bsg_equ_download": [vp, vp, vp, vp, vp],
             "bsg_solve_ldu": [vp, C.POINTER(SolverConfig), i32, vp, vp, vp, vp, vp, C.POINTER(SolveResult)],
             "bsg_pcg_jacobi_static": [i32, vp, vp, vp, vp, vp, vp, dbl, dbl, i32, C.POINTER(SolveResult)],
+            "bsg_system_create": [vp, i32, pp], "bsg_system_destroy": [vp],
+            "bsg_system_solve": [vp, C.POINTER(SolverConfig), vp, vp, vp, vp, vp, C.POINTER(SolveResult)],
+            "bsg_system_counters_read": [vp, C.POINTER(SystemCounters)],
             "bsg_simple_create": [vp, C.POINTER(SimpleConfig), pp],
             "bsg_simple_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_simple_set_fields": [vp, vp, vp],
             "bsg_simple_set_flux": [vp, vp],

@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (KEpsilonConfig, KOmegaConfig, PisoTurbulenceControls, SaConfig, MeshGeometry, Options, PisoConfig, PisoReport, SimpleConfig, SimpleReport, SolveResult, SolverConfig,
-                   check, f64, i32, lib, ptr)
+                   SystemCounters, check, f64, i32, lib, ptr)
 
 BC = {"fixedValue": 0, "fixedGradient": 1, "zeroGradient": 2, "inletOutlet": 3, "symmetry": 4}
 INTERP = {"linear": 0, "corrected": 1}
@@ -30,9 +30,10 @@ def options(interpolation="linear", gradient="greenGauss", convection="upwind", 
 
 
 def solver_config(ksp="cg", pc="jacobi", atol=1e-14, rtol=1e-10, max_iterations=1000, warm_start=False,
-                  amg_max_levels=12, amg_coarse_size=400, amg_smoothing_steps=1, precision=0) -> SolverConfig:
-    return SolverConfig(KSP[ksp], PC[pc], atol, rtol, max_iterations, int(warm_start), 8, 2.0, amg_max_levels,
-                        amg_coarse_size, amg_smoothing_steps, precision)
+                  amg_max_levels=12, amg_coarse_size=400, amg_smoothing_steps=1, precision=0, rebuild_interval=8,
+                  reuse_growth=2.0) -> SolverConfig:
+    return SolverConfig(KSP[ksp], PC[pc], atol, rtol, max_iterations, int(warm_start), rebuild_interval, reuse_growth,
+                        amg_max_levels, amg_coarse_size, amg_smoothing_steps, precision)
 
 
 class Context:
@@ -332,6 +333,36 @@ def solve_ldu(mesh: Mesh, cfg: SolverConfig, diag, upper, lower, source, x0=None
     check(lib().bsg_solve_ldu(mesh.h, C.byref(cfg), comps, ptr(f64(diag)), ptr(f64(upper)), ptr(f64(lower)),
                               ptr(src), ptr(x), res), mesh.ctx.h)
     return x, list(res)
+
+
+class LinearSystem:
+    """One equation's persistent linear system (bsg_system; PetscLinearSystem's lifecycle):
+    buffers and the AMG structure made once, exactly unchanged matrices skipped, AMG
+    hierarchies lagged and rebuilt on the reference's schedule."""
+
+    def __init__(self, mesh: Mesh, components: int = 1):
+        self.mesh, self.components = mesh, components
+        h = C.c_void_p()
+        check(lib().bsg_system_create(mesh.h, components, C.byref(h)), mesh.ctx.h)
+        self.h = h
+
+    def solve(self, cfg: SolverConfig, diag, upper, lower, source, x0=None):
+        src = f64(source)
+        x = f64(np.zeros_like(src) if x0 is None else x0).copy()
+        res = (SolveResult * self.components)()
+        check(lib().bsg_system_solve(self.h, C.byref(cfg), ptr(f64(diag)), ptr(f64(upper)), ptr(f64(lower)),
+                                     ptr(src), ptr(x), res), self.mesh.ctx.h)
+        return x, list(res)
+
+    def counters(self) -> dict:
+        k = SystemCounters()
+        check(lib().bsg_system_counters_read(self.h, C.byref(k)), self.mesh.ctx.h)
+        return {name: getattr(k, name) for name, _ in k._fields_}
+
+    def close(self):
+        if self.h:
+            lib().bsg_system_destroy(self.h)
+            self.h = None
 
 
 class _TurbulenceModels:

@@ -9,6 +9,7 @@
 #include "simple.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -17,9 +18,28 @@
 struct bsg_context {
     std::unique_ptr<bsg::Context> ctx;
 };
+// One equation's persistent linear system (PetscLinearSystem's role): device
+// buffers and the AMG structure live across solves, the matrix last uploaded is
+// kept on the host for the exact-equality skip of petsc_linear_system.cpp:257-282.
+struct bsg_system {
+    bsg_mesh* mesh = nullptr;
+    int comps = 1;
+    std::unique_ptr<bsg::DeviceField> unknown;
+    std::unique_ptr<bsg::DeviceEquation> eq;
+    std::unique_ptr<bsg::KrylovSolver> krylov;
+    std::unique_ptr<bsg::AmgPreconditioner> amg;
+    bsg::JacobiPreconditioner jacobi;
+    bsg::PcReusePolicy policy;
+    std::vector<double> diag, upper, lower;  // matrix values of the last update (caller's face order)
+    std::vector<double> slots;               // off-diagonal values in device slot order
+    bool ready = false;
+    bsg_system_counters counters{};
+};
 struct bsg_mesh {
     bsg_context* owner;
     std::unique_ptr<bsg::DeviceMesh> mesh;
+    // systems of bsg_solve_ldu (1 and 3 components); destroyed before the mesh
+    std::unique_ptr<bsg_system> ldu_system[2];
 };
 struct bsg_field {
     bsg_mesh* mesh;
@@ -209,14 +229,9 @@ void solveEquation(bsg_equation* e, const bsg::SolverConfig& cfg, bsg_solve_resu
         for (int c = 0; c < 3; ++c) toResult(o[c], results + c);
         return;
     }
-    if (cfg.solver != 0) {
-        // BiCGStab (and the GMRES types): Jacobi-preconditioned lockstep BiCGStab on one right-hand side
-        toResult(e->krylov->solveBicgstab(A, cfg, eq.src.data(), eq.x->v.data()), results);
-        return;
-    }
     std::unique_ptr<bsg::Preconditioner> jac;
     bsg::Preconditioner* pc = nullptr;
-    if (cfg.preconditioner == 2 || cfg.preconditioner == 3) {
+    if (cfg.solver != 1 && (cfg.preconditioner == 2 || cfg.preconditioner == 3)) {
         if (!e->amg) e->amg = std::make_unique<bsg::AmgPreconditioner>(m, cfg);
         e->amg->update(A, true);
         pc = e->amg.get();
@@ -229,6 +244,127 @@ void solveEquation(bsg_equation* e, const bsg::SolverConfig& cfg, bsg_solve_resu
     }
     const bsg::SolveOutcome o = e->krylov->solveScalar(A, cfg, pc, eq.src.data(), eq.x->v.data());
     toResult(o, results);
+}
+
+std::unique_ptr<bsg_system> makeSystem(bsg_mesh* mesh, int components) {
+    require(components == 1 || components == 3, "components must be 1 or 3");
+    bsg::DeviceMesh& m = *mesh->mesh;
+    auto s = std::make_unique<bsg_system>();
+    s->mesh = mesh;
+    s->comps = components;
+    s->unknown = std::make_unique<bsg::DeviceField>(m, 0, components);
+    s->eq = std::make_unique<bsg::DeviceEquation>(*s->unknown, bsg::Options{});
+    s->krylov = std::make_unique<bsg::KrylovSolver>(*m.ctx);
+    s->slots.assign(2 * static_cast<std::size_t>(m.n_interior), 0.0);
+    return s;
+}
+
+bool sameValues(const std::vector<double>& kept, const double* v, std::size_t n) {
+    if (kept.size() != n) return false;
+    for (std::size_t i = 0; i < n; ++i)
+        if (kept[i] != v[i]) return false;  // exact equality; NaN always counts as changed
+    return true;
+}
+
+double secondsSince(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+}
+
+// updateMatrix + prepare + solveRhs of PetscLinearSystem (petsc_linear_system.cpp:257-481)
+// for one call of the seam, every right-hand side of the system at once.
+void systemSolve(bsg_system* s, const bsg::SolverConfig& cfg, const double* diagonal, const double* upper,
+                 const double* lower, const double* source, double* x, bsg_solve_result* results) {
+    bsg::DeviceMesh& m = *s->mesh->mesh;
+    bsg::Context& ctx = *m.ctx;
+    const int N = m.n_cells, C = s->comps;
+    const std::size_t F = m.n_faces;
+    bsg_system_counters& k = s->counters;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < N; ++i)
+        if (!std::isfinite(diagonal[i])) bsg::fail(bsg::kNumeric, "nonfinite matrix diagonal");
+    const bool changed = !s->ready || !sameValues(s->diag, diagonal, N) || !sameValues(s->upper, upper, F) ||
+                         !sameValues(s->lower, lower, F);
+    if (changed) {
+        s->diag.assign(diagonal, diagonal + N);
+        s->upper.assign(upper, upper + F);
+        s->lower.assign(lower, lower + F);
+        for (int i = 0; i < m.n_interior; ++i) {
+            const int f = m.interior_ext[i];
+            s->slots[m.h_slot_own[i]] = upper[f];
+            s->slots[m.h_slot_nbr[i]] = lower[f];
+        }
+        s->eq->diag.upload(diagonal, N, ctx.stream);
+        s->eq->val.upload(s->slots, ctx.stream);
+        s->ready = true;
+        ++k.matrix_value_updates;
+    } else {
+        ++k.rhs_only_solves;
+    }
+    s->eq->src.upload(source, static_cast<std::size_t>(N) * C, ctx.stream);
+    s->unknown->v.upload(x, static_cast<std::size_t>(N) * C, ctx.stream);
+    k.matrix_update_seconds += secondsSince(t0);
+    const auto t1 = std::chrono::steady_clock::now();
+    bsg::Dcsr<double> A{N, m.cf_ptr.data(), m.cf_col.data(), s->eq->diag.data(), s->eq->val.data(),
+                        2LL * m.n_interior};
+    const bool use_amg = C == 1 && cfg.solver != 1 && (cfg.preconditioner == 2 || cfg.preconditioner == 3);
+    bool lagged = false;
+    if (use_amg) {
+        if (!s->amg) s->amg = std::make_unique<bsg::AmgPreconditioner>(m, cfg);
+        const bool rebuild = s->policy.needRebuild(changed, cfg);
+        if (rebuild || changed) s->amg->update(A, rebuild);
+        if (rebuild) ++k.preconditioner_setups;
+        lagged = s->policy.lagged();
+        if (lagged) ++k.preconditioner_reuses;
+        ctx.sync();
+    } else if (cfg.preconditioner != 0 && changed) {
+        ++k.preconditioner_setups;  // Jacobi-type: formed from the current diagonal
+    }
+    k.preconditioner_seconds += secondsSince(t1);
+    const auto t2 = std::chrono::steady_clock::now();
+    bsg::SolveOutcome o[3];
+    double* dx = s->unknown->v.data();
+    if (C == 3) {
+        s->krylov->solveVector3(A, cfg, s->eq->src.data(), dx, o);
+    } else {
+        bsg::Preconditioner* pc = nullptr;
+        if (use_amg) pc = s->amg.get();
+        else if (cfg.preconditioner != 0) {
+            s->jacobi.diag = s->eq->diag.data();
+            s->jacobi.n = N;
+            pc = &s->jacobi;
+        }
+        o[0] = s->krylov->solveScalar(A, cfg, pc, s->eq->src.data(), dx);
+        int attempt = o[0].iterations;
+        if (use_amg && lagged && o[0].status != 0) {
+            // a failed lagged solve is retried once from the same guess with a fresh hierarchy
+            const auto tr = std::chrono::steady_clock::now();
+            s->amg->update(A, true);
+            s->policy.rebuilt();
+            ++k.preconditioner_retries;
+            ++k.preconditioner_setups;
+            s->unknown->v.upload(x, N, ctx.stream);
+            k.preconditioner_seconds += secondsSince(tr);
+            const bsg::SolveOutcome first = o[0];
+            o[0] = s->krylov->solveScalar(A, cfg, pc, s->eq->src.data(), dx);
+            attempt = o[0].iterations;
+            o[0].iterations += first.iterations;
+            o[0].checks += first.checks;
+        }
+        if (use_amg) s->policy.afterSolve(o[0].status, attempt, o[0].iterations, cfg);
+    }
+    s->unknown->v.download(x, ctx.stream);
+    ctx.sync();
+    k.solve_seconds += secondsSince(t2);
+    for (int c = 0; c < C; ++c) {
+        toResult(o[c], results + c);
+        ++k.linear_solves;
+        k.krylov_iterations += static_cast<uint64_t>(std::max(o[c].iterations, 0));
+        k.true_residual_checks += static_cast<uint64_t>(std::max(o[c].checks, 0));
+        k.last_status = o[c].status;
+        k.last_initial_residual = o[c].initial;
+        k.last_final_residual = o[c].final_;
+        k.last_relative_residual = o[c].relative;
+    }
 }
 
 }  // namespace
@@ -781,37 +917,38 @@ int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t compo
     return guard(ctxOf(mesh), [&] {
         require(mesh && config && diagonal && upper && lower && source && x && results, "null argument");
         require(components == 1 || components == 3, "components must be 1 or 3");
-        bsg::DeviceMesh& m = *mesh->mesh;
-        bsg::Context& ctx = *m.ctx;
         const bsg::SolverConfig cfg = solverConfig(config);
-        // Pack the caller's LDU (face order) into the device slots.
-        std::vector<double> val(2 * static_cast<std::size_t>(m.n_interior));
-        for (int i = 0; i < m.n_interior; ++i) {
-            const int f = m.interior_ext[i];
-            val[m.h_slot_own[i]] = upper[f];
-            val[m.h_slot_nbr[i]] = lower[f];
-        }
-        for (int i = 0; i < m.n_cells; ++i)
-            if (!std::isfinite(diagonal[i])) bsg::fail(bsg::kNumeric, "nonfinite matrix diagonal");
-        bsg::DeviceField unknown(m, 0, components);
-        bsg::DeviceEquation eq(unknown, bsg::Options{});
-        eq.diag.upload(diagonal, m.n_cells, ctx.stream);
-        eq.val.upload(val, ctx.stream);
-        eq.src.upload(source, static_cast<std::size_t>(m.n_cells) * components, ctx.stream);
-        unknown.v.upload(x, static_cast<std::size_t>(m.n_cells) * components, ctx.stream);
-        bsg_field f{mesh, nullptr};
-        bsg_equation e;
-        e.unknown = &f;
-        e.eq.reset(&eq);
-        try {
-            solveEquation(&e, cfg, results);
-        } catch (...) {
-            e.eq.release();
-            throw;
-        }
-        e.eq.release();
-        unknown.v.download(x, ctx.stream);
-        ctx.sync();
+        std::unique_ptr<bsg_system>& sys = mesh->ldu_system[components == 3 ? 1 : 0];
+        if (!sys) sys = makeSystem(mesh, components);
+        systemSolve(sys.get(), cfg, diagonal, upper, lower, source, x, results);
+    });
+}
+
+int bsg_system_create(bsg_mesh* mesh, int32_t components, bsg_system** out) {
+    return guard(ctxOf(mesh), [&] {
+        require(mesh && out, "null argument");
+        *out = makeSystem(mesh, components).release();
+    });
+}
+
+int bsg_system_destroy(bsg_system* system) {
+    delete system;
+    return bsg::kOk;
+}
+
+int bsg_system_solve(bsg_system* system, const bsg_solver_config* config, const double* diagonal,
+                     const double* upper, const double* lower, const double* source, double* x,
+                     bsg_solve_result* results) {
+    return guard(system ? ctxOf(system->mesh) : nullptr, [&] {
+        require(system && config && diagonal && upper && lower && source && x && results, "null argument");
+        systemSolve(system, solverConfig(config), diagonal, upper, lower, source, x, results);
+    });
+}
+
+int bsg_system_counters_read(const bsg_system* system, bsg_system_counters* out) {
+    return guard(system ? ctxOf(system->mesh) : nullptr, [&] {
+        require(system && out, "null argument");
+        *out = system->counters;
     });
 }
 

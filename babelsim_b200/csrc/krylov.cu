@@ -530,6 +530,7 @@ struct KrylovSolver::Impl {
     DeviceArray<unsigned> ticket;  // arrivals of the current reduction (reduceThenFinish), zero between launches
     DeviceArray<PcgState> pst;
     DeviceArray<float> r32, s32, z32, p32a, p32b, q32, d32;  // FP32 inner solve of the refined path
+    GmresWorkspace gmres;
     // SELL-32 copy of the matrix the BiCGStab products read: the pattern of the
     // last CSR pattern seen (a solver's systems all live on one mesh's cell->face
     // pattern, so it is built once), the values re-scattered for every solve.
@@ -671,6 +672,7 @@ SolveOutcome KrylovSolver::solveRefined(const Dcsr<double>& A, const SolverConfi
     if (!cfg.warm_start) BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, ctx.stream));
     const double bnorm = hostNorm(ctx, b, n, m.partial);
     double rn = trueResidualNorm(ctx, A, b, x, m.r.data());
+    out.checks = 1;
     out.initial = rn;
     const double scale = residualScale(rn, bnorm);
     const double target = std::max(cfg.atol, cfg.rtol * scale);
@@ -697,6 +699,7 @@ SolveOutcome KrylovSolver::solveRefined(const Dcsr<double>& A, const SolverConfi
         ctx.launched();
         const double before = rn;
         rn = trueResidualNorm(ctx, A, b, x, m.r.data());  // synchronises; PcgState is in ctx.pinned
+        ++out.checks;
         PcgState r;
         std::memcpy(&r, ctx.pinned, sizeof(r));
         used += r.iterations;
@@ -786,11 +789,13 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
                 out.status = 0;
                 out.final_ = out.initial;
                 out.relative = out.initial / scale;
+                out.checks = 1;
                 return out;
             }
         }
         used += r.iterations;
         fin = trueResidualNorm(ctx, A, b, x, m.r.data());
+        ++out.checks;
         if (!std::isfinite(fin) || fin <= target || r.status == 2 || used >= cfg.max_iterations) break;
         // true-residual restart from this x with a halved internal target (petsc_linear_system.cpp:412-439)
         h.target2 = 0.25 * r.target2;
@@ -809,6 +814,10 @@ SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig
     Impl& m = *impl_;
     Context& ctx = m.ctx;
     const int n = A.n;
+    // kspType dispatch (LinearSolverType, petsc_linear_system.cpp:43-50): BiCGStab with the
+    // point-Jacobi preconditioner, GMRES / FGMRES with the given one, CG below.
+    if (cfg.solver == 1) return solveBicgstab(A, cfg, b, x);
+    if (cfg.solver == 2 || cfg.solver == 3) return gmresSolve(ctx, m.gmres, A, cfg, pc, b, x);
     if (persistent && cfg.solver == 0) {
         auto* amg = dynamic_cast<AmgPreconditioner*>(pc);
         auto* jac = dynamic_cast<JacobiPreconditioner*>(pc);
@@ -825,7 +834,7 @@ SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig
     const double target = std::max(cfg.atol, cfg.rtol * scale);
     out.initial = r0n;
     if (std::isfinite(r0n) && r0n <= target) {
-        out.status = 0; out.final_ = r0n; out.relative = r0n / scale;
+        out.status = 0; out.final_ = r0n; out.relative = r0n / scale; out.checks = 1;
         return out;
     }
     double inner = target;
@@ -888,6 +897,7 @@ SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig
             }
         }
         fin = trueResidualNorm(ctx, A, b, x, m.r.data());
+        ++out.checks;
         if ((std::isfinite(fin) && fin <= target) || !std::isfinite(fin)) break;
         inner *= 0.5;
     }
@@ -934,7 +944,10 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
         fin[c] = r0n[c];
         out[c] = SolveOutcome{};
         out[c].initial = r0n[c];
-        if (std::isfinite(r0n[c]) && r0n[c] <= target[c]) finished[c] = true;
+        if (std::isfinite(r0n[c]) && r0n[c] <= target[c]) {
+            finished[c] = true;
+            out[c].checks = 1;
+        }
     }
     for (int restart = 0; restart < 3; ++restart) {
         bool any = false;
@@ -986,6 +999,7 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
             if (finished[c]) continue;
             used[c] = h.iters[c];
             fin[c] = res[c];
+            ++out[c].checks;
             if (!std::isfinite(res[c]) || res[c] <= target[c] || h.done[c] == 2) finished[c] = true;
             else inner[c] *= 0.5;
         }
@@ -1000,7 +1014,35 @@ void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& c
 
 void KrylovSolver::solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                                 SolveOutcome out[3]) {
+    if (cfg.solver == 2 || cfg.solver == 3 || cfg.solver == 0) {
+        // GMRES / FGMRES (and CG) solve the three components one after another, as the
+        // reference's backend does (petsc_backend.cpp:165-195), with a point-Jacobi
+        // preconditioner unless none is configured.
+        JacobiPreconditioner jac;
+        jac.diag = A.diag;
+        jac.n = A.n;
+        Preconditioner* pc = cfg.preconditioner == 0 ? nullptr : &jac;
+        for (int c = 0; c < 3; ++c) {
+            if (cfg.solver == 0) out[c] = cgComponent(A, cfg, pc, c, b, x);
+            else out[c] = gmresComponent(impl_->ctx, impl_->gmres, A, cfg, pc, 3, c, b, x);
+        }
+        return;
+    }
     lockstepBicgstab<3>(A, cfg, b, x, out);
+}
+
+SolveOutcome KrylovSolver::cgComponent(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc, int c,
+                                       const double* b, double* x) {
+    // component c into contiguous buffers (the GMRES workspace's), CG, and back
+    Impl& m = *impl_;
+    Context& ctx = m.ctx;
+    const int n = A.n;
+    m.gmres.ensure(n, 1, false);
+    componentCopy(ctx, n, 3, c, b, m.gmres.bc.data(), true);
+    componentCopy(ctx, n, 3, c, x, m.gmres.xc.data(), true);
+    const SolveOutcome o = solveScalar(A, cfg, pc, m.gmres.bc.data(), m.gmres.xc.data());
+    componentCopy(ctx, n, 3, c, m.gmres.xc.data(), x, false);
+    return o;
 }
 
 SolveOutcome KrylovSolver::solveBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x) {

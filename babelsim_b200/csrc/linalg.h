@@ -40,6 +40,7 @@ struct SolveOutcome {
     int status = 2;            // 0 converged, 1 max iterations, 2 numerical failure
     int iterations = 0;
     double initial = 0.0, final_ = 0.0, relative = 0.0;
+    int checks = 0;            // true-residual evaluations (PetscLinearSystem's true_residual_checks)
 };
 
 class AmgPreconditioner;
@@ -52,7 +53,7 @@ class AmgPreconditioner;
 // that fails is retried once with a fresh preconditioner.
 struct PcReusePolicy {
     long long matrix_updates = 0, pc_matrix_update = -1, pc_setups = 0, rhs_solves = 0;
-    int fresh = 0;
+    int fresh[3] = {0, 0, 0};  // iterations of the fresh preconditioner, per right-hand side
     bool force_rebuild = true;
     // Before a solve: true when the preconditioner must be rebuilt for this matrix.
     bool needRebuild(bool matrix_changed, const SolverConfig& cfg) {
@@ -69,14 +70,15 @@ struct PcReusePolicy {
         ++pc_setups;
         pc_matrix_update = matrix_updates;
         rhs_solves = 0;
-        fresh = 0;
+        fresh[0] = fresh[1] = fresh[2] = 0;
     }
     bool lagged() const { return pc_matrix_update != matrix_updates; }
-    // After a solve with `attempt_iterations` iterations of the final attempt.
-    void afterSolve(int status, int attempt_iterations, int total_iterations, const SolverConfig& cfg) {
+    // After a solve of right-hand side `rhs` with `attempt_iterations` iterations of the final attempt.
+    void afterSolve(int status, int attempt_iterations, int total_iterations, const SolverConfig& cfg, int rhs = 0) {
+        int& f = fresh[rhs < 0 || rhs > 2 ? 0 : rhs];
         if (status == 0) {
-            if (!lagged()) fresh = std::max(fresh, attempt_iterations);
-            else if (attempt_iterations > cfg.reuse_growth * static_cast<double>(std::max(fresh, 1)))
+            if (!lagged()) f = std::max(f, attempt_iterations);
+            else if (attempt_iterations > cfg.reuse_growth * static_cast<double>(std::max(f, 1)))
                 force_rebuild = true;
         }
         if (total_iterations > 0) ++rhs_solves;
@@ -98,10 +100,13 @@ public:
     explicit KrylovSolver(Context& ctx);
     ~KrylovSolver();
     // Scalar system; x holds the guess on entry (warm start) and the solution on exit.
+    // cfg.solver selects the method: 0 CG (persistent kernel with AMG, Jacobi or no
+    // preconditioner), 1 BiCGStab (point Jacobi), 2 GMRES(30), 3 FGMRES(30) (with pc).
     SolveOutcome solveScalar(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc,
                              const double* b, double* x);
     // Three right-hand sides (xyz interleaved) sharing one matrix; Jacobi-preconditioned
-    // BiCGStab in lockstep, one matrix read per product for all three.
+    // BiCGStab in lockstep, one matrix read per product for all three (cfg.solver 1);
+    // GMRES / FGMRES / CG solve the components one after another.
     void solveVector3(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                       SolveOutcome out[3]);
     // One right-hand side, Jacobi-preconditioned BiCGStab (non-symmetric scalar systems:
@@ -122,11 +127,32 @@ private:
     template <int C>
     void lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                           SolveOutcome out[]);
+    SolveOutcome cgComponent(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc, int c,
+                             const double* b, double* x);
     SolveOutcome solvePersistent(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg,
                                  const double* jacobi_diag, const double* b, double* x);
     struct Impl;
     std::unique_ptr<Impl> impl_;
 };
+
+// Workspace of the restarted GMRES / FGMRES solver (gmres.cu): the Krylov basis
+// V ((m+1) x n), the preconditioned directions Z (FGMRES, m x n) and scratch.
+struct GmresWorkspace {
+    int restart = 30;  // m (the reference's PETSc default restart, at most 30 here)
+    DeviceArray<double> V, Z, w, r, zt, bc, xc, partial, coef;
+    void ensure(int n, int m, bool flexible);
+};
+
+// Restarted right-preconditioned GMRES(m) (cfg.solver 2) or FGMRES(m) (3) with the
+// reference's acceptance contract; pc may be nullptr (gmres.cu).
+SolveOutcome gmresSolve(Context& ctx, GmresWorkspace& ws, const Dcsr<double>& A, const SolverConfig& cfg,
+                        Preconditioner* pc, const double* b, double* x);
+// Component c of a C-component xyz-interleaved vector copied to (gather) or from a
+// contiguous n-vector (gmres.cu).
+void componentCopy(Context& ctx, int n, int C, int c, const double* in, double* out, bool gather);
+// gmresSolve for component c of C xyz-interleaved right-hand sides sharing A.
+SolveOutcome gmresComponent(Context& ctx, GmresWorkspace& ws, const Dcsr<double>& A, const SolverConfig& cfg,
+                            Preconditioner* pc, int C, int c, const double* b, double* x);
 
 // Jacobi preconditioner (point diagonal).
 struct JacobiPreconditioner : Preconditioner {

@@ -539,8 +539,7 @@ TransportResult KOmegaModel::solveTransport(DeviceField& U, DeviceField& phi) {
         JacobiPreconditioner jac;
         jac.diag = eq.diag.data();
         jac.n = N;
-        const SolveOutcome o = scfg.solver == 0 ? krylov_.solveScalar(A, scfg, &jac, eq.src.data(), x.v.data())
-                                                : krylov_.solveBicgstab(A, scfg, eq.src.data(), x.v.data());
+        const SolveOutcome o = krylov_.solveScalar(A, scfg, &jac, eq.src.data(), x.v.data());
         res.iterations += o.iterations;
         res.linear_converged = res.linear_converged && o.status == 0;
         res.healthy = res.healthy && o.status != 2 && std::isfinite(o.final_) && std::isfinite(r0);
@@ -620,8 +619,7 @@ TransportResult KOmegaModel::solveSpalartAllmaras(DeviceField& U, DeviceField& p
     jac.diag = eq.diag.data();
     jac.n = N;
     const SolverConfig& scfg = cfg_.omega_solver;
-    const SolveOutcome o = scfg.solver == 0 ? krylov_.solveScalar(A, scfg, &jac, eq.src.data(), omega_.v.data())
-                                            : krylov_.solveBicgstab(A, scfg, eq.src.data(), omega_.v.data());
+    const SolveOutcome o = krylov_.solveScalar(A, scfg, &jac, eq.src.data(), omega_.v.data());
     res.iterations = o.iterations;
     res.linear_converged = o.status == 0;
     res.residual = r0;

@@ -264,10 +264,55 @@ int bsg_equ_download(const bsg_equation* eq, double* diagonal, double* upper, do
  * Solves the LDU system given in host memory for 1 or 3 right-hand sides that
  * share one matrix.  x is the initial guess when warm_start and the solution
  * on return; source and x are xyz-interleaved for 3 components.  results gets
- * one entry per component. */
+ * one entry per component.  The mesh keeps one persistent system per component
+ * count for these calls (see bsg_system_solve); a caller with several
+ * equations should keep one bsg_system per equation instead. */
 int bsg_solve_ldu(bsg_mesh* mesh, const bsg_solver_config* config, int32_t components,
                   const double* diagonal, const double* upper, const double* lower,
                   const double* source, double* x, bsg_solve_result* results);
+
+/* One equation's persistent linear system (PetscLinearSystem,
+ * src/backend/petsc_linear_system.cpp; PetscBackend keeps one per equation
+ * identity "scalar:<equation>:<field>" / "vector:...", petsc_backend.cpp:201-213).
+ * Device buffers, the SELL copy and the AMG structure are made by the first
+ * solve and reused by every later one.  Each solve follows updateMatrix /
+ * prepare / solveRhs (petsc_linear_system.cpp:257-481): an exactly unchanged
+ * matrix is not re-uploaded (a right-hand-side-only solve); an AMG hierarchy is
+ * reused (lagged) until preconditioner_rebuild_interval matrix versions or
+ * right-hand-side solves have passed since its setup, rebuilt before the next
+ * solve after a lagged solve needed more than
+ * preconditioner_reuse_iteration_growth times the fresh iterations, and a
+ * lagged solve that fails is retried once from the same guess with a fresh
+ * hierarchy.  Jacobi-type preconditioners are formed from the current diagonal
+ * on every solve (free on the device), so only AMG setups are lagged.  Destroy
+ * every system before its mesh. */
+typedef struct bsg_system bsg_system;
+int bsg_system_create(bsg_mesh* mesh, int32_t components, bsg_system** out);
+int bsg_system_destroy(bsg_system* system);
+int bsg_system_solve(bsg_system* system, const bsg_solver_config* config, const double* diagonal,
+                     const double* upper, const double* lower, const double* source, double* x,
+                     bsg_solve_result* results);
+/* The EquationPerformanceCounters fields one system fills
+ * (include/babelsim/solver_control.h:37-60; PetscBackend::record*,
+ * petsc_backend.cpp:228-286); seconds are host wall time of each stage. */
+typedef struct {
+    uint64_t linear_solves;           /* one per right-hand side */
+    uint64_t krylov_iterations;
+    uint64_t matrix_value_updates;
+    uint64_t rhs_only_solves;
+    uint64_t preconditioner_setups;
+    uint64_t preconditioner_reuses;
+    uint64_t preconditioner_retries;
+    uint64_t true_residual_checks;
+    double matrix_update_seconds;
+    double preconditioner_seconds;
+    double solve_seconds;
+    int32_t last_status;
+    double last_initial_residual;
+    double last_final_residual;
+    double last_relative_residual;
+} bsg_system_counters;
+int bsg_system_counters_read(const bsg_system* system, bsg_system_counters* out);
 
 /* ---- allocation-free solve ---------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -193,3 +193,47 @@ def fields_at_reference_count(make_sim, n, target):
     U, p, _ = sim.fields()
     sim.close()
     return r, U, p
+
+
+class ReferenceCounters:
+    """PetscLinearSystem::updateMatrix / prepare / setup / solveRhs bookkeeping, one system."""
+
+    def __init__(self, interval=8, growth=2.0):
+        self.interval, self.growth = interval, growth
+        self.matrix_updates = 0
+        self.pc_matrix_update = 0
+        self.setups = 0
+        self.rhs_solves = 0
+        self.fresh = 0
+        self.setup_pending = True      # configure() (petsc_linear_system.cpp:190-194)
+        self.force_rebuild = True
+
+    def solve(self, changed, its, status):
+        if changed:                    # updateMatrix: values differ
+            self.matrix_updates += 1
+            self.setup_pending = True
+        rebuilt = False
+        if self.setup_pending or self.force_rebuild:     # prepare
+            reuse = (self.setups != 0 and not self.force_rebuild
+                     and self.matrix_updates - self.pc_matrix_update < self.interval
+                     and self.rhs_solves < self.interval)
+            if not reuse:                                # setup(false)
+                self.setups += 1
+                self.pc_matrix_update = self.matrix_updates
+                self.rhs_solves = 0
+                self.fresh = 0
+                rebuilt = True
+            self.setup_pending = False
+            self.force_rebuild = False
+        if status == 0:                                  # solveRhs after a converged attempt
+            if self.pc_matrix_update == self.matrix_updates:
+                self.fresh = max(self.fresh, its)
+            elif its > self.growth * max(self.fresh, 1):
+                self.force_rebuild = True
+        if its > 0:
+            self.rhs_solves += 1
+        return rebuilt
+
+    def lagged(self):
+        """After solve(): the solve ran with a preconditioner built for an older matrix."""
+        return self.pc_matrix_update != self.matrix_updates

@@ -11,6 +11,8 @@ import subprocess
 
 import pytest
 
+from helpers import ReferenceCounters
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA_INCLUDE = "/usr/local/cuda/include"
 
@@ -31,46 +33,6 @@ int main(int argc, char** argv) {
     return 0;
 }
 """
-
-
-class ReferenceCounters:
-    """PetscLinearSystem::updateMatrix / prepare / setup / solveRhs bookkeeping, one system."""
-
-    def __init__(self, interval=8, growth=2.0):
-        self.interval, self.growth = interval, growth
-        self.matrix_updates = 0
-        self.pc_matrix_update = 0
-        self.setups = 0
-        self.rhs_solves = 0
-        self.fresh = 0
-        self.setup_pending = True      # configure() (petsc_linear_system.cpp:190-194)
-        self.force_rebuild = True
-
-    def solve(self, changed, its, status):
-        if changed:                    # updateMatrix: values differ
-            self.matrix_updates += 1
-            self.setup_pending = True
-        rebuilt = False
-        if self.setup_pending or self.force_rebuild:     # prepare
-            reuse = (self.setups != 0 and not self.force_rebuild
-                     and self.matrix_updates - self.pc_matrix_update < self.interval
-                     and self.rhs_solves < self.interval)
-            if not reuse:                                # setup(false)
-                self.setups += 1
-                self.pc_matrix_update = self.matrix_updates
-                self.rhs_solves = 0
-                self.fresh = 0
-                rebuilt = True
-            self.setup_pending = False
-            self.force_rebuild = False
-        if status == 0:                                  # solveRhs after a converged attempt
-            if self.pc_matrix_update == self.matrix_updates:
-                self.fresh = max(self.fresh, its)
-            elif its > self.growth * max(self.fresh, 1):
-                self.force_rebuild = True
-        if its > 0:
-            self.rhs_solves += 1
-        return rebuilt
 
 
 @pytest.fixture(scope="module")
