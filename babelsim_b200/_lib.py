@@ -31,7 +31,7 @@ EXPORTS = [
     "bsg_system_create", "bsg_system_destroy", "bsg_system_solve", "bsg_system_counters_read",
     "bsg_simple_create",
     "bsg_simple_set_boundary", "bsg_simple_set_fields", "bsg_simple_set_flux", "bsg_simple_load_state",
-    "bsg_simple_iterate", "bsg_simple_enable_komega", "bsg_simple_enable_kepsilon",
+    "bsg_simple_iterate", "bsg_simple_set_segments", "bsg_simple_segment_report", "bsg_simple_enable_komega", "bsg_simple_enable_kepsilon",
     "bsg_simple_enable_spalart_allmaras", "bsg_simple_set_wall_distance", "bsg_simple_set_turbulence_fields",
     "bsg_simple_get_turbulence_fields", "bsg_simple_get_fields",
     "bsg_simple_destroy", "bsg_piso_create", "bsg_piso_set_boundary", "bsg_piso_set_fields", "bsg_piso_advance",
@@ -195,6 +195,8 @@ def lib():
             "bsg_simple_set_boundary": [vp, C.c_char_p, i32, i32, vp], "bsg_simple_set_fields": [vp, vp, vp],
             "bsg_simple_set_flux": [vp, vp],
             "bsg_simple_iterate": [vp, i32, C.POINTER(SimpleReport)],
+            "bsg_simple_set_segments": [vp, i32, vp, vp],
+            "bsg_simple_segment_report": [vp, i32, C.POINTER(SimpleReport)],
             "bsg_simple_enable_komega": [vp, C.POINTER(KOmegaConfig)],
             "bsg_simple_enable_kepsilon": [vp, C.POINTER(KEpsilonConfig)],
             "bsg_simple_enable_spalart_allmaras": [vp, C.POINTER(SaConfig)],

@@ -468,6 +468,18 @@ class Simple(_TurbulenceModels):
         check(lib().bsg_simple_iterate(self.h, max_iterations, C.byref(r)), self.mesh.ctx.h)
         return r
 
+    def set_segments(self, cell_offsets, viscosity):
+        """Block-diagonal batch: case k owns cells [cell_offsets[k], cell_offsets[k+1]) of a mesh
+        made by meshgen.concatenate, with dynamic viscosity viscosity[k] (before set_fields)."""
+        off = np.ascontiguousarray(cell_offsets, dtype=np.int32)
+        mu = f64(viscosity)
+        check(lib().bsg_simple_set_segments(self.h, len(mu), ptr(off), ptr(mu)), self.mesh.ctx.h)
+
+    def segment_report(self, k: int) -> SimpleReport:
+        r = SimpleReport()
+        check(lib().bsg_simple_segment_report(self.h, k, C.byref(r)), self.mesh.ctx.h)
+        return r
+
     def fields(self):
         m = self.mesh
         U, p, phi = np.zeros((m.n_cells, 3)), np.zeros(m.n_cells), np.zeros(m.n_faces)

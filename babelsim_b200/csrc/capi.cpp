@@ -1034,24 +1034,41 @@ int bsg_simple_load_state(bsg_simple* s, const double* U, const double* p, const
     });
 }
 
+void fillReport(const bsg::SimpleReport& r, bsg_simple_report* report) {
+    report->iterations = r.iterations;
+    report->converged = r.converged;
+    report->status = r.status;
+    report->mass = r.mass;
+    report->dU = r.dU;
+    report->rU = r.rU;
+    report->dP = r.dP;
+    report->linear_pressure_residual = r.linP;
+    report->momentum_iterations = r.momentum_iterations;
+    report->pressure_iterations = r.pressure_iterations;
+    report->turbulence_change = r.turbulence_change;
+    report->turbulence_residual = r.turbulence_residual;
+}
+
 int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report* report) {
     return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
         require(s && max_iterations >= 0, "bad argument");
         const bsg::SimpleReport r = s->solver->iterate(max_iterations);
-        if (report) {
-            report->iterations = r.iterations;
-            report->converged = r.converged;
-            report->status = r.status;
-            report->mass = r.mass;
-            report->dU = r.dU;
-            report->rU = r.rU;
-            report->dP = r.dP;
-            report->linear_pressure_residual = r.linP;
-            report->momentum_iterations = r.momentum_iterations;
-            report->pressure_iterations = r.pressure_iterations;
-            report->turbulence_change = r.turbulence_change;
-            report->turbulence_residual = r.turbulence_residual;
-        }
+        if (report) fillReport(r, report);
+    });
+}
+
+int bsg_simple_set_segments(bsg_simple* s, int32_t n_segments, const int32_t* cell_offsets, const double* viscosity) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && cell_offsets && viscosity && n_segments > 0, "bad argument");
+        s->solver->setSegments(std::vector<int>(cell_offsets, cell_offsets + n_segments + 1),
+                               std::vector<double>(viscosity, viscosity + n_segments));
+    });
+}
+
+int bsg_simple_segment_report(const bsg_simple* s, int32_t segment, bsg_simple_report* report) {
+    return guard(s ? ctxOf(s->mesh) : nullptr, [&] {
+        require(s && report, "null argument");
+        fillReport(s->solver->segmentReport(segment), report);
     });
 }
 

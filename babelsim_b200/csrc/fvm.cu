@@ -585,11 +585,11 @@ __global__ void kScaleArray(long long n, double f, double* __restrict__ a) {
 }
 
 // reference(Equation, value) row-sum test (procedural_equation.cpp:316-333).
-__global__ void kReferenceCheck(int n, const int* __restrict__ ptr, const double* __restrict__ diag,
+__global__ void kReferenceCheck(int row0, int n, const int* __restrict__ ptr, const double* __restrict__ diag,
                                 const double* __restrict__ val, int* __restrict__ all_constant) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = row0 + blockIdx.x * blockDim.x + threadIdx.x;
     int ok = 1;
-    if (i < n) {
+    if (i < row0 + n) {
         double row = diag[i], mag = fabs(diag[i]);
         for (int k = ptr[i]; k < ptr[i + 1]; ++k) { row += val[k]; mag += fabs(val[k]); }
         ok = isfinite(row) && fabs(row) <= 64.0 * kEps * mag;
@@ -598,13 +598,14 @@ __global__ void kReferenceCheck(int n, const int* __restrict__ ptr, const double
     if ((threadIdx.x & 31) == 0 && !warp_ok) atomicAnd(all_constant, 0);
 }
 
-// reference(Equation, cell 0, value) (procedural_equation.cpp:306-315).
-__global__ void kApplyReference(const int* __restrict__ flag, double value, double* __restrict__ diag,
+// reference(Equation, cell 0, value) (procedural_equation.cpp:306-315); cell `row0`, the
+// first cell of a segment, when the mesh holds several independent cases.
+__global__ void kApplyReference(int row0, const int* __restrict__ flag, double value, double* __restrict__ diag,
                                 double* __restrict__ src, int* __restrict__ error) {
     if (*flag) {
-        if (!(diag[0] > 0.0)) { *error = 1; return; }
-        src[0] += diag[0] * value;
-        diag[0] *= 2.0;
+        if (!(diag[row0] > 0.0)) { *error = 1; return; }
+        src[row0] += diag[row0] * value;
+        diag[row0] *= 2.0;
     }
 }
 
@@ -628,13 +629,13 @@ __global__ void kApply(int n, const int* __restrict__ ptr, const int* __restrict
 
 // Partial sums of ||b-Ax||^2, ||Ax||^2, ||b||^2 (relativeResidual, procedural_equation.cpp:429-433).
 template <int C>
-__global__ void kResidualNorms(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+__global__ void kResidualNorms(int row0, int n, const int* __restrict__ ptr, const int* __restrict__ col,
                                const double* __restrict__ diag, const double* __restrict__ val,
                                const double* __restrict__ src, const double* __restrict__ x,
                                double* __restrict__ partial) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = row0 + blockIdx.x * kBlock + threadIdx.x;
     double v[3] = {0.0, 0.0, 0.0};
-    if (i < n) {
+    if (i < row0 + n) {
         double acc[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) acc[c] = diag[i] * x[C * i + c];
@@ -655,11 +656,11 @@ __global__ void kResidualNorms(int n, const int* __restrict__ ptr, const int* __
 }
 
 // Flux balance per cell (fvm_execution.cpp:149-177): partial l1, l2^2, scale, and max.
-__global__ void kFluxBalance(MeshView m, const double* __restrict__ phi, double* __restrict__ partial) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+__global__ void kFluxBalance(int row0, int n, MeshView m, const double* __restrict__ phi, double* __restrict__ partial) {
+    const int i = row0 + blockIdx.x * kBlock + threadIdx.x;
     double v[3] = {0.0, 0.0, 0.0};
     double mx = 0.0;
-    if (i < m.n_cells) {
+    if (i < row0 + n) {
         double imb = 0.0, sc = 0.0;
         for (int k = m.cf_ptr[i]; k < m.cf_ptr[i + 1]; ++k) {
             const int f = m.cf_face[k];
@@ -1124,17 +1125,18 @@ void scale(DeviceEquation& eq, double f) {
     for (auto& s : eq.diffusion) s->factor *= f;
 }
 
-void referenceIfUnanchored(DeviceEquation& eq, double value, int* flag_dev) {
+void referenceIfUnanchored(DeviceEquation& eq, double value, int* flag_dev, int row0, int nrows) {
     if (eq.x->comps != 1) fail(kArgument, "reference requires a scalar equation");
     if (!std::isfinite(value)) fail(kArgument, "nonfinite equ coefficient");
     DeviceMesh& m = *eq.x->mesh;
     Context& ctx = *m.ctx;
+    const int n = nrows < 0 ? m.n_cells : nrows;
     // flag_dev[0] = all-constant flag, flag_dev[1] = error flag
     const int init[2] = {1, 0};
     BSG_CUDA(cudaMemcpyAsync(flag_dev, init, sizeof(init), cudaMemcpyHostToDevice, ctx.stream));
-    launch(ctx, kReferenceCheck, m.n_cells, m.n_cells, (const int*)m.cf_ptr.data(), (const double*)eq.diag.data(),
+    launch(ctx, kReferenceCheck, n, row0, n, (const int*)m.cf_ptr.data(), (const double*)eq.diag.data(),
            (const double*)eq.val.data(), flag_dev);
-    kApplyReference<<<1, 1, 0, ctx.stream>>>(flag_dev, value, eq.diag.data(), eq.src.data(), flag_dev + 1);
+    kApplyReference<<<1, 1, 0, ctx.stream>>>(row0, flag_dev, value, eq.diag.data(), eq.src.data(), flag_dev + 1);
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
 }
@@ -1169,27 +1171,29 @@ void faceFluxEquation(DeviceEquation& eq, const double* solution, DeviceArray<do
     }
 }
 
-void relativeResidualNorms(const DeviceEquation& eq, const double* x, Reducer& red) {
+void relativeResidualNorms(const DeviceEquation& eq, const double* x, Reducer& red, int row0, int nrows) {
     DeviceMesh& m = *eq.x->mesh;
     Context& ctx = *m.ctx;
-    const int blocks = static_cast<int>(gridFor(m.n_cells, kBlock));
+    const int n = nrows < 0 ? m.n_cells : nrows;
+    const int blocks = static_cast<int>(gridFor(n, kBlock));
     red.ensure(blocks, 3);
     if (eq.x->comps == 1)
-        launch(ctx, kResidualNorms<1>, m.n_cells, m.n_cells, (const int*)m.cf_ptr.data(), (const int*)m.cf_col.data(),
+        launch(ctx, kResidualNorms<1>, n, row0, n, (const int*)m.cf_ptr.data(), (const int*)m.cf_col.data(),
                eq.diag.data(), eq.val.data(), eq.src.data(), x, red.partial.data());
     else
-        launch(ctx, kResidualNorms<3>, m.n_cells, m.n_cells, (const int*)m.cf_ptr.data(), (const int*)m.cf_col.data(),
+        launch(ctx, kResidualNorms<3>, n, row0, n, (const int*)m.cf_ptr.data(), (const int*)m.cf_col.data(),
                eq.diag.data(), eq.val.data(), eq.src.data(), x, red.partial.data());
     kFinishReduce<<<1, 32 * 3, 0, ctx.stream>>>(blocks, 3, 0u, red.partial.data(), red.result.data());
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
 }
 
-void fluxBalance(DeviceMesh& m, const double* phi, Reducer& red) {
+void fluxBalance(DeviceMesh& m, const double* phi, Reducer& red, int row0, int nrows) {
     Context& ctx = *m.ctx;
-    const int blocks = static_cast<int>(gridFor(m.n_cells, kBlock));
+    const int n = nrows < 0 ? m.n_cells : nrows;
+    const int blocks = static_cast<int>(gridFor(n, kBlock));
     red.ensure(blocks, 4);
-    launch(ctx, kFluxBalance, m.n_cells, view(m), phi, red.partial.data());
+    launch(ctx, kFluxBalance, n, row0, n, view(m), phi, red.partial.data());
     kFinishReduce<<<1, 32 * 4, 0, ctx.stream>>>(blocks, 4, 0x8u, red.partial.data(), red.result.data());
     BSG_CUDA(cudaGetLastError());
     ctx.launched();

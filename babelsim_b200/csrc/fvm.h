@@ -108,16 +108,19 @@ void addReaction(DeviceEquation& eq, const double* coefficient, double c, double
 void checkValues(Context& ctx, const double* a, long long n, int* flags_dev, int out[2]);
 void scale(DeviceEquation& eq, double f);
 // Returns through *flag_dev (device int) whether the gauge was applied; host reads if asked.
-void referenceIfUnanchored(DeviceEquation& eq, double value, int* flag_dev);
+// With nrows >= 0 only cells [row0, row0 + nrows) are checked and cell row0 is the anchor
+// (one segment of a mesh that holds several independent cases).
+void referenceIfUnanchored(DeviceEquation& eq, double value, int* flag_dev, int row0 = 0, int nrows = -1);
 void applyEquation(const DeviceEquation& eq, const double* x, double* y);
 // y = b - A x (procedural_equation.cpp:291-296)
 void residualEquation(const DeviceEquation& eq, const double* x, double* y);
 void faceFluxEquation(DeviceEquation& eq, const double* solution, DeviceArray<double>& out_face);
-// ||b-Ax||, ||Ax||, ||b|| into red.result[0..2]
-void relativeResidualNorms(const DeviceEquation& eq, const double* x, Reducer& red);
+// ||b-Ax||, ||Ax||, ||b|| into red.result[0..2] (over cells [row0, row0 + nrows) when nrows >= 0)
+void relativeResidualNorms(const DeviceEquation& eq, const double* x, Reducer& red, int row0 = 0, int nrows = -1);
 
 // ---- device reductions and vector helpers ------------------------------------
-void fluxBalance(DeviceMesh& m, const double* phi, Reducer& red);          // l1, l2^2, scale, max
+// l1, l2^2, scale, max over cells [row0, row0 + nrows) (all cells when nrows < 0)
+void fluxBalance(DeviceMesh& m, const double* phi, Reducer& red, int row0 = 0, int nrows = -1);
 void relativeChangeNorms(Context& ctx, const double* a, const double* b, long long n, Reducer& red);  // |a-b|^2, |a|^2
 void copyAsync(Context& ctx, double* dst, const double* src, long long n);
 void axpyCell(Context& ctx, double* y, double a, const double* x, long long n);

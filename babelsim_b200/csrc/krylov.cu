@@ -908,6 +908,157 @@ SolveOutcome KrylovSolver::solveScalar(const Dcsr<double>& A, const SolverConfig
     return out;
 }
 
+namespace {
+// CTAs for each system of a batch: about two level-0 slices per warp, at least one CTA,
+// scaled down in proportion (keeping one each) when the batch exceeds the resident grid.
+std::vector<int> allotCtas(const std::vector<long long>& slices, int capacity) {
+    const int k = static_cast<int>(slices.size());
+    if (k > capacity) fail(kArgument, "batch larger than the resident grid: split it");
+    std::vector<int> c(k);
+    long long want = 0, total = 0;
+    for (int i = 0; i < k; ++i) {
+        c[i] = static_cast<int>(std::max<long long>(1, (slices[i] + 15) / 16));
+        want += c[i];
+        total += slices[i];
+    }
+    if (want > capacity) {
+        int used = 0;
+        for (int i = 0; i < k; ++i) {
+            c[i] = static_cast<int>(std::max<long long>(1, (capacity - k) * slices[i] / std::max<long long>(total, 1)));
+            used += c[i];
+        }
+        for (int i = 0; used > capacity; i = (i + 1) % k)
+            if (c[i] > 1) { --c[i]; --used; }
+    }
+    std::vector<int> begin(k + 1, 0);
+    for (int i = 0; i < k; ++i) begin[i + 1] = begin[i] + c[i];
+    return begin;
+}
+}  // namespace
+
+void KrylovSolver::solveBatch(Context& ctx, std::vector<BatchSolve>& items) {
+    const int K = static_cast<int>(items.size());
+    if (K == 0) return;
+    struct Track {
+        PcgState h{};
+        double scale = 1.0, target = 0.0, fin = 0.0;
+        int used = 0;
+        bool done = false;
+    };
+    std::vector<Track> t(K);
+    for (int k = 0; k < K; ++k) {
+        BatchSolve& it = items[k];
+        if (!it.amg || !it.solver || it.cfg.solver != 0 || it.cfg.precision == 1)
+            fail(kArgument, "batched solves take CG with the AMG preconditioner in FP64 or with an FP32 V-cycle");
+        Impl& m = *it.solver->impl_;
+        if (&m.ctx != &ctx) fail(kArgument, "batched solves must share one context");
+        m.ensure(it.A.n);
+        if (m.pst.size() < 1) m.pst.resize(1);
+        t[k].h.target2 = -1.0;
+        t[k].h.warm = it.cfg.warm_start ? 1 : 0;
+        t[k].h.max_iterations = it.cfg.max_iterations;
+        t[k].h.atol = it.cfg.atol;
+        t[k].h.rtol = it.cfg.rtol;
+        it.out = SolveOutcome{};
+    }
+    static thread_local DeviceArray<double> norms;
+    if (norms.size() < static_cast<std::size_t>(K)) norms.resize(K);
+    std::vector<PcgState> states(K);
+    std::vector<double> nrm(K);
+    const int capacity = sellBatchCapacity(ctx);
+    BatchLaunch<double, double> batch64;
+    BatchLaunch<double, float> batch32;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        std::vector<int> active;
+        for (int k = 0; k < K; ++k)
+            if (!t[k].done) active.push_back(k);
+        if (active.empty()) break;
+        // one launch per V-cycle precision
+        for (int fp32 = 0; fp32 < 2; ++fp32) {
+            std::vector<int> group;
+            std::vector<long long> slices;
+            for (int k : active)
+                if (items[k].amg->fp32VCycle() == (fp32 == 1)) {
+                    group.push_back(k);
+                    slices.push_back(items[k].amg->krylovMatrix().nslices);
+                }
+            if (group.empty()) continue;
+            for (int k : group)
+                BSG_CUDA(cudaMemcpyAsync(items[k].solver->impl_->pst.data(), &t[k].h, sizeof(PcgState),
+                                         cudaMemcpyHostToDevice, ctx.stream));
+            if (fp32 == 0) {
+                batch64.args.clear();
+                for (int k : group) {
+                    Impl& m = *items[k].solver->impl_;
+                    batch64.args.push_back({items[k].amg->krylovMatrix(), items[k].amg->sellView64(), items[k].b,
+                                            items[k].x, m.r.data(), m.z.data(), m.p.data(), m.v.data(), m.q.data(),
+                                            m.partial.data(), m.pst.data(), PhaseLog{}});
+                }
+                batch64.cta_begin = allotCtas(slices, capacity);
+                launchSellPcgBatch(ctx, batch64);
+            } else {
+                batch32.args.clear();
+                for (int k : group) {
+                    Impl& m = *items[k].solver->impl_;
+                    SellPcgArgs<double, float> a{items[k].amg->krylovMatrix(), items[k].amg->sellView32(),
+                                                 items[k].b, items[k].x, m.r.data(), m.z.data(), m.p.data(),
+                                                 m.v.data(), m.q.data(), m.partial.data(), m.pst.data(), PhaseLog{}, 1};
+                    batch32.args.push_back(a);
+                }
+                batch32.cta_begin = allotCtas(slices, capacity);
+                launchSellPcgBatch(ctx, batch32);
+            }
+        }
+        // solve states and true residuals of every system of this attempt, read back together
+        for (int k : active) {
+            BatchSolve& it = items[k];
+            Impl& m = *it.solver->impl_;
+            const int g = m.grid(it.A.n);
+            kResidual<<<g, kBlock, 0, ctx.stream>>>(it.A, it.b, it.x, m.r.data(), m.partial.data());
+            kFinishNorm<<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), norms.data() + k);
+            ctx.launches += 2;
+            BSG_CUDA(cudaMemcpyAsync(&states[k], m.pst.data(), sizeof(PcgState), cudaMemcpyDeviceToHost, ctx.stream));
+        }
+        BSG_CUDA(cudaGetLastError());
+        BSG_CUDA(cudaMemcpyAsync(nrm.data(), norms.data(), sizeof(double) * K, cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        for (int k : active) {
+            BatchSolve& it = items[k];
+            Track& tr = t[k];
+            const PcgState& r = states[k];
+            if (r.status == 3) fail(kCuda, "batched persistent PCG: a segment barrier wait ran past its bound");
+            ++it.out.checks;
+            if (attempt == 0) {
+                it.out.initial = std::sqrt(r.rr0);
+                tr.scale = residualScale(std::sqrt(r.rr0), std::sqrt(r.bb));
+                tr.target = std::max(it.cfg.atol, it.cfg.rtol * tr.scale);
+                if (r.iterations == 0 && r.status == 0) {
+                    it.out.status = 0;
+                    it.out.final_ = it.out.initial;
+                    it.out.relative = it.out.initial / tr.scale;
+                    tr.done = true;
+                    continue;
+                }
+            }
+            tr.used += r.iterations;
+            tr.fin = std::sqrt(nrm[k]);
+            if (!std::isfinite(tr.fin) || tr.fin <= tr.target || r.status == 2 || tr.used >= it.cfg.max_iterations ||
+                attempt == 2) {
+                tr.done = true;
+            } else {
+                // true-residual restart from this x with a halved internal target (petsc_linear_system.cpp:412-439)
+                tr.h.target2 = 0.25 * r.target2;
+                tr.h.warm = 1;
+                tr.h.max_iterations = it.cfg.max_iterations - tr.used;
+            }
+            it.out.iterations = tr.used;
+            it.out.final_ = tr.fin;
+            it.out.relative = tr.fin / tr.scale;
+            it.out.status = (std::isfinite(tr.fin) && tr.fin <= tr.target) ? 0 : (std::isfinite(tr.fin) ? 1 : 2);
+        }
+    }
+}
+
 template <int C>
 void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                                     SolveOutcome out[]) {

@@ -44,6 +44,18 @@ struct SolveOutcome {
 };
 
 class AmgPreconditioner;
+class KrylovSolver;
+
+// One system of a batched persistent CG + AMG solve (KrylovSolver::solveBatch).
+struct BatchSolve {
+    KrylovSolver* solver = nullptr;       // owns this system's vectors, partials and solve state
+    AmgPreconditioner* amg = nullptr;     // its hierarchy; level 0 is the Krylov matrix
+    Dcsr<double> A{};                     // the system, for the true-residual checks
+    const double* b = nullptr;
+    double* x = nullptr;
+    SolverConfig cfg{};
+    SolveOutcome out{};
+};
 
 // When a preconditioner built for an earlier matrix version is reused (lagged), as
 // PetscLinearSystem does (src/backend/petsc_linear_system.cpp:257-324, 446-470): a
@@ -112,6 +124,12 @@ public:
     // One right-hand side, Jacobi-preconditioned BiCGStab (non-symmetric scalar systems:
     // transported turbulence quantities, and any scalar equation configured with kspType bcgs).
     SolveOutcome solveBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x);
+    // Several independent CG + AMG systems (FP64, or FP64 CG with an FP32 V-cycle) solved
+    // together: each attempt of every unfinished system runs in one cooperative launch, on
+    // CTAs of its own, with the same acceptance loop per system as solveScalar (true-residual
+    // restarts with a halved internal target).  The true residuals of all systems are read
+    // back together.  Every item's solver must be on ctx.
+    static void solveBatch(Context& ctx, std::vector<BatchSolve>& items);
     int check_interval = 8;  // iterations between host convergence checks
     // CG with AMG, Jacobi or no preconditioner runs as one persistent cooperative
     // kernel per attempt (pcg_persistent.cu); set false to use per-kernel launches.

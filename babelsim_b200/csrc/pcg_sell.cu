@@ -21,14 +21,66 @@ constexpr int SB = BSG_SELL_SB;  // threads per block
 #define BSG_SELL_MIN_BLOCKS 3
 #endif
 
+// The CTAs that cooperate on one solve.  GridGroup: the whole cooperative grid,
+// synchronised by cooperative groups.  SegmentGroup: a contiguous range of the
+// grid's CTAs that owns one system of a batch; its barrier is a counter and a
+// generation word in global memory (all CTAs of a cooperative launch are
+// resident, so the spin always ends), and every wait is bounded: past
+// kBarrierCycles the group records an abort and its barriers stop waiting, so
+// the launch ends and the host reports the failure instead of hanging.
+struct GridGroup {
+    cg::grid_group g;
+    __device__ GridGroup() : g(cg::this_grid()) {}
+    __device__ __forceinline__ int rank() const { return blockIdx.x; }
+    __device__ __forceinline__ int size() const { return gridDim.x; }
+    __device__ __forceinline__ void sync() { g.sync(); }
+    __device__ __forceinline__ bool aborted() const { return false; }
+};
+
+constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s at the B200's clock
+
+struct SegmentGroup {
+    int cta0, ncta;
+    SegmentBarrier* bar;
+    __device__ __forceinline__ int rank() const { return blockIdx.x - cta0; }
+    __device__ __forceinline__ int size() const { return ncta; }
+    __device__ __forceinline__ bool aborted() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
+    __device__ void sync() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile unsigned* gen = &bar->generation;
+            const unsigned g0 = *gen;
+            __threadfence();
+            if (atomicAdd(&bar->count, 1u) == static_cast<unsigned>(ncta) - 1u) {
+                atomicExch(&bar->count, 0u);
+                __threadfence();
+                atomicAdd(&bar->generation, 1u);
+            } else {
+                const long long t0 = clock64();
+                while (*gen == g0) {
+                    if (aborted()) break;
+                    if (clock64() - t0 > kBarrierCycles) {
+                        atomicExch(&bar->abort, 1);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+    }
+};
+
 struct Lanes {
     int lane, gwarp, nwarps, gthread, nthreads;
 };
 
-__device__ __forceinline__ Lanes lanes() {
+template <class G>
+__device__ __forceinline__ Lanes lanes(const G& g) {
     Lanes c;
-    c.gthread = blockIdx.x * SB + threadIdx.x;
-    c.nthreads = gridDim.x * SB;
+    c.gthread = g.rank() * SB + threadIdx.x;
+    c.nthreads = g.size() * SB;
     c.lane = threadIdx.x & 31;
     c.gwarp = c.gthread >> 5;
     c.nwarps = c.nthreads >> 5;
@@ -38,11 +90,11 @@ __device__ __forceinline__ Lanes lanes() {
 // Deterministic grid sum of NV values (FP64); every block returns the same
 // totals.  `buf` alternates between two halves of `partial` so a fast block's
 // next write never overtakes a slow block's read of the previous sum.
-template <int NV>
-__device__ void gridSum(cg::grid_group& g, double v[NV], double* partial, int& buf) {
+template <int NV, class G>
+__device__ void gridSum(G& g, double v[NV], double* partial, int& buf) {
     __shared__ double sh[NV][SB / 32];
     __shared__ double tot[NV];
-    double* part = partial + static_cast<long long>(buf) * gridDim.x * NV;
+    double* part = partial + static_cast<long long>(buf) * g.size() * NV;
     buf ^= 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -58,14 +110,14 @@ __device__ void gridSum(cg::grid_group& g, double v[NV], double* partial, int& b
         for (int j = 0; j < NV; ++j) {
             double s = 0.0;
             for (int w = 0; w < SB / 32; ++w) s += sh[j][w];
-            part[blockIdx.x * NV + j] = s;
+            part[g.rank() * NV + j] = s;
         }
     }
     g.sync();
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
         double x = 0.0;
-        for (int b = threadIdx.x; b < gridDim.x; b += SB) x += part[b * NV + j];
+        for (int b = threadIdx.x; b < g.size(); b += SB) x += part[b * NV + j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0) sh[j][warp] = x;
@@ -137,9 +189,9 @@ __device__ __forceinline__ SplitUnit splitUnit(int u, int K, int lane) {
     return {u / K, (u % K) * rows + lane / K, lane % K};
 }
 
-template <class TK, class TV>
-__device__ double vcycle(cg::grid_group& g, const VCycleView<TV>& V, const TK* r, TK* z, const PhaseLog& log) {
-    const Lanes c = lanes();
+template <class TK, class TV, class G>
+__device__ double vcycle(G& g, const VCycleView<TV>& V, const TK* r, TK* z, const PhaseLog& log) {
+    const Lanes c = lanes(g);
     const int L = V.levels;
     // ---- down
     for (int l = 0; l < L - 1; ++l) {
@@ -278,10 +330,9 @@ __device__ __forceinline__ void seedLevel0(const VLevel<TV>& f0, int i, TK ri) {
     f0.w[i] = f0.rd[i] * rv;
 }
 
-template <class TK, class TV>
-__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<TK, TV> a) {
-    cg::grid_group g = cg::this_grid();
-    const Lanes c = lanes();
+template <class TK, class TV, class G>
+__device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
+    const Lanes c = lanes(g);
     const SellMat<TK>& A = a.A;
     const int n = A.n;
     int buf = 0;
@@ -320,7 +371,7 @@ __global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<
         const double t = fmax(atol, rtol * scale);
         target2 = t * t;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (g.rank() == 0 && threadIdx.x == 0) {
         st.rr0 = v[0];
         st.bb = v[1];
         st.target2 = target2;
@@ -329,10 +380,14 @@ __global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<
         st.status = 1;
     }
     if (isfinite(v[0]) && v[0] <= target2) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) st.status = 0;
+        if (g.rank() == 0 && threadIdx.x == 0) st.status = 0;
         return;
     }
     double w[1] = {vcycle<TK, TV>(g, a.V, a.r, a.z, a.log)};
+    if (g.aborted()) {
+        if (g.rank() == 0 && threadIdx.x == 0) st.status = 3;
+        return;
+    }
     gridSum<1>(g, w, a.partial, buf);
     mark(a.log, 4);
     double rz = w[0];
@@ -343,6 +398,7 @@ __global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<
     int status = 1;
     double rr = v[0];
     while (it < max_iterations) {
+        if (g.aborted()) { status = 3; break; }
         if (!isfinite(rz) || rz == 0.0) { status = 2; break; }
         // p_new = z + beta p_old and q = A p_new in one sweep (neighbours' p_new formed on the fly)
         const TK bk = static_cast<TK>(beta);
@@ -392,11 +448,34 @@ __global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<
         pold = pnew;
         pnew = tmp;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (g.rank() == 0 && threadIdx.x == 0) {
         st.rr = rr;
         st.iterations = it;
-        st.status = status;
+        st.status = g.aborted() ? 3 : status;
     }
+}
+
+template <class TK, class TV>
+__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<TK, TV> a) {
+    GridGroup g;
+    pcgBody<TK, TV>(g, a);
+}
+
+// A batch: CTAs [cta_begin[s], cta_begin[s+1]) solve system s with its own
+// arguments, barriers and reductions, independently of the other systems.
+template <class TK, class TV>
+__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS)
+    kPcgSellBatch(const SellPcgArgs<TK, TV>* __restrict__ segs, const int* __restrict__ cta_begin, int nsegs,
+                  SegmentBarrier* bars) {
+    int lo = 0, hi = nsegs - 1;  // the segment whose CTA range holds this block
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cta_begin[mid] <= static_cast<int>(blockIdx.x)) lo = mid;
+        else hi = mid - 1;
+    }
+    SegmentGroup g{cta_begin[lo], cta_begin[lo + 1] - cta_begin[lo], bars + lo};
+    const SellPcgArgs<TK, TV> a = segs[lo];
+    pcgBody<TK, TV>(g, a);
 }
 
 template <class TK, class TV>
@@ -422,6 +501,35 @@ void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& in) {
     ctx.launched();
 }
 
+int sellBatchCapacity(Context& ctx) { return sellGrid<double, double>(ctx); }
+
+template <class TK, class TV>
+void launchSellPcgBatch(Context& ctx, BatchLaunch<TK, TV>& batch) {
+    const int nsegs = static_cast<int>(batch.args.size());
+    if (nsegs == 0) return;
+    if (static_cast<int>(batch.cta_begin.size()) != nsegs + 1 || batch.cta_begin.front() != 0)
+        fail(kArgument, "batched PCG: CTA table does not match the systems");
+    for (int k = 0; k < nsegs; ++k)
+        if (batch.cta_begin[k + 1] <= batch.cta_begin[k]) fail(kArgument, "batched PCG: a system without CTAs");
+    const int total = batch.cta_begin.back();
+    if (total > sellGrid<TK, TV>(ctx)) fail(kArgument, "batched PCG: CTA allotment exceeds the resident grid");
+    batch.d_args.upload(batch.args, ctx.stream);
+    batch.d_cta.upload(batch.cta_begin, ctx.stream);
+    batch.d_bars.resize(nsegs);
+    batch.d_bars.zero(ctx.stream);
+    const SellPcgArgs<TK, TV>* segs = batch.d_args.data();
+    const int* cta = batch.d_cta.data();
+    SegmentBarrier* bars = batch.d_bars.data();
+    int ns = nsegs;
+    void* params[] = {&segs, &cta, &ns, &bars};
+    BSG_PROFILE(ctx, "pcg_amg_persistent_batch");
+    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgSellBatch<TK, TV>), total, SB, params, 0,
+                                         ctx.stream));
+    ctx.launched();
+}
+
+template void launchSellPcgBatch<double, double>(Context&, BatchLaunch<double, double>&);
+template void launchSellPcgBatch<double, float>(Context&, BatchLaunch<double, float>&);
 template void launchSellPcg<double, double>(Context&, const SellPcgArgs<double, double>&);
 template void launchSellPcg<double, float>(Context&, const SellPcgArgs<double, float>&);
 template void launchSellPcg<float, float>(Context&, const SellPcgArgs<float, float>&);

@@ -28,6 +28,8 @@
 #include "pcg_persistent.cuh"
 #include "sell.cuh"
 
+#include <vector>
+
 namespace bsg {
 
 template <class TV>
@@ -74,5 +76,32 @@ struct SellPcgArgs {
 // Launch (pcg_sell.cu); the grid is sized for co-residency.
 template <class TK, class TV>
 void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& args);
+
+// Barrier state of one system of a batch (zeroed before every launch).
+struct SegmentBarrier {
+    unsigned count;
+    unsigned generation;
+    int abort;   // set when a wait ran past its bound; the system's PcgState then has status 3
+    int pad;
+};
+
+// Several independent systems (each with its own matrix, V-cycle, vectors, partials
+// and PcgState, anywhere in device memory) solved by one cooperative launch: system s
+// runs on CTAs [cta_begin[s], cta_begin[s+1]) with barriers of its own, so the systems
+// neither wait for nor perturb one another, and each runs the kernel a single solve on
+// that many CTAs would run.  The host fills args and cta_begin; the launch uploads them.
+template <class TK, class TV>
+struct BatchLaunch {
+    std::vector<SellPcgArgs<TK, TV>> args;
+    std::vector<int> cta_begin;  // args.size() + 1 entries, first 0, last = total CTAs
+    DeviceArray<SellPcgArgs<TK, TV>> d_args;
+    DeviceArray<int> d_cta;
+    DeviceArray<SegmentBarrier> d_bars;
+};
+
+// CTAs one batched launch may use (the co-resident grid of the persistent kernel).
+int sellBatchCapacity(Context& ctx);
+template <class TK, class TV>
+void launchSellPcgBatch(Context& ctx, BatchLaunch<TK, TV>& batch);
 
 }  // namespace bsg

@@ -50,6 +50,26 @@ __global__ void kOwnerTrace(MeshView m, const double* __restrict__ x, double* __
 
 }  // namespace
 
+// One case of a batch (see SimpleSolver::setSegments).
+struct SimpleSegment {
+    int c0 = 0, n = 0;           // cells [c0, c0 + n)
+    int fi0 = 0, nfi = 0;        // interior faces in the device order (sorted by owner)
+    int fb0 = 0, nfb = 0;        // boundary faces in the device order (sorted by owner)
+    long long slot0 = 0, nslot = 0;  // off-diagonal matrix slots [slot0, slot0 + nslot)
+    DeviceArray<int> ptr, col;   // the case's cell->face pattern with local numbering
+    std::unique_ptr<KrylovSolver> mom, pres;
+    std::unique_ptr<AmgPreconditioner> amg;
+    PcReusePolicy preuse;
+    Reducer red, redU, redPP, redP, redM;
+    SimpleReport report;
+    bool frozen = false;         // converged: its state is kept while the others continue
+    DeviceArray<double> keepU, keepP, keepPhi;
+    // the case's rows of a matrix assembled on the whole mesh, in local numbering
+    Dcsr<double> view(const double* diag, const double* val) const {
+        return Dcsr<double>{n, ptr.data(), col.data(), diag + c0, val + slot0, nslot};
+    }
+};
+
 SimpleSolver::SimpleSolver(DeviceMesh& mesh, const SimpleConfig& cfg)
     : m_(mesh), ctx_(*mesh.ctx), cfg_(cfg), U_(mesh, 0, 3), p_(mesh, 0, 1), phi_(mesh, 1, 1), pP_(mesh, 0, 1),
       muEff_(mesh, 0, 1), rAU_(mesh, 0, 1), phiH_(mesh, 1, 1), krylov_(*mesh.ctx) {
@@ -67,7 +87,61 @@ SimpleSolver::SimpleSolver(DeviceMesh& mesh, const SimpleConfig& cfg)
     ctx_.sync();
 }
 
-SimpleSolver::~SimpleSolver() = default;
+SimpleSolver::~SimpleSolver() {
+    if (seg_pinned_) cudaFreeHost(seg_pinned_);
+}
+
+void SimpleSolver::setSegments(const std::vector<int>& off, const std::vector<double>& viscosity) {
+    if (started_) fail(kState, "segments must be set before the fields");
+    if (turb_) fail(kArgument, "batched cases are laminar");
+    const int K = static_cast<int>(off.size()) - 1;
+    if (K < 1 || static_cast<int>(viscosity.size()) != K || off.front() != 0 || off.back() != m_.n_cells)
+        fail(kArgument, "segment offsets must run from 0 to the cell count, one viscosity per segment");
+    if (K > 4096) fail(kArgument, "at most 4096 segments");
+    for (int k = 0; k < K; ++k) {
+        if (off[k + 1] <= off[k]) fail(kArgument, "every segment needs at least one cell");
+        if (!(viscosity[k] > 0.0) || !std::isfinite(viscosity[k])) fail(kArgument, "segment viscosity must be positive");
+    }
+    std::vector<int> seg_of(m_.n_cells);
+    for (int k = 0; k < K; ++k)
+        for (int i = off[k]; i < off[k + 1]; ++i) seg_of[i] = k;
+    for (int f = 0; f < m_.n_interior; ++f)
+        if (seg_of[m_.h_own[f]] != seg_of[m_.h_nbr[f]])
+            fail(kArgument, "an interior face connects two segments: segments must be independent meshes");
+    std::vector<double> mu(m_.n_cells);
+    segs_.clear();
+    int fi = 0, fb = 0;
+    for (int k = 0; k < K; ++k) {
+        auto sg = std::make_unique<SimpleSegment>();
+        sg->c0 = off[k];
+        sg->n = off[k + 1] - off[k];
+        sg->fi0 = fi;
+        while (fi < m_.n_interior && m_.h_own[fi] < off[k + 1]) ++fi;  // interior faces are sorted by owner
+        sg->nfi = fi - sg->fi0;
+        sg->fb0 = fb;
+        while (fb < m_.n_boundary && m_.h_bown[fb] < off[k + 1]) ++fb;
+        sg->nfb = fb - sg->fb0;
+        sg->slot0 = m_.h_cf_ptr[off[k]];
+        sg->nslot = m_.h_cf_ptr[off[k + 1]] - sg->slot0;
+        std::vector<int> ptr(sg->n + 1), col(std::max<long long>(sg->nslot, 1));
+        for (int i = 0; i <= sg->n; ++i) ptr[i] = static_cast<int>(m_.h_cf_ptr[off[k] + i] - sg->slot0);
+        for (long long q = 0; q < sg->nslot; ++q) col[q] = m_.h_cf_col[sg->slot0 + q] - off[k];
+        sg->ptr.upload(ptr, ctx_.stream);
+        sg->col.upload(col, ctx_.stream);
+        sg->mom = std::make_unique<KrylovSolver>(ctx_);
+        sg->pres = std::make_unique<KrylovSolver>(ctx_);
+        for (int i = off[k]; i < off[k + 1]; ++i) mu[i] = viscosity[k];
+        segs_.push_back(std::move(sg));
+    }
+    muEff_.v.upload(mu, ctx_.stream);
+    if (!seg_pinned_) BSG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&seg_pinned_), sizeof(double) * 16 * 4096));
+    ctx_.sync();
+}
+
+const SimpleReport& SimpleSolver::segmentReport(int k) const {
+    if (k < 0 || k >= static_cast<int>(segs_.size())) fail(kArgument, "segment index out of range");
+    return segs_[k]->report;
+}
 
 void SimpleSolver::enableKOmega(const KOmegaConfig& cfg) {
     if (started_) fail(kState, "the turbulence model must be chosen before the fields are set");
@@ -112,10 +186,202 @@ void SimpleSolver::loadState(const double* U, const double* p, const double* phi
 SimpleReport SimpleSolver::iterate(int max_iterations) {
     if (!started_) start();
     for (int k = 0; k < max_iterations; ++k) {
-        outerIteration();
+        if (segs_.empty()) outerIteration();
+        else outerIterationSegments();
         if (report_.converged || report_.status == 2) break;
     }
     return report_;
+}
+
+// outerIteration for a mesh of several independent cases: the same steps in the same order,
+// with the per-case parts (momentum solve, gauge, pressure solves, diagnostics, convergence)
+// done per segment and the pressure solves of all segments batched in one launch per attempt.
+void SimpleSolver::outerIterationSegments() {
+    const int N = m_.n_cells;
+    const int K = static_cast<int>(segs_.size());
+    const MeshView mv = view(m_);
+    copyAsync(ctx_, Uprev_.data(), U_.v.data(), 3LL * N);
+    DeviceEquation& mom = *mom_;
+    {
+        BSG_PROFILE(ctx_, "momentum_assembly");
+        mom.reset();
+        addConvection(mom, phi_, cfg_.rho, cfg_.momentum);
+        addLaplacian(mom, &muEff_, 0.0, -1.0, cfg_.momentum);
+        gradient(p_, cfg_.pressure.gradient, gradP_);
+        addSource(mom, gradP_.data(), -1.0);
+    }
+    for (auto& sg : segs_) relativeResidualNorms(mom, U_.v.data(), sg->red, sg->c0, sg->n);
+    relax(mom, Uprev_.data(), cfg_.alpha_u);
+    scale(mom, cfg_.alpha_u);
+    ratioVolume(m_, mom.diag.data(), rAU_.v.data());
+    kOwnerTrace<<<gridFor(m_.n_boundary, kBlock), kBlock, 0, ctx_.stream>>>(mv, rAU_.v.data(), rAU_.trace.data());
+    ctx_.launched();
+    // momentum: each active case on its own rows
+    std::vector<int> mom_ok(K, 1), p_ok(K, 1), mom_its(K, 0), p_its(K, 0);
+    std::vector<double> linP(K, 0.0);
+    bool failed = false;
+    {
+        BSG_PROFILE(ctx_, "bicgstab3_segments");
+        for (int k = 0; k < K; ++k) {
+            SimpleSegment& sg = *segs_[k];
+            if (sg.frozen) continue;
+            const Dcsr<double> A = sg.view(mom.diag.data(), mom.val.data());
+            SolveOutcome uo[3];
+            sg.mom->solveVector3(A, cfg_.momentum_solver, mom.src.data() + 3LL * sg.c0, U_.v.data() + 3LL * sg.c0, uo);
+            for (const auto& o : uo) {
+                mom_its[k] += o.iterations;
+                mom_ok[k] = mom_ok[k] && o.status == 0;
+                if (o.status == 2 || !std::isfinite(o.final_)) failed = true;
+            }
+        }
+    }
+    if (failed) { report_.status = 2; return; }
+    {
+        BSG_PROFILE(ctx_, "rhie_chow_flux");
+        faceFlux(U_, cfg_.momentum.interpolation, cfg_.momentum.gradient, phiH_);
+        kRhieChow<<<gridFor(m_.n_interior, kBlock), kBlock, 0, ctx_.stream>>>(
+            mv, p_.bcView(), rAU_.v.data(), gradP_.data(), p_.v.data(), cfg_.pressure.diffusion, phiH_.v.data());
+        ctx_.launched();
+        divFlux(phiH_, divPhiH_);
+    }
+    BSG_CUDA(cudaMemsetAsync(pP_.v.data(), 0, sizeof(double) * N, ctx_.stream));
+    const int pressure_solves = cfg_.pressure.diffusion == 0 ? 1 : cfg_.non_orthogonal_corrections + 1;
+    DeviceEquation& peq = *peq_;
+    const int pcType = cfg_.pressure_solver.preconditioner;
+    if (!(pcType == 2 || pcType == 3) || cfg_.pressure_solver.solver != 0 || cfg_.pressure_solver.precision == 1)
+        fail(kArgument, "batched cases solve the pressure with CG and the AMG preconditioner (FP64 or FP32 V-cycle)");
+    if (flags_.size() < static_cast<std::size_t>(2 * K)) flags_.resize(2 * K);
+    for (int corr = 0; corr < pressure_solves; ++corr) {
+        {
+            BSG_PROFILE(ctx_, "pressure_assembly");
+            peq.reset();
+            addLaplacian(peq, &rAU_, 0.0, -1.0, cfg_.pressure);
+            addSource(peq, divPhiH_.data(), -1.0);
+            for (int k = 0; k < K; ++k)
+                referenceIfUnanchored(peq, 0.0, flags_.data() + 2 * k, segs_[k]->c0, segs_[k]->n);
+        }
+        std::vector<BatchSolve> items;
+        std::vector<int> which;
+        std::vector<bool> lagged(K, false);
+        {
+            BSG_PROFILE(ctx_, "amg_numeric_setup");
+            for (int k = 0; k < K; ++k) {
+                SimpleSegment& sg = *segs_[k];
+                if (sg.frozen) continue;
+                const Dcsr<double> P = sg.view(peq.diag.data(), peq.val.data());
+                if (!sg.amg) sg.amg = std::make_unique<AmgPreconditioner>(m_, cfg_.pressure_solver);
+                sg.amg->update(P, sg.preuse.needRebuild(corr == 0, cfg_.pressure_solver));
+                lagged[k] = sg.preuse.lagged();
+                BatchSolve b;
+                b.solver = sg.pres.get();
+                b.amg = sg.amg.get();
+                b.A = P;
+                b.b = peq.src.data() + sg.c0;
+                b.x = pP_.v.data() + sg.c0;
+                b.cfg = cfg_.pressure_solver;
+                items.push_back(b);
+                which.push_back(k);
+            }
+        }
+        KrylovSolver::solveBatch(ctx_, items);
+        for (std::size_t q = 0; q < items.size(); ++q) {
+            const int k = which[q];
+            SimpleSegment& sg = *segs_[k];
+            SolveOutcome po = items[q].out;
+            int attempt = po.iterations;
+            if (lagged[k] && po.status != 0) {
+                // a failed lagged solve is retried once with a fresh preconditioner
+                const Dcsr<double> P = sg.view(peq.diag.data(), peq.val.data());
+                sg.amg->update(P, true);
+                sg.preuse.rebuilt();
+                const int first = po.iterations;
+                po = sg.pres->solveScalar(P, cfg_.pressure_solver, sg.amg.get(), peq.src.data() + sg.c0,
+                                          pP_.v.data() + sg.c0);
+                attempt = po.iterations;
+                po.iterations += first;
+            }
+            sg.preuse.afterSolve(po.status, attempt, po.iterations, cfg_.pressure_solver);
+            if (po.status == 2 || !std::isfinite(po.final_)) failed = true;
+            p_ok[k] = p_ok[k] && po.status == 0;
+            p_its[k] += po.iterations;
+            linP[k] = po.relative;
+        }
+        if (failed) { report_.status = 2; return; }
+    }
+    axpyCell(ctx_, p_.v.data(), cfg_.alpha_p, pP_.v.data(), N);
+    BSG_PROFILE(ctx_, "field_updates_diagnostics");
+    faceFluxEquation(peq, pP_.v.data(), pflux_);
+    gradient(pP_, cfg_.pressure.gradient, gradPP_);
+    subtractScaledGradient(m_, U_.v.data(), rAU_.v.data(), gradPP_.data());
+    addArrays(ctx_, phi_.v.data(), phiH_.v.data(), pflux_.data(), m_.n_faces);
+    for (auto& sg : segs_) {
+        relativeChangeNorms(ctx_, U_.v.data() + 3LL * sg->c0, Uprev_.data() + 3LL * sg->c0, 3LL * sg->n, sg->redU);
+        relativeChangeNorms(ctx_, pP_.v.data() + sg->c0, nullptr, sg->n, sg->redPP);
+        relativeChangeNorms(ctx_, p_.v.data() + sg->c0, nullptr, sg->n, sg->redP);
+        fluxBalance(m_, phi_.v.data(), sg->redM, sg->c0, sg->n);
+    }
+    double* h = seg_pinned_;
+    for (int k = 0; k < K; ++k) {
+        SimpleSegment& sg = *segs_[k];
+        double* hk = h + 16 * k;
+        BSG_CUDA(cudaMemcpyAsync(hk + 0, sg.red.result.data(), 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+        BSG_CUDA(cudaMemcpyAsync(hk + 4, sg.redU.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+        BSG_CUDA(cudaMemcpyAsync(hk + 6, sg.redPP.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+        BSG_CUDA(cudaMemcpyAsync(hk + 8, sg.redP.result.data(), 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+        BSG_CUDA(cudaMemcpyAsync(hk + 10, sg.redM.result.data(), 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+    }
+    ctx_.sync();
+    bool bad = false;
+    int total_mom = 0, total_p = 0;
+    const std::size_t Fi = m_.n_interior;
+    for (int k = 0; k < K; ++k) {
+        SimpleSegment& sg = *segs_[k];
+        if (sg.frozen) {
+            // keep the converged state: the batch's update touched these cells and faces too
+            copyAsync(ctx_, U_.v.data() + 3LL * sg.c0, sg.keepU.data(), 3LL * sg.n);
+            copyAsync(ctx_, p_.v.data() + sg.c0, sg.keepP.data(), sg.n);
+            copyAsync(ctx_, phi_.v.data() + sg.fi0, sg.keepPhi.data(), sg.nfi);
+            copyAsync(ctx_, phi_.v.data() + Fi + sg.fb0, sg.keepPhi.data() + sg.nfi, sg.nfb);
+            continue;
+        }
+        const double* hk = h + 16 * k;
+        SimpleReport& r = sg.report;
+        r.momentum_iterations = mom_its[k];
+        r.pressure_iterations = p_its[k];
+        r.linP = linP[k];
+        r.rU = std::sqrt(hk[0]) / std::max(std::sqrt(hk[1]) + std::sqrt(hk[2]), 1e-30);
+        r.dU = std::sqrt(hk[4]) / std::max(std::sqrt(hk[5]), 1e-30);
+        r.dP = std::sqrt(hk[6]) / std::max(std::sqrt(hk[9]), 1e-30);
+        r.mass = hk[10] / std::max(hk[12], 1e-30);
+        r.iterations += 1;
+        total_mom += mom_its[k];
+        total_p += p_its[k];
+        if (!(std::isfinite(r.rU) && std::isfinite(r.dU) && std::isfinite(r.dP) && std::isfinite(r.mass))) {
+            r.status = 2;
+            bad = true;
+            continue;
+        }
+        r.converged = mom_ok[k] && p_ok[k] && r.rU <= cfg_.momentum_tolerance && r.dU <= cfg_.velocity_tolerance &&
+                      r.dP <= cfg_.pressure_tolerance && r.mass <= cfg_.mass_tolerance;
+        r.status = r.converged ? 0 : 1;
+        if (r.converged) {
+            sg.frozen = true;
+            sg.keepU.resize(3 * static_cast<std::size_t>(sg.n));
+            sg.keepP.resize(sg.n);
+            sg.keepPhi.resize(std::max<std::size_t>(static_cast<std::size_t>(sg.nfi) + sg.nfb, 1));
+            copyAsync(ctx_, sg.keepU.data(), U_.v.data() + 3LL * sg.c0, 3LL * sg.n);
+            copyAsync(ctx_, sg.keepP.data(), p_.v.data() + sg.c0, sg.n);
+            copyAsync(ctx_, sg.keepPhi.data(), phi_.v.data() + sg.fi0, sg.nfi);
+            copyAsync(ctx_, sg.keepPhi.data() + sg.nfi, phi_.v.data() + Fi + sg.fb0, sg.nfb);
+        }
+    }
+    bool all = true;
+    for (auto& sg : segs_) all = all && sg->frozen;
+    report_.iterations += 1;
+    report_.momentum_iterations = total_mom;
+    report_.pressure_iterations = total_p;
+    report_.converged = all;
+    report_.status = bad ? 2 : (all ? 0 : 1);
 }
 
 void SimpleSolver::outerIteration() {

@@ -29,10 +29,24 @@ struct SimpleReport {
     double turbulence_change = 0, turbulence_residual = 0;
 };
 
+// One case of a batch: a contiguous cell range of the mesh that no interior face leaves.
+struct SimpleSegment;
+
 class SimpleSolver {
 public:
     SimpleSolver(DeviceMesh& mesh, const SimpleConfig& cfg);
     ~SimpleSolver();
+    // Several independent cases in one mesh (block-diagonal batching over a segment table):
+    // case s owns cells [cell_offsets[s], cell_offsets[s+1]) and has dynamic viscosity
+    // viscosity[s].  Every assembly, gradient, flux and update kernel runs once over all
+    // cases; the diagnostics, the gauge and the convergence tests are per case; each case's
+    // momentum system is solved on its own rows and all cases' pressure systems are solved
+    // together in one persistent launch per attempt (KrylovSolver::solveBatch), each with
+    // its own AMG hierarchy and preconditioner lag.  A case that has converged keeps its
+    // converged state while the others continue.  Call before start(); laminar only.
+    void setSegments(const std::vector<int>& cell_offsets, const std::vector<double>& viscosity);
+    int segments() const { return static_cast<int>(segs_.size()); }
+    const SimpleReport& segmentReport(int s) const;
     DeviceField& U() { return U_; }
     DeviceField& p() { return p_; }
     DeviceField& phi() { return phi_; }
@@ -49,6 +63,7 @@ public:
 
 private:
     void outerIteration();
+    void outerIterationSegments();
     DeviceMesh& m_;
     Context& ctx_;
     SimpleConfig cfg_;
@@ -64,6 +79,8 @@ private:
     DeviceArray<int> flags_;
     SimpleReport report_;
     bool started_ = false;
+    std::vector<std::unique_ptr<SimpleSegment>> segs_;
+    double* seg_pinned_ = nullptr;  // per-segment diagnostics read back together
 };
 
 }  // namespace bsg

@@ -261,3 +261,40 @@ def voronoi_cube(n: int, jitter: float = 0.3, seed: int = 20261007, names=None, 
     """Jittered-lattice Voronoi tessellation of the unit cube (see babelsim_b200.voronoi)."""
     from .voronoi import voronoi_cube as build
     return build(n, jitter, seed, names, kinds)
+
+
+def concatenate(meshes) -> tuple:
+    """Several independent meshes as one (the block-diagonal batch of bsg_simple_set_segments):
+    vertices, cells, faces and patches of mesh k follow those of meshes 0..k-1, its patches
+    named "<name>@k".  Returns (PolyMesh, cell_offsets, patch_offsets)."""
+    verts, ids, own, nbr, pat, names, kinds = [], [], [], [], [], [], []
+    v0 = c0 = p0 = 0
+    cell_offsets, patch_offsets = [0], [0]
+    for k, m in enumerate(meshes):
+        o, i = m.flat()
+        verts.append(np.asarray(m.vertices, np.float64))
+        ids.append(np.asarray(i, np.int64) + v0)
+        n = m.n_cells
+        own.append(np.asarray(m.owner, np.int64) + c0)
+        nb = np.asarray(m.neighbour, np.int64)
+        nbr.append(np.where(nb >= 0, nb + c0, -1))
+        pt = np.asarray(m.patch, np.int64)
+        pat.append(np.where(pt >= 0, pt + p0, -1))
+        names += [f"{nm}@{k}" for nm in m.patch_names]
+        kinds += list(m.patch_kinds)
+        v0 += len(m.vertices)
+        c0 += n
+        p0 += len(m.patch_names)
+        cell_offsets.append(c0)
+        patch_offsets.append(p0)
+    # ring offsets: each mesh's offsets shifted by the rings before it
+    flat_off = [np.zeros(1, np.int64)]
+    base = 0
+    for m in meshes:
+        o, _ = m.flat()
+        flat_off.append(np.asarray(o[1:], np.int64) + base)
+        base += int(o[-1])
+    pm = PolyMesh(np.concatenate(verts), None, np.concatenate(own).astype(np.int32),
+                  np.concatenate(nbr).astype(np.int32), np.concatenate(pat).astype(np.int32), names, kinds,
+                  offsets=np.concatenate(flat_off).astype(np.int32), ids=np.concatenate(ids).astype(np.int32))
+    return pm, np.array(cell_offsets, np.int32), np.array(patch_offsets, np.int32)

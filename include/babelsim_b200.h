@@ -422,6 +422,22 @@ int bsg_simple_set_flux(bsg_simple* s, const double* phi);
 int bsg_simple_load_state(bsg_simple* s, const double* U, const double* p, const double* phi);
 /* Run outer iterations until converged or max_iterations more have been done. */
 int bsg_simple_iterate(bsg_simple* s, int32_t max_iterations, bsg_simple_report* report);
+/* Block-diagonal batching (no counterpart in the reference, whose unit of work is one case per
+ * process, src/runtime/application.cpp:238-272): the mesh is several independent cases
+ * concatenated, case k owning cells [cell_offsets[k], cell_offsets[k+1]) (n_segments + 1
+ * offsets from 0 to the cell count; no interior face may join two cases; each case has its own
+ * patches) with dynamic viscosity viscosity[k].  Every assembly, gradient, flux and update
+ * kernel then runs once over all cases, each case's momentum system is solved on its own rows,
+ * the pressure systems of all cases are solved in one persistent launch per attempt (each on
+ * CTAs of its own, with its own AMG hierarchy and preconditioner lag), and the gauge,
+ * diagnostics and convergence tests are per case.  A converged case keeps its converged U, p
+ * and phi while the others continue; bsg_simple_iterate stops when every case has converged,
+ * and its report's iterations count the batch's outer iterations.  Call after create and
+ * before set_fields; laminar, with pressure CG + AMG (precision 0 or 2).  Up to 4096 cases. */
+int bsg_simple_set_segments(bsg_simple* s, int32_t n_segments, const int32_t* cell_offsets,
+                            const double* viscosity);
+/* The report of one case of a batch (its own outer iterations, residuals and status). */
+int bsg_simple_segment_report(const bsg_simple* s, int32_t segment, bsg_simple_report* report);
 /* turbulenceModel kOmega (src/physics/RANS/model.cpp:24-53): call after create and
  * before set_fields; then "k" and "omega" take boundary conditions through
  * bsg_simple_set_boundary and initial values through set_turbulence_fields. */
