@@ -1,5 +1,11 @@
 """Serving loop on the GPU: each request's result is the same alone and in the mix (the
-north star's serving test), and the loop retires every request."""
+north star's serving test), and the loop retires every request.
+
+In the mix, requests admitted together run as one block-diagonal cohort whose pressure
+systems share one persistent launch; each member's CTA share depends only on its own size
+(while the cohort fits the grid), so its arithmetic, and therefore its result, is bit for bit
+the one it has alone.  Against the unbatched path (its own launches on the whole grid, so a
+different dot-product order in the pressure solves) results agree to 1e-7 relative L2."""
 import numpy as np
 import pytest
 
@@ -31,6 +37,8 @@ def test_results_alone_and_in_the_mix_agree(ctx):
     for a, b in zip(alone, mix):
         assert a.iterations == b.iterations and a.converged == b.converged
         assert np.array_equal(a.U, b.U) and np.array_equal(a.p, b.p)
+    # the first three ran as one cohort: their outer iterations were shared launches
+    assert srv.batched
     # three slots: the fourth request waited for a retirement
     admitted = [e[1] for e in srv.log if e[0] == "admitted"]
     assert admitted == [0, 1, 2, 3]
@@ -50,3 +58,14 @@ def test_budget_queues_and_rejects(ctx):
             assert val <= budget
     rejected = {e[1] for e in srv.log if e[0] == "rejected"}
     assert rejected == {i for i, s in enumerate(sizes) if s > budget}
+
+
+def test_batched_and_unbatched_serving_agree(ctx):
+    reqs = _requests()
+    batched = serve.Server(ctx, slots=4, keep_fields=True).run(reqs)
+    each = serve.Server(ctx, slots=4, keep_fields=True, batched=False).run(reqs)
+    for a, b in zip(batched, each):
+        assert a.converged == b.converged
+        assert abs(a.iterations - b.iterations) <= 1
+        assert np.linalg.norm(a.U - b.U) <= 1e-7 * np.linalg.norm(b.U)
+        assert np.linalg.norm(a.p - b.p) <= 1e-7 * np.linalg.norm(b.p)

@@ -48,7 +48,7 @@ class Clock:
 
 
 def _server(budget, slots, needed, trace):
-    srv = serve.Server(ctx=None, hbm_budget=budget, slots=slots)
+    srv = serve.Server(ctx=None, hbm_budget=budget, slots=slots, batched=False)
     srv._start = lambda req: (FakeMesh(req.mesh.n_cells, 1), FakeSim(needed[req.id], trace, req.id))
     return srv
 
@@ -150,3 +150,52 @@ def test_two_ranks_agree_on_the_partition_over_gloo():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert sorted(gathered[0] + gathered[1]) == list(range(40)) and not set(gathered[0]) & set(gathered[1])
+
+
+class FakeBatch:
+    """A cohort's segmented solve: member k converges after needed[k] outer iterations and then
+    keeps its report (a converged segment is frozen)."""
+    def __init__(self, needed, trace, ids):
+        self.needed, self.it, self.trace, self.ids = needed, 0, trace, ids
+
+    def iterate(self, k):
+        self.it += k
+        self.trace.append(tuple(self.ids))
+        return FakeReport(self.it, self.it >= max(self.needed))
+
+    def segment_report(self, k):
+        it = min(self.it, self.needed[k])
+        return FakeReport(it, it >= self.needed[k])
+
+    def fields(self):
+        return None, None, None
+
+    def close(self):
+        pass
+
+
+def test_batched_cohorts_admit_as_slots_free_and_retire_members_individually():
+    reqs = [serve.Request(i, arrival=0.0 if i < 3 else 6.0, mesh=FakeMesh(1000, 3000)) for i in range(5)]
+    need = {0: 2, 1: 5, 2: 3, 3: 2, 4: 2}
+    trace = []
+    srv = serve.Server(ctx=None, hbm_budget=10 * serve.device_bytes(1000, 3000), slots=3, batched=True)
+
+    def start(members):
+        ids = [r.id for r, _, _ in members]
+        return serve._Cohort(list(members), FakeMesh(1000 * len(ids), 1), FakeBatch([need[i] for i in ids], trace, ids),
+                             np.arange(len(ids) + 1) * 1000, [False] * len(ids))
+    srv._start_cohort = start
+    res = srv.run(reqs, clock=Clock())
+    assert [r.id for r in res] == list(range(5))
+    assert all(r.converged for r in res)
+    assert [r.iterations for r in res] == [2, 5, 3, 2, 2]
+    # the first three arrive together and form one cohort; the later two join as slots free up
+    assert trace[0] == (0, 1, 2)
+    cohorts = {t for t in trace}
+    assert (0, 1, 2) in cohorts and any(3 in t for t in cohorts) and any(4 in t for t in cohorts)
+    # never more than three requests admitted and unretired at once
+    live = peak = 0
+    for kind, rid, _ in srv.log:
+        live += 1 if kind == "admitted" else (-1 if kind == "retired" else 0)
+        peak = max(peak, live)
+    assert peak <= 3
