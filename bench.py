@@ -69,12 +69,14 @@ def mesh_for(n: int):
     return pm
 
 
-def build_simple(bsg, mesh, s, precision=0):
+def build_simple(bsg, mesh, s, precision=0, boundaries=True):
     opts = bsg.options(s["interpolation"], s["gradient"], s["convection"], s["diffusion"])
     sim = bsg.Simple(mesh, s["rho"], s["mu"], s["alpha_u"], s["alpha_p"], s["non_orthogonal_corrections"],
                      1e-8, 1e-7, 1e-6, 1e-6, opts, opts,
                      bsg.solver_config("bcgs", "bjacobi", s["atol"], s["rtol"], 1000),
                      bsg.solver_config("cg", "hypre", s["atol"], s["rtol"], 1000, precision=precision))
+    if not boundaries:  # the caller sets boundaries (and segments) before the fields
+        return sim
     for patch in range(6):
         sim.set_boundary("U", patch, "fixedValue", (1.0, 0.0, 0.0) if patch == 3 else (0.0, 0.0, 0.0))
         sim.set_boundary("p", patch, "zeroGradient")
@@ -441,6 +443,103 @@ def run_piso_cylinder(args):
     ctx.close()
 
 
+def batched_cases():
+    """Uneven cavity cases of the batched workload: jittered-Voronoi cubes (the 1M-cell
+    workload's generator) and hex boxes, lid speed uniform 0.5-2 and viscosity log-uniform
+    1e-3-1e-2 from a seeded stream (the serving stream's distributions)."""
+    from babelsim_b200 import meshgen
+    rng = np.random.default_rng(SEED + 1)
+    meshes = [meshgen.voronoi_cube(n, 0.3, SEED + n) for n in (16, 20, 24, 28, 32, 40)]
+    meshes += [meshgen.hex_box(n, n, n, flat=True) for n in (20, 32)]
+    return [(m, float(rng.uniform(0.5, 2.0)), float(np.exp(rng.uniform(np.log(1e-3), np.log(1e-2)))))
+            for m in meshes]
+
+
+def run_batched(args):
+    """Block-diagonal batching: the uneven cases of batched_cases() advanced as one batch (one set
+    of launches per outer iteration, all pressure systems in one persistent launch per attempt)
+    against the same cases one after another, each with its own launches on the whole GPU."""
+    import babelsim_b200 as bsg
+    from babelsim_b200 import meshgen
+    s = case_settings()
+    cases = batched_cases()
+    ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    warm, steps = max(args.warmup, 3), args.steps
+
+    def configure(sim, patch0, lid):
+        for patch in range(6):
+            sim.set_boundary("U", patch0 + patch, "fixedValue", (lid, 0.0, 0.0) if patch == 3 else (0.0, 0.0, 0.0))
+            sim.set_boundary("p", patch0 + patch, "zeroGradient")
+
+    def simple(mesh, mu, precision):
+        t = dict(s, mu=mu)
+        return build_simple(bsg, mesh, t, precision=precision, boundaries=False)
+
+    # one after another: each case alone, its own kernels on the whole GPU
+    seq_ms, seq_fields, cells = 0.0, [], 0
+    for poly, lid, mu in cases:
+        mesh = bsg.Mesh.from_polyhedral(ctx, poly)
+        sim = simple(mesh, mu, 0)
+        configure(sim, 0, lid)
+        sim.set_fields(np.zeros((mesh.n_cells, 3)), np.zeros(mesh.n_cells))
+        sim.iterate(warm)
+        ctx.synchronize()
+        ctx.record(0)
+        sim.iterate(steps)
+        ctx.record(1)
+        seq_ms += ctx.elapsed_ms(0, 1)
+        seq_fields.append(sim.fields()[:2])
+        cells += mesh.n_cells
+        sim.close()
+        mesh.close()
+    seq_value = cells * steps / (seq_ms / 1e3)
+    poly, offsets, patches = meshgen.concatenate([c[0] for c in cases])
+    mesh = bsg.Mesh.from_polyhedral(ctx, poly)
+    out = {}
+    for precision in (0, 2):
+        sim = simple(mesh, cases[0][2], precision)
+        sim.set_segments(offsets, [c[2] for c in cases])
+        for k, (_, lid, _) in enumerate(cases):
+            configure(sim, int(patches[k]), lid)
+        sim.set_fields(np.zeros((mesh.n_cells, 3)), np.zeros(mesh.n_cells))
+        sim.iterate(warm)
+        ctx.synchronize()
+        launches0 = ctx.launches()
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            ctx.record(2)
+            sim.iterate(steps)
+            ctx.record(3)
+            ms = ctx.elapsed_ms(2, 3)
+        U, p, _ = sim.fields()
+        dev = []
+        for k, (Us, ps) in enumerate(seq_fields):
+            a, b = int(offsets[k]), int(offsets[k + 1])
+            dev.append(max(float(np.linalg.norm(U[a:b] - Us) / max(np.linalg.norm(Us), 1e-300)),
+                           float(np.linalg.norm(p[a:b] - ps) / max(np.linalg.norm(ps), 1e-300))))
+        out[precision] = {"value": cells * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                          "launches_per_step": (ctx.launches() - launches0) / steps, "clocks": clocks.summary(),
+                          "max_rel_l2_vs_one_after_another": max(dev)}
+        sim.close()
+    mesh.close()
+    ctx.close()
+    b64 = out[0]
+    line = {"metric": "cell-iters/s (uneven steady SIMPLE cavities, block-diagonal batch)", "value": b64["value"],
+            "unit": "cell-iters/s", "n_gpus": 1, "steps": steps, "warmup": warm, "ms_per_step": b64["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{len(cases)} cavities, {cells} cells in total (jittered-Voronoi cubes "
+                                   f"16^3-40^3 and hex boxes 20^3, 32^3), lid 0.5-2, nu 1e-3-1e-2, linearUpwind, "
+                                   f"least squares, corrected diffusion, 2 non-orthogonal correctors, pressure CG + "
+                                   f"AMG and momentum BiCGStab to rtol 1e-10", "cases": len(cases), "cells": cells},
+            "one_after_another": {"value": seq_value, "ms_per_step": seq_ms / steps},
+            "speedup_vs_one_after_another": b64["value"] / seq_value,
+            "launches_per_step": b64["launches_per_step"], "clocks": b64["clocks"],
+            "max_rel_l2_vs_one_after_another": b64["max_rel_l2_vs_one_after_another"],
+            "fp32_vcycle": {"value": out[2]["value"], "ms_per_step": out[2]["ms_per_step"],
+                            "vs_fp64_batch": out[2]["value"] / b64["value"],
+                            "max_rel_l2_vs_fp64_one_after_another": out[2]["max_rel_l2_vs_one_after_another"]}}
+    print(json.dumps(line))
+
+
 def run_komega_channel(args):
     """Steady SIMPLE with k-omega in a plane channel (2 pi x 2 x pi, tanh wall clustering),
     inlet/outlet (the reference has no periodic patches), nu 1e-4; metric cell-iters/s."""
@@ -504,7 +603,7 @@ def main():
     ap.add_argument("--cells", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison run")
-    ap.add_argument("--workload", default="cavity", choices=["cavity", "serving", "piso-cylinder", "komega-channel"])
+    ap.add_argument("--workload", default="cavity", choices=["cavity", "serving", "piso-cylinder", "komega-channel", "batched"])
     ap.add_argument("--theta-cells", type=int, default=2000)
     ap.add_argument("--dt", type=float, default=0.001)
     ap.add_argument("--radial-cells", type=int, default=100)
@@ -523,6 +622,8 @@ def main():
         return run_piso_cylinder(args)
     if args.workload == "komega-channel":
         return run_komega_channel(args)
+    if args.workload == "batched":
+        return run_batched(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
