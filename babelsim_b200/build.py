@@ -34,8 +34,11 @@ def nvcc():
 
 
 def flags():
+    # BSG_NVCC_FLAGS: extra nvcc flags for a tuning build (e.g. -DBSG_SELL_BATCH=8); objects are
+    # rebuilt when it changes
+    extra = os.environ.get("BSG_NVCC_FLAGS", "").split()
     return ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
-                   "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+                   "-I" + os.path.join(ROOT, "include"), "-I" + CSRC] + extra
 
 
 def compile_one(src):
@@ -43,13 +46,17 @@ def compile_one(src):
     path = os.path.join(CSRC, src)
     deps = [path] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "babelsim_b200.h"))
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
+    stamp = obj + ".flags"
+    same_flags = os.path.exists(stamp) and open(stamp).read() == " ".join(flags())
+    if same_flags and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
     lang = ["-x", "cu"] if src.endswith(".cu") else []
     cmd = [nvcc()] + flags() + EXTRA.get(src, []) + lang + ["-c", path, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{res.stdout}\n{res.stderr}")
+    with open(stamp, "w") as f:
+        f.write(" ".join(flags()))
     return obj
 
 
