@@ -7,6 +7,7 @@
 // reads a convergence word every `check_interval` iterations; kernels of
 // iterations issued after convergence return immediately.
 #include "amg.h"
+#include "bicgstab_sell.cuh"
 #include "pcg_sell.cuh"
 #include "sell.cuh"
 #include "bsg_device.cuh"
@@ -527,6 +528,7 @@ struct KrylovSolver::Impl {
     Context& ctx;
     DeviceArray<double> r, z, p, q, r0, v, ph, sh, t, partial, tmp;
     DeviceArray<Scalars> sc;
+    DeviceArray<BicgState> bst;    // state of the persistent BiCGStab
     DeviceArray<unsigned> ticket;  // arrivals of the current reduction (reduceThenFinish), zero between launches
     DeviceArray<PcgState> pst;
     DeviceArray<float> r32, s32, z32, p32a, p32b, q32, d32;  // FP32 inner solve of the refined path
@@ -746,12 +748,12 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
             // FP64 Krylov vectors and products, FP32 V-cycle, flexible beta
             SellPcgArgs<double, float> args{amg->krylovMatrix(), amg->sellView32(), b, x, m.r.data(), m.z.data(),
                                             m.p.data(), m.v.data(), m.q.data(), m.partial.data(), m.pst.data(),
-                                            PhaseLog{}, 1};
+                                            PhaseLog{}, 1, m.t.data()};
             launchSellPcg(ctx, args);
         } else if (amg) {
             SellPcgArgs<double, double> args{amg->krylovMatrix(), amg->sellView64(), b, x, m.r.data(), m.z.data(),
                                              m.p.data(), m.v.data(), m.q.data(), m.partial.data(), m.pst.data(),
-                                             PhaseLog{}};
+                                             PhaseLog{}, 0, m.t.data()};
             launchSellPcg(ctx, args);
         } else {
             launchPersistentPcg(ctx, A, view, jacobi_diag, b, x, m.r.data(), m.z.data(), m.p.data(), m.v.data(),
@@ -774,7 +776,10 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
                                    : (jacobi_diag ? 32.0 * N : 24.0 * N);
             const double it = r.iterations;
             const double applications = (r.iterations == 0 && r.status == 0) ? 0.0 : std::max(1.0, it);
-            const double bytes = init + applications * pre + it * (M0 + 80.0 * N);
+            // with one smoothing step the update of x and r shares its pass with the next level-0
+            // residual sweep, which then no longer reads the level-0 right-hand side and iterate
+            const bool fused = amg && amg->levels() >= 2 && cfg.amg_smoothing_steps < 2;
+            const double bytes = init + applications * pre + it * (M0 + 80.0 * N) - (fused ? 16.0 * N * it : 0.0);
             ctx.profileNote("pcg_amg_persistent", bytes, it);
             if (trace_solves())
                 std::fprintf(stderr, "bsg persistent pcg: rows %d iterations %d status %d algorithmic_bytes %.0f\n", n,
@@ -992,7 +997,7 @@ void KrylovSolver::solveBatch(Context& ctx, std::vector<BatchSolve>& items) {
                     Impl& m = *items[k].solver->impl_;
                     batch64.args.push_back({items[k].amg->krylovMatrix(), items[k].amg->sellView64(), items[k].b,
                                             items[k].x, m.r.data(), m.z.data(), m.p.data(), m.v.data(), m.q.data(),
-                                            m.partial.data(), m.pst.data(), PhaseLog{}});
+                                            m.partial.data(), m.pst.data(), PhaseLog{}, 0, m.t.data()});
                 }
                 batch64.cta_begin = allotCtas(slices, capacity);
                 launchSellPcgBatch(ctx, batch64);
@@ -1002,7 +1007,8 @@ void KrylovSolver::solveBatch(Context& ctx, std::vector<BatchSolve>& items) {
                     Impl& m = *items[k].solver->impl_;
                     SellPcgArgs<double, float> a{items[k].amg->krylovMatrix(), items[k].amg->sellView32(),
                                                  items[k].b, items[k].x, m.r.data(), m.z.data(), m.p.data(),
-                                                 m.v.data(), m.q.data(), m.partial.data(), m.pst.data(), PhaseLog{}, 1};
+                                                 m.v.data(), m.q.data(), m.partial.data(), m.pst.data(), PhaseLog{}, 1,
+                                                 m.t.data()};
                     batch32.args.push_back(a);
                 }
                 batch32.cta_begin = allotCtas(slices, capacity);
@@ -1059,9 +1065,116 @@ void KrylovSolver::solveBatch(Context& ctx, std::vector<BatchSolve>& items) {
     }
 }
 
+void KrylovSolver::solveVector3Batch(Context& ctx, std::vector<BicgItem>& items, bool batched) {
+    const int K = static_cast<int>(items.size());
+    if (K == 0) return;
+    struct Track {
+        BicgState h{};
+        double scale[3] = {1, 1, 1}, target[3] = {0, 0, 0}, fin[3] = {0, 0, 0};
+        bool finished[3] = {false, false, false};
+    };
+    std::vector<Track> t(K);
+    std::vector<SellMat<double>> sell(K);
+    for (int k = 0; k < K; ++k) {
+        BicgItem& it = items[k];
+        if (!it.solver || &it.solver->impl_->ctx != &ctx) fail(kArgument, "batched BiCGStab: solvers must share ctx");
+        Impl& m = *it.solver->impl_;
+        const int n = it.A.n;
+        m.ensure(3 * static_cast<std::size_t>(n));
+        if (m.bst.size() < 1) m.bst.resize(1);
+        sell[k] = m.sellOf(it.A);
+        if (!it.cfg.warm_start) BSG_CUDA(cudaMemsetAsync(it.x, 0, sizeof(double) * 3 * n, ctx.stream));
+        BicgState& h = t[k].h;
+        for (int c = 0; c < 3; ++c) {
+            h.target2[c] = -1.0;
+            h.done[c] = 0;
+            h.iters[c] = 0;
+            it.out[c] = SolveOutcome{};
+        }
+        h.atol = it.cfg.atol;
+        h.rtol = it.cfg.rtol;
+        h.max_iters = it.cfg.max_iterations;
+    }
+    std::vector<BicgState> res(K);
+    BicgBatch<3> batch;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        std::vector<int> active;
+        for (int k = 0; k < K; ++k)
+            if (!(t[k].finished[0] && t[k].finished[1] && t[k].finished[2])) active.push_back(k);
+        if (active.empty()) break;
+        std::vector<long long> slices;
+        batch.args.clear();
+        for (int k : active) {
+            Impl& m = *items[k].solver->impl_;
+            BSG_CUDA(cudaMemcpyAsync(m.bst.data(), &t[k].h, sizeof(BicgState), cudaMemcpyHostToDevice, ctx.stream));
+            batch.args.push_back({sell[k], items[k].b, items[k].x, m.r.data(), m.r0.data(), m.p.data(), m.v.data(),
+                                  m.ph.data(), m.sh.data(), m.t.data(), m.partial.data(), m.bst.data()});
+            slices.push_back(sell[k].nslices);
+        }
+        if (batched) {
+            batch.cta_begin = allotCtas(slices, bicgstabGrid(ctx));
+            launchBicgstabBatch<3>(ctx, batch);
+        } else {
+            for (const auto& a : batch.args) launchBicgstab<3>(ctx, a);
+        }
+        for (int k : active)
+            BSG_CUDA(cudaMemcpyAsync(&res[k], items[k].solver->impl_->bst.data(), sizeof(BicgState),
+                                     cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        for (int k : active) {
+            BicgItem& it = items[k];
+            Track& tr = t[k];
+            const BicgState& r = res[k];
+            if (r.status == 3) fail(kCuda, "persistent BiCGStab: a barrier wait ran past its bound");
+            for (int c = 0; c < 3; ++c) {
+                if (tr.finished[c]) continue;
+                SolveOutcome& o = it.out[c];
+                ++o.checks;
+                if (attempt == 0) {
+                    // zero initial guess unless warm start: r0 = b (petsc_linear_system.cpp:383-391)
+                    o.initial = std::sqrt(r.rr0[c]);
+                    tr.scale[c] = residualScale(std::sqrt(r.rr0[c]), std::sqrt(r.bb[c]));
+                    tr.target[c] = std::max(it.cfg.atol, it.cfg.rtol * tr.scale[c]);
+                }
+                tr.fin[c] = std::sqrt(r.fin2[c]);
+                o.iterations = r.iters[c];
+                o.final_ = tr.fin[c];
+                o.relative = tr.fin[c] / tr.scale[c];
+                const bool ok = std::isfinite(tr.fin[c]) && tr.fin[c] <= tr.target[c];
+                o.status = ok ? 0 : (std::isfinite(tr.fin[c]) && r.done[c] != 2 ? 1 : 2);
+                if (ok || !std::isfinite(tr.fin[c]) || r.done[c] == 2 || r.iters[c] >= it.cfg.max_iterations) {
+                    tr.finished[c] = true;
+                    tr.h.done[c] = 1;
+                } else {
+                    // true-residual restart with a halved internal target (petsc_linear_system.cpp:412-439)
+                    tr.h.target2[c] = 0.25 * r.target2[c];
+                    tr.h.done[c] = 0;
+                }
+                tr.h.iters[c] = r.iters[c];
+            }
+            for (int c = 0; c < 3; ++c)
+                if (tr.finished[c]) tr.h.done[c] = 1;
+            // a restart recomputes r = b - A x from the current x; targets already set stay
+            for (int c = 0; c < 3; ++c)
+                if (!tr.finished[c] && tr.h.target2[c] < 0.0) tr.h.target2[c] = r.target2[c];
+        }
+    }
+}
+
 template <int C>
 void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                                     SolveOutcome out[]) {
+    if (persistent && C == 3) {
+        std::vector<BicgItem> one(1);
+        one[0].solver = this;
+        one[0].A = A;
+        one[0].b = b;
+        one[0].x = x;
+        one[0].cfg = cfg;
+        solveVector3Batch(impl_->ctx, one, false);
+        for (int c = 0; c < C; ++c) out[c] = one[0].out[c];
+        return;
+    }
     Impl& m = *impl_;
     Context& ctx = m.ctx;
     const int n = A.n;

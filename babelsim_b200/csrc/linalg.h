@@ -57,6 +57,16 @@ struct BatchSolve {
     SolveOutcome out{};
 };
 
+// One 3-component system of a batched persistent BiCGStab solve (KrylovSolver::solveVector3Batch).
+struct BicgItem {
+    KrylovSolver* solver = nullptr;       // owns this system's vectors, SELL copy and solve state
+    Dcsr<double> A{};
+    const double* b = nullptr;            // xyz-interleaved
+    double* x = nullptr;
+    SolverConfig cfg{};
+    SolveOutcome out[3]{};
+};
+
 // When a preconditioner built for an earlier matrix version is reused (lagged), as
 // PetscLinearSystem does (src/backend/petsc_linear_system.cpp:257-324, 446-470): a
 // rebuild is due when rebuild_interval matrix versions or right-hand-side solves
@@ -130,6 +140,11 @@ public:
     // restarts with a halved internal target).  The true residuals of all systems are read
     // back together.  Every item's solver must be on ctx.
     static void solveBatch(Context& ctx, std::vector<BatchSolve>& items);
+    // Several 3-component BiCGStab systems (Jacobi preconditioner, the momentum equations of
+    // a batch) solved by the persistent BiCGStab kernel: with `batched` all unfinished systems
+    // of an attempt share one cooperative launch, each on CTAs of its own; otherwise each
+    // system gets the whole grid in turn.  The reference's acceptance loop per component.
+    static void solveVector3Batch(Context& ctx, std::vector<BicgItem>& items, bool batched = true);
     int check_interval = 8;  // iterations between host convergence checks
     // CG with AMG, Jacobi or no preconditioner runs as one persistent cooperative
     // kernel per attempt (pcg_persistent.cu); set false to use per-kernel launches.

@@ -1,12 +1,9 @@
 // Persistent cooperative PCG + AMG V-cycle on SELL-32 levels (see pcg_sell.cuh).
-#include <cooperative_groups.h>
-
+#include "group.cuh"
 #include "pcg_sell.cuh"
 
 #include <algorithm>
 #include <cmath>
-
-namespace cg = cooperative_groups;
 
 namespace bsg {
 namespace {
@@ -20,122 +17,6 @@ constexpr int SB = BSG_SELL_SB;  // threads per block
 #ifndef BSG_SELL_MIN_BLOCKS
 #define BSG_SELL_MIN_BLOCKS 3
 #endif
-
-// The CTAs that cooperate on one solve.  GridGroup: the whole cooperative grid,
-// synchronised by cooperative groups.  SegmentGroup: a contiguous range of the
-// grid's CTAs that owns one system of a batch; its barrier is a counter and a
-// generation word in global memory (all CTAs of a cooperative launch are
-// resident, so the spin always ends), and every wait is bounded: past
-// kBarrierCycles the group records an abort and its barriers stop waiting, so
-// the launch ends and the host reports the failure instead of hanging.
-struct GridGroup {
-    cg::grid_group g;
-    __device__ GridGroup() : g(cg::this_grid()) {}
-    __device__ __forceinline__ int rank() const { return blockIdx.x; }
-    __device__ __forceinline__ int size() const { return gridDim.x; }
-    __device__ __forceinline__ void sync() { g.sync(); }
-    __device__ __forceinline__ bool aborted() const { return false; }
-};
-
-constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s at the B200's clock
-
-struct SegmentGroup {
-    int cta0, ncta;
-    SegmentBarrier* bar;
-    __device__ __forceinline__ int rank() const { return blockIdx.x - cta0; }
-    __device__ __forceinline__ int size() const { return ncta; }
-    __device__ __forceinline__ bool aborted() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
-    __device__ void sync() {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            volatile unsigned* gen = &bar->generation;
-            const unsigned g0 = *gen;
-            __threadfence();
-            if (atomicAdd(&bar->count, 1u) == static_cast<unsigned>(ncta) - 1u) {
-                atomicExch(&bar->count, 0u);
-                __threadfence();
-                atomicAdd(&bar->generation, 1u);
-            } else {
-                const long long t0 = clock64();
-                while (*gen == g0) {
-                    if (aborted()) break;
-                    if (clock64() - t0 > kBarrierCycles) {
-                        atomicExch(&bar->abort, 1);
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
-            __threadfence();
-        }
-        __syncthreads();
-    }
-};
-
-struct Lanes {
-    int lane, gwarp, nwarps, gthread, nthreads;
-};
-
-template <class G>
-__device__ __forceinline__ Lanes lanes(const G& g) {
-    Lanes c;
-    c.gthread = g.rank() * SB + threadIdx.x;
-    c.nthreads = g.size() * SB;
-    c.lane = threadIdx.x & 31;
-    c.gwarp = c.gthread >> 5;
-    c.nwarps = c.nthreads >> 5;
-    return c;
-}
-
-// Deterministic grid sum of NV values (FP64); every block returns the same
-// totals.  `buf` alternates between two halves of `partial` so a fast block's
-// next write never overtakes a slow block's read of the previous sum.
-template <int NV, class G>
-__device__ void gridSum(G& g, double v[NV], double* partial, int& buf) {
-    __shared__ double sh[NV][SB / 32];
-    __shared__ double tot[NV];
-    double* part = partial + static_cast<long long>(buf) * g.size() * NV;
-    buf ^= 1;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-        double x = v[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) sh[j][warp] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) {
-            double s = 0.0;
-            for (int w = 0; w < SB / 32; ++w) s += sh[j][w];
-            part[g.rank() * NV + j] = s;
-        }
-    }
-    g.sync();
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-        double x = 0.0;
-        for (int b = threadIdx.x; b < g.size(); b += SB) x += part[b * NV + j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) sh[j][warp] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) {
-            double s = 0.0;
-            for (int w = 0; w < SB / 32; ++w) s += sh[j][w];
-            tot[j] = s;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < NV; ++j) v[j] = tot[j];
-    __syncthreads();
-}
 
 __device__ __forceinline__ void mark(const PhaseLog& log, int id) {
     if (log.entries && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -190,43 +71,47 @@ __device__ __forceinline__ SplitUnit splitUnit(int u, int K, int lane) {
 }
 
 template <class TK, class TV, class G>
-__device__ double vcycle(G& g, const VCycleView<TV>& V, const TK* r, TK* z, const PhaseLog& log) {
-    const Lanes c = lanes(g);
+__device__ double vcycle(G& g, const VCycleView<TV>& V, const TK* r, TK* z, const PhaseLog& log,
+                         bool level0_residual_done = false) {
+    const Lanes c = lanes<SB>(g);
     const int L = V.levels;
     // ---- down
     for (int l = 0; l < L - 1; ++l) {
         const VLevel<TV> f = V.lv[l];
-        if (V.nu >= 2) {
-            for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
-                const int i = 32 * s + c.lane;
-                const TV* w = f.w;
-                const TV aw = sellRow(f.A, s, c.lane, [&](int j) { return w[j]; });
-                if (i < f.A.n) {
-                    const TV wi = w[i];
-                    f.x[i] = wi + f.rd[i] * (f.b[i] - (f.A.diag[i] * wi + aw));
+        // t of level 0 may have come with the Krylov update (fused sweep in pcgBody)
+        if (!(l == 0 && level0_residual_done)) {
+            if (V.nu >= 2) {
+                for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+                    const int i = 32 * s + c.lane;
+                    const TV* w = f.w;
+                    const TV aw = sellRow(f.A, s, c.lane, [&](int j) { return w[j]; });
+                    if (i < f.A.n) {
+                        const TV wi = w[i];
+                        f.x[i] = wi + f.rd[i] * (f.b[i] - (f.A.diag[i] * wi + aw));
+                    }
+                }
+                g.sync();
+                mark(log, 10 + l);
+            }
+            const TV* xs = V.nu >= 2 ? f.x : f.w;
+            const int K = splitOf(f.A.nslices, c.nwarps);
+            if (K == 1) {
+                for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
+                    const int i = 32 * s + c.lane;
+                    const TV ax = sellRow(f.A, s, c.lane, [&](int j) { return xs[j]; });
+                    if (i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
+                }
+            } else {
+                for (int u = c.gwarp; u < f.A.nslices * K; u += c.nwarps) {
+                    const SplitUnit su = splitUnit(u, K, c.lane);
+                    const int i = 32 * su.s + su.r;
+                    const TV ax = sellRowSplit(f.A, su.s, su.r, su.q, K, [&](int j) { return xs[j]; });
+                    if (su.q == 0 && i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
                 }
             }
             g.sync();
-            mark(log, 10 + l);
+            mark(log, 30 + l);
         }
-        const TV* xs = V.nu >= 2 ? f.x : f.w;
-        const int K = splitOf(f.A.nslices, c.nwarps);
-        if (K == 1) {
-            for (int s = c.gwarp; s < f.A.nslices; s += c.nwarps) {
-                const int i = 32 * s + c.lane;
-                const TV ax = sellRow(f.A, s, c.lane, [&](int j) { return xs[j]; });
-                if (i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
-            }
-        } else {
-            for (int u = c.gwarp; u < f.A.nslices * K; u += c.nwarps) {
-                const SplitUnit su = splitUnit(u, K, c.lane);
-                const int i = 32 * su.s + su.r;
-                const TV ax = sellRowSplit(f.A, su.s, su.r, su.q, K, [&](int j) { return xs[j]; });
-                if (su.q == 0 && i < f.A.n) f.t[i] = f.b[i] - (f.A.diag[i] * xs[i] + ax);
-            }
-        }
-        g.sync();
-        mark(log, 30 + l);
         const VLevel<TV> cl = V.lv[l + 1];
         for (int I = c.gthread; I < cl.A.n; I += c.nthreads) {
             TV s = TV(0);
@@ -332,7 +217,7 @@ __device__ __forceinline__ void seedLevel0(const VLevel<TV>& f0, int i, TK ri) {
 
 template <class TK, class TV, class G>
 __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
-    const Lanes c = lanes(g);
+    const Lanes c = lanes<SB>(g);
     const SellMat<TK>& A = a.A;
     const int n = A.n;
     int buf = 0;
@@ -361,7 +246,7 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
             v[1] += static_cast<double>(a.b[i]) * static_cast<double>(a.b[i]);
         }
     }
-    gridSum<2>(g, v, a.partial, buf);
+    gridSum<2, SB>(g, v, a.partial, buf);
     mark(a.log, 1);
     double target2 = target2_in;
     if (target2 < 0.0) {
@@ -388,12 +273,15 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
         if (g.rank() == 0 && threadIdx.x == 0) st.status = 3;
         return;
     }
-    gridSum<1>(g, w, a.partial, buf);
+    gridSum<1, SB>(g, w, a.partial, buf);
     mark(a.log, 4);
     double rz = w[0];
     double beta = 0.0;
     TK* pold = a.p0;
     TK* pnew = a.p1;
+    const bool fuse = a.r2 != nullptr && a.V.nu < 2 && a.V.levels >= 2;
+    TK* rcur = a.r;
+    TK* rnext = a.r2;
     int it = 0;
     int status = 1;
     double rr = v[0];
@@ -417,21 +305,46 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
                 pq[0] += static_cast<double>(pi) * static_cast<double>(qi);
             }
         }
-        gridSum<1>(g, pq, a.partial, buf);
+        gridSum<1, SB>(g, pq, a.partial, buf);
         mark(a.log, 2);
         if (!(fabs(pq[0]) > 0.0) || !isfinite(pq[0])) { status = 2; break; }
         const double alpha = rz / pq[0];
         const TK ak = static_cast<TK>(alpha);
         double nr[2] = {0.0, 0.0};
-        for (int i = c.gthread; i < n; i += c.nthreads) {
-            a.x[i] += ak * pnew[i];
-            const TK ri = a.r[i] - ak * a.q[i];
-            a.r[i] = ri;
-            seedLevel0<TK, TV>(f0, i, ri);
-            nr[0] += static_cast<double>(ri) * static_cast<double>(ri);
-            if (a.flexible) nr[1] += static_cast<double>(ri) * static_cast<double>(a.z[i]);  // r_new . z_old
+        if (fuse) {
+            // x += alpha p, r_new = r - alpha q, the level-0 seeds b = r_new, w = rd b, and the
+            // level-0 residual t = b - A w with the neighbours' w formed from their r and q
+            const TK* rc = rcur;
+            const TK* qq = a.q;
+            const TV* rd0 = f0.rd;
+            for (int s = c.gwarp; s < f0.A.nslices; s += c.nwarps) {
+                const int i = 32 * s + c.lane;
+                const TV aw = sellRow(f0.A, s, c.lane,
+                                      [&](int j) { return rd0[j] * static_cast<TV>(rc[j] - ak * qq[j]); });
+                if (i < n) {
+                    a.x[i] += ak * pnew[i];
+                    const TK ri = rc[i] - ak * qq[i];
+                    rnext[i] = ri;
+                    const TV rv = static_cast<TV>(ri);
+                    const TV wi = rd0[i] * rv;
+                    f0.b[i] = rv;
+                    f0.w[i] = wi;
+                    f0.t[i] = rv - (f0.A.diag[i] * wi + aw);
+                    nr[0] += static_cast<double>(ri) * static_cast<double>(ri);
+                    if (a.flexible) nr[1] += static_cast<double>(ri) * static_cast<double>(a.z[i]);
+                }
+            }
+        } else {
+            for (int i = c.gthread; i < n; i += c.nthreads) {
+                a.x[i] += ak * pnew[i];
+                const TK ri = a.r[i] - ak * a.q[i];
+                a.r[i] = ri;
+                seedLevel0<TK, TV>(f0, i, ri);
+                nr[0] += static_cast<double>(ri) * static_cast<double>(ri);
+                if (a.flexible) nr[1] += static_cast<double>(ri) * static_cast<double>(a.z[i]);  // r_new . z_old
+            }
         }
-        gridSum<2>(g, nr, a.partial, buf);
+        gridSum<2, SB>(g, nr, a.partial, buf);
         mark(a.log, 3);
         rr = nr[0];
         const double rz_old_new = nr[1];
@@ -439,14 +352,19 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
         if (!isfinite(rr)) { status = 2; break; }
         if (rr <= target2) { status = 0; break; }
         if (it >= max_iterations) break;
-        double zr[1] = {vcycle<TK, TV>(g, a.V, a.r, a.z, a.log)};
-        gridSum<1>(g, zr, a.partial, buf);
+        double zr[1] = {vcycle<TK, TV>(g, a.V, fuse ? rnext : a.r, a.z, a.log, fuse)};
+        gridSum<1, SB>(g, zr, a.partial, buf);
         mark(a.log, 4);
         beta = a.flexible ? (zr[0] - rz_old_new) / rz : zr[0] / rz;
         rz = zr[0];
         TK* tmp = pold;
         pold = pnew;
         pnew = tmp;
+        if (fuse) {
+            TK* t2 = rcur;
+            rcur = rnext;
+            rnext = t2;
+        }
     }
     if (g.rank() == 0 && threadIdx.x == 0) {
         st.rr = rr;

@@ -25,6 +25,7 @@
 // bit for bit.
 #pragma once
 
+#include "group.cuh"
 #include "pcg_persistent.cuh"
 #include "sell.cuh"
 
@@ -71,19 +72,17 @@ struct SellPcgArgs {
     // preconditioner that is not exactly the same linear operator every iteration
     // (an FP32 V-cycle); 0: beta = r_new.z_new / r_old.z_old.
     int flexible = 0;
+    // Second residual buffer.  When given (and the V-cycle has one smoothing step and at
+    // least two levels) the Krylov update of x and r is fused with the level-0 residual
+    // sweep of the next V-cycle: neighbours' r are read from one buffer while the new r
+    // goes to the other, saving one grid-wide phase and one pass over the vectors per
+    // CG iteration.
+    TK* r2 = nullptr;
 };
 
 // Launch (pcg_sell.cu); the grid is sized for co-residency.
 template <class TK, class TV>
 void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& args);
-
-// Barrier state of one system of a batch (zeroed before every launch).
-struct SegmentBarrier {
-    unsigned count;
-    unsigned generation;
-    int abort;   // set when a wait ran past its bound; the system's PcgState then has status 3
-    int pad;
-};
 
 // Several independent systems (each with its own matrix, V-cycle, vectors, partials
 // and PcgState, anywhere in device memory) solved by one cooperative launch: system s

@@ -221,11 +221,25 @@ void SimpleSolver::outerIterationSegments() {
     std::vector<double> linP(K, 0.0);
     bool failed = false;
     {
-        BSG_PROFILE(ctx_, "bicgstab3_segments");
+        // BiCGStab (kspType bcgs): every active case's momentum system in one persistent launch
+        // per attempt; other Krylov types solve case by case
+        std::vector<BicgItem> items;
+        std::vector<int> which;
         for (int k = 0; k < K; ++k) {
             SimpleSegment& sg = *segs_[k];
             if (sg.frozen) continue;
             const Dcsr<double> A = sg.view(mom.diag.data(), mom.val.data());
+            if (cfg_.momentum_solver.solver == 1) {
+                BicgItem it;
+                it.solver = sg.mom.get();
+                it.A = A;
+                it.b = mom.src.data() + 3LL * sg.c0;
+                it.x = U_.v.data() + 3LL * sg.c0;
+                it.cfg = cfg_.momentum_solver;
+                items.push_back(it);
+                which.push_back(k);
+                continue;
+            }
             SolveOutcome uo[3];
             sg.mom->solveVector3(A, cfg_.momentum_solver, mom.src.data() + 3LL * sg.c0, U_.v.data() + 3LL * sg.c0, uo);
             for (const auto& o : uo) {
@@ -234,6 +248,14 @@ void SimpleSolver::outerIterationSegments() {
                 if (o.status == 2 || !std::isfinite(o.final_)) failed = true;
             }
         }
+        KrylovSolver::solveVector3Batch(ctx_, items, true);
+        for (std::size_t q = 0; q < items.size(); ++q)
+            for (const auto& o : items[q].out) {
+                const int k = which[q];
+                mom_its[k] += o.iterations;
+                mom_ok[k] = mom_ok[k] && o.status == 0;
+                if (o.status == 2 || !std::isfinite(o.final_)) failed = true;
+            }
     }
     if (failed) { report_.status = 2; return; }
     {
