@@ -182,6 +182,10 @@ struct DeviceMesh {
     DeviceArray<int> slot_own, slot_nbr;
     // scratch for the first Green-Gauss pass (3*9*n_cells doubles at most)
     DeviceArray<double> ws_grad_pass1;
+    // per cell, for a mesh that holds several independent cases (a batch): 1 where the cell's
+    // case has orthogonal geometry, so the second Green-Gauss pass leaves its cells alone as a
+    // solo run of that case would; empty when the mesh's own flag applies to every cell
+    DeviceArray<unsigned char> cell_orth;
     // per-slot records of the face pass of diffusion assembly ((1 + C) * 2 n_interior doubles)
     DeviceArray<double> ws_slots;
     // external geometry copy for bsg_mesh_export (host; filled on first export when the

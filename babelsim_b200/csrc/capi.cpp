@@ -4,6 +4,7 @@
 #include "amg.h"
 #include "fvm.h"
 #include "linalg.h"
+#include "mesh_io.h"
 #include "piso.h"
 #include "results.h"
 #include "simple.h"
@@ -542,6 +543,45 @@ int bsg_mesh_create_polyhedral_host(bsg_context* ctx, int32_t n_vertices, const 
             throw;
         }
         *out = m;
+    });
+}
+
+int bsg_mesh_create_from_file(bsg_context* ctx, const char* path, bsg_mesh** out) {
+    return guard(ctx, [&] {
+        require(ctx && path && out, "null argument");
+        const bsg::PolyFile f = bsg::readPolyFile(path);
+        auto m = std::make_unique<bsg_mesh>();
+        m->owner = ctx;
+        try {
+            m->mesh = bsg::buildDeviceMeshPolyhedral(*ctx->ctx, static_cast<int>(f.vertices.size() / 3),
+                                                     f.vertices.data(), static_cast<int>(f.owner.size()),
+                                                     f.offsets.data(), f.ids.data(), f.owner.data(),
+                                                     f.neighbour.data(), f.patch.data(),
+                                                     static_cast<int>(f.patch_names.size()));
+        } catch (const bsg::Error& e) {
+            if (e.code != bsg::kArgument) throw;
+            bsg::fail(bsg::kArgument, std::string("invalid BabelSim mesh file ") + path + ": " + e.what());
+        }
+        *out = m.release();
+    });
+}
+
+int bsg_mesh_file_info(const char* path, int64_t out[4], char* patches, int32_t capacity) {
+    return guard(nullptr, [&] {
+        require(path && out, "null argument");
+        const bsg::PolyFile f = bsg::readPolyFile(path);
+        out[0] = f.n_cells;
+        out[1] = static_cast<int64_t>(f.owner.size());
+        out[2] = static_cast<int64_t>(f.vertices.size() / 3);
+        out[3] = static_cast<int64_t>(f.patch_names.size());
+        if (patches && capacity > 0) {
+            static const char* kinds[] = {"generic", "wall", "inlet", "outlet", "symmetry", "processor"};
+            std::string text;
+            for (std::size_t p = 0; p < f.patch_names.size(); ++p)
+                text += f.patch_names[p] + " " + kinds[f.patch_kinds[p]] + "\n";
+            require(static_cast<int32_t>(text.size()) < capacity, "patch list buffer too small");
+            std::memcpy(patches, text.c_str(), text.size() + 1);
+        }
     });
 }
 

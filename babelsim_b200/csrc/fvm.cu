@@ -19,11 +19,18 @@ constexpr double kEps = 2.220446049250313e-16;
 // ---------------------------------------------------------------- gradients
 // greenGaussGradient (operators.cpp:275-316 scalar, 365-405 vector); PASS2 is
 // the skew-corrected second pass that uses the first-pass gradient g1.
+// orth_cells (second pass only, may be nullptr): cells whose case of a batch has orthogonal
+// geometry keep the first-pass gradient.
 template <int C, bool PASS2>
 __global__ void kGradGauss(MeshView m, BcView b, const double* __restrict__ x, const double* __restrict__ g1,
-                           double* __restrict__ out) {
+                           double* __restrict__ out, const unsigned char* __restrict__ orth_cells) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.n_cells) return;
+    if (PASS2 && orth_cells && orth_cells[i]) {
+#pragma unroll
+        for (int j = 0; j < 3 * C; ++j) out[3 * C * i + j] = g1[3 * C * i + j];
+        return;
+    }
     double acc[3 * C];
 #pragma unroll
     for (int j = 0; j < 3 * C; ++j) acc[j] = 0.0;
@@ -894,19 +901,21 @@ void gradient(DeviceField& x, int method, DeviceArray<double>& out) {
         return;
     }
     if (method != 0) fail(kArgument, "unsupported gradient method");
+    const unsigned char* none = nullptr;
     if (m.orthogonal) {
-        if (C == 1) launch(ctx, kGradGauss<1, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, out.data());
-        else launch(ctx, kGradGauss<3, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, out.data());
+        if (C == 1) launch(ctx, kGradGauss<1, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, out.data(), none);
+        else launch(ctx, kGradGauss<3, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, out.data(), none);
         return;
     }
     DeviceArray<double>& first = m.ws_grad_pass1;  // persistent scratch: no allocation per call
     if (first.size() < out.size()) first.resize(out.size());
+    const unsigned char* oc = m.cell_orth.size() ? m.cell_orth.data() : nullptr;
     if (C == 1) {
-        launch(ctx, kGradGauss<1, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, first.data());
-        launch(ctx, kGradGauss<1, true>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)first.data(), out.data());
+        launch(ctx, kGradGauss<1, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, first.data(), none);
+        launch(ctx, kGradGauss<1, true>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)first.data(), out.data(), oc);
     } else {
-        launch(ctx, kGradGauss<3, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, first.data());
-        launch(ctx, kGradGauss<3, true>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)first.data(), out.data());
+        launch(ctx, kGradGauss<3, false>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)nullptr, first.data(), none);
+        launch(ctx, kGradGauss<3, true>, m.n_cells, mv, b, (const double*)x.v.data(), (const double*)first.data(), out.data(), oc);
     }
 }
 

@@ -41,6 +41,33 @@ __global__ void kRhieChow(MeshView m, BcView bp, const double* __restrict__ rAU,
     phiH[f] = v;
 }
 
+// Per case of a batch: cleared when one of its faces is non-orthogonal by Mesh::polyhedral's
+// test (|k| > 1e-12 |Sf|, or for an interior face |skew| > 1e-12 |d|; the host geometry's
+// criterion), so each case gets the orthogonal flag its own mesh would have.
+__global__ void kCaseOrthogonal(MeshView m, const int* __restrict__ case_of, int* __restrict__ orth) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < m.n_interior) {
+        const double k0 = m.kvec[3 * f], k1 = m.kvec[3 * f + 1], k2 = m.kvec[3 * f + 2];
+        bool ortho = !(sqrt(k0 * k0 + k1 * k1 + k2 * k2) > 1e-12 * m.area[f]);
+        const int o = m.own[f], n = m.nbr[f];
+        const double d0 = m.xc[3 * n] - m.xc[3 * o], d1 = m.xc[3 * n + 1] - m.xc[3 * o + 1],
+                     d2 = m.xc[3 * n + 2] - m.xc[3 * o + 2];
+        const double s0 = m.skew[3 * f], s1 = m.skew[3 * f + 1], s2 = m.skew[3 * f + 2];
+        if (sqrt(s0 * s0 + s1 * s1 + s2 * s2) > 1e-12 * sqrt(d0 * d0 + d1 * d1 + d2 * d2)) ortho = false;
+        if (!ortho) atomicAnd(orth + case_of[o], 0);
+    } else if (f < m.n_interior + m.n_boundary) {
+        const int fb = f - m.n_interior;
+        const double k0 = m.bk[3 * fb], k1 = m.bk[3 * fb + 1], k2 = m.bk[3 * fb + 2];
+        if (sqrt(k0 * k0 + k1 * k1 + k2 * k2) > 1e-12 * m.barea[fb]) atomicAnd(orth + case_of[m.bown[fb]], 0);
+    }
+}
+
+__global__ void kCellOrthogonal(int n, const int* __restrict__ case_of, const int* __restrict__ orth,
+                                unsigned char* __restrict__ cell) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cell[i] = orth[case_of[i]] ? 1 : 0;
+}
+
 // Traces of a calculated cell field whose constraints are the default
 // zeroGradient ones: the owner value (geometry.cpp values(), field.h:264-272).
 __global__ void kOwnerTrace(MeshView m, const double* __restrict__ x, double* __restrict__ trace) {
@@ -135,6 +162,22 @@ void SimpleSolver::setSegments(const std::vector<int>& off, const std::vector<do
     }
     muEff_.v.upload(mu, ctx_.stream);
     if (!seg_pinned_) BSG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&seg_pinned_), sizeof(double) * 16 * 4096));
+    // the second Green-Gauss pass follows each case's own orthogonality, not the batch mesh's
+    m_.cell_orth.release();
+    if (!m_.orthogonal) {
+        DeviceArray<int> d_case, d_orth;
+        d_case.upload(seg_of, ctx_.stream);
+        std::vector<int> ones(K, 1);
+        d_orth.upload(ones, ctx_.stream);
+        kCaseOrthogonal<<<gridFor(static_cast<long long>(m_.n_interior) + m_.n_boundary, kBlock), kBlock, 0,
+                          ctx_.stream>>>(view(m_), d_case.data(), d_orth.data());
+        m_.cell_orth.resize(m_.n_cells);
+        kCellOrthogonal<<<gridFor(m_.n_cells, kBlock), kBlock, 0, ctx_.stream>>>(m_.n_cells, d_case.data(),
+                                                                                 d_orth.data(), m_.cell_orth.data());
+        BSG_CUDA(cudaGetLastError());
+        ctx_.launches += 2;
+        ctx_.sync();
+    }
     ctx_.sync();
 }
 

@@ -181,6 +181,13 @@ int bsg_mesh_create_polyhedral_host(bsg_context* ctx, int32_t n_vertices, const 
                                     const int32_t* face_point_ids, const int32_t* owner,
                                     const int32_t* neighbour, const int32_t* patch, int32_t n_patches,
                                     bsg_mesh** out);
+/* The reference's mesh file (BABELSIM_MESH 3, readMeshFile, src/io/mesh_reader.cpp:44-111) read
+ * natively on the host and built as bsg_mesh_create_polyhedral builds it (geometry on the device).
+ * A bad file is rejected with the reference's message, "invalid BabelSim mesh file <path>: ...". */
+int bsg_mesh_create_from_file(bsg_context* ctx, const char* path, bsg_mesh** out);
+/* Host only: reads and checks a mesh file.  out = {cells, faces, vertices, patches}; when `patches`
+ * is given, one "<name> <kind>" line per patch in file order. */
+int bsg_mesh_file_info(const char* path, int64_t out[4], char* patches, int32_t capacity);
 int bsg_mesh_destroy(bsg_mesh* mesh);
 /* Host-only check of a polyhedral description: computes the geometry exactly as
  * bsg_mesh_create_polyhedral does (no device needed) and reports the first
