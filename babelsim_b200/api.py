@@ -29,6 +29,16 @@ def options(interpolation="linear", gradient="greenGauss", convection="upwind", 
                    -1 if coefficient_gradient is None else GRAD[coefficient_gradient])
 
 
+def file_info(path) -> dict:
+    """Host-only read of a BABELSIM_MESH 3 file by the native reader: sizes and patches."""
+    out = np.zeros(4, np.int64)
+    buf = C.create_string_buffer(1 << 20)
+    check(lib().bsg_mesh_file_info(str(path).encode(), ptr(out), buf, len(buf)))
+    lines = [ln.split() for ln in buf.value.decode().splitlines() if ln.strip()]
+    return {"cells": int(out[0]), "faces": int(out[1]), "vertices": int(out[2]),
+            "patches": [(ln[0], ln[1]) for ln in lines]}
+
+
 def solver_config(ksp="cg", pc="jacobi", atol=1e-14, rtol=1e-10, max_iterations=1000, warm_start=False,
                   amg_max_levels=12, amg_coarse_size=400, amg_smoothing_steps=1, precision=0, rebuild_interval=8,
                   reuse_growth=2.0) -> SolverConfig:
@@ -130,6 +140,17 @@ class Mesh:
                      ptr(patch), len(poly.patch_names), C.byref(h)), ctx.h)
         m = cls(ctx, h, len(poly.patch_names))
         m.patch_names = list(poly.patch_names)
+        return m
+
+    @classmethod
+    def from_file(cls, ctx: Context, path: str):
+        """The reference's mesh file (BABELSIM_MESH 3) read by the library's native reader,
+        geometry on the device."""
+        info = file_info(path)
+        h = C.c_void_p()
+        check(lib().bsg_mesh_create_from_file(ctx.h, str(path).encode(), C.byref(h)), ctx.h)
+        m = cls(ctx, h, len(info["patches"]))
+        m.patch_names = [name for name, _ in info["patches"]]
         return m
 
     @classmethod

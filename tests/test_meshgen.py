@@ -80,3 +80,35 @@ def test_library_geometry_rejects_what_the_reference_rejects():
     pm.vertices[ring[1]] = pm.vertices[ring[0]]   # collapse an edge of one face: zero-area triangle
     with pytest.raises(Exception):
         validate_polyhedral(pm)
+
+
+def test_native_mesh_reader_matches_the_python_reader(tmp_path):
+    """bsg_mesh_file_info (the native BABELSIM_MESH 3 reader, host only) on files the Python
+    writer made and on the reference-format cavity fixture mesh."""
+    from babelsim_b200.api import file_info
+    for pm in (meshgen.voronoi_cube(5, 0.3, 11), meshgen.cavity_2d(6)):
+        path = tmp_path / "m.mesh"
+        meshgen.write_mesh(path, pm)
+        info = file_info(path)
+        assert info["cells"] == pm.n_cells and info["faces"] == len(pm.owner)
+        assert info["vertices"] == len(pm.vertices)
+        assert [n for n, _ in info["patches"]] == list(pm.patch_names)
+        assert [k for _, k in info["patches"]] == list(pm.patch_kinds)
+
+
+@pytest.mark.parametrize("edit,message", [
+    (lambda t: t.replace("BABELSIM_MESH 3", "BABELSIM_MESH 2", 1), "only BABELSIM_MESH version 3 is supported"),
+    (lambda t: t.replace("\nend", "\nend extra"), "unexpected trailing token extra"),
+    (lambda t: t.replace("minus_x\ngeneric", "minus_x\nplasma"), "unknown patch kind plasma"),
+    (lambda t: t.replace("\nfaces\n", "\nfacez\n"), "expected faces"),
+    (lambda t: t[:t.index("patches")], "missing patches keyword"),
+])
+def test_native_mesh_reader_rejects_bad_files_with_the_references_messages(tmp_path, edit, message):
+    from babelsim_b200 import BsgError
+    from babelsim_b200.api import file_info
+    path = tmp_path / "bad.mesh"
+    meshgen.write_mesh(path, meshgen.hex_box(2, 2, 2))
+    path.write_text(edit(path.read_text()))
+    with pytest.raises(BsgError) as err:
+        file_info(path)
+    assert f"invalid BabelSim mesh file {path}: {message}" in str(err.value)
