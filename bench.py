@@ -224,6 +224,41 @@ def cpu_baseline(seconds_budget=25.0, iterations=4, n=CPU_SAMPLE_SIDE):
             "preconditioner_setups": info.get("preconditioner_setups")}
 
 
+# Phase ids of the persistent pressure solver's timeline (bsg_context_phase_log).
+PHASE_NAMES = {1: "initial residual", 2: "CG product + p.q", 3: "x, r update + norm (+ level-0 residual)",
+               4: "level-0 post sweep + r.z", 50: "coarsest solve"}
+
+
+def pressure_phases(ctx, sim, iterations=2):
+    """Device time between the persistent pressure solver's grid barriers over `iterations` more
+    outer iterations (device %globaltimer), per CG iteration and phase."""
+    ctx.phase_log(1 << 20)
+    sim.iterate(iterations)
+    ctx.synchronize()
+    ent = ctx.phase_log_read()
+    ctx.phase_log(0)
+    acc, cg = {}, 0
+    for k in range(1, len(ent)):
+        pid = int(ent[k, 0])
+        if pid == 1:
+            continue  # the gap before a launch's first barrier includes the host's work between solves
+        cg += pid == 2
+        acc[pid] = acc.get(pid, 0.0) + (ent[k, 1] - ent[k - 1, 1]) / 1e3
+    cg = max(cg, 1)
+
+    def name(pid):
+        if pid in PHASE_NAMES:
+            return PHASE_NAMES[pid]
+        kind = {1: "pre-smooth", 3: "residual", 6: "first post sweep", 8: "post sweep + prolong"}.get(pid // 10, None)
+        if pid >= 100:
+            return f"restrict {pid - 100}->{pid - 99}"
+        return f"level {pid % 10} {kind}" if kind else str(pid)
+    out = {name(p): round(v / cg, 2) for p, v in sorted(acc.items())}
+    out["total"] = round(sum(acc.values()) / cg, 2)
+    out["cg_iterations"] = cg
+    return out
+
+
 def device_on_sample(bsg, ctx, s, warmup, steps=5):
     """The device path on the CPU baseline's own sample (the same mesh and settings), so the
     two throughputs can be compared case for case as well as per cell."""
@@ -284,7 +319,7 @@ def run_serving(args):
         t += rng.exponential(1.0 / args.arrival_rate)
         reqs.append(serve.Request(i, t, pool[k], speed=float(rng.uniform(0.5, 2.0)),
                                   nu=float(np.exp(rng.uniform(np.log(1e-3), np.log(1e-2)))),
-                                  max_iterations=args.max_outer, tolerance=1e-4))
+                                  max_iterations=args.max_outer, tolerance=args.tolerance))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
@@ -295,7 +330,8 @@ def run_serving(args):
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     mine = serve.shard(reqs, world, rank)
     ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
-    srv = serve.Server(ctx, hbm_budget=150 * 2**30, slots=args.slots)
+    srv = serve.Server(ctx, hbm_budget=150 * 2**30, slots=args.slots, solver_precision=args.precision,
+                       batched=not args.unbatched)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -317,7 +353,8 @@ def run_serving(args):
         # each request solved alone on the same GPU (arrival at 0, nothing else running)
         alone = []
         for r in reqs:
-            solo = serve.Server(ctx, hbm_budget=150 * 2**30, slots=1)
+            solo = serve.Server(ctx, hbm_budget=150 * 2**30, slots=1, solver_precision=args.precision,
+                                batched=not args.unbatched)
             rr = solo.run([serve.Request(r.id, 0.0, r.mesh, r.speed, r.nu, r.max_iterations, r.tolerance)])[0]
             alone.append(rr.latency)
         ratio = np.array([res[i].latency / alone[i] for i in range(len(reqs))])
@@ -326,8 +363,11 @@ def run_serving(args):
             "scaling": "strong",
             "config": {"workload": f"{args.requests} seeded requests, cells log-uniform 4k-100k (hex and "
                                    f"jittered-Voronoi cubes), Poisson arrivals {args.arrival_rate}/s, "
-                                   f"{args.slots} slots, 150 GiB budget, outer tolerance 1e-4 or "
-                                   f"{args.max_outer} iterations", "slots": args.slots},
+                                   f"{args.slots} slots, 150 GiB budget, outer tolerance {args.tolerance} or "
+                                   f"{args.max_outer} iterations, pressure V-cycle "
+                                   f"{'fp32' if args.precision == 2 else 'fp64'}, "
+                                   f"{'one solve per request' if args.unbatched else 'cohorts as block-diagonal batches'}",
+                       "slots": args.slots, "batched": not args.unbatched},
             "p50_latency_s": out["p50_latency_s"], "p99_latency_s": out["p99_latency_s"],
             "converged": out["converged"], "cell_iters_per_s": out["cell_iters_per_s"], "wall_s": wall,
             "parallelism": f"requests sharded over {world} GPU(s) by predicted cell-iterations, no data exchange",
@@ -603,6 +643,7 @@ def main():
     ap.add_argument("--cells", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison run")
+    ap.add_argument("--phases", action="store_true", help="add the pressure solver's phase timeline to the line")
     ap.add_argument("--workload", default="cavity", choices=["cavity", "serving", "piso-cylinder", "komega-channel", "batched"])
     ap.add_argument("--theta-cells", type=int, default=2000)
     ap.add_argument("--dt", type=float, default=0.001)
@@ -612,6 +653,9 @@ def main():
     ap.add_argument("--arrival-rate", type=float, default=8.0)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--max-outer", type=int, default=150)
+    ap.add_argument("--tolerance", type=float, default=1e-4, help="serving: outer-loop tolerance")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 2], help="serving: pressure V-cycle precision")
+    ap.add_argument("--unbatched", action="store_true", help="serving: one solve per request, no cohorts")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -683,6 +727,7 @@ def main():
             return rec[2] / rec[0]
         return algorithmic_bytes(name, N, 2 * Fi, amg_rows)
 
+    phases = pressure_phases(ctx, sim) if args.phases else None
     candidates = {k: v for k, v in prof.items() if launch_bytes(k, v)}
     top = max(candidates, key=lambda k: candidates[k][1]) if candidates else None
     peak, peak_kind = load_peaks()
@@ -771,6 +816,7 @@ def main():
                 "mixed_precision": mixed,
                 "gpu_launches": launches, "mesh_ingest": ingest,
                 "clocks": clocks.summary(), "profile_ms_one_step": {k: round(v[1], 3) for k, v in prof.items()},
+                "pressure_phases_us_per_cg_iteration": phases,
                 "pressure_iterations_per_solve": round(prof["pcg_amg_persistent"][3] / prof["pcg_amg_persistent"][0], 1)
                 if "pcg_amg_persistent" in prof else None,
                 "last_report": {"momentum_iterations": rep.momentum_iterations,
