@@ -20,7 +20,7 @@ EXPORTS = [
     "bsg_context_synchronize", "bsg_context_profile", "bsg_context_profile_report", "bsg_context_phase_log",
     "bsg_context_phase_log_read", "bsg_context_event_record",
     "bsg_context_event_elapsed", "bsg_mesh_create", "bsg_mesh_create_polyhedral", "bsg_mesh_create_polyhedral_host",
-    "bsg_mesh_destroy", "bsg_mesh_create_from_file", "bsg_mesh_file_info",
+    "bsg_mesh_destroy", "bsg_mesh_create_from_file", "bsg_mesh_file_info", "bsg_mesh_locality_order",
     "bsg_mesh_validate_polyhedral", "bsg_write_results",
     "bsg_mesh_sizes", "bsg_mesh_export", "bsg_field_create", "bsg_field_destroy", "bsg_field_set_boundary",
     "bsg_field_upload", "bsg_field_download", "bsg_field_set_boundary_flux", "bsg_math_grad",
@@ -168,7 +168,8 @@ def lib():
             "bsg_mesh_create_polyhedral": [vp, i32, vp, i32, vp, vp, vp, vp, vp, i32, pp],
             "bsg_mesh_create_polyhedral_host": [vp, i32, vp, i32, vp, vp, vp, vp, vp, i32, pp],
             "bsg_mesh_destroy": [vp], "bsg_mesh_create_from_file": [vp, C.c_char_p, pp],
-            "bsg_mesh_file_info": [C.c_char_p, vp, C.c_char_p, i32], "bsg_mesh_sizes": [vp, vp], "bsg_mesh_export": [vp, C.c_char_p, vp],
+            "bsg_mesh_file_info": [C.c_char_p, vp, C.c_char_p, i32],
+            "bsg_mesh_locality_order": [i32, i32, vp, vp, vp, C.POINTER(i32)], "bsg_mesh_sizes": [vp, vp], "bsg_mesh_export": [vp, C.c_char_p, vp],
             "bsg_mesh_validate_polyhedral": [i32, vp, i32, vp, vp, vp, vp, vp, i32, C.POINTER(i32), C.POINTER(i32)],
             "bsg_write_results": [C.c_char_p, C.c_char_p, i32, vp, i32, vp, vp, vp, vp, vp, i32, i32, vp, vp, vp],
             "bsg_field_create": [vp, i32, i32, pp], "bsg_field_destroy": [vp],

@@ -29,6 +29,17 @@ def options(interpolation="linear", gradient="greenGauss", convection="upwind", 
                    -1 if coefficient_gradient is None else GRAD[coefficient_gradient])
 
 
+def locality_order(poly):
+    """(order, applied): the cell numbering the library uses inside for this polyhedral mesh,
+    order[internal] = caller cell (reverse Cuthill-McKee when the caller's order is poor)."""
+    owner, nbr = i32(poly.owner), i32(poly.neighbour)
+    n = poly.n_cells
+    order = np.zeros(n, np.int32)
+    applied = C.c_int32()
+    check(lib().bsg_mesh_locality_order(n, len(owner), ptr(owner), ptr(nbr), ptr(order), C.byref(applied)))
+    return order, bool(applied.value)
+
+
 def file_info(path) -> dict:
     """Host-only read of a BABELSIM_MESH 3 file by the native reader: sizes and patches."""
     out = np.zeros(4, np.int64)

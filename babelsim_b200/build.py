@@ -20,7 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libbabelsim_b200.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["mesh.cpp", "mesh_io.cpp", "geometry.cu", "fvm.cu", "krylov.cu", "gmres.cu", "amg.cu", "pcg_persistent.cu", "pcg_sell.cu", "bicgstab_sell.cu", "simple.cu", "piso.cu", "rans.cu", "results.cpp", "capi.cpp"]
+SOURCES = ["mesh.cpp", "mesh_io.cpp", "renumber.cpp", "geometry.cu", "fvm.cu", "krylov.cu", "gmres.cu", "amg.cu", "pcg_persistent.cu", "pcg_sell.cu", "bicgstab_sell.cu", "simple.cu", "piso.cu", "rans.cu", "results.cpp", "capi.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # The device geometry reproduces the host geometry bit for bit: no FMA contraction there.
 EXTRA = {"geometry.cu": ["-fmad=false"]}

@@ -167,6 +167,11 @@ struct DeviceMesh {
     std::vector<int> face_slot;          // per external face: index in interior or boundary list
     std::vector<int> interior_ext, boundary_ext;
     DeviceArray<int> face_perm;          // caller face -> internal position (interior faces first)
+    // caller cell -> internal cell when the cells were renumbered for locality (empty: the
+    // caller's numbering is kept); cell arrays crossing the ABI go through cell_stage
+    std::vector<int> h_cell_perm;
+    DeviceArray<int> cell_perm;
+    DeviceArray<double> cell_stage;
     DeviceArray<double> face_stage;      // staging for face fields crossing the ABI
     // host copies kept for setup work (AMG aggregation, exports)
     std::vector<int> h_own, h_nbr, h_cf_ptr, h_cf_col, h_cf_face, h_bown, h_cb_ptr;

@@ -6,6 +6,7 @@
 #include "linalg.h"
 #include "mesh_io.h"
 #include "piso.h"
+#include "renumber.h"
 #include "results.h"
 #include "simple.h"
 
@@ -247,6 +248,53 @@ void solveEquation(bsg_equation* e, const bsg::SolverConfig& cfg, bsg_solve_resu
     toResult(o, results);
 }
 
+// The locality renumbering of a polyhedral description's cells (renumber.cpp): owner and
+// neighbour in the internal numbering when it applies.
+struct CellOrder {
+    bool applied = false;
+    std::vector<int> order, owner, neighbour;  // order[internal] = caller cell
+};
+
+CellOrder cellOrder(int n_vertices, int n_faces, const int* offsets, const int* ids, const int* owner,
+                    const int* neighbour, const int* patch, int n_patches) {
+    CellOrder r;
+    const int N = bsg::validatePolyhedralTopology(n_vertices, n_faces, offsets, ids, owner, neighbour, patch, n_patches);
+    r.order = bsg::localityOrder(N, n_faces, owner, neighbour, &r.applied);
+    if (!r.applied) return r;
+    std::vector<int> pos(N);
+    for (int i = 0; i < N; ++i) pos[r.order[i]] = i;
+    r.owner.resize(n_faces);
+    r.neighbour.resize(n_faces);
+    for (int f = 0; f < n_faces; ++f) {
+        r.owner[f] = pos[owner[f]];
+        r.neighbour[f] = neighbour[f] < 0 ? -1 : pos[neighbour[f]];
+    }
+    return r;
+}
+
+// A mesh built on renumbered cells: the caller-to-internal map for cell arrays crossing the
+// ABI, and the exported topology and cell geometry back in the caller's numbering.
+void applyCellOrder(bsg::DeviceMesh& m, const CellOrder& r) {
+    if (!r.applied) return;
+    const int N = m.n_cells;
+    m.h_cell_perm.assign(N, 0);
+    for (int i = 0; i < N; ++i) m.h_cell_perm[r.order[i]] = i;
+    m.cell_perm.upload(m.h_cell_perm, m.ctx->stream);
+    for (int& o : m.ext_owner) o = r.order[o];
+    for (int& n : m.ext_nbr)
+        if (n >= 0) n = r.order[n];
+    if (!m.ext_V.empty()) {
+        std::vector<double> V(N), xc(3LL * N);
+        for (int i = 0; i < N; ++i) {
+            V[r.order[i]] = m.ext_V[i];
+            for (int c = 0; c < 3; ++c) xc[3LL * r.order[i] + c] = m.ext_xc[3LL * i + c];
+        }
+        m.ext_V = std::move(V);
+        m.ext_xc = std::move(xc);
+    }
+    m.ctx->sync();
+}
+
 std::unique_ptr<bsg_system> makeSystem(bsg_mesh* mesh, int components) {
     require(components == 1 || components == 3, "components must be 1 or 3");
     bsg::DeviceMesh& m = *mesh->mesh;
@@ -294,15 +342,18 @@ void systemSolve(bsg_system* s, const bsg::SolverConfig& cfg, const double* diag
             s->slots[m.h_slot_own[i]] = upper[f];
             s->slots[m.h_slot_nbr[i]] = lower[f];
         }
-        s->eq->diag.upload(diagonal, N, ctx.stream);
+        s->eq->diag.resize(N);
+        bsg::uploadCells(m, s->eq->diag.data(), diagonal, 1);
         s->eq->val.upload(s->slots, ctx.stream);
         s->ready = true;
         ++k.matrix_value_updates;
     } else {
         ++k.rhs_only_solves;
     }
-    s->eq->src.upload(source, static_cast<std::size_t>(N) * C, ctx.stream);
-    s->unknown->v.upload(x, static_cast<std::size_t>(N) * C, ctx.stream);
+    s->eq->src.resize(static_cast<std::size_t>(N) * C);
+    bsg::uploadCells(m, s->eq->src.data(), source, C);
+    s->unknown->v.resize(static_cast<std::size_t>(N) * C);
+    bsg::uploadCells(m, s->unknown->v.data(), x, C);
     k.matrix_update_seconds += secondsSince(t0);
     const auto t1 = std::chrono::steady_clock::now();
     bsg::Dcsr<double> A{N, m.cf_ptr.data(), m.cf_col.data(), s->eq->diag.data(), s->eq->val.data(),
@@ -343,7 +394,7 @@ void systemSolve(bsg_system* s, const bsg::SolverConfig& cfg, const double* diag
             s->policy.rebuilt();
             ++k.preconditioner_retries;
             ++k.preconditioner_setups;
-            s->unknown->v.upload(x, N, ctx.stream);
+            bsg::uploadCells(m, s->unknown->v.data(), x, 1);
             k.preconditioner_seconds += secondsSince(tr);
             const bsg::SolveOutcome first = o[0];
             o[0] = s->krylov->solveScalar(A, cfg, pc, s->eq->src.data(), dx);
@@ -353,8 +404,7 @@ void systemSolve(bsg_system* s, const bsg::SolverConfig& cfg, const double* diag
         }
         if (use_amg) s->policy.afterSolve(o[0].status, attempt, o[0].iterations, cfg);
     }
-    s->unknown->v.download(x, ctx.stream);
-    ctx.sync();
+    bsg::downloadCells(m, s->unknown->v.data(), x, C);
     k.solve_seconds += secondsSince(t2);
     for (int c = 0; c < C; ++c) {
         toResult(o[c], results + c);
@@ -515,10 +565,13 @@ int bsg_mesh_create_polyhedral(bsg_context* ctx, int32_t n_vertices, const doubl
                                const int32_t* neighbour, const int32_t* patch, int32_t n_patches, bsg_mesh** out) {
     return guard(ctx, [&] {
         require(ctx && vertices && offsets && ids && owner && neighbour && patch && out, "null argument");
+        const CellOrder r = cellOrder(n_vertices, n_faces, offsets, ids, owner, neighbour, patch, n_patches);
         auto* m = new bsg_mesh{ctx, nullptr};
         try {
-            m->mesh = bsg::buildDeviceMeshPolyhedral(*ctx->ctx, n_vertices, vertices, n_faces, offsets, ids, owner,
-                                                     neighbour, patch, n_patches);
+            m->mesh = bsg::buildDeviceMeshPolyhedral(*ctx->ctx, n_vertices, vertices, n_faces, offsets, ids,
+                                                     r.applied ? r.owner.data() : owner,
+                                                     r.applied ? r.neighbour.data() : neighbour, patch, n_patches);
+            applyCellOrder(*m->mesh, r);
         } catch (...) {
             delete m;
             throw;
@@ -533,11 +586,14 @@ int bsg_mesh_create_polyhedral_host(bsg_context* ctx, int32_t n_vertices, const 
                                     bsg_mesh** out) {
     return guard(ctx, [&] {
         require(ctx && vertices && offsets && ids && owner && neighbour && patch && out, "null argument");
-        const bsg::HostGeometry h = bsg::computePolyhedralGeometry(n_vertices, vertices, n_faces, offsets, ids, owner,
-                                                                    neighbour, patch, n_patches);
+        const CellOrder r = cellOrder(n_vertices, n_faces, offsets, ids, owner, neighbour, patch, n_patches);
+        const bsg::HostGeometry h = bsg::computePolyhedralGeometry(
+            n_vertices, vertices, n_faces, offsets, ids, r.applied ? r.owner.data() : owner,
+            r.applied ? r.neighbour.data() : neighbour, patch, n_patches);
         auto* m = new bsg_mesh{ctx, nullptr};
         try {
             m->mesh = bsg::buildDeviceMesh(*ctx->ctx, h);
+            applyCellOrder(*m->mesh, r);
         } catch (...) {
             delete m;
             throw;
@@ -553,11 +609,15 @@ int bsg_mesh_create_from_file(bsg_context* ctx, const char* path, bsg_mesh** out
         auto m = std::make_unique<bsg_mesh>();
         m->owner = ctx;
         try {
-            m->mesh = bsg::buildDeviceMeshPolyhedral(*ctx->ctx, static_cast<int>(f.vertices.size() / 3),
-                                                     f.vertices.data(), static_cast<int>(f.owner.size()),
-                                                     f.offsets.data(), f.ids.data(), f.owner.data(),
-                                                     f.neighbour.data(), f.patch.data(),
-                                                     static_cast<int>(f.patch_names.size()));
+            const int nv = static_cast<int>(f.vertices.size() / 3), nf = static_cast<int>(f.owner.size());
+            const int np = static_cast<int>(f.patch_names.size());
+            const CellOrder r = cellOrder(nv, nf, f.offsets.data(), f.ids.data(), f.owner.data(), f.neighbour.data(),
+                                          f.patch.data(), np);
+            m->mesh = bsg::buildDeviceMeshPolyhedral(*ctx->ctx, nv, f.vertices.data(), nf, f.offsets.data(),
+                                                     f.ids.data(), r.applied ? r.owner.data() : f.owner.data(),
+                                                     r.applied ? r.neighbour.data() : f.neighbour.data(),
+                                                     f.patch.data(), np);
+            applyCellOrder(*m->mesh, r);
         } catch (const bsg::Error& e) {
             if (e.code != bsg::kArgument) throw;
             bsg::fail(bsg::kArgument, std::string("invalid BabelSim mesh file ") + path + ": " + e.what());
@@ -582,6 +642,19 @@ int bsg_mesh_file_info(const char* path, int64_t out[4], char* patches, int32_t 
             require(static_cast<int32_t>(text.size()) < capacity, "patch list buffer too small");
             std::memcpy(patches, text.c_str(), text.size() + 1);
         }
+    });
+}
+
+int bsg_mesh_locality_order(int32_t n_cells, int32_t n_faces, const int32_t* owner, const int32_t* neighbour,
+                            int32_t* order, int32_t* applied) {
+    return guard(nullptr, [&] {
+        require(owner && neighbour && order && applied && n_cells > 0 && n_faces > 0, "bad argument");
+        for (int f = 0; f < n_faces; ++f)
+            require(owner[f] >= 0 && owner[f] < n_cells && neighbour[f] < n_cells, "owner or neighbour out of range");
+        bool a = false;
+        const std::vector<int> o = bsg::localityOrder(n_cells, n_faces, owner, neighbour, &a);
+        std::memcpy(order, o.data(), sizeof(int) * o.size());
+        *applied = a ? 1 : 0;
     });
 }
 
@@ -931,11 +1004,11 @@ int bsg_equ_download(const bsg_equation* e, double* diagonal, double* upper, dou
     return guard(e ? ctxOf(e->unknown) : nullptr, [&] {
         require(e != nullptr, "null equation");
         const bsg::DeviceEquation& eq = *e->eq;
-        const bsg::DeviceMesh& m = *eq.x->mesh;
+        bsg::DeviceMesh& m = *eq.x->mesh;
         bsg::Context& ctx = *m.ctx;
         std::vector<double> val(eq.val.size());
-        if (diagonal) eq.diag.download(diagonal, ctx.stream);
-        if (source) eq.src.download(source, ctx.stream);
+        if (diagonal) bsg::downloadCells(m, eq.diag.data(), diagonal, 1);
+        if (source) bsg::downloadCells(m, eq.src.data(), source, eq.x->comps);
         eq.val.download(val.data(), ctx.stream);
         ctx.sync();
         for (int f = 0; f < m.n_faces; ++f) {

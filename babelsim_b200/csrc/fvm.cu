@@ -800,12 +800,42 @@ BcView DeviceField::bcView() {
     return BcView{d_bcs.data(), calculated ? trace.data() : nullptr, has_flux ? bflux.data() : nullptr};
 }
 
+void uploadCells(DeviceMesh& m, double* device, const double* host, int C) {
+    Context& ctx = *m.ctx;
+    const std::size_t n = static_cast<std::size_t>(m.n_cells) * C;
+    if (m.cell_perm.size() == 0) {
+        if (n) BSG_CUDA(cudaMemcpyAsync(device, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+        ctx.sync();
+        return;
+    }
+    if (m.cell_stage.size() < n) m.cell_stage.resize(n);
+    if (n) BSG_CUDA(cudaMemcpyAsync(m.cell_stage.data(), host, n * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+    launch(ctx, kPermuteFaces, m.n_cells, m.n_cells, C, (const int*)m.cell_perm.data(),
+           (const double*)m.cell_stage.data(), device, 1);
+    ctx.sync();
+}
+
+void downloadCells(DeviceMesh& m, const double* device, double* host, int C) {
+    Context& ctx = *m.ctx;
+    const std::size_t n = static_cast<std::size_t>(m.n_cells) * C;
+    if (m.cell_perm.size() == 0) {
+        if (n) BSG_CUDA(cudaMemcpyAsync(host, device, n * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        return;
+    }
+    if (m.cell_stage.size() < n) m.cell_stage.resize(n);
+    launch(ctx, kPermuteFaces, m.n_cells, m.n_cells, C, (const int*)m.cell_perm.data(), device,
+           m.cell_stage.data(), 0);
+    if (n) BSG_CUDA(cudaMemcpyAsync(host, m.cell_stage.data(), n * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+}
+
 void DeviceField::uploadExternal(const double* host) {
     const int C = comps;
     Context& ctx = *mesh->ctx;
     if (location == 0) {
-        v.upload(host, static_cast<std::size_t>(mesh->n_cells) * C, ctx.stream);
-        ctx.sync();
+        v.resize(static_cast<std::size_t>(mesh->n_cells) * C);
+        uploadCells(*mesh, v.data(), host, C);
         return;
     }
     // copy in caller order, then scatter to the internal face order on the device
@@ -821,8 +851,7 @@ void DeviceField::downloadExternal(double* host) const {
     const int C = comps;
     Context& ctx = *mesh->ctx;
     if (location == 0) {
-        v.download(host, ctx.stream);
-        ctx.sync();
+        downloadCells(*mesh, v.data(), host, C);
         return;
     }
     const std::size_t n = static_cast<std::size_t>(mesh->n_faces) * C;

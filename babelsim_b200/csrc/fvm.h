@@ -77,6 +77,11 @@ struct Reducer {
     void ensure(int blocks, int nv);
 };
 
+// Cell arrays between the caller's numbering (host) and the device's (C values per cell):
+// a plain copy, or through the mesh's locality renumbering when it has one.
+void uploadCells(DeviceMesh& m, double* device, const double* host, int C);
+void downloadCells(DeviceMesh& m, const double* device, double* host, int C);
+
 // ---- explicit operators ---------------------------------------------------
 void gradient(DeviceField& x, int method, DeviceArray<double>& out);
 void interpolate(DeviceField& x, int interp, int grad, DeviceArray<double>& out_face,

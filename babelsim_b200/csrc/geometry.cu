@@ -684,6 +684,16 @@ void ensureExternalGeometry(DeviceMesh& m) {
             m.ext_k[3LL * f + c] = bk[3LL * i + c];
         }
     }
+    if (!m.h_cell_perm.empty()) {  // renumbered cells: back to the caller's numbering
+        std::vector<double> Vc(N), xcc(3LL * N);
+        for (int c = 0; c < N; ++c) {
+            const int i = m.h_cell_perm[c];
+            Vc[c] = V[i];
+            for (int q = 0; q < 3; ++q) xcc[3LL * c + q] = xc[3LL * i + q];
+        }
+        V.swap(Vc);
+        xc.swap(xcc);
+    }
     m.ext_V = std::move(V);
     m.ext_xc = std::move(xc);
 }

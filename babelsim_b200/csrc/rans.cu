@@ -418,7 +418,8 @@ void KOmegaModel::setWallDistance(const double* host) {
     if (cfg_.kind != 2) fail(kState, "a wall distance belongs to the Spalart-Allmaras model");
     for (int i = 0; i < m_.n_cells; ++i)
         if (!std::isfinite(host[i])) fail(kNumeric, "wall distance must be finite");
-    wallDist_.upload(host, m_.n_cells, ctx_.stream);
+    wallDist_.resize(m_.n_cells);
+    uploadCells(m_, wallDist_.data(), host, 1);
     wall_set_ = true;
 }
 

@@ -163,6 +163,11 @@ void SimpleSolver::setSegments(const std::vector<int>& off, const std::vector<do
     muEff_.v.upload(mu, ctx_.stream);
     if (!seg_pinned_) BSG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&seg_pinned_), sizeof(double) * 16 * 4096));
     // the second Green-Gauss pass follows each case's own orthogonality, not the batch mesh's
+    if (!m_.h_cell_perm.empty())
+        for (int k = 0; k < K; ++k)
+            for (int i = off[k]; i < off[k + 1]; ++i)
+                if (m_.h_cell_perm[i] < off[k] || m_.h_cell_perm[i] >= off[k + 1])
+                    fail(kArgument, "segments must keep their cell ranges: each case must be one connected mesh");
     m_.cell_orth.release();
     if (!m_.orthogonal) {
         DeviceArray<int> d_case, d_orth;
@@ -219,9 +224,8 @@ void SimpleSolver::start() {
 
 void SimpleSolver::loadState(const double* U, const double* p, const double* phi) {
     if (!started_) fail(kState, "load_state requires a started SIMPLE solver (set_fields first)");
-    const std::size_t N = m_.n_cells;
-    U_.v.upload(U, 3 * N, ctx_.stream);
-    p_.v.upload(p, N, ctx_.stream);
+    U_.uploadExternal(U);
+    p_.uploadExternal(p);
     // phi arrives in the caller's face numbering; the device keeps interior faces first.
     phi_.uploadExternal(phi);
 }

@@ -188,6 +188,16 @@ int bsg_mesh_create_from_file(bsg_context* ctx, const char* path, bsg_mesh** out
 /* Host only: reads and checks a mesh file.  out = {cells, faces, vertices, patches}; when `patches`
  * is given, one "<name> <kind>" line per patch in file order. */
 int bsg_mesh_file_info(const char* path, int64_t out[4], char* patches, int32_t capacity);
+/* Locality renumbering (no counterpart in the reference, which keeps the file's numbering).
+ * Every polyhedral mesh (bsg_mesh_create_polyhedral, _host, _from_file) is renumbered inside
+ * the library when its cells are poorly ordered: reverse Cuthill-McKee on the cell graph per
+ * connected component (components in the order of their lowest cell), applied when it cuts the
+ * mean |i - j| over interior faces more than twofold.  Every array crossing the ABI stays in the
+ * caller's numbering.  Host only: the order the library uses, order[internal] = caller cell,
+ * and whether it applies (a mesh built from given geometry, bsg_mesh_create, is never
+ * renumbered). */
+int bsg_mesh_locality_order(int32_t n_cells, int32_t n_faces, const int32_t* owner, const int32_t* neighbour,
+                            int32_t* order, int32_t* applied);
 int bsg_mesh_destroy(bsg_mesh* mesh);
 /* Host-only check of a polyhedral description: computes the geometry exactly as
  * bsg_mesh_create_polyhedral does (no device needed) and reports the first

@@ -112,3 +112,36 @@ def test_native_mesh_reader_rejects_bad_files_with_the_references_messages(tmp_p
     with pytest.raises(BsgError) as err:
         file_info(path)
     assert f"invalid BabelSim mesh file {path}: {message}" in str(err.value)
+
+
+def shuffled(pm, seed=5):
+    """The same mesh with its cells numbered at random (owner / neighbour remapped)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(pm.n_cells)          # caller cell c -> shuffled number perm[c]
+    nb = np.asarray(pm.neighbour)
+    own = perm[np.asarray(pm.owner)].astype(np.int32)
+    nbr = np.where(nb >= 0, perm[np.maximum(nb, 0)], -1).astype(np.int32)
+    off, ids = pm.flat()
+    return meshgen.PolyMesh(pm.vertices, None, own, nbr, pm.patch, pm.patch_names, pm.patch_kinds,
+                            offsets=off, ids=ids), perm
+
+
+def test_locality_order_keeps_lattice_meshes_and_reorders_shuffled_ones():
+    from babelsim_b200.api import locality_order
+    pm = meshgen.voronoi_cube(8, 0.3, 20261007)
+    order, applied = locality_order(pm)
+    assert not applied and np.array_equal(order, np.arange(pm.n_cells))
+    sh, _ = shuffled(pm)
+    order, applied = locality_order(sh)
+    assert applied and np.array_equal(np.sort(order), np.arange(pm.n_cells))
+    pos = np.empty_like(order)
+    pos[order] = np.arange(len(order))
+    inn = sh.neighbour >= 0
+    span = np.abs(pos[sh.owner[inn]] - pos[sh.neighbour[inn]]).mean()
+    raw = np.abs(sh.owner[inn] - sh.neighbour[inn]).mean()
+    assert span * 3 < raw
+    # independent cases concatenated keep their cell ranges
+    cat, cells, _ = meshgen.concatenate([sh, meshgen.cavity_2d(5)])
+    order, applied = locality_order(cat)
+    assert applied
+    assert set(order[:cells[1]]) == set(range(cells[1]))
