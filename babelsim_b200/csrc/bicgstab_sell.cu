@@ -268,8 +268,8 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
 }
 
 template <int C>
-__global__ void __launch_bounds__(BB, 3) kBicgSell(BicgArgs<C> a) {
-    GridGroup g;
+__global__ void __launch_bounds__(BB, 3) kBicgSell(BicgArgs<C> a, SegmentBarrier* bar) {
+    GridGroup g{bar};
     bicgBody<C>(g, a);
 }
 
@@ -305,7 +305,9 @@ int bicgstabGrid(Context& ctx) {
 template <int C>
 void launchBicgstab(Context& ctx, const BicgArgs<C>& in) {
     BicgArgs<C> args = in;
-    void* params[] = {&args};
+    SegmentBarrier* bar = ctx.grid_barrier;
+    BSG_CUDA(cudaMemsetAsync(bar, 0, sizeof(SegmentBarrier), ctx.stream));
+    void* params[] = {&args, &bar};
     BSG_PROFILE(ctx, "bicgstab3_persistent");
     BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kBicgSell<C>), bicgstabGrid(ctx), BB, params, 0,
                                          ctx.stream));

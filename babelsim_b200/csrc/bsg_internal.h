@@ -95,6 +95,16 @@ private:
 
 // One device, one stream, a launch counter, pinned scratch for scalars read
 // back by the host, and optional per-kernel CUDA-event timing.
+// Barrier word of one group of CTAs in a persistent solver launch (zeroed before
+// the launch): the arrival count, whose top bit flips once per phase, and the
+// flag a wait that ran past its bound sets.
+struct SegmentBarrier {
+    unsigned count;
+    unsigned generation;  // unused; keeps the struct 16 bytes
+    int abort;
+    int pad;
+};
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -102,6 +112,7 @@ struct Context {
     long long launches = 0;
     std::string last_error;
     double* pinned = nullptr;            // 64 doubles of pinned host memory
+    SegmentBarrier* grid_barrier = nullptr;  // device: the barrier of whole-grid persistent launches
     // Per-kernel timing: while `profiling`, every instrumented launch is
     // bracketed by two events on `stream`; profileReport() resolves them.
     bool profiling = false;

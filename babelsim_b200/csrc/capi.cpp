@@ -78,6 +78,7 @@ Context::Context(int dev) : device(dev) {
     sm_count = prop.multiProcessorCount;
     checkCuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&pinned), 64 * sizeof(double)), "cudaMallocHost");
+    checkCuda(cudaMalloc(reinterpret_cast<void**>(&grid_barrier), sizeof(SegmentBarrier)), "cudaMalloc");
 }
 
 Context::~Context() {
@@ -88,6 +89,7 @@ Context::~Context() {
     if (phase_entries) cudaFree(phase_entries);
     if (phase_count) cudaFree(phase_count);
     if (pinned) cudaFreeHost(pinned);
+    if (grid_barrier) cudaFree(grid_barrier);
     if (stream) cudaStreamDestroy(stream);
 }
 

@@ -4,43 +4,60 @@
 // phases by barriers instead of kernel launches.  GridGroup is the whole
 // cooperative grid; SegmentGroup is a contiguous range of its CTAs that owns one
 // system of a batch, so one launch can solve several independent systems side by
-// side.  gridSum is the deterministic reduction both use.
+// side.  Both synchronise through groupBarrier, whose every wait is bounded, and
+// gridSum is the deterministic reduction both use.
 #pragma once
-
-#include <cooperative_groups.h>
 
 #include "bsg_internal.h"
 
 namespace bsg {
 
-// Barrier state of one system of a batch (zeroed before every launch).
-struct SegmentBarrier {
-    unsigned count;
-    unsigned generation;
-    int abort;   // set when a wait ran past its bound; the system then reports status 3
-    int pad;
-};
-
 #ifdef __CUDACC__
-namespace cgx = cooperative_groups;
+constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s at the B200's clock
 
-// The CTAs that cooperate on one solve.  GridGroup: the whole cooperative grid,
-// synchronised by cooperative groups.  SegmentGroup: a contiguous range of the
-// grid's CTAs that owns one system of a batch; its barrier is a counter and a
-// generation word in global memory (all CTAs of a cooperative launch are
-// resident, so the spin always ends), and every wait is bounded: past
-// kBarrierCycles the group records an abort and its barriers stop waiting, so
-// the launch ends and the host reports the failure instead of hanging.
+// Barrier of n CTAs on one word.  Every CTA adds to `count` once per phase: the
+// leader adds 2^31 - (n - 1), the others 1, so the n arrivals add exactly 2^31 and
+// the top bit flips when the last one lands, while the low 31 bits come back to
+// where they were (zero: the word is zeroed before each launch).  A CTA leaves
+// when the top bit differs from the value its own add returned.  All CTAs of a
+// cooperative launch are resident, so the flip always comes unless a CTA skipped
+// the barrier; the wait is bounded all the same: past kBarrierCycles the CTA
+// records an abort and returns, and later barriers of the group stop waiting, so
+// the launch ends and the host reports status 3 instead of hanging the GPU.
+__device__ __forceinline__ void groupBarrier(SegmentBarrier* bar, bool leader, int n) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned add = leader ? 0x80000000u - static_cast<unsigned>(n - 1) : 1u;
+        __threadfence();  // this CTA's writes before its arrival
+        const unsigned old = atomicAdd(&bar->count, add);
+        volatile unsigned* word = &bar->count;
+        volatile int* abort = &bar->abort;
+        long long t0 = 0;
+        for (unsigned spins = 1; ((*word ^ old) & 0x80000000u) == 0u; ++spins) {
+            if ((spins & 255u) != 0u) continue;
+            if (*abort) break;
+            const long long now = clock64();
+            if (spins == 256u) t0 = now;
+            else if (now - t0 > kBarrierCycles) {
+                atomicExch(&bar->abort, 1);
+                break;
+            }
+        }
+        __threadfence();  // the other CTAs' writes before this CTA reads them
+    }
+    __syncthreads();
+}
+
+// The CTAs that cooperate on one solve.  GridGroup: the whole cooperative grid.
+// SegmentGroup: a contiguous range of the grid's CTAs that owns one system of a
+// batch.  Each has its own zeroed SegmentBarrier.
 struct GridGroup {
-    cgx::grid_group g;
-    __device__ GridGroup() : g(cgx::this_grid()) {}
+    SegmentBarrier* bar;
     __device__ __forceinline__ int rank() const { return blockIdx.x; }
     __device__ __forceinline__ int size() const { return gridDim.x; }
-    __device__ __forceinline__ void sync() { g.sync(); }
-    __device__ __forceinline__ bool aborted() const { return false; }
+    __device__ __forceinline__ bool aborted() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
+    __device__ __forceinline__ void sync() { groupBarrier(bar, blockIdx.x == 0, gridDim.x); }
 };
-
-constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s at the B200's clock
 
 struct SegmentGroup {
     int cta0, ncta;
@@ -48,31 +65,7 @@ struct SegmentGroup {
     __device__ __forceinline__ int rank() const { return blockIdx.x - cta0; }
     __device__ __forceinline__ int size() const { return ncta; }
     __device__ __forceinline__ bool aborted() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
-    __device__ void sync() {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            volatile unsigned* gen = &bar->generation;
-            const unsigned g0 = *gen;
-            __threadfence();
-            if (atomicAdd(&bar->count, 1u) == static_cast<unsigned>(ncta) - 1u) {
-                atomicExch(&bar->count, 0u);
-                __threadfence();
-                atomicAdd(&bar->generation, 1u);
-            } else {
-                const long long t0 = clock64();
-                while (*gen == g0) {
-                    if (aborted()) break;
-                    if (clock64() - t0 > kBarrierCycles) {
-                        atomicExch(&bar->abort, 1);
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
-            __threadfence();
-        }
-        __syncthreads();
-    }
+    __device__ __forceinline__ void sync() { groupBarrier(bar, rank() == 0, ncta); }
 };
 
 struct Lanes {

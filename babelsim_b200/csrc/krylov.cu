@@ -704,6 +704,7 @@ SolveOutcome KrylovSolver::solveRefined(const Dcsr<double>& A, const SolverConfi
         ++out.checks;
         PcgState r;
         std::memcpy(&r, ctx.pinned, sizeof(r));
+        if (r.status == 3) fail(kCuda, "persistent PCG: a barrier wait ran past its bound");
         used += r.iterations;
         if (ctx.profiling || trace_solves()) {
             const double N = n;
@@ -763,6 +764,7 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
         ctx.sync();
         PcgState r;
         std::memcpy(&r, ctx.pinned, sizeof(r));
+        if (r.status == 3) fail(kCuda, "persistent PCG: a barrier wait ran past its bound");
         if (ctx.profiling || trace_solves()) {
             // algorithmic bytes of this launch: initial residual, preconditioner
             // applications and per-iteration SpMV + vector updates

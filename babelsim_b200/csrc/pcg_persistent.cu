@@ -1,6 +1,5 @@
 // Persistent cooperative PCG + AMG V-cycle (see pcg_persistent.cuh).
-#include <cooperative_groups.h>
-
+#include "group.cuh"
 #include "linalg.h"
 #include "pcg_persistent.cuh"
 
@@ -8,8 +7,6 @@
 #include <cmath>
 #include <cstring>
 #include <string>
-
-namespace cg = cooperative_groups;
 
 namespace bsg {
 namespace {
@@ -43,7 +40,7 @@ __device__ __forceinline__ double groupSum(double v, unsigned mask) {
 // `buf` alternates between two halves of `partial` so a fast block's next write
 // never overtakes a slow block's read.
 template <int NV>
-__device__ void gridReduce(cg::grid_group& g, double v[NV], double* partial, int& buf) {
+__device__ void gridReduce(GridGroup& g, double v[NV], double* partial, int& buf) {
     __shared__ double sh[NVMAX][PB / 32];
     __shared__ double tot[NVMAX];
     double* part = partial + static_cast<long long>(buf) * gridDim.x * NVMAX;
@@ -114,7 +111,7 @@ __device__ __forceinline__ double rowApply(const int* __restrict__ ptr, const in
 }
 
 // One V-cycle: z = M r.  Returns this thread's partial of r.z (lane 0 of each row group).
-__device__ double vcycle(cg::grid_group& g, const AmgView<double>& a, const double* __restrict__ r,
+__device__ double vcycle(GridGroup& g, const AmgView<double>& a, const double* __restrict__ r,
                          double* __restrict__ z, const PhaseLog& log) {
     const Cursor c = cursor();
     const int L = a.levels;
@@ -233,7 +230,7 @@ struct PcgArgs {
 };
 
 // z = M r and the partial of r.z
-__device__ double precondition(cg::grid_group& g, const PcgArgs& a) {
+__device__ double precondition(GridGroup& g, const PcgArgs& a) {
     if (a.amg.levels > 0) return vcycle(g, a.amg, a.r, a.z, a.log);
     const Cursor c = cursor();
     double rz = 0.0;
@@ -245,8 +242,8 @@ __device__ double precondition(cg::grid_group& g, const PcgArgs& a) {
     return rz;
 }
 
-__global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
-    cg::grid_group g = cg::this_grid();
+__global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a, SegmentBarrier* bar) {
+    GridGroup g{bar};
     const Cursor c = cursor();
     const int n = a.A.n;
     int buf = 0;
@@ -304,6 +301,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
     int status = 1;
     double rr = v[0];
     while (it < max_iterations) {
+        if (g.aborted()) { status = 3; break; }
         if (!isfinite(rz) || rz == 0.0) { status = 2; break; }
         // p_new = z + beta p_old and q = A p_new in one pass (neighbours' p_new formed on the fly)
         double pq[1] = {0.0};
@@ -349,7 +347,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st.rr = rr;
         st.iterations = it;
-        st.status = status;
+        st.status = g.aborted() ? 3 : status;
     }
 }
 
@@ -393,11 +391,13 @@ constexpr int kStaticMaxRows = 131072;
 constexpr int kStaticMaxBlocks = 4096;
 static __device__ __align__(256) double g_static_scratch[5 * kStaticMaxRows + 2 * NVMAX * kStaticMaxBlocks];
 static __device__ __align__(256) PcgState g_static_state;
+static __device__ __align__(16) SegmentBarrier g_static_barrier;
 
 namespace {
 struct StaticScratch {
     double* base = nullptr;
     PcgState* state = nullptr;
+    SegmentBarrier* barrier = nullptr;
 };
 
 // Device addresses of the static scratch on the current device.
@@ -407,8 +407,11 @@ StaticScratch staticScratch() {
     checkCuda(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(scratch)");
     void* q = nullptr;
     checkCuda(cudaGetSymbolAddress(&q, g_static_state), "cudaGetSymbolAddress(state)");
+    void* w = nullptr;
+    checkCuda(cudaGetSymbolAddress(&w, g_static_barrier), "cudaGetSymbolAddress(barrier)");
     s.base = static_cast<double*>(p);
     s.state = static_cast<PcgState*>(q);
+    s.barrier = static_cast<SegmentBarrier*>(w);
     return s;
 }
 }  // namespace
@@ -446,12 +449,15 @@ SolveOutcome staticJacobiPcg(int n, const int* row_ptr, const int* cols, const d
     int used = 0;
     auto run = [&](PcgState in) {
         checkCuda(cudaMemcpy(s.state, &in, sizeof(in), cudaMemcpyHostToDevice), "cudaMemcpy(state)");
+        checkCuda(cudaMemset(s.barrier, 0, sizeof(SegmentBarrier)), "cudaMemset(barrier)");
         PcgArgs args{A, AmgView<double>{}, diag, b, x, r, z, p0, p1, q, partial, s.state, PhaseLog{}};
-        void* params[] = {&args};
+        SegmentBarrier* bar = s.barrier;
+        void* params[] = {&args, &bar};
         checkCuda(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgPersistent), grid, PB, params, 0, 0),
                   "cudaLaunchCooperativeKernel");
         PcgState res;
         checkCuda(cudaMemcpy(&res, s.state, sizeof(res), cudaMemcpyDeviceToHost), "cudaMemcpy(result)");
+        if (res.status == 3) fail(kCuda, "persistent PCG: a barrier wait ran past its bound");
         return res;
     };
     for (int attempt = 0; attempt < 3; ++attempt) {
@@ -492,7 +498,9 @@ void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<doub
                          double* partial, PcgState* st) {
     const PhaseLog log{ctx.phase_entries, ctx.phase_capacity, ctx.phase_count};
     PcgArgs args{A, amg, jac, b, x, r, z, p0, p1, q, partial, st, log};
-    void* params[] = {&args};
+    SegmentBarrier* bar = ctx.grid_barrier;
+    BSG_CUDA(cudaMemsetAsync(bar, 0, sizeof(SegmentBarrier), ctx.stream));
+    void* params[] = {&args, &bar};
     const int grid = persistentGrid(ctx);
     BSG_PROFILE(ctx, "pcg_amg_persistent");
     BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgPersistent), grid, PB, params, 0, ctx.stream));

@@ -374,8 +374,8 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
 }
 
 template <class TK, class TV>
-__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<TK, TV> a) {
-    GridGroup g;
+__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<TK, TV> a, SegmentBarrier* bar) {
+    GridGroup g{bar};
     pcgBody<TK, TV>(g, a);
 }
 
@@ -412,7 +412,9 @@ template <class TK, class TV>
 void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& in) {
     SellPcgArgs<TK, TV> args = in;
     args.log = PhaseLog{ctx.phase_entries, ctx.phase_capacity, ctx.phase_count};
-    void* params[] = {&args};
+    SegmentBarrier* bar = ctx.grid_barrier;
+    BSG_CUDA(cudaMemsetAsync(bar, 0, sizeof(SegmentBarrier), ctx.stream));
+    void* params[] = {&args, &bar};
     const int grid = sellGrid<TK, TV>(ctx);
     BSG_PROFILE(ctx, "pcg_amg_persistent");
     BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgSell<TK, TV>), grid, SB, params, 0, ctx.stream));

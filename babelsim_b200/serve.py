@@ -115,6 +115,13 @@ class Server:
     solver_precision: int = 0
     batched: bool = True
     log: list = field(default_factory=list)
+    trace: bool = False         # also print every log entry to stderr as it happens
+
+    def _note(self, entry):
+        self.log.append(entry)
+        if self.trace:
+            import sys
+            print("serve:", *entry, file=sys.stderr, flush=True)
 
     def _simple(self, mesh, nu, tolerance):
         import babelsim_b200 as bsg
@@ -179,14 +186,14 @@ class Server:
                 if need > self.hbm_budget:
                     heapq.heappop(queue)
                     results.append(Result(req.id, req.mesh.n_cells, req.arrival, now, now, 0, False))
-                    self.log.append(("rejected", req.id, need))
+                    self._note(("rejected", req.id, need))
                     continue
                 if used + need > self.hbm_budget or (members and req.tolerance != members[0][0].tolerance):
                     break
                 heapq.heappop(queue)
                 used += need
                 members.append((req, clock() - t0, need))
-                self.log.append(("admitted", req.id, need))
+                self._note(("admitted", req.id, need))
             if members:
                 cohorts.append(self._start_cohort(members))
                 busy += len(members)
@@ -216,7 +223,7 @@ class Server:
                         busy -= 1
                         results.append(Result(req.id, req.mesh.n_cells, req.arrival, admitted, clock() - t0,
                                               rep.iterations, bool(rep.converged), U, p))
-                        self.log.append(("retired", req.id, rep.iterations))
+                        self._note(("retired", req.id, rep.iterations))
                 if all(c.done):
                     c.sim.close()
                     c.mesh.close()
@@ -244,7 +251,7 @@ class Server:
                 if need > self.hbm_budget:
                     heapq.heappop(queue)
                     results.append(Result(req.id, req.mesh.n_cells, req.arrival, now, now, 0, False))
-                    self.log.append(("rejected", req.id, need))
+                    self._note(("rejected", req.id, need))
                     continue
                 if used + need > self.hbm_budget:
                     break
@@ -252,7 +259,7 @@ class Server:
                 m, sim = self._start(req)
                 used += need
                 active.append(_Active(req, m, sim, clock() - t0, need))
-                self.log.append(("admitted", req.id, need))
+                self._note(("admitted", req.id, need))
             if not active:
                 if i < len(pending):  # idle until the next arrival
                     wait = pending[i].arrival - (clock() - t0)
@@ -276,7 +283,7 @@ class Server:
                 active.remove(a)
                 results.append(Result(a.req.id, a.req.mesh.n_cells, a.req.arrival, a.admitted, clock() - t0,
                                       a.iterations, bool(rep.converged), U, p))
-                self.log.append(("retired", a.req.id, a.iterations))
+                self._note(("retired", a.req.id, a.iterations))
             turn += 1
         return sorted(results, key=lambda r: r.id)
 

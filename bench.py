@@ -331,7 +331,7 @@ def run_serving(args):
     mine = serve.shard(reqs, world, rank)
     ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
     srv = serve.Server(ctx, hbm_budget=150 * 2**30, slots=args.slots, solver_precision=args.precision,
-                       batched=not args.unbatched)
+                       batched=not args.unbatched, trace=args.trace)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -357,6 +357,8 @@ def run_serving(args):
                                 batched=not args.unbatched)
             rr = solo.run([serve.Request(r.id, 0.0, r.mesh, r.speed, r.nu, r.max_iterations, r.tolerance)])[0]
             alone.append(rr.latency)
+            if args.trace:
+                print(f"serve: alone {r.id} {rr.iterations} {rr.latency:.3f}", file=sys.stderr, flush=True)
         ratio = np.array([res[i].latency / alone[i] for i in range(len(reqs))])
     line = {"metric": "served solves/s (steady SIMPLE cavity requests)", "value": out["solves_per_s"],
             "unit": "solves/s", "n_gpus": world, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
@@ -656,6 +658,7 @@ def main():
     ap.add_argument("--tolerance", type=float, default=1e-4, help="serving: outer-loop tolerance")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 2], help="serving: pressure V-cycle precision")
     ap.add_argument("--unbatched", action="store_true", help="serving: one solve per request, no cohorts")
+    ap.add_argument("--trace", action="store_true", help="serving: print admissions and retirements to stderr")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
