@@ -263,7 +263,7 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
             st.iters[c] = iters[c];
             st.fin2[c] = fr[c];
         }
-        st.status = g.aborted() ? 3 : 0;
+        st.status = g.failed() ? 3 : 0;
     }
 }
 
@@ -306,11 +306,11 @@ template <int C>
 void launchBicgstab(Context& ctx, const BicgArgs<C>& in) {
     BicgArgs<C> args = in;
     SegmentBarrier* bar = ctx.grid_barrier;
-    BSG_CUDA(cudaMemsetAsync(bar, 0, sizeof(SegmentBarrier), ctx.stream));
+    const int grid = bicgstabGrid(ctx);
+    resetBarriers(ctx, bar, 1, grid);
     void* params[] = {&args, &bar};
     BSG_PROFILE(ctx, "bicgstab3_persistent");
-    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kBicgSell<C>), bicgstabGrid(ctx), BB, params, 0,
-                                         ctx.stream));
+    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kBicgSell<C>), grid, BB, params, 0, ctx.stream));
     ctx.launched();
 }
 
@@ -327,7 +327,7 @@ void launchBicgstabBatch(Context& ctx, BicgBatch<C>& batch) {
     batch.d_args.upload(batch.args, ctx.stream);
     batch.d_cta.upload(batch.cta_begin, ctx.stream);
     batch.d_bars.resize(nsegs);
-    batch.d_bars.zero(ctx.stream);
+    resetBarriers(ctx, batch.d_bars.data(), nsegs, total, batch.cta_begin.data());
     const BicgArgs<C>* segs = batch.d_args.data();
     const int* cta = batch.d_cta.data();
     SegmentBarrier* bars = batch.d_bars.data();

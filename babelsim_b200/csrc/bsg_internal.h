@@ -95,15 +95,34 @@ private:
 
 // One device, one stream, a launch counter, pinned scratch for scalars read
 // back by the host, and optional per-kernel CUDA-event timing.
-// Barrier word of one group of CTAs in a persistent solver launch (zeroed before
-// the launch): the arrival count, whose top bit flips once per phase, and the
-// flag a wait that ran past its bound sets.
+// Barrier of one group of CTAs in a persistent solver launch (set by
+// resetBarriers before the launch): the arrival count, whose top bit flips once
+// per phase; the flag a wait that ran past its bound sets, with what that wait
+// saw; and where each CTA of the launch last arrived.
 struct SegmentBarrier {
     unsigned count;
-    unsigned generation;  // unused; keeps the struct 16 bytes
     int abort;
+    int who;              // 1 + grid rank of the first CTA whose wait ran out (0: none)
+    unsigned where;       // that CTA's barrier number (1 = its first barrier)
+    unsigned seen;        // the count word it last read
+    int cta0, ncta;       // the group's CTAs (grid ranks)
     int pad;
+    unsigned* progress;   // per CTA of the launch (grid rank): number of its latest barrier; may be null
 };
+
+constexpr int kMaxPersistentCtas = 8192;  // CTAs of one persistent launch, at most
+
+struct Context;
+// Sets `n` device barriers to their launch state (no arrivals, no abort, progress
+// recorded in ctx.progress, whose first `ctas` entries are zeroed), in stream order.
+// Barrier k covers CTAs [cta_begin[k], cta_begin[k+1]); without cta_begin, the one
+// barrier covers all `ctas`.
+void resetBarriers(Context& ctx, SegmentBarrier* dev, int n, int ctas, const int* cta_begin = nullptr);
+// After a launch reported status 3 (the stream synchronised): which CTAs of the
+// barrier's group stopped where, for the error message.
+std::string barrierReport(const SegmentBarrier* dev);
+// The same for the first of `n` barriers of a batched launch whose wait ran out.
+std::string barrierReport(const SegmentBarrier* dev, int n);
 
 struct Context {
     int device = 0;
@@ -113,6 +132,7 @@ struct Context {
     std::string last_error;
     double* pinned = nullptr;            // 64 doubles of pinned host memory
     SegmentBarrier* grid_barrier = nullptr;  // device: the barrier of whole-grid persistent launches
+    unsigned* progress = nullptr;            // device, kMaxPersistentCtas: barrier numbers per CTA
     // Per-kernel timing: while `profiling`, every instrumented launch is
     // bracketed by two events on `stream`; profileReport() resolves them.
     bool profiling = false;

@@ -79,6 +79,7 @@ Context::Context(int dev) : device(dev) {
     checkCuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&pinned), 64 * sizeof(double)), "cudaMallocHost");
     checkCuda(cudaMalloc(reinterpret_cast<void**>(&grid_barrier), sizeof(SegmentBarrier)), "cudaMalloc");
+    checkCuda(cudaMalloc(reinterpret_cast<void**>(&progress), sizeof(unsigned) * kMaxPersistentCtas), "cudaMalloc");
 }
 
 Context::~Context() {
@@ -90,7 +91,55 @@ Context::~Context() {
     if (phase_count) cudaFree(phase_count);
     if (pinned) cudaFreeHost(pinned);
     if (grid_barrier) cudaFree(grid_barrier);
+    if (progress) cudaFree(progress);
     if (stream) cudaStreamDestroy(stream);
+}
+
+void resetBarriers(Context& ctx, SegmentBarrier* dev, int n, int ctas, const int* cta_begin) {
+    if (ctas > kMaxPersistentCtas) fail(kArgument, "persistent launch larger than its progress record");
+    std::vector<SegmentBarrier> h(static_cast<std::size_t>(n));
+    for (int k = 0; k < n; ++k) {
+        const int c0 = cta_begin ? cta_begin[k] : 0, c1 = cta_begin ? cta_begin[k + 1] : ctas;
+        h[k] = SegmentBarrier{0u, 0, 0, 0u, 0u, c0, c1 - c0, 0, ctx.progress};
+    }
+    // pageable source: the call returns once the bytes are staged, so `h` may go
+    BSG_CUDA(cudaMemcpyAsync(dev, h.data(), sizeof(SegmentBarrier) * h.size(), cudaMemcpyHostToDevice, ctx.stream));
+    BSG_CUDA(cudaMemsetAsync(ctx.progress, 0, sizeof(unsigned) * ctas, ctx.stream));
+}
+
+std::string barrierReport(const SegmentBarrier* dev) {
+    SegmentBarrier b{};
+    if (cudaMemcpy(&b, dev, sizeof(b), cudaMemcpyDeviceToHost) != cudaSuccess) return "";
+    std::string out = " (group of CTAs " + std::to_string(b.cta0) + ".." + std::to_string(b.cta0 + b.ncta - 1);
+    if (b.who > 0)
+        out += "; CTA " + std::to_string(b.who - 1) + " gave up at its barrier " + std::to_string(b.where) + " with " +
+               std::to_string(b.seen & 0x7fffffffu) + " arrivals counted";
+    if (b.progress && b.ncta > 0) {
+        std::vector<unsigned> prog(static_cast<std::size_t>(b.ncta));
+        if (cudaMemcpy(prog.data(), b.progress + b.cta0, sizeof(unsigned) * prog.size(), cudaMemcpyDeviceToHost) ==
+            cudaSuccess) {
+            const unsigned lo = *std::min_element(prog.begin(), prog.end());
+            const unsigned hi = *std::max_element(prog.begin(), prog.end());
+            int behind = 0, first = -1;
+            for (int k = 0; k < b.ncta; ++k)
+                if (prog[k] == lo) {
+                    ++behind;
+                    if (first < 0) first = b.cta0 + k;
+                }
+            out += "; barriers reached " + std::to_string(lo) + ".." + std::to_string(hi) + ", " +
+                   std::to_string(behind) + " CTA(s) at " + std::to_string(lo) + " from CTA " + std::to_string(first);
+        }
+    }
+    return out + ")";
+}
+
+std::string barrierReport(const SegmentBarrier* dev, int n) {
+    std::vector<SegmentBarrier> h(static_cast<std::size_t>(std::max(n, 0)));
+    if (n <= 0 || cudaMemcpy(h.data(), dev, sizeof(SegmentBarrier) * h.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return "";
+    for (int k = 0; k < n; ++k)
+        if (h[k].abort || h[k].who) return " in system " + std::to_string(k) + " of the launch" + barrierReport(dev + k);
+    return "";
 }
 
 cudaEvent_t Context::takeEvent() {

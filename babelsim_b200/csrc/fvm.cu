@@ -605,14 +605,15 @@ __global__ void kReferenceCheck(int row0, int n, const int* __restrict__ ptr, co
     if ((threadIdx.x & 31) == 0 && !warp_ok) atomicAnd(all_constant, 0);
 }
 
-// reference(Equation, cell 0, value) (procedural_equation.cpp:306-315); cell `row0`, the
-// first cell of a segment, when the mesh holds several independent cases.
-__global__ void kApplyReference(int row0, const int* __restrict__ flag, double value, double* __restrict__ diag,
+// reference(Equation, cell 0, value) (procedural_equation.cpp:306-315) on row `ref`: the
+// caller's cell 0 (or first cell of a segment, when the mesh holds several independent
+// cases) in the internal numbering.
+__global__ void kApplyReference(int ref, const int* __restrict__ flag, double value, double* __restrict__ diag,
                                 double* __restrict__ src, int* __restrict__ error) {
     if (*flag) {
-        if (!(diag[row0] > 0.0)) { *error = 1; return; }
-        src[row0] += diag[row0] * value;
-        diag[row0] *= 2.0;
+        if (!(diag[ref] > 0.0)) { *error = 1; return; }
+        src[ref] += diag[ref] * value;
+        diag[ref] *= 2.0;
     }
 }
 
@@ -1174,7 +1175,11 @@ void referenceIfUnanchored(DeviceEquation& eq, double value, int* flag_dev, int 
     BSG_CUDA(cudaMemcpyAsync(flag_dev, init, sizeof(init), cudaMemcpyHostToDevice, ctx.stream));
     launch(ctx, kReferenceCheck, n, row0, n, (const int*)m.cf_ptr.data(), (const double*)eq.diag.data(),
            (const double*)eq.val.data(), flag_dev);
-    kApplyReference<<<1, 1, 0, ctx.stream>>>(row0, flag_dev, value, eq.diag.data(), eq.src.data(), flag_dev + 1);
+    // the anchored cell is the caller's first cell of the range, wherever renumbering put it
+    // (a renumbered segment keeps its cell range)
+    const int ref = m.h_cell_perm.empty() ? row0 : m.h_cell_perm[row0];
+    if (ref < row0 || ref >= row0 + n) fail(kState, "reference cell outside its cell range");
+    kApplyReference<<<1, 1, 0, ctx.stream>>>(ref, flag_dev, value, eq.diag.data(), eq.src.data(), flag_dev + 1);
     BSG_CUDA(cudaGetLastError());
     ctx.launched();
 }

@@ -18,54 +18,144 @@ constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s at the B200's c
 // Barrier of n CTAs on one word.  Every CTA adds to `count` once per phase: the
 // leader adds 2^31 - (n - 1), the others 1, so the n arrivals add exactly 2^31 and
 // the top bit flips when the last one lands, while the low 31 bits come back to
-// where they were (zero: the word is zeroed before each launch).  A CTA leaves
-// when the top bit differs from the value its own add returned.  All CTAs of a
-// cooperative launch are resident, so the flip always comes unless a CTA skipped
-// the barrier; the wait is bounded all the same: past kBarrierCycles the CTA
-// records an abort and returns, and later barriers of the group stop waiting, so
-// the launch ends and the host reports status 3 instead of hanging the GPU.
-__device__ __forceinline__ void groupBarrier(SegmentBarrier* bar, bool leader, int n) {
+// where they were (zero: the word is reset before each launch).  A CTA leaves
+// when the top bit differs from the value its own add returned.  The add is a
+// gpu-scope release (after __syncthreads, so it covers the whole CTA's writes)
+// and the poll a gpu-scope acquire, so no separate fences are needed.  All CTAs
+// of a cooperative launch are resident, so the flip always comes unless a CTA
+// skipped the barrier; the wait is bounded all the same: past kBarrierCycles the
+// CTA records an abort (and, first of all, where it was and what it saw) and
+// returns, and later barriers of the group stop waiting, so the launch ends and
+// the host reports status 3 instead of hanging the GPU.
+__device__ __forceinline__ unsigned arriveRelease(unsigned* word, unsigned add) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(word), "r"(add) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned loadRelaxed(const unsigned* word) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned loadAcquire(const unsigned* word) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+    return v;
+}
+
+// Thread 0's barrier bookkeeping lives in shared memory, out of the registers of
+// the kernels' hot loops: the number of this CTA's latest barrier and where the
+// launch records it.
+struct BarrierBook {
+    unsigned seq;
+    unsigned* progress;
+};
+__device__ __forceinline__ BarrierBook& barrierBook() {
+    __shared__ BarrierBook book;
+    return book;
+}
+__device__ __forceinline__ void openBarrierBook(const SegmentBarrier* bar) {
+    if (threadIdx.x == 0) barrierBook() = BarrierBook{0u, bar->progress};
+}
+
+#ifndef BSG_BARRIER_POLL
+#define BSG_BARRIER_POLL 1  // 0: acquire loads; 1: relaxed loads, one acquire fence after; 2: volatile + fence.sc
+#endif
+#ifndef BSG_BARRIER_PROGRESS
+#define BSG_BARRIER_PROGRESS 1
+#endif
+#if BSG_BARRIER_NOINLINE
+#define BSG_BARRIER_INLINE static __noinline__
+#else
+#define BSG_BARRIER_INLINE __forceinline__
+#endif
+
+// Returns 1 when thread 0 left the wait on the group's abort (its own timeout or
+// another CTA's), 0 when the phase completed: the same value for every thread of
+// the CTA, so a loop that stops on it stops in all of them.
+__device__ BSG_BARRIER_INLINE int groupBarrier(SegmentBarrier* bar, bool leader, int n) {
+    __shared__ int aborted;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned add = leader ? 0x80000000u - static_cast<unsigned>(n - 1) : 1u;
-        __threadfence();  // this CTA's writes before its arrival
+#if BSG_BARRIER_POLL == 2
+        __threadfence();
         const unsigned old = atomicAdd(&bar->count, add);
-        volatile unsigned* word = &bar->count;
-        volatile int* abort = &bar->abort;
+#else
+        const unsigned old = arriveRelease(&bar->count, add);
+#endif
+        BarrierBook& book = barrierBook();
+        const unsigned seq = ++book.seq;
+        // recorded after the arrival, so the release above never waits on this store
+        if (BSG_BARRIER_PROGRESS && book.progress) book.progress[blockIdx.x] = seq;
         long long t0 = 0;
-        for (unsigned spins = 1; ((*word ^ old) & 0x80000000u) == 0u; ++spins) {
+        int stop = 0;
+        for (unsigned spins = 1;; ++spins) {
+#if BSG_BARRIER_POLL == 0
+            const unsigned cur = loadAcquire(&bar->count);
+#elif BSG_BARRIER_POLL == 1
+            const unsigned cur = loadRelaxed(&bar->count);
+#else
+            const unsigned cur = *reinterpret_cast<volatile unsigned*>(&bar->count);
+#endif
+            if ((cur ^ old) & 0x80000000u) break;
             if ((spins & 255u) != 0u) continue;
-            if (*abort) break;
+            if (*reinterpret_cast<volatile int*>(&bar->abort)) {
+                stop = 1;
+                break;
+            }
             const long long now = clock64();
-            if (spins == 256u) t0 = now;
-            else if (now - t0 > kBarrierCycles) {
+            if (spins == 256u) {
+                t0 = now;
+            } else if (now - t0 > kBarrierCycles) {
+                if (atomicCAS(&bar->who, 0, static_cast<int>(blockIdx.x) + 1) == 0) {
+                    bar->where = seq;
+                    bar->seen = cur;
+                }
+                __threadfence();
                 atomicExch(&bar->abort, 1);
+                stop = 1;
                 break;
             }
         }
-        __threadfence();  // the other CTAs' writes before this CTA reads them
+#if BSG_BARRIER_POLL == 1
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");  // the acquire that pairs with the last arrival
+#elif BSG_BARRIER_POLL == 2
+        __threadfence();
+#endif
+        aborted = stop;
     }
     __syncthreads();
+    // the next write to `aborted` comes after the next barrier's first __syncthreads,
+    // which every thread reaches only after this read
+    return aborted;
 }
 
-// The CTAs that cooperate on one solve.  GridGroup: the whole cooperative grid.
-// SegmentGroup: a contiguous range of the grid's CTAs that owns one system of a
-// batch.  Each has its own zeroed SegmentBarrier.
+// aborted(): this CTA has left a wait on the group's abort (sticky, uniform within
+// the CTA; for stopping loops).  failed(): the group's flag in memory, read once
+// at the end for the launch's status, since a CTA may pass every barrier it
+// reaches after another CTA gave up.
 struct GridGroup {
     SegmentBarrier* bar;
+    int stop = 0;
+    __device__ explicit GridGroup(SegmentBarrier* b) : bar(b) { openBarrierBook(b); }
     __device__ __forceinline__ int rank() const { return blockIdx.x; }
     __device__ __forceinline__ int size() const { return gridDim.x; }
-    __device__ __forceinline__ bool aborted() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
-    __device__ __forceinline__ void sync() { groupBarrier(bar, blockIdx.x == 0, gridDim.x); }
+    __device__ __forceinline__ bool aborted() const { return stop != 0; }
+    __device__ __forceinline__ bool failed() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
+    __device__ __forceinline__ void sync() { stop |= groupBarrier(bar, blockIdx.x == 0, gridDim.x); }
 };
 
 struct SegmentGroup {
     int cta0, ncta;
     SegmentBarrier* bar;
+    int stop = 0;
+    __device__ SegmentGroup(int c0, int n, SegmentBarrier* b) : cta0(c0), ncta(n), bar(b) { openBarrierBook(b); }
     __device__ __forceinline__ int rank() const { return blockIdx.x - cta0; }
     __device__ __forceinline__ int size() const { return ncta; }
-    __device__ __forceinline__ bool aborted() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
-    __device__ __forceinline__ void sync() { groupBarrier(bar, rank() == 0, ncta); }
+    __device__ __forceinline__ bool aborted() const { return stop != 0; }
+    __device__ __forceinline__ bool failed() const { return *reinterpret_cast<volatile int*>(&bar->abort) != 0; }
+    __device__ __forceinline__ void sync() { stop |= groupBarrier(bar, rank() == 0, ncta); }
 };
 
 struct Lanes {
@@ -113,7 +203,9 @@ __device__ void gridSum(G& g, double v[NV], double* partial, int& buf) {
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
         double x = 0.0;
-        for (int b = threadIdx.x; b < g.size(); b += BS) x += part[b * NV + j];
+        // read at L2 (ld.global.cg): every CTA must see exactly the totals the others see,
+        // whatever its SM's L1 still holds of the previous sum on this half
+        for (int b = threadIdx.x; b < g.size(); b += BS) x += __ldcg(part + b * NV + j);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0) sh[j][warp] = x;

@@ -704,7 +704,8 @@ SolveOutcome KrylovSolver::solveRefined(const Dcsr<double>& A, const SolverConfi
         ++out.checks;
         PcgState r;
         std::memcpy(&r, ctx.pinned, sizeof(r));
-        if (r.status == 3) fail(kCuda, "persistent PCG: a barrier wait ran past its bound");
+        if (r.status == 3)
+            fail(kCuda, "persistent PCG: a barrier wait ran past its bound" + barrierReport(ctx.grid_barrier));
         used += r.iterations;
         if (ctx.profiling || trace_solves()) {
             const double N = n;
@@ -764,7 +765,8 @@ SolveOutcome KrylovSolver::solvePersistent(const Dcsr<double>& A, const SolverCo
         ctx.sync();
         PcgState r;
         std::memcpy(&r, ctx.pinned, sizeof(r));
-        if (r.status == 3) fail(kCuda, "persistent PCG: a barrier wait ran past its bound");
+        if (r.status == 3)
+            fail(kCuda, "persistent PCG: a barrier wait ran past its bound" + barrierReport(ctx.grid_barrier));
         if (ctx.profiling || trace_solves()) {
             // algorithmic bytes of this launch: initial residual, preconditioner
             // applications and per-iteration SpMV + vector updates
@@ -1034,7 +1036,10 @@ void KrylovSolver::solveBatch(Context& ctx, std::vector<BatchSolve>& items) {
             BatchSolve& it = items[k];
             Track& tr = t[k];
             const PcgState& r = states[k];
-            if (r.status == 3) fail(kCuda, "batched persistent PCG: a segment barrier wait ran past its bound");
+            if (r.status == 3)
+                fail(kCuda, "batched persistent PCG: a segment barrier wait ran past its bound" +
+                                barrierReport(batch64.d_bars.data(), static_cast<int>(batch64.args.size())) +
+                                barrierReport(batch32.d_bars.data(), static_cast<int>(batch32.args.size())));
             ++it.out.checks;
             if (attempt == 0) {
                 it.out.initial = std::sqrt(r.rr0);
@@ -1132,7 +1137,10 @@ void KrylovSolver::solveVector3Batch(Context& ctx, std::vector<BicgItem>& items,
             BicgItem& it = items[k];
             Track& tr = t[k];
             const BicgState& r = res[k];
-            if (r.status == 3) fail(kCuda, "persistent BiCGStab: a barrier wait ran past its bound");
+            if (r.status == 3)
+                fail(kCuda, "persistent BiCGStab: a barrier wait ran past its bound" +
+                                (batched ? barrierReport(batch.d_bars.data(), static_cast<int>(batch.args.size()))
+                                         : barrierReport(ctx.grid_barrier)));
             for (int c = 0; c < 3; ++c) {
                 if (tr.finished[c]) continue;
                 SolveOutcome& o = it.out[c];

@@ -66,7 +66,7 @@ __device__ void gridReduce(GridGroup& g, double v[NV], double* partial, int& buf
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
         double x = 0.0;
-        for (int b = threadIdx.x; b < gridDim.x; b += PB) x += part[b * NVMAX + j];
+        for (int b = threadIdx.x; b < gridDim.x; b += PB) x += __ldcg(part + b * NVMAX + j);  // at L2
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0) sh[j][warp] = x;
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(PB) kPcgPersistent(PcgArgs a, SegmentBarrier* 
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st.rr = rr;
         st.iterations = it;
-        st.status = g.aborted() ? 3 : status;
+        st.status = g.failed() ? 3 : status;
     }
 }
 
@@ -391,7 +391,7 @@ constexpr int kStaticMaxRows = 131072;
 constexpr int kStaticMaxBlocks = 4096;
 static __device__ __align__(256) double g_static_scratch[5 * kStaticMaxRows + 2 * NVMAX * kStaticMaxBlocks];
 static __device__ __align__(256) PcgState g_static_state;
-static __device__ __align__(16) SegmentBarrier g_static_barrier;
+static __device__ __align__(16) SegmentBarrier g_static_barrier;  // zeroed before each launch: no progress record
 
 namespace {
 struct StaticScratch {
@@ -499,9 +499,9 @@ void launchPersistentPcg(Context& ctx, const Dcsr<double>& A, const AmgView<doub
     const PhaseLog log{ctx.phase_entries, ctx.phase_capacity, ctx.phase_count};
     PcgArgs args{A, amg, jac, b, x, r, z, p0, p1, q, partial, st, log};
     SegmentBarrier* bar = ctx.grid_barrier;
-    BSG_CUDA(cudaMemsetAsync(bar, 0, sizeof(SegmentBarrier), ctx.stream));
-    void* params[] = {&args, &bar};
     const int grid = persistentGrid(ctx);
+    resetBarriers(ctx, bar, 1, grid);
+    void* params[] = {&args, &bar};
     BSG_PROFILE(ctx, "pcg_amg_persistent");
     BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgPersistent), grid, PB, params, 0, ctx.stream));
     ctx.launched();

@@ -369,7 +369,7 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
     if (g.rank() == 0 && threadIdx.x == 0) {
         st.rr = rr;
         st.iterations = it;
-        st.status = g.aborted() ? 3 : status;
+        st.status = g.failed() ? 3 : status;
     }
 }
 
@@ -413,9 +413,9 @@ void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& in) {
     SellPcgArgs<TK, TV> args = in;
     args.log = PhaseLog{ctx.phase_entries, ctx.phase_capacity, ctx.phase_count};
     SegmentBarrier* bar = ctx.grid_barrier;
-    BSG_CUDA(cudaMemsetAsync(bar, 0, sizeof(SegmentBarrier), ctx.stream));
-    void* params[] = {&args, &bar};
     const int grid = sellGrid<TK, TV>(ctx);
+    resetBarriers(ctx, bar, 1, grid);
+    void* params[] = {&args, &bar};
     BSG_PROFILE(ctx, "pcg_amg_persistent");
     BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kPcgSell<TK, TV>), grid, SB, params, 0, ctx.stream));
     ctx.launched();
@@ -436,7 +436,7 @@ void launchSellPcgBatch(Context& ctx, BatchLaunch<TK, TV>& batch) {
     batch.d_args.upload(batch.args, ctx.stream);
     batch.d_cta.upload(batch.cta_begin, ctx.stream);
     batch.d_bars.resize(nsegs);
-    batch.d_bars.zero(ctx.stream);
+    resetBarriers(ctx, batch.d_bars.data(), nsegs, total, batch.cta_begin.data());
     const SellPcgArgs<TK, TV>* segs = batch.d_args.data();
     const int* cta = batch.d_cta.data();
     SegmentBarrier* bars = batch.d_bars.data();
