@@ -20,8 +20,8 @@ constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s at the B200's c
 // the top bit flips when the last one lands, while the low 31 bits come back to
 // where they were (zero: the word is reset before each launch).  A CTA leaves
 // when the top bit differs from the value its own add returned.  The add is a
-// gpu-scope release (after __syncthreads, so it covers the whole CTA's writes)
-// and the poll a gpu-scope acquire, so no separate fences are needed.  All CTAs
+// gpu-scope release (after __syncthreads, so it covers the whole CTA's writes);
+// the poll uses relaxed loads and one acquire fence follows the flip.  All CTAs
 // of a cooperative launch are resident, so the flip always comes unless a CTA
 // skipped the barrier; the wait is bounded all the same: past kBarrierCycles the
 // CTA records an abort (and, first of all, where it was and what it saw) and
@@ -35,11 +35,6 @@ __device__ __forceinline__ unsigned arriveRelease(unsigned* word, unsigned add) 
 __device__ __forceinline__ unsigned loadRelaxed(const unsigned* word) {
     unsigned v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
-    return v;
-}
-__device__ __forceinline__ unsigned loadAcquire(const unsigned* word) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
     return v;
 }
 
@@ -58,73 +53,51 @@ __device__ __forceinline__ void openBarrierBook(const SegmentBarrier* bar) {
     if (threadIdx.x == 0) barrierBook() = BarrierBook{0u, bar->progress};
 }
 
-#ifndef BSG_BARRIER_POLL
-#define BSG_BARRIER_POLL 1  // 0: acquire loads; 1: relaxed loads, one acquire fence after; 2: volatile + fence.sc
-#endif
-#ifndef BSG_BARRIER_PROGRESS
-#define BSG_BARRIER_PROGRESS 1
-#endif
-#if BSG_BARRIER_NOINLINE
-#define BSG_BARRIER_INLINE static __noinline__
-#else
-#define BSG_BARRIER_INLINE __forceinline__
-#endif
+// Thread 0's part of a barrier: arrive, wait for the flip (bounded), acquire.
+// Returns 1 when it left on the group's abort (its own timeout or another CTA's).
+__device__ __forceinline__ int arriveAndWait(SegmentBarrier* bar, bool leader, int n) {
+    const unsigned add = leader ? 0x80000000u - static_cast<unsigned>(n - 1) : 1u;
+    const unsigned old = arriveRelease(&bar->count, add);
+    BarrierBook& book = barrierBook();
+    const unsigned seq = ++book.seq;
+    // recorded after the arrival, so the release above never waits on this store
+    if (book.progress) book.progress[blockIdx.x] = seq;
+    long long t0 = 0;
+    int stop = 0;
+    for (unsigned spins = 1;; ++spins) {
+        const unsigned cur = loadRelaxed(&bar->count);
+        if ((cur ^ old) & 0x80000000u) break;
+        if ((spins & 255u) != 0u) continue;
+        if (*reinterpret_cast<volatile int*>(&bar->abort)) {
+            stop = 1;
+            break;
+        }
+        const long long now = clock64();
+        if (spins == 256u) {
+            t0 = now;
+        } else if (now - t0 > kBarrierCycles) {
+            if (atomicCAS(&bar->who, 0, static_cast<int>(blockIdx.x) + 1) == 0) {
+                bar->where = seq;
+                bar->seen = cur;
+            }
+            __threadfence();
+            atomicExch(&bar->abort, 1);
+            stop = 1;
+            break;
+        }
+    }
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");  // the acquire that pairs with the last arrival
+    return stop;
+}
 
-// Returns 1 when thread 0 left the wait on the group's abort (its own timeout or
-// another CTA's), 0 when the phase completed: the same value for every thread of
-// the CTA, so a loop that stops on it stops in all of them.
-__device__ BSG_BARRIER_INLINE int groupBarrier(SegmentBarrier* bar, bool leader, int n) {
+// Returns thread 0's result of arriveAndWait: the same value for every thread of
+// the CTA, so a loop that stops on it stops in all of them.  Out of line: on the
+// 1M-cell pressure solves every inlined copy slowed the sweeps between barriers
+// (52.4 against 47.3 ms per SIMPLE iteration), while the call costs nothing visible.
+__device__ static __noinline__ int groupBarrier(SegmentBarrier* bar, bool leader, int n) {
     __shared__ int aborted;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned add = leader ? 0x80000000u - static_cast<unsigned>(n - 1) : 1u;
-#if BSG_BARRIER_POLL == 2
-        __threadfence();
-        const unsigned old = atomicAdd(&bar->count, add);
-#else
-        const unsigned old = arriveRelease(&bar->count, add);
-#endif
-        BarrierBook& book = barrierBook();
-        const unsigned seq = ++book.seq;
-        // recorded after the arrival, so the release above never waits on this store
-        if (BSG_BARRIER_PROGRESS && book.progress) book.progress[blockIdx.x] = seq;
-        long long t0 = 0;
-        int stop = 0;
-        for (unsigned spins = 1;; ++spins) {
-#if BSG_BARRIER_POLL == 0
-            const unsigned cur = loadAcquire(&bar->count);
-#elif BSG_BARRIER_POLL == 1
-            const unsigned cur = loadRelaxed(&bar->count);
-#else
-            const unsigned cur = *reinterpret_cast<volatile unsigned*>(&bar->count);
-#endif
-            if ((cur ^ old) & 0x80000000u) break;
-            if ((spins & 255u) != 0u) continue;
-            if (*reinterpret_cast<volatile int*>(&bar->abort)) {
-                stop = 1;
-                break;
-            }
-            const long long now = clock64();
-            if (spins == 256u) {
-                t0 = now;
-            } else if (now - t0 > kBarrierCycles) {
-                if (atomicCAS(&bar->who, 0, static_cast<int>(blockIdx.x) + 1) == 0) {
-                    bar->where = seq;
-                    bar->seen = cur;
-                }
-                __threadfence();
-                atomicExch(&bar->abort, 1);
-                stop = 1;
-                break;
-            }
-        }
-#if BSG_BARRIER_POLL == 1
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");  // the acquire that pairs with the last arrival
-#elif BSG_BARRIER_POLL == 2
-        __threadfence();
-#endif
-        aborted = stop;
-    }
+    if (threadIdx.x == 0) aborted = arriveAndWait(bar, leader, n);
     __syncthreads();
     // the next write to `aborted` comes after the next barrier's first __syncthreads,
     // which every thread reaches only after this read

@@ -12,11 +12,18 @@ namespace {
 #define BSG_SELL_SB 256
 #endif
 constexpr int SB = BSG_SELL_SB;  // threads per block
-// Minimum resident blocks per SM the register budget must allow: 3 (80 registers)
-// measured faster than 4 (64) on the 1M-cell pressure solves, 2 (128) slower.
+// Minimum resident blocks per SM the register budget must allow.  The FP64
+// single-system kernel: 4 (64 registers, no spills) measured 2 % faster than 3 (80)
+// on the 1M-cell pressure solves, 2 (128) slower.  The FP32 V-cycle variants and the
+// batched kernel keep 3: at 64 registers they spill.
 #ifndef BSG_SELL_MIN_BLOCKS
-#define BSG_SELL_MIN_BLOCKS 3
+#define BSG_SELL_MIN_BLOCKS 4
 #endif
+#ifndef BSG_SELL_BATCH_MIN_BLOCKS
+#define BSG_SELL_BATCH_MIN_BLOCKS 3
+#endif
+template <class TK, class TV>
+constexpr int kSellMinBlocks = (sizeof(TK) == 8 && sizeof(TV) == 8) ? BSG_SELL_MIN_BLOCKS : 3;
 
 __device__ __forceinline__ void mark(const PhaseLog& log, int id) {
     if (log.entries && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -374,7 +381,7 @@ __device__ void pcgBody(G& g, const SellPcgArgs<TK, TV>& a) {
 }
 
 template <class TK, class TV>
-__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<TK, TV> a, SegmentBarrier* bar) {
+__global__ void __launch_bounds__(SB, (kSellMinBlocks<TK, TV>)) kPcgSell(SellPcgArgs<TK, TV> a, SegmentBarrier* bar) {
     GridGroup g{bar};
     pcgBody<TK, TV>(g, a);
 }
@@ -382,7 +389,7 @@ __global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS) kPcgSell(SellPcgArgs<
 // A batch: CTAs [cta_begin[s], cta_begin[s+1]) solve system s with its own
 // arguments, barriers and reductions, independently of the other systems.
 template <class TK, class TV>
-__global__ void __launch_bounds__(SB, BSG_SELL_MIN_BLOCKS)
+__global__ void __launch_bounds__(SB, BSG_SELL_BATCH_MIN_BLOCKS)
     kPcgSellBatch(const SellPcgArgs<TK, TV>* __restrict__ segs, const int* __restrict__ cta_begin, int nsegs,
                   SegmentBarrier* bars) {
     int lo = 0, hi = nsegs - 1;  // the segment whose CTA range holds this block
@@ -406,6 +413,19 @@ int sellGrid(Context& ctx) {
     return ctx.sm_count * std::min(per_sm, 8);
 }
 
+// Resident CTAs of the batched kernels: the smaller of the two precisions' grids.
+int batchGrid(Context& ctx) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        int a = 0, b = 0;
+        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kPcgSellBatch<double, double>, SB, 0));
+        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kPcgSellBatch<double, float>, SB, 0));
+        per_sm = std::min(a, b);
+        if (per_sm <= 0) fail(kCuda, "batched SELL PCG kernel cannot be resident");
+    }
+    return ctx.sm_count * std::min(per_sm, 8);
+}
+
 }  // namespace
 
 template <class TK, class TV>
@@ -421,7 +441,7 @@ void launchSellPcg(Context& ctx, const SellPcgArgs<TK, TV>& in) {
     ctx.launched();
 }
 
-int sellBatchCapacity(Context& ctx) { return sellGrid<double, double>(ctx); }
+int sellBatchCapacity(Context& ctx) { return batchGrid(ctx); }
 
 template <class TK, class TV>
 void launchSellPcgBatch(Context& ctx, BatchLaunch<TK, TV>& batch) {
@@ -432,7 +452,7 @@ void launchSellPcgBatch(Context& ctx, BatchLaunch<TK, TV>& batch) {
     for (int k = 0; k < nsegs; ++k)
         if (batch.cta_begin[k + 1] <= batch.cta_begin[k]) fail(kArgument, "batched PCG: a system without CTAs");
     const int total = batch.cta_begin.back();
-    if (total > sellGrid<TK, TV>(ctx)) fail(kArgument, "batched PCG: CTA allotment exceeds the resident grid");
+    if (total > batchGrid(ctx)) fail(kArgument, "batched PCG: CTA allotment exceeds the resident grid");
     batch.d_args.upload(batch.args, ctx.stream);
     batch.d_cta.upload(batch.cta_begin, ctx.stream);
     batch.d_bars.resize(nsegs);
