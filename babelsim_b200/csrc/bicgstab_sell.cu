@@ -21,19 +21,18 @@ namespace {
 constexpr int BB = 256;  // threads per block
 
 // (A x)_i for the C components of row i of slice sl (lane = row within the slice).
-template <int C>
-__device__ __forceinline__ void sellProduct(const SellMat<double>& S, int sl, int lane, const double* __restrict__ x,
-                                            double acc[C]) {
+template <int C, class T>
+__device__ __forceinline__ void sellProduct(const SellMat<T>& S, int sl, int lane, const T* __restrict__ x, T acc[C]) {
     const int beg = S.sptr[sl], w = (S.sptr[sl + 1] - beg) >> 5;
     const int* __restrict__ cp = S.col + beg + lane;
-    const double* __restrict__ vp = S.val + beg + lane;
-    double a[C];
+    const T* __restrict__ vp = S.val + beg + lane;
+    T a[C];
 #pragma unroll
-    for (int c = 0; c < C; ++c) a[c] = 0.0;
+    for (int c = 0; c < C; ++c) a[c] = T(0);
     int k = 0;
     for (; k + 4 <= w; k += 4) {
         int cc[4];
-        double vv[4];
+        T vv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             cc[u] = __ldg(cp + 32 * (k + u));
@@ -46,30 +45,39 @@ __device__ __forceinline__ void sellProduct(const SellMat<double>& S, int sl, in
     }
     for (; k < w; ++k) {
         const int j = __ldg(cp + 32 * k);
-        const double v = __ldg(vp + 32 * k);
+        const T v = __ldg(vp + 32 * k);
 #pragma unroll
         for (int c = 0; c < C; ++c) a[c] += v * x[C * j + c];
     }
     const int i = 32 * sl + lane;
-    const double d = i < S.n ? S.diag[i] : 0.0;
+    const T d = i < S.n ? S.diag[i] : T(0);
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[c] = (i < S.n ? d * x[C * i + c] : 0.0) + a[c];
+    for (int c = 0; c < C; ++c) acc[c] = (i < S.n ? d * x[C * i + c] : T(0)) + a[c];
 }
 
-template <int C, class G>
-__device__ void bicgBody(G& g, const BicgArgs<C>& a) {
+// Products of vector entries are summed in FP64 whatever the vectors' type.
+template <class T>
+__device__ __forceinline__ double dd(T x) {
+    return static_cast<double>(x);
+}
+
+template <int C, class T, class G>
+__device__ void bicgBody(G& g, const BicgArgs<C, T>& a) {
     const Lanes ln = lanes<BB>(g);
-    const SellMat<double>& A = a.A;
+    const SellMat<T>& A = a.A;
     const int n = A.n;
     BicgState& st = *a.st;
     int buf = 0;
     double rho[C], alpha[C], omega[C], beta[C], target2[C];
     int done[C], iters[C];
+    double target2_in[C];
     const int max_iters = st.max_iters;
+    // inputs are read before block 0 writes any result into the same struct
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         done[c] = st.done[c];
         iters[c] = st.iters[c];
+        target2_in[c] = st.target2[c];
         alpha[c] = 1.0;
         omega[c] = 1.0;
         beta[c] = 0.0;
@@ -80,19 +88,19 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
 #pragma unroll
     for (int j = 0; j < 2 * C; ++j) nb[j] = 0.0;
     for (int sl = ln.gwarp; sl < A.nslices; sl += ln.nwarps) {
-        double acc[C];
-        sellProduct<C>(A, sl, ln.lane, a.x, acc);
+        T acc[C];
+        sellProduct<C, T>(A, sl, ln.lane, a.x, acc);
         const int i = 32 * sl + ln.lane;
         if (i < n) {
 #pragma unroll
             for (int c = 0; c < C; ++c) {
-                const double bi = a.b[C * i + c], ri = bi - acc[c];
+                const T bi = a.b[C * i + c], ri = bi - acc[c];
                 a.r[C * i + c] = ri;
                 a.r0[C * i + c] = ri;
-                a.p[C * i + c] = 0.0;
-                a.v[C * i + c] = 0.0;
-                nb[c] += ri * ri;
-                nb[C + c] += bi * bi;
+                a.p[C * i + c] = T(0);
+                a.v[C * i + c] = T(0);
+                nb[c] += dd(ri) * dd(ri);
+                nb[C + c] += dd(bi) * dd(bi);
             }
         }
     }
@@ -100,14 +108,14 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         rho[c] = nb[c];
-        if (st.target2[c] < 0.0) {
+        if (target2_in[c] < 0.0) {
             // the reference's contract: max(atol, rtol * max(||r0||, ||b||)) (solver_control.h:199-210)
             double scale = fmax(sqrt(nb[c]), sqrt(nb[C + c]));
             if (!(scale > 0.0)) scale = 1.0;
             const double tg = fmax(st.atol, st.rtol * scale);
             target2[c] = tg * tg;
         } else {
-            target2[c] = st.target2[c];
+            target2[c] = target2_in[c];
         }
         if (done[c] == 0 && (!(nb[c] > 0.0) || nb[c] <= target2[c])) done[c] = 1;
     }
@@ -126,11 +134,12 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
         if (!any || g.aborted()) break;
         // p = r + beta (p - omega v), ph = p / d
         for (int i = ln.gthread; i < n; i += ln.nthreads) {
-            const double rd = 1.0 / A.diag[i];
+            const T rd = T(1) / A.diag[i];
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 if (!active(c)) continue;
-                const double pi = a.r[C * i + c] + beta[c] * (a.p[C * i + c] - omega[c] * a.v[C * i + c]);
+                const T pi = a.r[C * i + c] +
+                             static_cast<T>(beta[c]) * (a.p[C * i + c] - static_cast<T>(omega[c]) * a.v[C * i + c]);
                 a.p[C * i + c] = pi;
                 a.ph[C * i + c] = pi * rd;
             }
@@ -141,14 +150,14 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
 #pragma unroll
         for (int c = 0; c < C; ++c) r0v[c] = 0.0;
         for (int sl = ln.gwarp; sl < A.nslices; sl += ln.nwarps) {
-            double acc[C];
-            sellProduct<C>(A, sl, ln.lane, a.ph, acc);
+            T acc[C];
+            sellProduct<C, T>(A, sl, ln.lane, a.ph, acc);
             const int i = 32 * sl + ln.lane;
             if (i < n) {
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
                     a.v[C * i + c] = acc[c];
-                    r0v[c] += a.r0[C * i + c] * acc[c];
+                    r0v[c] += dd(a.r0[C * i + c]) * dd(acc[c]);
                 }
             }
         }
@@ -164,14 +173,14 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
 #pragma unroll
         for (int c = 0; c < C; ++c) ss[c] = 0.0;
         for (int i = ln.gthread; i < n; i += ln.nthreads) {
-            const double rd = 1.0 / A.diag[i];
+            const T rd = T(1) / A.diag[i];
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 if (!active(c)) continue;
-                const double si = a.r[C * i + c] - alpha[c] * a.v[C * i + c];
+                const T si = a.r[C * i + c] - static_cast<T>(alpha[c]) * a.v[C * i + c];
                 a.r[C * i + c] = si;
                 a.sh[C * i + c] = si * rd;
-                ss[c] += si * si;
+                ss[c] += dd(si) * dd(si);
             }
         }
         gridSum<C, BB>(g, ss, a.partial, buf);
@@ -186,15 +195,15 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
 #pragma unroll
         for (int j = 0; j < 2 * C; ++j) ts[j] = 0.0;
         for (int sl = ln.gwarp; sl < A.nslices; sl += ln.nwarps) {
-            double acc[C];
-            sellProduct<C>(A, sl, ln.lane, a.sh, acc);
+            T acc[C];
+            sellProduct<C, T>(A, sl, ln.lane, a.sh, acc);
             const int i = 32 * sl + ln.lane;
             if (i < n) {
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
                     a.t[C * i + c] = acc[c];
-                    ts[2 * c] += acc[c] * acc[c];
-                    ts[2 * c + 1] += acc[c] * a.r[C * i + c];
+                    ts[2 * c] += dd(acc[c]) * dd(acc[c]);
+                    ts[2 * c + 1] += dd(acc[c]) * dd(a.r[C * i + c]);
                 }
             }
         }
@@ -214,14 +223,14 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
             for (int c = 0; c < C; ++c) {
                 if (mode[c] == 0) continue;
                 if (mode[c] == 2) {
-                    a.x[C * i + c] += alpha[c] * a.ph[C * i + c];
+                    a.x[C * i + c] += static_cast<T>(alpha[c]) * a.ph[C * i + c];
                     continue;
                 }
-                a.x[C * i + c] += alpha[c] * a.ph[C * i + c] + omega[c] * a.sh[C * i + c];
-                const double ri = a.r[C * i + c] - omega[c] * a.t[C * i + c];
+                a.x[C * i + c] += static_cast<T>(alpha[c]) * a.ph[C * i + c] + static_cast<T>(omega[c]) * a.sh[C * i + c];
+                const T ri = a.r[C * i + c] - static_cast<T>(omega[c]) * a.t[C * i + c];
                 a.r[C * i + c] = ri;
-                nr[2 * c] += ri * ri;
-                nr[2 * c + 1] += a.r0[C * i + c] * ri;
+                nr[2 * c] += dd(ri) * dd(ri);
+                nr[2 * c + 1] += dd(a.r0[C * i + c]) * dd(ri);
             }
         }
         gridSum<2 * C, BB>(g, nr, a.partial, buf);
@@ -244,14 +253,14 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
     for (int c = 0; c < C; ++c) fr[c] = 0.0;
     g.sync();
     for (int sl = ln.gwarp; sl < A.nslices; sl += ln.nwarps) {
-        double acc[C];
-        sellProduct<C>(A, sl, ln.lane, a.x, acc);
+        T acc[C];
+        sellProduct<C, T>(A, sl, ln.lane, a.x, acc);
         const int i = 32 * sl + ln.lane;
         if (i < n) {
 #pragma unroll
             for (int c = 0; c < C; ++c) {
-                const double ri = a.b[C * i + c] - acc[c];
-                fr[c] += ri * ri;
+                const T ri = a.b[C * i + c] - acc[c];
+                fr[c] += dd(ri) * dd(ri);
             }
         }
     }
@@ -267,10 +276,10 @@ __device__ void bicgBody(G& g, const BicgArgs<C>& a) {
     }
 }
 
-template <int C>
-__global__ void __launch_bounds__(BB, 3) kBicgSell(BicgArgs<C> a, SegmentBarrier* bar) {
+template <int C, class T>
+__global__ void __launch_bounds__(BB, 3) kBicgSell(BicgArgs<C, T> a, SegmentBarrier* bar) {
     GridGroup g{bar};
-    bicgBody<C>(g, a);
+    bicgBody<C, T>(g, a);
 }
 
 template <int C>
@@ -285,7 +294,7 @@ __global__ void __launch_bounds__(BB, 3)
     }
     SegmentGroup g{cta_begin[lo], cta_begin[lo + 1] - cta_begin[lo], bars + lo};
     const BicgArgs<C> a = segs[lo];
-    bicgBody<C>(g, a);
+    bicgBody<C, double>(g, a);
 }
 
 }  // namespace
@@ -293,7 +302,7 @@ __global__ void __launch_bounds__(BB, 3)
 int bicgstabGrid(Context& ctx) {
     static int per_sm = -1;
     if (per_sm < 0) {
-        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kBicgSell<3>, BB, 0));
+        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kBicgSell<3, double>, BB, 0));
         int b = 0;
         BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kBicgSellBatch<3>, BB, 0));
         per_sm = std::min(per_sm, b);
@@ -302,15 +311,28 @@ int bicgstabGrid(Context& ctx) {
     return ctx.sm_count * std::min(per_sm, 4);
 }
 
-template <int C>
-void launchBicgstab(Context& ctx, const BicgArgs<C>& in) {
-    BicgArgs<C> args = in;
+namespace {
+// Resident CTAs of one whole-grid launch of kBicgSell<C, T>.
+template <int C, class T>
+int singleGrid(Context& ctx) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kBicgSell<C, T>, BB, 0));
+        if (per_sm <= 0) fail(kCuda, "persistent BiCGStab kernel cannot be resident");
+    }
+    return ctx.sm_count * std::min(per_sm, 4);
+}
+}  // namespace
+
+template <int C, class T>
+void launchBicgstab(Context& ctx, const BicgArgs<C, T>& in) {
+    BicgArgs<C, T> args = in;
     SegmentBarrier* bar = ctx.grid_barrier;
-    const int grid = bicgstabGrid(ctx);
+    const int grid = singleGrid<C, T>(ctx);
     resetBarriers(ctx, bar, 1, grid);
     void* params[] = {&args, &bar};
-    BSG_PROFILE(ctx, "bicgstab3_persistent");
-    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kBicgSell<C>), grid, BB, params, 0, ctx.stream));
+    BSG_PROFILE(ctx, sizeof(T) == 4 ? "bicgstab3_persistent_fp32" : "bicgstab3_persistent");
+    BSG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kBicgSell<C, T>), grid, BB, params, 0, ctx.stream));
     ctx.launched();
 }
 
@@ -339,8 +361,10 @@ void launchBicgstabBatch(Context& ctx, BicgBatch<C>& batch) {
     ctx.launched();
 }
 
-template void launchBicgstab<3>(Context&, const BicgArgs<3>&);
-template void launchBicgstab<1>(Context&, const BicgArgs<1>&);
+template void launchBicgstab<3, double>(Context&, const BicgArgs<3, double>&);
+template void launchBicgstab<1, double>(Context&, const BicgArgs<1, double>&);
+template void launchBicgstab<3, float>(Context&, const BicgArgs<3, float>&);
+template void launchBicgstab<1, float>(Context&, const BicgArgs<1, float>&);
 template void launchBicgstabBatch<3>(Context&, BicgBatch<3>&);
 
 }  // namespace bsg

@@ -33,12 +33,14 @@ struct BicgState {
     int status;         // out: 0 ok, 3 a barrier wait ran past its bound
 };
 
-template <int C>
+// T: the type of the matrix copy, the vectors and their arithmetic (double, or float for
+// the inner iterations of a mixed-precision solve); reductions are summed in FP64.
+template <int C, class T = double>
 struct BicgArgs {
-    SellMat<double> A;       // SELL-32 copy of the matrix (diag included)
-    const double* b;         // C-interleaved right-hand sides
-    double* x;               // C-interleaved initial guess / solution
-    double *r, *r0, *p, *v, *ph, *sh, *t;  // C * n each
+    SellMat<T> A;            // SELL-32 copy of the matrix (diag included)
+    const T* b;              // C-interleaved right-hand sides
+    T* x;                    // C-interleaved initial guess / solution
+    T *r, *r0, *p, *v, *ph, *sh, *t;  // C * n each
     double* partial;         // 2 * ctas * 2C doubles
     BicgState* st;
 };
@@ -54,8 +56,8 @@ struct BicgBatch {
 
 // Resident CTAs of the persistent BiCGStab kernel (the grid of one solve).
 int bicgstabGrid(Context& ctx);
-template <int C>
-void launchBicgstab(Context& ctx, const BicgArgs<C>& args);
+template <int C, class T>
+void launchBicgstab(Context& ctx, const BicgArgs<C, T>& args);
 template <int C>
 void launchBicgstabBatch(Context& ctx, BicgBatch<C>& batch);
 

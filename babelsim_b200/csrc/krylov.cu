@@ -532,6 +532,9 @@ struct KrylovSolver::Impl {
     DeviceArray<unsigned> ticket;  // arrivals of the current reduction (reduceThenFinish), zero between launches
     DeviceArray<PcgState> pst;
     DeviceArray<float> r32, s32, z32, p32a, p32b, q32, d32;  // FP32 inner solve of the refined path
+    // FP32 inner BiCGStab of the refined path: matrix copy (SELL values, diagonal) and
+    // the C-interleaved right-hand side, correction and Krylov vectors
+    DeviceArray<float> bval32, bdiag32, bb32, bx32, br32, br032, bp32, bv32, bph32, bsh32, bt32;
     GmresWorkspace gmres;
     // SELL-32 copy of the matrix the BiCGStab products read: the pattern of the
     // last CSR pattern seen (a solver's systems all live on one mesh's cell->face
@@ -1127,7 +1130,7 @@ void KrylovSolver::solveVector3Batch(Context& ctx, std::vector<BicgItem>& items,
             batch.cta_begin = allotCtas(slices, bicgstabGrid(ctx));
             launchBicgstabBatch<3>(ctx, batch);
         } else {
-            for (const auto& a : batch.args) launchBicgstab<3>(ctx, a);
+            for (const auto& a : batch.args) launchBicgstab<3, double>(ctx, a);
         }
         for (int k : active)
             BSG_CUDA(cudaMemcpyAsync(&res[k], items[k].solver->impl_->bst.data(), sizeof(BicgState),
@@ -1176,9 +1179,124 @@ void KrylovSolver::solveVector3Batch(Context& ctx, std::vector<BicgItem>& items,
     }
 }
 
+// Mixed precision (precision 1) for the Jacobi BiCGStab solves (momentum, transport):
+// r = b - A x and the acceptance test in FP64; each pass solves A d = r with the FP32
+// persistent BiCGStab (FP32 matrix copy and vectors, FP64 reductions) to a relative
+// target, then x += d in FP64, until every component's FP64 residual meets
+// max(atol, rtol max(||r0||, ||b||)), the iteration budget is spent, or a pass stops
+// reducing the residual.
+template <int C>
+void KrylovSolver::refinedBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                                   SolveOutcome out[]) {
+    Impl& m = *impl_;
+    Context& ctx = m.ctx;
+    const int n = A.n;
+    const long long cn = static_cast<long long>(C) * n;
+    m.ensure(cn);
+    if (m.bst.size() < 1) m.bst.resize(1);
+    const SellMat<double> S = m.sellOf(A);
+    const long long entries = static_cast<long long>(m.sell.sval.size());
+    for (DeviceArray<float>* a : {&m.bb32, &m.bx32, &m.br32, &m.br032, &m.bp32, &m.bv32, &m.bph32, &m.bsh32, &m.bt32})
+        if (a->size() < static_cast<std::size_t>(cn)) a->resize(cn);
+    if (m.bval32.size() < static_cast<std::size_t>(entries)) m.bval32.resize(entries);
+    if (m.bdiag32.size() < static_cast<std::size_t>(n)) m.bdiag32.resize(n);
+    auto toFloat = [&](long long count, const double* from, float* to) {
+        for (long long o = 0; o < count; o += (1LL << 30)) {
+            const int k = static_cast<int>(std::min<long long>(count - o, 1LL << 30));
+            kToFloat32<<<(k + 255) / 256, 256, 0, ctx.stream>>>(k, from + o, to + o);
+            ctx.launched();
+        }
+    };
+    toFloat(entries, S.val, m.bval32.data());
+    toFloat(n, A.diag, m.bdiag32.data());
+    const SellMat<float> S32{n, S.nslices, S.sptr, S.col, m.bval32.data(), m.bdiag32.data()};
+    if (!cfg.warm_start) BSG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * cn, ctx.stream));
+    const int g = m.grid(n);
+    double* result = m.partial.data() + 8 * 4096 - 8;
+    auto residual = [&](double res[C], double bres[C]) {
+        kResidualC<C><<<g, kBlock, 0, ctx.stream>>>(A, b, x, m.r.data(), m.partial.data());
+        kFinishN<2 * C><<<1, 32, 0, ctx.stream>>>(g, m.partial.data(), result);
+        ctx.launches += 2;
+        BSG_CUDA(cudaGetLastError());
+        BSG_CUDA(cudaMemcpyAsync(ctx.pinned, result, 2 * C * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        for (int c = 0; c < C; ++c) {
+            res[c] = std::sqrt(ctx.pinned[c]);
+            if (bres) bres[c] = std::sqrt(ctx.pinned[C + c]);
+        }
+    };
+    double rn[C], bn[C], scale[C], target[C];
+    int used[C] = {};
+    bool finished[C] = {};
+    residual(rn, bn);
+    for (int c = 0; c < C; ++c) {
+        scale[c] = residualScale(rn[c], bn[c]);
+        target[c] = std::max(cfg.atol, cfg.rtol * scale[c]);
+        out[c] = SolveOutcome{};
+        out[c].initial = rn[c];
+        out[c].checks = 1;
+        finished[c] = !std::isfinite(rn[c]) || rn[c] <= target[c];
+    }
+    for (int pass = 0; pass < max_refinements; ++pass) {
+        bool any = false;
+        for (int c = 0; c < C; ++c) any = any || (!finished[c] && used[c] < cfg.max_iterations);
+        if (!any) break;
+        // the FP32 system A d = r, from d = 0, to a relative target per component
+        toFloat(cn, m.r.data(), m.bb32.data());
+        BSG_CUDA(cudaMemsetAsync(m.bx32.data(), 0, sizeof(float) * cn, ctx.stream));
+        BicgState h{};
+        int budget = cfg.max_iterations;
+        for (int c = 0; c < C; ++c) {
+            const bool on = !finished[c] && used[c] < cfg.max_iterations;
+            h.done[c] = on ? 0 : 1;
+            h.iters[c] = 0;
+            const double want = std::max(refine_inner_rtol, 0.5 * target[c] / rn[c]);
+            const double t = want * rn[c];
+            h.target2[c] = t * t;
+            if (on) budget = std::min(budget, cfg.max_iterations - used[c]);
+        }
+        h.atol = 0.0;
+        h.rtol = refine_inner_rtol;
+        h.max_iters = std::max(budget, 1);
+        BSG_CUDA(cudaMemcpyAsync(m.bst.data(), &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
+        BicgArgs<C, float> args{S32, m.bb32.data(), m.bx32.data(), m.br32.data(), m.br032.data(), m.bp32.data(),
+                                m.bv32.data(), m.bph32.data(), m.bsh32.data(), m.bt32.data(), m.partial.data(),
+                                m.bst.data()};
+        launchBicgstab<C, float>(ctx, args);
+        BicgState res;
+        BSG_CUDA(cudaMemcpyAsync(&res, m.bst.data(), sizeof(res), cudaMemcpyDeviceToHost, ctx.stream));
+        // x += d for the components still solving (the others' d stayed zero)
+        const int gc = static_cast<int>((cn + 255) / 256);
+        kAddCorrection<<<gc, 256, 0, ctx.stream>>>(static_cast<int>(cn), x, m.bx32.data());
+        ctx.launched();
+        double next[C];
+        residual(next, nullptr);  // synchronises; `res` is in place
+        if (res.status == 3)
+            fail(kCuda, "persistent BiCGStab: a barrier wait ran past its bound" + barrierReport(ctx.grid_barrier));
+        for (int c = 0; c < C; ++c) {
+            if (finished[c] || h.done[c]) continue;
+            used[c] += res.iters[c];
+            ++out[c].checks;
+            const bool stalled = !(next[c] < rn[c]);
+            rn[c] = next[c];
+            if (!std::isfinite(rn[c]) || rn[c] <= target[c] || stalled) finished[c] = true;
+        }
+    }
+    for (int c = 0; c < C; ++c) {
+        out[c].iterations = used[c];
+        out[c].final_ = rn[c];
+        out[c].relative = rn[c] / scale[c];
+        out[c].status = (std::isfinite(rn[c]) && rn[c] <= target[c]) ? 0 : (std::isfinite(rn[c]) ? 1 : 2);
+    }
+}
+
 template <int C>
 void KrylovSolver::lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                                     SolveOutcome out[]) {
+    if (cfg.precision == 1) {
+        refinedBicgstab<C>(A, cfg, b, x, out);
+        return;
+    }
     // the persistent kernel saves the launches and host checks that dominate small systems;
     // large ones stream faster through the per-phase kernels' higher occupancy
     if (persistent && C == 3 && A.n <= kPersistentBicgstabRows) {

@@ -160,6 +160,9 @@ private:
     template <int C>
     void lockstepBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
                           SolveOutcome out[]);
+    template <int C>
+    void refinedBicgstab(const Dcsr<double>& A, const SolverConfig& cfg, const double* b, double* x,
+                         SolveOutcome out[]);
     SolveOutcome cgComponent(const Dcsr<double>& A, const SolverConfig& cfg, Preconditioner* pc, int c,
                              const double* b, double* x);
     SolveOutcome solvePersistent(const Dcsr<double>& A, const SolverConfig& cfg, AmgPreconditioner* amg,

@@ -268,15 +268,16 @@ void SimpleSolver::outerIterationSegments() {
     std::vector<double> linP(K, 0.0);
     bool failed = false;
     {
-        // BiCGStab (kspType bcgs): every active case's momentum system in one persistent launch
-        // per attempt; other Krylov types solve case by case
+        // BiCGStab (kspType bcgs) in FP64: every active case's momentum system in one persistent
+        // launch per attempt; other Krylov types, and FP32 inner iterations with FP64 refinement
+        // (precision 1), solve case by case
         std::vector<BicgItem> items;
         std::vector<int> which;
         for (int k = 0; k < K; ++k) {
             SimpleSegment& sg = *segs_[k];
             if (sg.frozen) continue;
             const Dcsr<double> A = sg.view(mom.diag.data(), mom.val.data());
-            if (cfg_.momentum_solver.solver == 1) {
+            if (cfg_.momentum_solver.solver == 1 && cfg_.momentum_solver.precision != 1) {
                 BicgItem it;
                 it.solver = sg.mom.get();
                 it.A = A;

@@ -69,11 +69,11 @@ def mesh_for(n: int):
     return pm
 
 
-def build_simple(bsg, mesh, s, precision=0, boundaries=True):
+def build_simple(bsg, mesh, s, precision=0, boundaries=True, momentum_precision=0):
     opts = bsg.options(s["interpolation"], s["gradient"], s["convection"], s["diffusion"])
     sim = bsg.Simple(mesh, s["rho"], s["mu"], s["alpha_u"], s["alpha_p"], s["non_orthogonal_corrections"],
                      1e-8, 1e-7, 1e-6, 1e-6, opts, opts,
-                     bsg.solver_config("bcgs", "bjacobi", s["atol"], s["rtol"], 1000),
+                     bsg.solver_config("bcgs", "bjacobi", s["atol"], s["rtol"], 1000, precision=momentum_precision),
                      bsg.solver_config("cg", "hypre", s["atol"], s["rtol"], 1000, precision=precision))
     if not boundaries:  # the caller sets boundaries (and segments) before the fields
         return sim
@@ -777,12 +777,16 @@ def main():
     mixed = None
     if not args.no_mixed:
         U64, p64, _ = sim.fields()
-        steps64 = max(args.warmup, 3) + steps_done + 1 + e2e_steps
+        steps64 = sim.iterate(0).iterations  # every outer iteration of the FP64 run so far
         mixed = {}
         for mode, label in ((2, "fp64 flexible PCG + fp32 AMG V-cycle"),
-                            (1, "fp32 inner PCG + fp32 AMG V-cycle, fp64 refinement")):
+                            (1, "fp32 inner PCG + fp32 AMG V-cycle, fp64 refinement"),
+                            ("1_momentum", "fp32 inner BiCGStab in fp64 refinement for momentum, fp64 pressure"),
+                            ("1_all", "fp32 inner iterations in fp64 refinement for pressure (PCG + AMG) "
+                                      "and momentum (BiCGStab)")):
             sim.close()
-            sim = build_simple(bsg, mesh, s, precision=mode)
+            sim = build_simple(bsg, mesh, s, precision={"1_all": 1, "1_momentum": 0}.get(mode, mode),
+                               momentum_precision=1 if mode in ("1_all", "1_momentum") else 0)
             sim.iterate(max(args.warmup, 3))
             ctx.synchronize()
             ctx.record(4)

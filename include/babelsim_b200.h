@@ -83,7 +83,11 @@ typedef struct {
 } bsg_options;
 
 /* LinearSolverConfig, include/babelsim/solver_control.h:165-184, plus the
- * precision of the inner iterations. */
+ * precision of the inner iterations: 0 FP64; 1 FP32 inner iterations inside FP64
+ * iterative refinement (CG + AMG pressure solves, and the Jacobi BiCGStab solves of
+ * momentum and transport equations), the acceptance test always on the FP64
+ * residual; 2 FP64 Krylov iterations around an FP32 AMG V-cycle (CG + AMG only;
+ * other solvers run in FP64). */
 typedef struct {
     int32_t solver;
     int32_t preconditioner;
