@@ -19,8 +19,9 @@ namespace bsg {
 
 constexpr int kSellC = 32;
 // Entries each thread loads before it gathers (memory-level parallelism of a row sweep).
+// 8 against 4: 39.5 against 40.5 ms per outer iteration on the 1M-cell cavity (6: 39.8).
 #ifndef BSG_SELL_BATCH
-#define BSG_SELL_BATCH 4
+#define BSG_SELL_BATCH 8
 #endif
 constexpr int kSellBatch = BSG_SELL_BATCH;
 
