@@ -12,10 +12,10 @@ namespace {
 #define BSG_SELL_SB 256
 #endif
 constexpr int SB = BSG_SELL_SB;  // threads per block
-// Minimum resident blocks per SM the register budget must allow.  The FP64
-// single-system kernel: 4 (64 registers, no spills) measured 2 % faster than 3 (80)
-// on the 1M-cell pressure solves, 2 (128) slower.  The FP32 V-cycle variants and the
-// batched kernel keep 3: at 64 registers they spill.
+// Minimum resident blocks per SM the register budget must allow.  The single-system
+// kernels: 4 (64 registers) measured faster than 3 (80) on the 1M-cell cavity (FP64:
+// 2 %; FP32 V-cycle: 42.4 -> 40.3 ms per outer iteration; FP32 inner PCG: 49.6 ->
+// 45.5), 2 (128) slower.  The batched kernel keeps 3: at 64 registers it spills heavily.
 #ifndef BSG_SELL_MIN_BLOCKS
 #define BSG_SELL_MIN_BLOCKS 4
 #endif
@@ -31,9 +31,12 @@ constexpr int SB = BSG_SELL_SB;  // threads per block
 #define BSG_RESTRICT_ROWS 20000
 #endif
 constexpr int kRestrictRows = BSG_RESTRICT_ROWS;
-constexpr int kRowLanes = 8;
+#ifndef BSG_ROW_LANES
+#define BSG_ROW_LANES 8
+#endif
+constexpr int kRowLanes = BSG_ROW_LANES;
 template <class TK, class TV>
-constexpr int kSellMinBlocks = (sizeof(TK) == 8 && sizeof(TV) == 8) ? BSG_SELL_MIN_BLOCKS : 3;
+constexpr int kSellMinBlocks = BSG_SELL_MIN_BLOCKS;
 
 __device__ __forceinline__ void mark(const PhaseLog& log, int id) {
     if (log.entries && blockIdx.x == 0 && threadIdx.x == 0) {
