@@ -276,8 +276,13 @@ __device__ void bicgBody(G& g, const BicgArgs<C, T>& a) {
     }
 }
 
+// Whole-grid kernel at 4 blocks per SM (64 registers, no spills); the batched kernel keeps
+// 3 (80 registers).
+#ifndef BSG_BICG_MIN_BLOCKS
+#define BSG_BICG_MIN_BLOCKS 4
+#endif
 template <int C, class T>
-__global__ void __launch_bounds__(BB, 3) kBicgSell(BicgArgs<C, T> a, SegmentBarrier* bar) {
+__global__ void __launch_bounds__(BB, BSG_BICG_MIN_BLOCKS) kBicgSell(BicgArgs<C, T> a, SegmentBarrier* bar) {
     GridGroup g{bar};
     bicgBody<C, T>(g, a);
 }

@@ -1076,9 +1076,12 @@ void KrylovSolver::solveBatch(Context& ctx, std::vector<BatchSolve>& items) {
 }
 
 // Largest system the single-system momentum solve runs on the persistent BiCGStab kernel
-// (110 592-cell Voronoi cube: 8.07 against 8.77 ms per SIMPLE iteration; 1M cells: 5.45
-// against 3.86 ms of momentum solve per iteration).
-constexpr int kPersistentBicgstabRows = 300000;
+// (110 592-cell Voronoi cube: 8.07 against 8.77 ms per SIMPLE iteration; 1M cells, at 4
+// blocks per SM: 39.24 against 39.93 ms per SIMPLE iteration with the per-phase kernels).
+#ifndef BSG_PERSISTENT_BICGSTAB_ROWS
+#define BSG_PERSISTENT_BICGSTAB_ROWS 2000000
+#endif
+constexpr int kPersistentBicgstabRows = BSG_PERSISTENT_BICGSTAB_ROWS;
 
 void KrylovSolver::solveVector3Batch(Context& ctx, std::vector<BicgItem>& items, bool batched) {
     const int K = static_cast<int>(items.size());
