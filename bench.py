@@ -158,9 +158,9 @@ def algorithmic_bytes(name, N, nnz_off, amg_rows):
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte,
 # measured by one ncu capture of the kernel: kPcgSell, first pressure solve of the
 # 512000-cell Voronoi cavity of the same generator and settings (30 CG iterations),
-# 15.47 GB of DRAM traffic for 17.10 GB of algorithmic bytes.  Both grow with cells
+# 15.58 GB of DRAM traffic for 17.10 GB of algorithmic bytes.  Both grow with cells
 # and CG iterations in proportion, so the ratio scales the 1M-cell launches.
-DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.905}
+DRAM_PER_ALGORITHMIC_BYTE = {"pcg_amg_persistent": 0.911}
 
 
 def load_peaks():
