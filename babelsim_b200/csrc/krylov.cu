@@ -659,8 +659,8 @@ inline double residualScale(double initial, double rhs) {
 }
 }  // namespace
 
-// FP64 iterative refinement around FP32 persistent PCG + FP32 V-cycle (north-star
-// form (c)): r = b - A x in FP64; solve A d = r in FP32 to a relative target;
+// FP64 iterative refinement around FP32 persistent PCG + FP32 V-cycle (precision 1):
+// r = b - A x in FP64; solve A d = r in FP32 to a relative target;
 // x += d in FP64; repeat until the FP64 true residual meets the reference's
 // acceptance contract (petsc_linear_system.cpp:355-481 semantics: zero start
 // unless warm, target max(atol, rtol max(||r0||, ||b||))).

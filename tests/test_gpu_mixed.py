@@ -6,8 +6,8 @@ inside FP64 refinement for the momentum systems (precision 1 on the momentum sol
 Tolerances: the refined solve meets the same FP64 true-residual contract as
 the FP64 path, so solutions agree with a direct solve to 1e-8 (rtol 1e-12) and
 converged SIMPLE fields with the reference's to 1e-8 after the reference's own number of
-outer iterations (outer tolerance 1e-6); the
-north star's bound for the mixed path is 1e-6 relative L2 of the FP64 result.
+outer iterations (outer tolerance 1e-6); the bound asked of the mixed path is 1e-6
+relative L2 of the FP64 result.
 """
 import numpy as np
 import pytest

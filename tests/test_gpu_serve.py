@@ -1,5 +1,5 @@
-"""Serving loop on the GPU: each request's result is the same alone and in the mix (the
-north star's serving test), and the loop retires every request.
+"""Serving loop on the GPU: each request's result is the same alone and in the mix, and the
+loop retires every request.
 
 In the mix, requests admitted together run as one block-diagonal cohort whose pressure
 systems share one persistent launch; each member's CTA share depends only on its own size
